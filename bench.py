@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""bench.py -- density + force particle-updates/s on one or more B200s.
+
+Workload (the lattice-100 density + force configuration): the close-packed unit-box
+lattice with npartx = 100 (1,403,000 particles), 1% of particles (seeded uniform pick)
+with h scaled by U[0.65, 1.35], velocities N(0, 0.1^2) per component, u = 1,
+gamma = 5/3, alpha_AV = 1, beta = 2, alphau = 0, cubic kernel, hfact 1.2, tolh 1e-4,
+open boundaries (the reference driver's boundary choice).  Synthetic, seeded.
+
+A step is one density solve (tree + Newton-Raphson + gradient sweep) followed by one
+force pass, both through the library's C-ABI.  Particle-updates per step = the sum over
+Newton iterations of the particles updated + the live particles of the force pass.
+
+  value   device-timed, inputs resident in HBM (no host transfers in the timed region)
+  e2e     the same step through the C-ABI from pinned host buffers, with every step's
+          uploads (POS, HSML, VEL, ACCEL, THERMO) and downloads (HSML, DENS_OUT,
+          GRAD_OUT, FORCE_OUT) inside the timed region
+Multi-GPU: one process per GPU (torchrun), each an independent replica of the workload
+(the path has no exchange step); value = all ranks' updates / the slowest rank's time.
+
+--impl reference times the CPU oracle (the reference cannot be built here: its
+Cornerstone dependency is absent) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "density+force particle-updates/s (lattice 100 + jiggle, plain FP64)"
+UNIT = "particle-updates/s"
+FLOP_PER_DENSITY_PAIR = 30.0
+FLOP_PER_NR_UPDATE = 30.0
+BYTES_PER_DENSITY_UPDATE = 56.0
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", local))
+        dist = td
+    return rank, world, local, dist
+
+
+def barrier(dist, local):
+    if dist is not None:
+        import torch
+        t = torch.zeros(1, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        torch.cuda.synchronize(local)
+
+
+def max_over_ranks(dist, local, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, local, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 100 ms during the timed region."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(gpu), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(", ") for r in self.f.read().strip().splitlines() if r.count(",") >= 9]
+        os.unlink(self.f.name)
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].strip() == "Active"})
+        busy = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)]
+        return {"sm_mhz": statistics.median(busy or sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def workload(npartx):
+    from cosmosphere_b200 import inputs
+    return inputs.lattice100_workload(npartx)
+
+
+def cpu_oracle_step(p, threads=0):
+    """One density (+gradients) + force step of the CPU oracle; returns (updates, seconds)."""
+    from oracle import oracle as O
+    o = O.Oracle(threads=threads)
+    n = p.n
+    vel = np.stack([p["vx"], p["vy"], p["vz"]])
+    t0 = time.perf_counter()
+    st = o.density(p["x"], p["y"], p["z"], p["h"], p["pmass"], vel=vel, acc=np.zeros((3, n)), max_iter=100)
+    assert st == 0, st
+    o.force(np.stack([p["pro2"], p["cs"], p["alpha"], p["u"]]), beta=2.0, alphau=0.0)
+    dt = time.perf_counter() - t0
+    upd = float(o.array("activePerIter").sum() + o.scalar("nAlive"))
+    return upd, dt, O.max_threads()
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "MEASURED_PEAKS.json"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    return None
+
+
+def run_reference(args, rank, world, local, dist):
+    """The CPU arm: the oracle port of the path, all host threads, a bounded sample."""
+    if rank != 0:
+        return
+    sample_npx = args.ref_npartx
+    p = workload(sample_npx)
+    for _ in range(args.warmup):
+        cpu_oracle_step(p)
+    upd = 0.0
+    t = 0.0
+    cores = 0
+    for _ in range(args.steps):
+        u, dt, cores = cpu_oracle_step(p)
+        upd += u
+        t += dt
+    v = upd / t
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"lattice {sample_npx} + 1% jiggle, density+force (sample of lattice 100)",
+                       "particles": p.n, "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"lattice-{sample_npx} instance of the lattice-100 generator ({p.n} particles), "
+                                       "one density+force step per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--npartx", type=int, default=100)
+    ap.add_argument("--ref-npartx", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, rank, world, local, dist)
+        return
+
+    from cosmosphere_b200 import capi
+    c = capi.Cosmo()
+    c.set_device(local)
+    p = workload(args.npartx)
+    n = p.n
+    pm = p["pmass"]
+    pos = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]))
+    hsml = np.ascontiguousarray(p["h"])
+    vel = np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]]))
+    acc = np.zeros((3, n))
+    thermo = np.ascontiguousarray(np.stack([p["pro2"], p["cs"], p["alpha"], p["u"]]))
+    outs = {capi.HSML: np.empty((1, n)), capi.DENS_OUT: np.empty((2, n)), capi.GRAD_OUT: np.empty((3, n)),
+            capi.FORCE_OUT: np.empty((6, n))}
+    for a in [pos, hsml, vel, acc, thermo] + list(outs.values()):
+        c.pin(a)
+    c.arrays_init(n)
+
+    def upload_inputs():
+        c.upload(capi.POS, pos, n)
+        c.upload(capi.HSML, hsml, n)
+        c.upload(capi.VEL, vel, n)
+        c.upload(capi.ACCEL, acc, n)
+
+    def step_resident():
+        c.density(n, pm, tolh=1e-4, hfact=1.2)
+        c.force(n, pm, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
+
+    def step_e2e():
+        upload_inputs()
+        c.density(n, pm, tolh=1e-4, hfact=1.2)
+        c.upload(capi.THERMO, thermo, n, sorted_=True)
+        c.force(n, pm, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
+        for slot, buf in outs.items():
+            c.download(slot, n, buf)
+
+    # inputs resident; THERMO gathered into Hilbert order once (every step sorts the same input)
+    upload_inputs()
+    c.density(n, pm, tolh=1e-4, hfact=1.2)
+    c.upload(capi.THERMO, thermo, n, sorted_=True)
+
+    # ---------------- device-resident timing
+    for _ in range(args.warmup):
+        step_resident()
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    barrier(dist, local)
+    c.sync()
+    launches0 = c.launches()
+    upd_step = 0.0
+    t_nr = t_fk = 0.0
+    pairs = nr_upd = 0.0
+    nr_launches = 0
+    c.mark(0)
+    for _ in range(args.steps):
+        step_resident()
+        act = c.array("activePerIter")
+        upd_step = float(act.sum() + c.scalar("nAlive"))
+        nr_upd += float(act.sum())
+        nr_launches += len(act)
+        t_nr += c.scalar("t_nrkern")
+        t_fk += c.scalar("t_fkern")
+        pairs += c.scalar("pairsDensity")
+    c.mark(1)
+    t_dev = c.elapsed(0, 1)
+    c.sync()
+    barrier(dist, local)
+    clk = clocks.stop()
+    launches = c.launches() - launches0
+    t_max = max_over_ranks(dist, local, t_dev)
+    upd_total = sum_over_ranks(dist, local, upd_step * args.steps)
+    value = upd_total / t_max
+
+    # ---------------- end to end through the C-ABI
+    for _ in range(args.warmup):
+        step_e2e()
+    barrier(dist, local)
+    c.sync()
+    c.mark(2)
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    c.mark(3)
+    t_e2e_dev = c.elapsed(2, 3)
+    t_e2e_wall = time.perf_counter() - w0
+    barrier(dist, local)
+    t_e2e = max_over_ranks(dist, local, max(t_e2e_dev, t_e2e_wall))
+    e2e_value = upd_total / t_e2e
+    h2d = 8 * n * (3 + 1 + 3 + 3 + 4)
+    d2h = 8 * n * (1 + 2 + 3 + 6)
+
+    # ---------------- roofline of the Newton density kernel (dominant launch)
+    fp64_peak = c.fp64_peak_tflops()
+    flops = FLOP_PER_DENSITY_PAIR * pairs + FLOP_PER_NR_UPDATE * nr_upd
+    achieved = flops / t_nr / 1e12
+    peaks, src = measured_peaks()
+    hbm_achieved = BYTES_PER_DENSITY_UPDATE * nr_upd / t_nr / 1e9
+    traffic = ncu_traffic("density_nr_kernel")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cp = workload(args.ref_npartx)
+        u, dt, cores = cpu_oracle_step(cp)
+        cpu = {"value": u / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"lattice-{args.ref_npartx} instance of the same generator ({cp.n} particles), "
+                         "one density+force step of the CPU oracle (FP64, OpenMP)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"lattice {args.npartx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, "
+                                   "cubic, open boundaries",
+                       "particles": n, "particles_per_gpu": n, "nr_iterations": len(act),
+                       "updates_per_step": upd_step, "parallelism": f"replicas x{world}",
+                       "l2": "working set ~0.4 GB > 126 MB L2 (no flush needed)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1e3 * t_e2e / args.steps},
+            "roofline": {"kernel": "density_nr_kernel", "bound": "fp64", "achieved": achieved,
+                         "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                         "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
+                         "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
+                         "traffic": traffic,
+                         "hbm": {"achieved": hbm_achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                                 "frac": hbm_achieved / peaks.get("hbm_gbs"), "source": src,
+                                 "byte_convention": "56 B per particle-update"},
+                         "launch_ms": 1e3 * t_nr / max(1, nr_launches)},
+            "kernel_ms_per_step": {"density_nr": 1e3 * t_nr / args.steps, "force": 1e3 * t_fk / args.steps},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+"""ctypes binding of libcosmoSPHere's C-ABI (include/cosmosphere.h).
+
+Every call goes to the CUDA library; nothing here computes.  The library aborts the
+process with a "FATAL:" line on misuse, exactly as the reference's C-ABI does, so tests
+of those paths run it in a child process.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+
+POS, HSML, VEL, ACCEL, DENS_OUT, GRAD_OUT, THERMO, FORCE_OUT = range(1, 9)
+NCOMP = {POS: 3, HSML: 1, VEL: 3, ACCEL: 3, DENS_OUT: 2, GRAD_OUT: 3, THERMO: 4, FORCE_OUT: 6}
+
+EXPORTS = [
+    "cosmo_arrays_init", "cosmo_slot_ncomp", "cosmo_upload", "cosmo_upload_sorted", "cosmo_download",
+    "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
+    "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
+    "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
+]
+
+_DT = {0: np.float64, 1: np.int32, 2: np.uint32, 3: np.uint64, 4: np.int64}
+
+
+def lib_path(quintic: bool = False) -> str:
+    return os.path.join(LIBDIR, "libcosmoSPHere_quintic.so" if quintic else "libcosmoSPHere.so")
+
+
+def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
+    I, D, P = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    L.cosmo_arrays_init.argtypes = [I]
+    L.cosmo_slot_ncomp.argtypes = [I]
+    L.cosmo_slot_ncomp.restype = I
+    for f in (L.cosmo_upload, L.cosmo_upload_sorted, L.cosmo_download):
+        f.argtypes = [I, P, I]
+    L.cosmo_pin_host.argtypes = [P, ctypes.c_size_t]
+    L.cosmo_unpin_host.argtypes = [P]
+    L.cosmo_kernel_radius.restype = D
+    L.densityiterate_gpu_c.argtypes = [I, D, I, P, D, D]
+    L.force_gpu_c.argtypes = [I, D, D, D, I, I, I]
+    L.cosmo_x_set_max_iter.argtypes = [I]
+    L.cosmo_x_density.argtypes = [I, D, I, P, D, D, I, I]
+    L.cosmo_x_density.restype = I
+    L.cosmo_x_scalar.argtypes = [ctypes.c_char_p]
+    L.cosmo_x_scalar.restype = D
+    L.cosmo_x_array.argtypes = [ctypes.c_char_p, P, ctypes.POINTER(I)]
+    L.cosmo_x_array.restype = ctypes.c_long
+    L.cosmo_x_set_device.argtypes = [I]
+    L.cosmo_x_mark.argtypes = [I]
+    L.cosmo_x_mark_elapsed.argtypes = [I, I]
+    L.cosmo_x_mark_elapsed.restype = D
+    L.cosmo_x_launches.restype = ctypes.c_ulonglong
+    L.cosmo_x_fp64_peak.restype = D
+    return L
+
+
+_libs: dict = {}
+
+
+def load(quintic: bool = False) -> ctypes.CDLL:
+    """Load the CUDA library; raises if it has not been built (no fallback)."""
+    key = bool(quintic)
+    if key not in _libs:
+        path = lib_path(quintic)
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with __graft_entry__.build() "
+                               "(make -C cosmosphere_b200); there is no CPU fallback")
+        _libs[key] = _bind(ctypes.CDLL(path))
+    return _libs[key]
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Cosmo:
+    """The C-ABI, one call per method; arrays are numpy float64, slots component-major."""
+
+    def __init__(self, quintic: bool = False):
+        self.L = load(quintic)
+        self.quintic = quintic
+
+    def arrays_init(self, n: int):
+        self.L.cosmo_arrays_init(int(n))
+
+    def slot_ncomp(self, slot: int) -> int:
+        return int(self.L.cosmo_slot_ncomp(int(slot)))
+
+    def upload(self, slot: int, data, n: int | None = None, sorted_: bool = False):
+        a = _c(data).reshape(-1)
+        n = a.size // NCOMP[slot] if n is None else n
+        f = self.L.cosmo_upload_sorted if sorted_ else self.L.cosmo_upload
+        f(int(slot), a.ctypes.data, int(n))
+
+    def download(self, slot: int, n: int, out=None) -> np.ndarray:
+        nc = NCOMP[slot]
+        if out is None:
+            out = np.empty((nc, n), dtype=np.float64)
+        self.L.cosmo_download(int(slot), out.ctypes.data, int(n))
+        return out
+
+    def density(self, n, pmass, *, periodic_box=None, tolh=1e-4, hfact=-1.0):
+        box = _c(periodic_box if periodic_box is not None else np.zeros(6))
+        self.L.densityiterate_gpu_c(int(n), float(pmass), 1 if periodic_box is not None else 0,
+                                    box.ctypes.data, float(tolh), float(hfact))
+
+    def density_status(self, n, pmass, *, periodic_box=None, tolh=1e-4, hfact=-1.0, max_iter=0,
+                       with_gradients=True) -> int:
+        box = _c(periodic_box if periodic_box is not None else np.zeros(6))
+        return int(self.L.cosmo_x_density(int(n), float(pmass), 1 if periodic_box is not None else 0,
+                                          box.ctypes.data, float(tolh), float(hfact), int(max_iter),
+                                          1 if with_gradients else 0))
+
+    def force(self, n, pmass, *, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1):
+        self.L.force_gpu_c(int(n), float(pmass), float(beta), float(alphau), int(disc), int(pdv), int(shock))
+
+    def kernel_radius(self) -> float:
+        return float(self.L.cosmo_kernel_radius())
+
+    def pin(self, a: np.ndarray):
+        self.L.cosmo_pin_host(a.ctypes.data, a.nbytes)
+
+    def unpin(self, a: np.ndarray):
+        self.L.cosmo_unpin_host(a.ctypes.data)
+
+    def set_max_iter(self, m: int):
+        self.L.cosmo_x_set_max_iter(int(m))
+
+    def sync(self):
+        self.L.cosmo_x_sync()
+
+    def set_device(self, dev: int):
+        self.L.cosmo_x_set_device(int(dev))
+
+    def mark(self, i: int):
+        self.L.cosmo_x_mark(int(i))
+
+    def elapsed(self, a: int, b: int) -> float:
+        return float(self.L.cosmo_x_mark_elapsed(int(a), int(b)))
+
+    def launches(self) -> int:
+        return int(self.L.cosmo_x_launches())
+
+    def fp64_peak_tflops(self) -> float:
+        return float(self.L.cosmo_x_fp64_peak())
+
+    def scalar(self, name: str) -> float:
+        return float(self.L.cosmo_x_scalar(name.encode()))
+
+    def array(self, name: str) -> np.ndarray:
+        dt = ctypes.c_int(0)
+        n = self.L.cosmo_x_array(name.encode(), None, ctypes.byref(dt))
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, dtype=_DT[dt.value])
+        self.L.cosmo_x_array(name.encode(), out.ctypes.data if n else None, ctypes.byref(dt))
+        return out

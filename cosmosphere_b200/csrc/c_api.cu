@@ -1,0 +1,633 @@
+/*
+ * c_api.cu -- the drop-in C-ABI (declared in include/cosmosphere.h) and the state
+ * plumbing behind it: sizing, the slot table, host <-> device transfers through the
+ * Hilbert ordering, pinning, the compute entry points, and their stderr statistics.
+ *
+ * Semantics follow the reference's src/arrays_c_api.cu, src/dens_c_api.cu,
+ * src/force_c_api.cu, src/pin_c_api.cu and src/gpu_state.cu: one process-wide state on
+ * one device, every call synchronous with respect to the host, errors abort with a
+ * "FATAL:" line.  Test and harness hooks are exported with the cosmo_x_ prefix.
+ */
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstring>
+#include <string>
+
+#include "state.hpp"
+#include "../../include/cosmosphere.h"
+#include "../../include/cosmo_density.hpp"
+
+namespace cosmo {
+
+unsigned long long g_launches = 0;
+
+// FP64 throughput probe: independent FMA chains per thread, no memory traffic.
+__global__ void fp64_peak_kernel(double* out, int iters, double a, double b)
+{
+    double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-3, x2 = x0 + 2e-3, x3 = x0 + 3e-3;
+    double x4 = x0 + 4e-3, x5 = x0 + 5e-3, x6 = x0 + 6e-3, x7 = x0 + 7e-3;
+    for (int k = 0; k < iters; ++k)
+    {
+        x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+        x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+    const double r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (r == 12345.0) out[0] = r;   // keeps the chains live
+}
+
+void fatal(const char* fmt, ...)
+{
+    std::fprintf(stderr, "FATAL: ");
+    va_list ap;
+    va_start(ap, fmt);
+    std::vfprintf(stderr, fmt, ap);
+    va_end(ap);
+    std::fprintf(stderr, "\n");
+    std::fflush(stderr);
+    std::abort();
+}
+
+// Deliberately leaked (src/gpu_state.cu:1-19): no device memory is released during
+// static teardown, after the CUDA runtime may have unloaded.
+State& state()
+{
+    static State* s = new State();
+    return *s;
+}
+
+void ensure_init(State& s)
+{
+    if (s.st) return;
+    COSMO_CUDA(cudaGetDevice(&s.device));
+    COSMO_CUDA(cudaDeviceGetAttribute(&s.numSMs, cudaDevAttrMultiProcessorCount, s.device));
+    COSMO_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+    s.dscal.resize(1, s.st);
+    COSMO_CUDA(cudaMallocHost(&s.hscal, sizeof(DevScalars)));
+    COSMO_CUDA(cudaMallocHost(&s.hsmall, 64 * sizeof(int)));
+    std::memset(s.hscal, 0, sizeof(DevScalars));
+    s.box.resize(1, s.st);
+    if (const char* e = std::getenv("COSMO_MAX_ITER")) s.maxIter = std::max(1, std::atoi(e));
+}
+
+// src/gpu_state.cu:21-46: every particle-length array, sized once per count.
+void size_particle_arrays(State& s, int n)
+{
+    ensure_init(s);
+    if (s.sizedFor == n) return;
+    for (auto* b : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
+                    &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF})
+        b->resize(n, s.st);
+    for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB}) b->resize(n, s.st);
+    s.xfer.resize(size_t(6) * n, s.st);
+    s.keysA.resize(n, s.st);
+    s.keysB.resize(n, s.st);
+    for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged}) b->resize(n, s.st);
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    s.sizedFor = n;
+}
+
+void read_scalars(State& s)
+{
+    COSMO_CUDA(cudaMemcpyAsync(s.hscal, s.dscal.get(), sizeof(DevScalars), cudaMemcpyDeviceToHost, s.st));
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+}
+
+void check_dev_err(State& s, const char* where)
+{
+    read_scalars(s);
+    const int e = s.hscal->err;
+    if (e)
+        fatal("%s: device error 0x%x (%s%s%s%s)", where, e, (e & kErrSortSpin) ? "sort look-back timeout " : "",
+              (e & kErrListCap) ? "j-list capacity " : "", (e & kErrStageWait) ? "staging wait timeout " : "",
+              (e & kErrQueueWait) ? "queue wait timeout" : "");
+}
+
+namespace {
+constexpr int kEvPool = 1024;
+cudaEvent_t gEv[kEvPool];
+int gEvNext = 0;
+bool gEvInit = false;
+}
+
+cudaEvent_t ev(State& s)
+{
+    if (!gEvInit)
+    {
+        for (auto& e : gEv) COSMO_CUDA(cudaEventCreate(&e));
+        gEvInit = true;
+    }
+    cudaEvent_t e = gEv[gEvNext];
+    gEvNext = (gEvNext + 1) % kEvPool;
+    COSMO_CUDA(cudaEventRecord(e, s.st));
+    return e;
+}
+
+void ev_reset() { gEvNext = 0; }
+
+double elapsed_s(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.0f;
+    COSMO_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms * 1e-3;
+}
+
+// ------------------------------------------------------------------ slots
+struct Comp
+{
+    double* base;   // Hilbert-order device array
+    int stride;     // in doubles
+    double* caller; // caller-order upload target, or nullptr
+};
+
+static int slot_components(State& s, int slot, Comp* c)
+{
+    auto d4 = [](DBuf<double4>& b, int off) { return reinterpret_cast<double*>(b.get()) + off; };
+    switch (slot)
+    {
+        case COSMO_POS:
+            c[0] = {d4(s.xyzh, 0), 4, s.ux.get()};
+            c[1] = {d4(s.xyzh, 1), 4, s.uy.get()};
+            c[2] = {d4(s.xyzh, 2), 4, s.uz.get()};
+            return 3;
+        case COSMO_HSML: c[0] = {d4(s.xyzh, 3), 4, s.uh.get()}; return 1;
+        case COSMO_VEL:
+            c[0] = {d4(s.vel4, 0), 4, s.uvx.get()};
+            c[1] = {d4(s.vel4, 1), 4, s.uvy.get()};
+            c[2] = {d4(s.vel4, 2), 4, s.uvz.get()};
+            return 3;
+        case COSMO_ACCEL:
+            c[0] = {d4(s.acc4, 0), 4, s.uax.get()};
+            c[1] = {d4(s.acc4, 1), 4, s.uay.get()};
+            c[2] = {d4(s.acc4, 2), 4, s.uaz.get()};
+            return 3;
+        case COSMO_DENS_OUT:
+            c[0] = {s.rho.get(), 1, nullptr};
+            c[1] = {s.gradh.get(), 1, nullptr};
+            return 2;
+        case COSMO_GRAD_OUT:
+            c[0] = {s.divv.get(), 1, nullptr};
+            c[1] = {s.xi.get(), 1, nullptr};
+            c[2] = {s.ddivvdt.get(), 1, nullptr};
+            return 3;
+        case COSMO_THERMO:
+            for (int k = 0; k < 4; ++k) c[k] = {d4(s.thermo4, k), 4, nullptr};
+            return 4;
+        case COSMO_FORCE_OUT:
+            c[0] = {s.fx.get(), 1, nullptr};
+            c[1] = {s.fy.get(), 1, nullptr};
+            c[2] = {s.fz.get(), 1, nullptr};
+            c[3] = {s.f4.get(), 1, nullptr};
+            c[4] = {s.vsigmax.get(), 1, nullptr};
+            c[5] = {s.divvF.get(), 1, nullptr};
+            return 6;
+        default: return 0;
+    }
+}
+
+static int slot_ncomp_static(int slot)
+{
+    switch (slot)
+    {
+        case COSMO_POS: return 3;
+        case COSMO_HSML: return 1;
+        case COSMO_VEL: return 3;
+        case COSMO_ACCEL: return 3;
+        case COSMO_DENS_OUT: return 2;
+        case COSMO_GRAD_OUT: return 3;
+        case COSMO_THERMO: return 4;
+        case COSMO_FORCE_OUT: return 6;
+        default: return 0;
+    }
+}
+
+struct CompSet
+{
+    double* base[6];
+    int stride[6];
+};
+
+// dst component c at sorted k  <-  xfer[c*n + order[k]]   (cosmo_upload_sorted)
+__global__ void gather_slot_kernel(CompSet cs, int nc, const int* __restrict__ order, int n,
+                                   const double* __restrict__ xfer)
+{
+    const long k = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int src = order[k];
+    for (int c = 0; c < nc; ++c) cs.base[c][size_t(k) * cs.stride[c]] = xfer[size_t(c) * n + src];
+}
+
+// xfer[c*n + order[k]]  <-  src component c at sorted k   (cosmo_download)
+__global__ void scatter_slot_kernel(CompSet cs, int nc, const int* __restrict__ order, int n,
+                                    double* __restrict__ xfer)
+{
+    const long k = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int dst = order[k];
+    for (int c = 0; c < nc; ++c) xfer[size_t(c) * n + dst] = cs.base[c][size_t(k) * cs.stride[c]];
+}
+
+// dst component c at k  <-  xfer[c*n + k]   (raw upload of a result slot, no permutation)
+__global__ void copy_slot_kernel(CompSet cs, int nc, int n, const double* __restrict__ xfer)
+{
+    const long k = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    for (int c = 0; c < nc; ++c) cs.base[c][size_t(k) * cs.stride[c]] = xfer[size_t(c) * n + k];
+}
+
+static void check_sized(State& s, int slot, int n, const char* what, Comp* comps, int& nc)
+{
+    if (s.sizedFor != n)
+        fatal("%s(slot=%d) with n=%d but the device arrays are sized for %d", what, slot, n, s.sizedFor);
+    nc = slot_components(s, slot, comps);
+    if (nc == 0) fatal("%s called for slot %d, which has no arrays", what, slot);
+}
+
+static void require_order(State& s, int slot, int n, const char* what)
+{
+    if (s.orderFor != n)
+        fatal("%s(slot=%d) with no ordering: a density solve must have run first", what, slot);
+}
+
+struct XferTimer
+{
+    State& s;
+    double& sink;
+    cudaEvent_t a;
+    XferTimer(State& st, double& k) : s(st), sink(k) { a = ev(s); }
+    ~XferTimer()
+    {
+        cudaEvent_t b = ev(s);
+        COSMO_CUDA(cudaEventSynchronize(b));
+        sink += elapsed_s(a, b);
+    }
+};
+
+static void upload_slot(int slot, const double* host, int n, bool sorted, const char* what)
+{
+    State& s = state();
+    if (n <= 0) return;
+    Comp comps[6];
+    int nc = 0;
+    check_sized(s, slot, n, what, comps, nc);
+    if (sorted) require_order(s, slot, n, what);
+    XferTimer timer(s, s.uploadSeconds);
+    const size_t bytes = size_t(n) * sizeof(double);
+    if (!sorted && comps[0].caller)
+    {
+        for (int c = 0; c < nc; ++c)
+            COSMO_CUDA(cudaMemcpyAsync(comps[c].caller, host + size_t(c) * n, bytes, cudaMemcpyHostToDevice, s.st));
+        return;
+    }
+    COSMO_CUDA(cudaMemcpyAsync(s.xfer.get(), host, bytes * nc, cudaMemcpyHostToDevice, s.st));
+    CompSet cs{};
+    for (int c = 0; c < nc; ++c) { cs.base[c] = comps[c].base; cs.stride[c] = comps[c].stride; }
+    if (sorted) gather_slot_kernel<<<iceil(n, 256), 256, 0, s.st>>>(cs, nc, s.orderA.get(), n, s.xfer.get());
+    else copy_slot_kernel<<<iceil(n, 256), 256, 0, s.st>>>(cs, nc, n, s.xfer.get());
+    COSMO_LAUNCHED();
+}
+
+// ------------------------------------------------------------------ stats lines
+static bool env_on(const char* k) { return std::getenv(k) != nullptr; }
+
+} // namespace cosmo
+
+using namespace cosmo;
+
+// ====================================================================== the C-ABI
+extern "C" {
+
+void cosmo_arrays_init(int n)
+{
+    if (n <= 0) return;
+    size_particle_arrays(state(), n);
+}
+
+int cosmo_slot_ncomp(int slot) { return slot_ncomp_static(slot); }
+
+void cosmo_upload(int slot, const double* host, int n) { upload_slot(slot, host, n, false, "cosmo_upload"); }
+
+void cosmo_upload_sorted(int slot, const double* host, int n)
+{
+    upload_slot(slot, host, n, true, "cosmo_upload_sorted");
+}
+
+void cosmo_download(int slot, double* host, int n)
+{
+    State& s = state();
+    if (n <= 0) return;
+    Comp comps[6];
+    int nc = 0;
+    check_sized(s, slot, n, "cosmo_download", comps, nc);
+    require_order(s, slot, n, "cosmo_download");
+    XferTimer timer(s, s.downloadSeconds);
+    CompSet cs{};
+    for (int c = 0; c < nc; ++c) { cs.base[c] = comps[c].base; cs.stride[c] = comps[c].stride; }
+    scatter_slot_kernel<<<iceil(n, 256), 256, 0, s.st>>>(cs, nc, s.orderA.get(), n, s.xfer.get());
+    COSMO_LAUNCHED();
+    COSMO_CUDA(cudaMemcpyAsync(host, s.xfer.get(), size_t(n) * nc * sizeof(double), cudaMemcpyDeviceToHost, s.st));
+}
+
+void cosmo_pin_host(void* ptr, size_t nbytes)
+{
+    if (ptr == nullptr || nbytes == 0) return;
+    if (cudaHostRegister(ptr, nbytes, cudaHostRegisterDefault) != cudaSuccess) (void)cudaGetLastError();
+}
+
+void cosmo_unpin_host(void* ptr)
+{
+    if (ptr == nullptr) return;
+    if (cudaHostUnregister(ptr) != cudaSuccess) (void)cudaGetLastError();
+}
+
+double cosmo_kernel_radius(void) { return kRadKernel; }
+
+void densityiterate_gpu_c(int n, double pmass, int periodic, const double* box, double tolh, double hfact)
+{
+    State& s = state();
+    if (s.sizedFor != n)
+        fatal("%s called with n=%d but the device arrays are sized for %d "
+              "(cosmo_arrays_init not called, or called with a different count)",
+              "densityiterate_gpu_c", n, s.sizedFor);
+    if (n <= 0) return;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    const DensResult r = solve_density(s, n, pmass, periodic ? box : nullptr, tolh, hfact, s.maxIter, true);
+    const auto t1 = clk::now();
+    if (r.status == 1)
+        fatal("solveDensH: unconverged=%d jlist_trunc=%d stack_drops=%d (iters=%d)", r.unconverged, 0, 0,
+              r.itersRun);
+    if (r.status == 2)
+        fatal("solveDensH: kernel support %gh reaches half the periodic box; too few particles for this box",
+              kRadKernel);
+    static bool memReported = false;
+    if (!memReported && env_on("COSMO_MEM"))
+    {
+        memReported = true;
+        size_t fr = 0, tot = 0;
+        COSMO_CUDA(cudaMemGetInfo(&fr, &tot));
+        std::fprintf(stderr, "COSMO_MEM n=%d device_used=%.2f GB of %.2f GB (%.0f bytes/particle)\n", n,
+                     (tot - fr) / 1e9, tot / 1e9, double(tot - fr) / n);
+    }
+    static const bool stats = env_on("COSMO_DENS_STATS");
+    if (stats)
+    {
+        const Timings& t = s.t;
+        const double gpu = 1e3 * (t.bbox + t.keysSort + t.tree + t.nodes + t.jbuild + t.nrkern + t.gjbuild + t.gradkern);
+        const double solve = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        std::fprintf(stderr,
+                     "COSMO_STATS n=%d leaves=%d iters=%d | upload=%.2f bbox=%.2f keysort=%.2f tree=%.2f nodes=%.2f "
+                     "jbuild=%.2f nrkern=%.2f gjbuild=%.2f gradkern=%.2f download=%.2f | gpusum=%.2f solve=%.2f "
+                     "unaccounted=%.2f\n",
+                     n, s.nLeaves, s.itersRun, 1e3 * s.uploadSeconds, 1e3 * t.bbox, 1e3 * t.keysSort, 1e3 * t.tree,
+                     1e3 * t.nodes, 1e3 * t.jbuild, 1e3 * t.nrkern, 1e3 * t.gjbuild, 1e3 * t.gradkern,
+                     1e3 * s.downloadSeconds, gpu, solve, solve - gpu);
+    }
+    s.uploadSeconds = 0.0;
+    s.downloadSeconds = 0.0;
+}
+
+void force_gpu_c(int n, double pmass, double beta, double alphau, int disc_viscosity, int pdv_heating,
+                 int shock_heating)
+{
+    State& s = state();
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    if (s.sizedFor != n)
+        fatal("%s called with n=%d but the device arrays are sized for %d "
+              "(cosmo_arrays_init not called, or called with a different count)",
+              "force_gpu_c", n, s.sizedFor);
+    if (!(s.ngas == n && s.token != 0))
+        fatal("force_gpu_c called with no GPU density solve for this particle set (n=%d state.ngas=%d token=%llu)",
+              n, s.ngas, (unsigned long long)s.token);
+    s.t.upsweep = s.t.fjbuild = s.t.prep = s.t.fkern = 0.0;
+    compute_forces(s, pmass, beta, alphau, disc_viscosity != 0, pdv_heating > 0, shock_heating > 0);
+    static const bool stats = env_on("COSMO_DENS_STATS");
+    if (stats)
+    {
+        const double wall = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        const Timings& t = s.t;
+        const double gpu = 1e3 * (t.upsweep + t.fjbuild + t.prep + t.fkern);
+        std::fprintf(stderr,
+                     "COSMO_FORCE n=%d leaves=%d | upsweep=%.2f jbuild=%.2f prep=%.2f kernel=%.2f | gpusum=%.2f "
+                     "wall=%.2f unaccounted=%.2f\n",
+                     s.ngas, s.nLeaves, 1e3 * t.upsweep, 1e3 * t.fjbuild, 1e3 * t.prep, 1e3 * t.fkern, gpu, wall,
+                     wall - gpu);
+    }
+}
+
+// ---------------------------------------------------------------- harness hooks
+void cosmo_x_set_max_iter(int m) { state().maxIter = std::max(1, m); }
+
+void cosmo_x_set_device(int dev) { COSMO_CUDA(cudaSetDevice(dev)); }
+
+static cudaEvent_t g_marks[16];
+static bool g_marksInit = false;
+
+void cosmo_x_mark(int id)
+{
+    State& s = state();
+    ensure_init(s);
+    if (!g_marksInit)
+    {
+        for (auto& e : g_marks) COSMO_CUDA(cudaEventCreate(&e));
+        g_marksInit = true;
+    }
+    COSMO_CUDA(cudaEventRecord(g_marks[id & 15], s.st));
+}
+
+double cosmo_x_mark_elapsed(int a, int b)
+{
+    COSMO_CUDA(cudaEventSynchronize(g_marks[b & 15]));
+    float ms = 0.0f;
+    COSMO_CUDA(cudaEventElapsedTime(&ms, g_marks[a & 15], g_marks[b & 15]));
+    return ms * 1e-3;
+}
+
+unsigned long long cosmo_x_launches(void) { return g_launches; }
+
+// Measured FP64 FMA throughput of this GPU in TFLOP/s (2 flops per FMA).
+double cosmo_x_fp64_peak(void)
+{
+    State& s = state();
+    ensure_init(s);
+    double* out = nullptr;
+    COSMO_CUDA(cudaMalloc(&out, sizeof(double)));
+    const int threads = 256, blocks = s.numSMs * 8, iters = 1 << 14;
+    fp64_peak_kernel<<<blocks, threads, 0, s.st>>>(out, iters, 0.999999, 1e-7);
+    COSMO_LAUNCHED();
+    cudaEvent_t a = ev(s);
+    fp64_peak_kernel<<<blocks, threads, 0, s.st>>>(out, iters, 0.999999, 1e-7);
+    COSMO_LAUNCHED();
+    cudaEvent_t b = ev(s);
+    COSMO_CUDA(cudaEventSynchronize(b));
+    const double t = elapsed_s(a, b);
+    COSMO_CUDA(cudaFree(out));
+    return 2.0 * 8.0 * double(iters) * threads * blocks / t / 1e12;
+}
+
+// Density solve that reports instead of aborting: 0 ok, 1 unconverged, 2 periodic support.
+int cosmo_x_density(int n, double pmass, int periodic, const double* box, double tolh, double hfact, int maxIter,
+                    int withGradients)
+{
+    State& s = state();
+    if (s.sizedFor != n || n <= 0) return -1;
+    const DensResult r = solve_density(s, n, pmass, periodic ? box : nullptr, tolh, hfact,
+                                       maxIter > 0 ? maxIter : s.maxIter, withGradients != 0);
+    return r.status;
+}
+
+void cosmo_x_sync(void)
+{
+    State& s = state();
+    if (s.st) COSMO_CUDA(cudaStreamSynchronize(s.st));
+}
+
+double cosmo_x_scalar(const char* name)
+{
+    State& s = state();
+    const std::string k(name);
+    if (k == "nAlive") return s.nAlive;
+    if (k == "nLeaves") return s.nLeaves;
+    if (k == "numNodes") return s.numNodes;
+    if (k == "itersRun") return s.itersRun;
+    if (k == "token") return double(s.token);
+    if (k == "hfact") return s.hfact;
+    if (k == "maxIter") return s.maxIter;
+    if (s.hscal)
+    {
+        read_scalars(s);
+        if (k == "pairsDensity") return double(s.hscal->pairs[0]);
+        if (k == "pairsGrad") return double(s.hscal->pairs[1]);
+        if (k == "pairsForce") return double(s.hscal->pairs[2]);
+        if (k == "candDensity") return double(s.hscal->pairs[3]);
+        if (k == "unconverged") return s.hscal->unconverged;
+    }
+    const Timings& t = s.t;
+    if (k == "t_bbox") return t.bbox;
+    if (k == "t_keysort") return t.keysSort;
+    if (k == "t_tree") return t.tree;
+    if (k == "t_nodes") return t.nodes;
+    if (k == "t_jbuild") return t.jbuild;
+    if (k == "t_nrkern") return t.nrkern;
+    if (k == "t_gjbuild") return t.gjbuild;
+    if (k == "t_gradkern") return t.gradkern;
+    if (k == "t_upsweep") return t.upsweep;
+    if (k == "t_fjbuild") return t.fjbuild;
+    if (k == "t_prep") return t.prep;
+    if (k == "t_fkern") return t.fkern;
+    return NAN;
+}
+
+// Copy a named device array to the host.  Returns the element count (or -1 if unknown);
+// *dtype: 0 f64, 1 i32, 2 u32, 3 u64, 4 i64.  out == nullptr only queries.
+long cosmo_x_array(const char* name, void* out, int* dtype)
+{
+    State& s = state();
+    const std::string k(name);
+    auto put = [&](const void* dev, size_t cnt, size_t es, int code, size_t stride = 1, size_t off = 0) -> long {
+        if (dtype) *dtype = code;
+        if (out && cnt)
+        {
+            if (stride == 1)
+                COSMO_CUDA(cudaMemcpyAsync(out, static_cast<const char*>(dev) + off * es, cnt * es,
+                                           cudaMemcpyDeviceToHost, s.st));
+            else
+                COSMO_CUDA(cudaMemcpy2DAsync(out, es, static_cast<const char*>(dev) + off * es, stride * es, es, cnt,
+                                             cudaMemcpyDeviceToHost, s.st));
+            COSMO_CUDA(cudaStreamSynchronize(s.st));
+        }
+        return long(cnt);
+    };
+    const size_t n = size_t(s.ngas), nL = size_t(s.nLeaves), nN = size_t(s.numNodes);
+    if (k == "x") return put(s.xyzh.get(), n, 8, 0, 4, 0);
+    if (k == "y") return put(s.xyzh.get(), n, 8, 0, 4, 1);
+    if (k == "z") return put(s.xyzh.get(), n, 8, 0, 4, 2);
+    if (k == "h") return put(s.xyzh.get(), n, 8, 0, 4, 3);
+    if (k == "vx") return put(s.vel4.get(), n, 8, 0, 4, 0);
+    if (k == "vy") return put(s.vel4.get(), n, 8, 0, 4, 1);
+    if (k == "vz") return put(s.vel4.get(), n, 8, 0, 4, 2);
+    if (k == "rho") return put(s.rho.get(), n, 8, 0);
+    if (k == "gradh") return put(s.gradh.get(), n, 8, 0);
+    if (k == "divv") return put(s.divv.get(), n, 8, 0);
+    if (k == "xi") return put(s.xi.get(), n, 8, 0);
+    if (k == "ddivvdt") return put(s.ddivvdt.get(), n, 8, 0);
+    if (k == "fx") return put(s.fx.get(), n, 8, 0);
+    if (k == "fy") return put(s.fy.get(), n, 8, 0);
+    if (k == "fz") return put(s.fz.get(), n, 8, 0);
+    if (k == "f4") return put(s.f4.get(), n, 8, 0);
+    if (k == "vsigmax") return put(s.vsigmax.get(), n, 8, 0);
+    if (k == "divvF") return put(s.divvF.get(), n, 8, 0);
+    if (k == "converged") return put(s.converged.get(), n, 4, 1);
+    if (k == "keys") return put(s.keysA.get(), n, 8, 3);
+    if (k == "order") return put(s.orderA.get(), n, 4, 1);
+    if (k == "particleLeaf") return put(s.particleLeaf.get(), size_t(s.nAlive), 4, 1);
+    if (k == "csTree") return put(s.csTree.get(), nL + 1, 8, 3);
+    if (k == "counts") return put(s.counts.get(), nL, 4, 2);
+    if (k == "layout") return put(s.layout.get(), nL + 1, 4, 2);
+    if (k == "prefixes") return put(s.bfsPrefix.get(), nN, 8, 3);
+    if (k == "childOffsets") return put(s.childOffsets.get(), nN, 4, 1);
+    if (k == "internalToLeaf") return put(s.internalToLeaf.get(), nN, 4, 1);
+    if (k == "levelRange") return put(s.levelRange.get(), kMaxLevel + 2, 4, 1);
+    if (k == "leafToInternal") return put(s.leafToInternal.get(), nL, 4, 1);
+    if (k == "centers") return put(s.centers.get(), 3 * nN, 8, 0);
+    if (k == "sizes") return put(s.sizes.get(), 3 * nN, 8, 0);
+    if (k == "hmax_leaf") return put(s.hmaxLeaf.get(), nL, 8, 0);
+    if (k == "hmax_node") return put(s.hmaxNode.get(), nN, 8, 0);
+    if (k == "jcount") return put(s.jcount.get(), nL, 4, 2);
+    if (k == "jOffset") return put(s.jOffset.get(), nL + 1, 4, 2);
+    if (k == "jlist")
+    {
+        uint32_t tot = 0;
+        if (nL)
+        {
+            COSMO_CUDA(cudaMemcpy(&tot, s.jOffset.get() + nL, 4, cudaMemcpyDeviceToHost));
+        }
+        return put(s.jlist.get(), tot, 4, 1);
+    }
+    if (k == "activePerIter")
+    {
+        if (dtype) *dtype = 4;
+        if (out) std::memcpy(out, s.activePerIter.data(), s.activePerIter.size() * 8);
+        return long(s.activePerIter.size());
+    }
+    if (dtype) *dtype = -1;
+    return -1;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- C++ entry point
+// The reference's own C++ API (include/density.hpp:85-91), used by its standalone driver.
+// Both kernel modes run this library's warp-per-leaf Newton kernel.
+DensTimings solveDensH(int n, double pmass, KernelMode mode, bool withGradients, const double* periodicBox,
+                       double tolh, double hfact)
+{
+    State& s = state();
+    if (s.sizedFor != n)
+        fatal("solveDensH called with n=%d but the device arrays are sized for %d", n, s.sizedFor);
+    DensTimings t{};
+    t.kernelMode = mode;
+    t.nParticles = n;
+    if (n <= 0) return t;
+    const DensResult r = solve_density(s, n, pmass, periodicBox, tolh, hfact, s.maxIter, withGradients);
+    if (r.status == 1)
+        fatal("solveDensH: unconverged=%d jlist_trunc=%d stack_drops=%d (iters=%d)", r.unconverged, 0, 0,
+              r.itersRun);
+    if (r.status == 2) fatal("solveDensH: kernel support reaches half the periodic box");
+    t.upload = s.uploadSeconds;
+    s.uploadSeconds = 0.0;
+    t.bboxAndSetup = s.t.bbox;
+    t.keysAndSort = s.t.keysSort;
+    t.treeBuild = s.t.tree;
+    t.nodeCenters = s.t.nodes;
+    t.jleafBuild = s.t.jbuild;
+    t.densKernel = s.t.nrkern;
+    t.gradJleafBuild = s.t.gjbuild;
+    t.gradKernel = s.t.gradkern;
+    t.download = s.downloadSeconds;
+    s.downloadSeconds = 0.0;
+    t.itersRun = r.itersRun;
+    t.nLeavesOut = s.nLeaves;
+    return t;
+}

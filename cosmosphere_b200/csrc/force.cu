@@ -1,0 +1,251 @@
+/*
+ * force.cu -- the SPH force pass over the symmetric j-leaf lists: per-particle factors
+ * (src/force.cu:92-137), pressure + artificial-viscosity accelerations, du/dt, vsigmax
+ * and div v (src/force.cu:145-383), and the list rebuild with its hmax upsweep
+ * (src/force.cu:19-88).  One warp per i-leaf; j runs in ascending Hilbert index, as the
+ * oracle's, so the plain FP64 results agree with it bit for bit.
+ */
+#include <algorithm>
+
+#include "state.hpp"
+
+namespace cosmo {
+
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kThreads = 32 * kWarpsPerBlock;
+
+__global__ void force_prep_kernel(const double4* __restrict__ xyzh, const double* __restrict__ gradh,
+                                  const double4* __restrict__ thermo4, int n, double pmass, double alphau,
+                                  double hfact, double4* __restrict__ prepA, double4* __restrict__ prepB)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double hi = xyzh[i].w;
+    if (!(hi > 0.0))
+    {
+        prepA[i] = make_double4(0, 0, 0, 0);
+        prepB[i] = make_double4(0, 0, 0, 0);
+        return;
+    }
+    const double hsq = 1.0 / (hi * hi);
+    const double h4 = hsq * hsq;
+    const double hfoh = hfact / hi;
+    const double rho = pmass * hfoh * hfoh * hfoh;
+    const double dhdrho = -hi / (3.0 * rho);
+    const double omega = 1.0 - dhdrho * gradh[i];
+    const double oinv = (omega > 0.0) ? (1 / omega) : 1.0;
+    const double pro2 = thermo4[i].x;
+    prepA[i] = make_double4(hsq, 1.0 / hi, rho, 1.0 / rho);
+    prepB[i] = make_double4(h4 * kCnormk * oinv, pro2 * rho * rho, 0.5 * pmass * (1.0 / rho) * alphau,
+                            kCnormk * oinv * h4 / rho);
+}
+
+template<bool Periodic, bool Disc>
+__global__ void __launch_bounds__(kThreads)
+force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __restrict__ jOffset,
+             const uint32_t* __restrict__ jcount, const int* __restrict__ jlist, const double4* __restrict__ xyzh,
+             const double4* __restrict__ vel4, const double4* __restrict__ thermo4,
+             const double4* __restrict__ prepA, const double4* __restrict__ prepB, double* __restrict__ fx,
+             double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ f4,
+             double* __restrict__ vsigmax, double* __restrict__ divvF, double pmass, double beta, int pdv,
+             int shock, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nWarps = (gridDim.x * blockDim.x) >> 5;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    unsigned long long pairs = 0;
+    const double pm = pmass;
+    for (int leaf = warpGlobal; leaf < nL; leaf += nWarps)
+    {
+        const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
+        const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
+        for (uint32_t g = p0; g < p1; g += 32)
+        {
+            const uint32_t i = g + lane;
+            const bool mine = i < p1;
+            const uint32_t ii = mine ? i : p0;
+            const double4 pi = xyzh[ii];
+            const double4 vi = vel4[ii];
+            const double4 ti = thermo4[ii];
+            const double4 ai = prepA[ii];
+            const double4 bi = prepB[ii];
+            const double hi = pi.w;
+            const double pro2i = ti.x, vwavei = ti.y, alphai = ti.z, eni = ti.w;
+            const double hsqinvi = ai.x, hinvi = ai.y, rhoi = ai.z, rho1i = ai.w;
+            const double grkfaci = bi.x, pri = bi.y, autermi = bi.z;
+            double itx = 0, ity = 0, itz = 0, jtx = 0, jty = 0, jtz = 0;
+            double f4s = 0.0, vsm = 0.0, divs = 0.0;
+            unsigned int gp = 0;
+            for (uint32_t jl = 0; jl < nj; ++jl)
+            {
+                const int jLeaf = jlist[jb + jl];
+                const uint32_t q0 = layout[jLeaf], q1 = layout[jLeaf + 1];
+                for (uint32_t j = q0; j < q1; ++j)
+                {
+                    const double4 pj = ldg4(xyzh + j);
+                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                    const double dr2 = pair_r2(dx, dy, dz);
+                    if (!(dr2 > 0.0)) continue;
+                    const double hj = pj.w;
+                    {
+                        const double rmax2 = kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10);
+                        if (dr2 >= rmax2) continue;
+                    }
+                    const double4 aj = ldg4(prepA + j);
+                    const double qi2 = dr2 * hsqinvi;
+                    const double qj2 = dr2 * aj.x;
+                    const double dr = sqrt(dr2);
+                    const double rij1 = 1.0 / dr;
+                    const double rx = dx * rij1, ry = dy * rij1, rz = dz * rij1;
+                    const double4 vj = ldg4(vel4 + j);
+                    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+                    const double projv = dvx * rx + dvy * ry + dvz * rz;
+                    const double4 tj = ldg4(thermo4 + j);
+                    const double4 bj = ldg4(prepB + j);
+                    const double rhoj = aj.z, rho1j = aj.w, pro2j = tj.x;
+                    const double vwavej = tj.y, alphaj = tj.z, enj = tj.w;
+                    const double prj = bj.y, autermj = bj.z;
+                    const double vsigi = fmax(vwavei - beta * projv, 0.0);
+                    const double vsigavi = fmax(alphai * vwavei - beta * projv, 0.0);
+                    const double vsigj = fmax(vwavej - beta * projv, 0.0);
+                    const double vsigavj = fmax(alphaj * vwavej - beta * projv, 0.0);
+                    const double pvs = fmax(vsigi, vsigj);
+                    double qr2i = 0.0, qr2j = 0.0;
+                    const double denij = eni - enj;
+                    const double vsigu = sqrt(fabs(pri - prj) * (2.0 / (rhoi + rhoj)));
+                    if (Disc)
+                    {
+                        const double hori = hi * rij1, horj = hj * rij1;
+                        if (projv < 0.0)
+                        {
+                            qr2i = -0.5 * rho1i * (alphai * vwavei - beta * projv) * hori * projv;
+                            qr2j = -0.5 * rho1j * (alphaj * vwavej - beta * projv) * horj * projv;
+                        }
+                        else
+                        {
+                            qr2i = -0.5 * rho1i * alphai * vwavei * hori * projv;
+                            qr2j = -0.5 * rho1j * alphaj * vwavej * horj * projv;
+                        }
+                    }
+                    else if (projv < 0.0)
+                    {
+                        qr2i = -0.5 * rho1i * vsigavi * projv;
+                        qr2j = -0.5 * rho1j * vsigavj * projv;
+                    }
+                    bool took = false;
+                    if (qi2 < kRadK2)
+                    {
+                        took = true;
+                        vsm = fmax(vsm, pvs);
+                        double wk, dwk;
+                        const double q = dr * hinvi;
+                        sph_kernel(qi2, q, wk, dwk);
+                        divs += pm * dwk * projv;
+                        const double gki = dwk * grkfaci;
+                        const double gpi = pm * (pro2i + qr2i) * gki;
+                        itx += -gpi * rx; ity += -gpi * ry; itz += -gpi * rz;
+                        const double pdvi = pm * pro2i * projv * gki;
+                        const double dissi = Disc
+                            ? -0.5 * pm * rho1i * alphai * vwavei * (hi * rij1) * projv * projv * gki
+                            : pm * qr2i * projv * gki;
+                        const double condi = vsigu * denij * autermi * gki;
+                        if (pdv) f4s += pdvi;
+                        if (shock) f4s += dissi;
+                        f4s += condi;
+                    }
+                    if (qj2 < kRadK2)
+                    {
+                        took = true;
+                        vsm = fmax(vsm, pvs);
+                        double wk, dwk;
+                        const double q = dr * aj.y;
+                        sph_kernel(qj2, q, wk, dwk);
+                        const double gkj = dwk * bj.x;
+                        const double gpj = pm * (pro2j + qr2j) * gkj;
+                        jtx -= gpj * rx; jty -= gpj * ry; jtz -= gpj * rz;
+                        f4s += vsigu * denij * autermj * gkj;
+                    }
+                    if (took) ++gp;
+                }
+            }
+            if (!mine) continue;
+            pairs += gp;
+            fx[i] = itx + jtx;
+            fy[i] = ity + jty;
+            fz[i] = itz + jtz;
+            f4[i] = f4s;
+            vsigmax[i] = vsm;
+            divvF[i] = -divs * bi.w;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    if (lane == 0) atomicAdd(&ds->pairs[2], pairs);
+}
+
+// Dead particles: no force (src/force.cu:191-200).
+__global__ void force_dead_kernel(int nAlive, int n, double* fx, double* fy, double* fz, double* f4,
+                                  double* vsigmax, double* divvF)
+{
+    const long i = nAlive + long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    fx[i] = 0.0; fy[i] = 0.0; fz[i] = 0.0; f4[i] = 0.0; vsigmax[i] = 0.0; divvF[i] = 0.0;
+}
+
+} // namespace
+
+void compute_forces(State& s, double pmass, double beta, double alphau, bool disc, bool pdv, bool shock)
+{
+    const int n = s.ngas;
+    DevScalars* ds = s.dscal.get();
+    COSMO_CUDA(cudaMemsetAsync(&ds->pairs[2], 0, sizeof(unsigned long long), s.st));
+    cudaEvent_t e0 = ev(s);
+    // The symmetric list is cached per tree (src/force.cu:19-24).
+    if (s.jlistToken != s.token)
+    {
+        hmax_upsweep(s);
+        cudaEvent_t e1 = ev(s);
+        build_lists(s, true);
+        s.jlistToken = s.token;
+        cudaEvent_t e2 = ev(s);
+        COSMO_CUDA(cudaStreamSynchronize(s.st));
+        s.t.upsweep += elapsed_s(e0, e1);
+        s.t.fjbuild += elapsed_s(e1, e2);
+    }
+    cudaEvent_t p0 = ev(s);
+    force_prep_kernel<<<iceil(n, 256), 256, 0, s.st>>>(s.xyzh.get(), s.gradh.get(), s.thermo4.get(), n, pmass,
+                                                       alphau, s.hfact, s.prepA.get(), s.prepB.get());
+    COSMO_LAUNCHED();
+    cudaEvent_t p1 = ev(s);
+    const int nL = s.nLeaves;
+    const int grid = std::max(1, std::min(s.numSMs * 8, iceil(nL, kWarpsPerBlock)));
+    auto launch = [&](auto kern) {
+        kern<<<grid, kThreads, 0, s.st>>>(nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
+                                          s.xyzh.get(), s.vel4.get(), s.thermo4.get(), s.prepA.get(),
+                                          s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(),
+                                          s.vsigmax.get(), s.divvF.get(), pmass, beta, pdv ? 1 : 0,
+                                          shock ? 1 : 0, s.box.get(), ds);
+    };
+    if (s.periodic) { if (disc) launch(force_kernel<true, true>); else launch(force_kernel<true, false>); }
+    else { if (disc) launch(force_kernel<false, true>); else launch(force_kernel<false, false>); }
+    COSMO_LAUNCHED();
+    if (n > s.nAlive)
+    {
+        force_dead_kernel<<<iceil(n - s.nAlive, 256), 256, 0, s.st>>>(s.nAlive, n, s.fx.get(), s.fy.get(),
+                                                                      s.fz.get(), s.f4.get(), s.vsigmax.get(),
+                                                                      s.divvF.get());
+        COSMO_LAUNCHED();
+    }
+    cudaEvent_t p2 = ev(s);
+    read_scalars(s);
+    s.t.prep += elapsed_s(p0, p1);
+    s.t.fkern += elapsed_s(p1, p2);
+    check_dev_err(s, "force_gpu_c");
+}
+
+} // namespace cosmo

@@ -1,0 +1,163 @@
+/*
+ * state.hpp -- the persistent device state behind the C-ABI: the B200 counterpart of the
+ * reference's GpuState (include/gpu_state.hpp:36-123).
+ *
+ * Layout in HBM (all Hilbert-ordered arrays are indexed by sorted position k):
+ *   caller order   ux uy uz uh | uvx uvy uvz | uax uay uaz    upload targets (f64 SoA)
+ *   Hilbert order  xyzh   double4 (x, y, z, h)                 TMA/128-bit friendly
+ *                  vel4   double4 (vx, vy, vz, 0), acc4 likewise
+ *                  thermo4 double4 (pro2, cs, alpha, u)
+ *                  prepA  double4 (1/h^2, 1/h, rho(h), 1/rho)   force per-particle factors
+ *                  prepB  double4 (grkfac, P, auterm, divfac)
+ *                  rho gradh divv xi ddivvdt, fx fy fz f4 vsigmax divvF   f64 SoA
+ *   tree           cornerstone leaf array, linked octree (BFS), pre-order walk arrays,
+ *                  CSR j-leaf lists
+ * Buffers grow and are never freed: like the reference's state, it is deliberately
+ * leaked so no CUDA call runs during static teardown.
+ */
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace cosmo {
+
+template<class T>
+struct DBuf
+{
+    T*     p   = nullptr;
+    size_t n   = 0;
+    size_t cap = 0;
+
+    // Grow to hold c elements.  Contents are kept only when keep is set; new memory is
+    // zeroed, as the reference's thrust::device_vector value-initialises.
+    void resize(size_t c, cudaStream_t st, bool keep = false)
+    {
+        if (c > cap)
+        {
+            T* q = nullptr;
+            const size_t newCap = c + c / 8 + 16;
+            COSMO_CUDA(cudaMalloc(&q, newCap * sizeof(T)));
+            COSMO_CUDA(cudaMemsetAsync(q, 0, newCap * sizeof(T), st));
+            if (keep && p && n) COSMO_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            if (p)
+            {
+                COSMO_CUDA(cudaStreamSynchronize(st));
+                COSMO_CUDA(cudaFree(p));
+            }
+            p = q;
+            cap = newCap;
+        }
+        n = c;
+    }
+    T* get() const { return p; }
+};
+
+// Device-side scalars, one block, so a solve reads its counters with one copy.
+struct DevScalars
+{
+    int nAlive;
+    int err;                     // DevErr bits
+    int nextActive;              // active-leaf appends of the current NR iteration
+    int unconverged;             // particles left unconverged by the current iteration
+    int workCounter[4];          // dynamic work distribution for persistent kernels
+    unsigned long long pairs[4]; // accepted pairs: density, gradient, force, candidates
+    unsigned int sortTiles[16];  // onesweep tile tickets, one per digit pass
+    int pad[8];
+};
+
+struct Timings
+{
+    double bbox = 0, keysSort = 0, tree = 0, nodes = 0, jbuild = 0, nrkern = 0, gjbuild = 0,
+           gradkern = 0, upsweep = 0, fjbuild = 0, prep = 0, fkern = 0;
+};
+
+struct State
+{
+    cudaStream_t st = nullptr;
+    int device = -1;
+    int numSMs = 148;
+
+    int sizedFor = 0;      // particle count the arrays were sized for (cosmo_arrays_init)
+    int orderFor = 0;      // particle count the current Hilbert ordering belongs to
+    int ngas = 0, nAlive = 0, nLeaves = 0, numNodes = 0;
+    double pmass = 0.0, hfact = 0.0;
+    int periodic = 0;
+    double boxHost[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t token = 0, jlistToken = 0;
+    int itersRun = 0, maxIter = 100;
+    std::vector<long long> activePerIter;
+    double uploadSeconds = 0.0, downloadSeconds = 0.0;
+    Timings t;
+
+    // caller-order upload targets
+    DBuf<double> ux, uy, uz, uh, uvx, uvy, uvz, uax, uay, uaz;
+    // Hilbert-order particle data
+    DBuf<double4> xyzh, vel4, acc4, thermo4, prepA, prepB;
+    DBuf<double> rho, gradh, divv, xi, ddivvdt, fx, fy, fz, f4, vsigmax, divvF;
+    DBuf<double> xfer;                          // 6n: one slot's worth of host traffic
+    DBuf<uint64_t> keysA, keysB;
+    DBuf<int> orderA, orderB, particleLeaf, converged;
+
+    // tree
+    DBuf<DevBox> box;
+    DBuf<uint64_t> csTree, csTree2;
+    DBuf<uint32_t> counts, ops, opsScan, layout;
+    DBuf<uint64_t> prePrefix, bfsPrefix;
+    DBuf<uint32_t> nodeCount, leafPreStart;
+    DBuf<int> preLeaf, preSkip, bfsToPre, preToBfs;
+    DBuf<int> childOffsets, internalToLeaf, levelRange, leafToInternal;
+    DBuf<double> centers, sizes;                // 3 per BFS node
+    DBuf<double4> preCenter, preHalf;           // pre-order copies for the walk
+    DBuf<double> hmaxLeaf, hmaxNode, hmaxPre;
+    DBuf<uint32_t> jcount, jOffset;
+    DBuf<int> jlist;
+    DBuf<int> activeA, activeB, allLeaves;
+
+    // scratch
+    DBuf<uint32_t> scanTmp, sortHist, sortBase, sortLookback;
+    DBuf<uint64_t> nodeKeysTmp;
+    DBuf<int> nodeValsTmp;
+    DBuf<double> redTmp;
+    DBuf<DevScalars> dscal;
+    DevScalars* hscal = nullptr;                // pinned host mirror
+    int* hsmall = nullptr;                      // pinned scratch for small reads (64 ints)
+};
+
+State& state();
+void ensure_init(State& s);
+void size_particle_arrays(State& s, int n);
+
+// tree.cu
+void build_tree(State& s, const double* periodicBox, bool alsoSortVA);
+void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
+void build_lists(State& s, bool symmetric);
+void hmax_upsweep(State& s);
+void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int n, bool iotaValues);
+uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool readTotal);
+
+// density.cu
+struct DensResult { int itersRun; int unconverged; int status; };
+DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh,
+                         double hfact, int maxIter, bool withGradients);
+
+// force.cu
+void compute_forces(State& s, double pmass, double beta, double alphau, bool disc, bool pdv,
+                    bool shock);
+
+// timing helpers
+struct EventPair
+{
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+double elapsed_s(cudaEvent_t a, cudaEvent_t b);
+cudaEvent_t ev(State& s);            // record an event on the state's stream (pooled)
+void ev_reset();
+
+void read_scalars(State& s);         // dscal -> hscal, synchronising the stream
+void check_dev_err(State& s, const char* where);
+
+} // namespace cosmo

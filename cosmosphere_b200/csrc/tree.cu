@@ -1,0 +1,898 @@
+/*
+ * tree.cu -- Hilbert keys, the onesweep radix sort, the cornerstone leaf tree, the linked
+ * octree with node geometry, hmax, and the j-leaf list walk.  The B200 counterpart of the
+ * reference's src/tree.cu and include/tree.cuh, written without Thrust or Cornerstone.
+ *
+ * Parity notes (the oracle restates the same definitions):
+ *   keys     21-bit quantisation of (x - lo) * 2^21/len, Skilling's Hilbert curve;
+ *            h <= 0 (or NaN) gives ~0, which sorts last (include/tree.cuh:89-105).
+ *   sort     stable LSD radix sort of (key, index): the order is the unique stable one.
+ *   leaves   split from the root while a node holds more than 64 particles (a level-21
+ *            node never splits): the fixed point of src/tree.cu:126-136 from its seed.
+ *   octree   BFS order = placeholder prefixes sorted, as Cornerstone's OctreeData;
+ *            childOffsets 0 marks a leaf, internalToLeaf is -1 for internal nodes.
+ *   lists    the reference's accept tests (include/tree.cuh:228-252); leaves emitted in
+ *            ascending order by a stackless pre-order scan (no stack, nothing dropped).
+ */
+#include <algorithm>
+
+#include "state.hpp"
+
+namespace cosmo {
+
+namespace {
+
+constexpr int kBlk = 256;
+
+__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+// ------------------------------------------------------------------ scan (3 phase)
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems   = 4;
+constexpr int kScanTile    = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive prefix and
+// the block total in *total.
+__device__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
+{
+    __shared__ uint32_t sw[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    const uint32_t inc = warp_incl_scan(v);
+    if (lane == 31) sw[warp] = inc;
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint32_t s = lane < nw ? sw[lane] : 0;
+        s = warp_incl_scan(s);
+        sw[lane] = s;
+    }
+    __syncthreads();
+    const uint32_t before = warp ? sw[warp - 1] : 0;
+    *total = sw[nw - 1];
+    __syncthreads();
+    return before + inc - v;
+}
+
+__global__ void scan_reduce_kernel(const uint32_t* __restrict__ in, int n, uint32_t* __restrict__ bsum)
+{
+    const long base = long(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) s += in[base + k];
+    uint32_t tot;
+    block_excl_scan(s, &tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void scan_blocks_kernel(uint32_t* bsum, int nb, uint32_t* totalOut)
+{
+    // one block of kScanThreads; nb <= kScanTile
+    const int base = threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+    {
+        v[k] = (base + k < nb) ? bsum[base + k] : 0;
+        s += v[k];
+    }
+    uint32_t tot;
+    uint32_t run = block_excl_scan(s, &tot);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < nb)
+        {
+            bsum[base + k] = run;
+            run += v[k];
+        }
+    if (threadIdx.x == 0) *totalOut = tot;
+}
+
+__global__ void scan_apply_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int n,
+                                  const uint32_t* __restrict__ boff)
+{
+    const long base = long(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+    {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    uint32_t tot;
+    uint32_t run = block_excl_scan(s, &tot) + boff[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n)
+        {
+            out[base + k] = run;
+            run += v[k];
+        }
+}
+
+// ------------------------------------------------------------------ onesweep radix sort
+constexpr int kSortThreads = 256;
+constexpr int kSortIpt     = 16;
+constexpr int kSortTile    = kSortThreads * kSortIpt;
+constexpr int kSortWarps   = kSortThreads / 32;
+constexpr int kSortPasses  = 8;
+constexpr uint32_t kLbAgg  = 1u << 30, kLbInc = 2u << 30, kLbMask = (1u << 30) - 1;
+
+__global__ void digit_hist_kernel(const uint64_t* __restrict__ keys, int n, uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t s[kSortPasses][256];
+    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) (&s[0][0])[i] = 0;
+    __syncthreads();
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const uint64_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < kSortPasses; ++p) atomicAdd(&s[p][(k >> (8 * p)) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x)
+        if ((&s[0][0])[i]) atomicAdd(&hist[i], (&s[0][0])[i]);
+}
+
+__global__ void digit_base_kernel(const uint32_t* __restrict__ hist, uint32_t* __restrict__ base)
+{
+    // block p scans the 256 bins of pass p
+    const uint32_t v = hist[blockIdx.x * 256 + threadIdx.x];
+    uint32_t tot;
+    base[blockIdx.x * 256 + threadIdx.x] = block_excl_scan(v, &tot);
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+onesweep_kernel(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uint64_t* __restrict__ kout,
+                int* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ binBase,
+                uint32_t* lookback, unsigned int* tileTicket, int* err)
+{
+    __shared__ uint32_t sHist[kSortWarps][256];
+    __shared__ uint32_t sBase[256];
+    __shared__ int sTile;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < kSortWarps * 256; i += kSortThreads) (&sHist[0][0])[i] = 0;
+    if (tid == 0) sTile = int(atomicAdd(tileTicket, 1u));
+    __syncthreads();
+    const int tile = sTile;
+    const long base = long(tile) * kSortTile + long(warp) * 32 * kSortIpt;
+
+    uint64_t k[kSortIpt];
+    int v[kSortIpt];
+    uint32_t rank[kSortIpt];
+#pragma unroll
+    for (int it = 0; it < kSortIpt; ++it)
+    {
+        const long idx = base + it * 32 + lane;
+        if (idx < n) { k[it] = kin[idx]; v[it] = vin ? vin[idx] : int(idx); }
+        else { k[it] = 0; v[it] = 0; }
+    }
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int it = 0; it < kSortIpt; ++it)
+    {
+        const bool valid = (base + it * 32 + lane) < n;
+        const uint32_t d = valid ? uint32_t(k[it] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t c = 0;
+        if (valid) c = sHist[warp][d];
+        __syncwarp();
+        rank[it] = c + __popc(peers & lt);
+        if (valid && (peers & lt) == 0u) sHist[warp][d] = c + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const int d = tid;
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+        {
+            const uint32_t c = sHist[w][d];
+            sHist[w][d] = total;
+            total += c;
+        }
+        uint32_t* mine = lookback + size_t(tile) * 256 + d;
+        if (tile == 0)
+        {
+            atomicExch(mine, kLbInc | total);
+            sBase[d] = binBase[d];
+        }
+        else
+        {
+            atomicExch(mine, kLbAgg | total);
+            uint32_t excl = 0;
+            int p = tile - 1;
+            long long spins = 0;
+            while (p >= 0)
+            {
+                const uint32_t s = ld_volatile_u32(lookback + size_t(p) * 256 + d);
+                if ((s & ~kLbMask) == 0u)
+                {
+                    if (++spins > kSpinLimit) { atomicOr(err, int(kErrSortSpin)); break; }
+                    continue;
+                }
+                excl += s & kLbMask;
+                if (s & kLbInc) break;
+                --p;
+            }
+            atomicExch(mine, kLbInc | (excl + total));
+            sBase[d] = binBase[d] + excl;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kSortIpt; ++it)
+    {
+        const long idx = base + it * 32 + lane;
+        if (idx < n)
+        {
+            const uint32_t d = uint32_t(k[it] >> shift) & 255u;
+            const uint32_t pos = sBase[d] + sHist[warp][d] + rank[it];
+            kout[pos] = k[it];
+            vout[pos] = v[it];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ bbox and keys
+__global__ void bbox_partial_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                                    const double* __restrict__ z, int n, double* __restrict__ part)
+{
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+    {
+        const double c[3] = {x[i], y[i], z[i]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { mn[d] = fmin(mn[d], c[d]); mx[d] = fmax(mx[d], c[d]); }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    __shared__ double s[8][6];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) { s[warp][d] = mn[d]; s[warp][3 + d] = mx[d]; }
+    __syncthreads();
+    if (threadIdx.x < 6)
+    {
+        const int c = threadIdx.x;
+        double v = s[0][c];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) v = (c < 3) ? fmin(v, s[w][c]) : fmax(v, s[w][c]);
+        part[blockIdx.x * 6 + c] = v;
+    }
+}
+
+// Open boundaries (src/tree.cu:54-72): a cube of side 1.00001 x the largest span,
+// centred on the particles.
+__global__ void bbox_final_kernel(const double* __restrict__ part, int nb, DevBox* box)
+{
+    if (threadIdx.x != 0) return;
+    double mn[3], mx[3];
+    for (int d = 0; d < 3; ++d) { mn[d] = part[d]; mx[d] = part[3 + d]; }
+    for (int b = 1; b < nb; ++b)
+        for (int d = 0; d < 3; ++d) { mn[d] = fmin(mn[d], part[6 * b + d]); mx[d] = fmax(mx[d], part[6 * b + 3 + d]); }
+    const double sx = mx[0] - mn[0], sy = mx[1] - mn[1], sz = mx[2] - mn[2];
+    double span = (sx < sy) ? sy : sx;
+    span = (span < sz) ? sz : span;
+    span = span * 1.00001;
+    const double half = 0.5 * span;
+    DevBox b;
+    for (int d = 0; d < 3; ++d)
+    {
+        const double ctr = 0.5 * (mn[d] + mx[d]);
+        b.lo[d] = ctr - half;
+        b.hi[d] = ctr + half;
+    }
+    b.periodic = 0;
+    box_finish(b);
+    *box = b;
+}
+
+__global__ void set_box_kernel(double x0, double x1, double y0, double y1, double z0, double z1, DevBox* box)
+{
+    if (threadIdx.x != 0) return;
+    DevBox b;
+    b.lo[0] = x0; b.hi[0] = x1; b.lo[1] = y0; b.hi[1] = y1; b.lo[2] = z0; b.hi[2] = z1;
+    b.periodic = 1;
+    box_finish(b);
+    *box = b;
+}
+
+__global__ void keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
+                            const double* __restrict__ z, const double* __restrict__ h, int n,
+                            const DevBox* __restrict__ box, uint64_t* __restrict__ keys)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DevBox b = *box;
+    uint64_t k = kDeadKey;
+    if (h[i] > 0.0)
+        k = hilbert_key(quantise(x[i], b.lo[0], b.scale[0]), quantise(y[i], b.lo[1], b.scale[1]),
+                        quantise(z[i], b.lo[2], b.scale[2]));
+    keys[i] = k;
+}
+
+// nAlive = first dead key (keys sorted).
+__global__ void alive_kernel(const uint64_t* __restrict__ keys, int n, DevScalars* ds)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool dead = keys[i] == kDeadKey;
+    const bool prevAlive = (i == 0) ? true : keys[i - 1] != kDeadKey;
+    if (dead && prevAlive) ds->nAlive = int(i);
+    if (!dead && i == n - 1) ds->nAlive = n;
+}
+
+__global__ void gather_particles_kernel(const int* __restrict__ order, int n,
+                                        const double* __restrict__ ux, const double* __restrict__ uy,
+                                        const double* __restrict__ uz, const double* __restrict__ uh,
+                                        double4* __restrict__ xyzh, const double* __restrict__ uvx,
+                                        const double* __restrict__ uvy, const double* __restrict__ uvz,
+                                        const double* __restrict__ uax, const double* __restrict__ uay,
+                                        const double* __restrict__ uaz, double4* __restrict__ vel4,
+                                        double4* __restrict__ acc4, int alsoVA)
+{
+    const long k = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = order[k];
+    xyzh[k] = make_double4(ux[i], uy[i], uz[i], uh[i]);
+    if (alsoVA)
+    {
+        vel4[k] = make_double4(uvx[i], uvy[i], uvz[i], 0.0);
+        acc4[k] = make_double4(uax[i], uay[i], uaz[i], 0.0);
+    }
+}
+
+// ------------------------------------------------------------------ leaf tree
+__device__ __forceinline__ uint32_t lower_bound_u64(const uint64_t* a, uint32_t n, uint64_t v)
+{
+    uint32_t lo = 0, hi = n;
+    while (lo < hi)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void leaf_count_kernel(const uint64_t* __restrict__ tree, int nL, const uint64_t* __restrict__ keys,
+                                  const DevScalars* __restrict__ ds, uint32_t* __restrict__ counts,
+                                  uint32_t* __restrict__ ops)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nL) return;
+    const uint32_t na = uint32_t(ds->nAlive);
+    const uint64_t a = tree[i], b = tree[i + 1];
+    const uint32_t c = lower_bound_u64(keys, na, b) - lower_bound_u64(keys, na, a);
+    counts[i] = c;
+    const int L = level_of_range(b - a);
+    ops[i] = (c > kBucket && L < kMaxLevel) ? 8u : 1u;
+}
+
+__global__ void leaf_split_kernel(const uint64_t* __restrict__ tree, int nL, const uint32_t* __restrict__ ops,
+                                  const uint32_t* __restrict__ pos, uint64_t* __restrict__ out)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i > nL) return;
+    if (i == nL) { out[pos[nL]] = kKeyEnd; return; }
+    const uint64_t a = tree[i];
+    const uint32_t p = pos[i];
+    if (ops[i] == 8u)
+    {
+        const uint64_t child = (tree[i + 1] - a) >> 3;
+        for (int o = 0; o < 8; ++o) out[p + o] = a + uint64_t(o) * child;
+    }
+    else out[p] = a;
+}
+
+// ------------------------------------------------------------------ linked octree
+__device__ __forceinline__ int first_aligned_level(uint64_t k)
+{
+    if (k == 0) return 0;
+    const int tz = __ffsll((long long)k) - 1;
+    const int L0 = kMaxLevel - tz / 3;
+    return L0 < 0 ? 0 : L0;
+}
+
+__global__ void node_count_kernel(const uint64_t* __restrict__ tree, int nL, uint32_t* __restrict__ cnt)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nL) return;
+    const uint64_t k = tree[i];
+    const int L = level_of_range(tree[i + 1] - k);
+    const int L0 = first_aligned_level(k);
+    cnt[i] = uint32_t((L > L0 ? L - L0 : 0) + 1);
+}
+
+// Pre-order emission: each leaf writes the internal nodes that start at its key
+// (shallowest first) and then itself.  skip = size of the node's subtree in pre-order.
+__global__ void node_emit_kernel(const uint64_t* __restrict__ tree, int nL, const uint32_t* __restrict__ start,
+                                 int numNodes, uint64_t* __restrict__ prePrefix, int* __restrict__ preLeaf,
+                                 int* __restrict__ preSkip)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nL) return;
+    const uint64_t k = tree[i];
+    const int L = level_of_range(tree[i + 1] - k);
+    const int L0 = first_aligned_level(k);
+    uint32_t pos = start[i];
+    for (int a = (L0 < L ? L0 : L); a <= L; ++a, ++pos)
+    {
+        prePrefix[pos] = encode_prefix(k, a);
+        preLeaf[pos] = (a == L) ? int(i) : -1;
+        const uint64_t end = k + node_range(a);
+        const uint32_t endLeaf = lower_bound_u64(tree, uint32_t(nL + 1), end);
+        const uint32_t next = (endLeaf < uint32_t(nL)) ? start[endLeaf] : uint32_t(numNodes);
+        preSkip[pos] = int(next - pos);
+    }
+}
+
+__global__ void bfs_link_kernel(const uint64_t* __restrict__ bfsPrefix, const int* __restrict__ bfsToPre,
+                                int numNodes, const int* __restrict__ preLeaf, int* __restrict__ preToBfs,
+                                int* __restrict__ childOffsets, int* __restrict__ internalToLeaf,
+                                int* __restrict__ leafToInternal, int* __restrict__ levelRange,
+                                const DevBox* __restrict__ box, double* __restrict__ centers,
+                                double* __restrict__ sizes, double4* __restrict__ preCenter,
+                                double4* __restrict__ preHalf)
+{
+    const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (b >= numNodes) return;
+    const uint64_t p = bfsPrefix[b];
+    const int pre = bfsToPre[b];
+    preToBfs[pre] = int(b);
+    const int leaf = preLeaf[pre];
+    const int L = prefix_level(p);
+    if (leaf >= 0)
+    {
+        childOffsets[b] = 0;
+        internalToLeaf[b] = leaf;
+        leafToInternal[leaf] = int(b);
+    }
+    else
+    {
+        childOffsets[b] = int(lower_bound_u64(bfsPrefix, uint32_t(numNodes), p << 3));
+        internalToLeaf[b] = -1;
+    }
+    const int Lprev = (b == 0) ? -1 : prefix_level(bfsPrefix[b - 1]);
+    for (int l = Lprev + 1; l <= L; ++l) levelRange[l] = int(b);
+    if (b == numNodes - 1)
+        for (int l = L + 1; l <= kMaxLevel + 1; ++l) levelRange[l] = numNodes;
+
+    // Node geometry (include/tree.cuh:110-125): centre and half-size of the node's cube.
+    uint32_t ic[3];
+    hilbert_cell(prefix_start(p), ic[0], ic[1], ic[2]);
+    const uint32_t side = 1u << (kMaxLevel - L);
+    const double sd = double(side);
+    const DevBox bx = *box;
+    double c[3], s[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        const double corner = double(ic[d] & ~(side - 1u));
+        c[d] = bx.lo[d] + (corner + 0.5 * sd) * bx.unit[d];
+        s[d] = 0.5 * sd * bx.unit[d];
+        centers[3 * b + d] = c[d];
+        sizes[3 * b + d] = s[d];
+    }
+    preCenter[pre] = make_double4(c[0], c[1], c[2], 0.0);
+    preHalf[pre] = make_double4(s[0], s[1], s[2], 0.0);
+}
+
+__global__ void particle_leaf_kernel(const uint32_t* __restrict__ layout, int nL, int nAliveMax,
+                                     const DevScalars* __restrict__ ds, int* __restrict__ particleLeaf)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nAliveMax || i >= ds->nAlive) return;
+    // last leaf whose start <= i, skipping empty leaves: upper_bound(layout, i) - 1
+    uint32_t lo = 0, hi = uint32_t(nL + 1);
+    while (lo < hi)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (layout[mid] <= uint32_t(i)) lo = mid + 1;
+        else hi = mid;
+    }
+    particleLeaf[i] = int(lo) - 1;
+}
+
+__global__ void iota_kernel(int* __restrict__ a, int n)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = int(i);
+}
+
+// ------------------------------------------------------------------ hmax
+// include/tree.cuh:177-191: largest finite h of each listed leaf.
+__global__ void hmax_leaf_kernel(const double4* __restrict__ xyzh, const uint32_t* __restrict__ layout,
+                                 const int* __restrict__ leaves, int nActive, double* __restrict__ hmax)
+{
+    const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= nActive) return;
+    const int l = leaves[t];
+    double hm = 0.0;
+    for (uint32_t j = layout[l]; j < layout[l + 1]; ++j)
+    {
+        const double hj = xyzh[j].w;
+        if (isfinite(hj)) hm = fmax(hm, hj);
+    }
+    hmax[l] = hm;
+}
+
+// include/tree.cuh:196-217, one level, deepest first.
+__global__ void hmax_level_kernel(int first, int last, const int* __restrict__ childOffsets,
+                                  const int* __restrict__ internalToLeaf, const double* __restrict__ hmaxLeaf,
+                                  double* __restrict__ hmaxNode, const int* __restrict__ bfsToPre,
+                                  double* __restrict__ hmaxPre)
+{
+    const int i = first + int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= last) return;
+    const int c = childOffsets[i];
+    double m;
+    if (c == 0)
+    {
+        const double hm = hmaxLeaf[internalToLeaf[i]];
+        m = (isfinite(hm) && hm > 0.0) ? hm : 0.0;
+    }
+    else
+    {
+        m = 0.0;
+        for (int o = 0; o < 8; ++o) m = fmax(m, hmaxNode[c + o]);
+    }
+    hmaxNode[i] = m;
+    hmaxPre[bfsToPre[i]] = m;
+}
+
+// ------------------------------------------------------------------ j-leaf list walk
+// One warp per i-leaf.  The tree is scanned in pre-order 32 nodes at a time: every lane
+// tests one node; the nodes before the first rejected one are all reached (an accepted
+// node is followed by its successor in pre-order), so their leaves are emitted in order,
+// and the scan resumes after the rejected node's subtree.  Accepted leaves therefore come
+// out in ascending order, nothing is stacked, and nothing can be dropped.
+template<bool Symmetric, bool Periodic, bool Fill>
+__global__ void __launch_bounds__(kBlk)
+list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
+                 const double* __restrict__ centers, const double* __restrict__ sizes,
+                 const double* __restrict__ hmaxLeaf, const double4* __restrict__ preCenter,
+                 const double4* __restrict__ preHalf, const int* __restrict__ preSkip,
+                 const int* __restrict__ preLeaf, const double* __restrict__ hmaxPre,
+                 const DevBox* __restrict__ box, uint32_t* __restrict__ jcount,
+                 const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err)
+{
+    const int lane = threadIdx.x & 31;
+    const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (leaf >= nL) return;
+    const int iNode = leafToInternal[leaf];
+    const double icx = centers[3 * iNode], icy = centers[3 * iNode + 1], icz = centers[3 * iNode + 2];
+    const double isx = sizes[3 * iNode], isy = sizes[3 * iNode + 1], isz = sizes[3 * iNode + 2];
+    double hmax = hmaxLeaf[leaf];
+    if (!isfinite(hmax) || hmax <= 0.0) hmax = 0.0;
+    const double radHi = kRadKernel * hmax;
+    // gather: the i-box inflated by radHi; symmetric: the raw i-box
+    const double ax = Symmetric ? isx : isx + radHi;
+    const double ay = Symmetric ? isy : isy + radHi;
+    const double az = Symmetric ? isz : isz + radHi;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+
+    uint32_t count = 0, base = 0, cap = 0;
+    if (Fill) { base = jOffset[leaf]; cap = jOffset[leaf + 1] - base; }
+    const uint32_t lt = (1u << lane) - 1u;
+
+    int p = 0;
+    while (p < numNodes)
+    {
+        const int idx = p + lane;
+        const bool valid = idx < numNodes;
+        bool accept = false;
+        int skip = 1, pl = -1;
+        if (valid)
+        {
+            const double4 c = preCenter[idx];
+            const double4 s = preHalf[idx];
+            double dd[3] = {fabs(icx - c.x), fabs(icy - c.y), fabs(icz - c.z)};
+            if (Periodic)
+            {
+                dd[0] = fmin(dd[0], lx - dd[0]);
+                dd[1] = fmin(dd[1], ly - dd[1]);
+                dd[2] = fmin(dd[2], lz - dd[2]);
+            }
+            const double g0 = dd[0] - ax - s.x, g1 = dd[1] - ay - s.y, g2 = dd[2] - az - s.z;
+            const double d0 = (g0 > 0.0) ? g0 : 0.0, d1 = (g1 > 0.0) ? g1 : 0.0, d2 = (g2 > 0.0) ? g2 : 0.0;
+            const double n2 = d0 * d0 + d1 * d1 + d2 * d2;
+            if (Symmetric)
+            {
+                const double rs = fmax(radHi, kRadKernel * hmaxPre[idx]);
+                accept = n2 <= rs * rs;
+            }
+            else accept = n2 <= 0.0;
+            skip = preSkip[idx];
+            pl = preLeaf[idx];
+        }
+        const uint32_t validMask = __ballot_sync(0xffffffffu, valid);
+        const uint32_t rejMask = __ballot_sync(0xffffffffu, valid && !accept);
+        // Walk the window: runs of reached nodes end at a rejection, after which the scan
+        // jumps over that node's subtree; a jump that lands inside the window continues.
+        int pos = 0;        // offset of the next reached node in this window
+        int next = p + 32;  // where the following window starts
+        for (;;)
+        {
+            const uint32_t fromPos = (pos >= 32) ? 0u : (0xffffffffu << pos);
+            const uint32_t rej = rejMask & fromPos;
+            const int r = rej ? (__ffs(rej) - 1) : 32;
+            // lanes [pos, r) are reached and accepted
+            const uint32_t runMask = validMask & fromPos & ((r >= 32) ? 0xffffffffu : ((1u << r) - 1u));
+            const uint32_t emitMask = __ballot_sync(0xffffffffu, ((runMask >> lane) & 1u) && pl >= 0);
+            if (Fill)
+            {
+                if ((emitMask >> lane) & 1u)
+                {
+                    const uint32_t slot = count + __popc(emitMask & lt);
+                    if (slot < cap) jlist[base + slot] = pl;
+                    else atomicOr(err, int(kErrListCap));
+                }
+            }
+            count += __popc(emitMask);
+            if (r >= 32) { next = p + 32; break; }
+            int rskip = __shfl_sync(0xffffffffu, skip, r);
+            if (rskip < 1) rskip = 1;   // a subtree holds its root: the scan always advances
+            const int target = p + r + rskip;
+            if (target >= p + 32 || target >= numNodes) { next = target; break; }
+            pos = target - p;
+        }
+        p = next;
+    }
+    if (lane == 0)
+    {
+        if (Fill) { if (count != cap) atomicOr(err, int(kErrListCap)); }
+        else jcount[leaf] = count;
+    }
+}
+
+} // namespace
+
+// ====================================================================== host side
+uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool readTotal)
+{
+    const int nb = std::max(1, iceil(n, kScanTile));
+    if (nb > kScanTile) fatal("scan_exclusive: %d elements exceed the scan capacity", n);
+    s.scanTmp.resize(size_t(nb) + 1, s.st);
+    uint32_t* bsum = s.scanTmp.get();
+    scan_reduce_kernel<<<nb, kScanThreads, 0, s.st>>>(in, n, bsum);
+    COSMO_LAUNCHED();
+    scan_blocks_kernel<<<1, kScanThreads, 0, s.st>>>(bsum, nb, out + n);
+    COSMO_LAUNCHED();
+    scan_apply_kernel<<<nb, kScanThreads, 0, s.st>>>(in, out, n, bsum);
+    COSMO_LAUNCHED();
+    if (!readTotal) return 0;
+    COSMO_CUDA(cudaMemcpyAsync(s.hsmall, out + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    return uint32_t(s.hsmall[0]);
+}
+
+void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int n, bool iotaValues)
+{
+    if (n <= 0) return;
+    const int tiles = iceil(n, kSortTile);
+    s.sortHist.resize(kSortPasses * 256, s.st);
+    s.sortBase.resize(kSortPasses * 256, s.st);
+    s.sortLookback.resize(size_t(kSortPasses) * tiles * 256, s.st);
+    DevScalars* ds = s.dscal.get();
+    COSMO_CUDA(cudaMemsetAsync(s.sortHist.get(), 0, kSortPasses * 256 * sizeof(uint32_t), s.st));
+    COSMO_CUDA(cudaMemsetAsync(s.sortLookback.get(), 0, size_t(kSortPasses) * tiles * 256 * sizeof(uint32_t), s.st));
+    COSMO_CUDA(cudaMemsetAsync(&ds->sortTiles[0], 0, sizeof(ds->sortTiles), s.st));
+    digit_hist_kernel<<<std::min(iceil(n, kBlk), 4 * s.numSMs), kBlk, 0, s.st>>>(kA, n, s.sortHist.get());
+    COSMO_LAUNCHED();
+    digit_base_kernel<<<kSortPasses, 256, 0, s.st>>>(s.sortHist.get(), s.sortBase.get());
+    COSMO_LAUNCHED();
+    uint64_t* ki = kA; uint64_t* ko = kB;
+    int* vi = iotaValues ? nullptr : vA; int* vo = vB;
+    for (int p = 0; p < kSortPasses; ++p)
+    {
+        onesweep_kernel<<<tiles, kSortThreads, 0, s.st>>>(
+            ki, vi, ko, vo, n, 8 * p, s.sortBase.get() + 256 * p,
+            s.sortLookback.get() + size_t(p) * tiles * 256, &ds->sortTiles[p], &ds->err);
+        COSMO_LAUNCHED();
+        std::swap(ki, ko);
+        vi = vo;
+        vo = (vo == vB) ? vA : vB;
+    }
+    // eight passes: the result is back in kA / vA
+}
+
+void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
+{
+    const int n = s.ngas;
+    DevScalars* ds = s.dscal.get();
+    cudaEvent_t e0 = ev(s);
+
+    // bounding box (src/tree.cu:47-72)
+    if (periodicBox)
+    {
+        set_box_kernel<<<1, 32, 0, s.st>>>(periodicBox[0], periodicBox[1], periodicBox[2], periodicBox[3],
+                                            periodicBox[4], periodicBox[5], s.box.get());
+    }
+    else
+    {
+        const int nb = std::min(iceil(n, kBlk), 2 * s.numSMs);
+        s.redTmp.resize(size_t(nb) * 6, s.st);
+        bbox_partial_kernel<<<nb, kBlk, 0, s.st>>>(s.ux.get(), s.uy.get(), s.uz.get(), n, s.redTmp.get());
+        COSMO_LAUNCHED();
+        bbox_final_kernel<<<1, 32, 0, s.st>>>(s.redTmp.get(), nb, s.box.get());
+    }
+    COSMO_LAUNCHED();
+    cudaEvent_t e1 = ev(s);
+
+    // keys and sort (src/tree.cu:82-108)
+    keys_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.ux.get(), s.uy.get(), s.uz.get(), s.uh.get(), n,
+                                                  s.box.get(), s.keysA.get());
+    COSMO_LAUNCHED();
+    radix_sort_u64(s, s.keysA.get(), s.keysB.get(), s.orderA.get(), s.orderB.get(), n, true);
+    alive_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.keysA.get(), n, ds);
+    COSMO_LAUNCHED();
+    gather_particles_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(
+        s.orderA.get(), n, s.ux.get(), s.uy.get(), s.uz.get(), s.uh.get(), s.xyzh.get(), s.uvx.get(),
+        s.uvy.get(), s.uvz.get(), s.uax.get(), s.uay.get(), s.uaz.get(), s.vel4.get(), s.acc4.get(),
+        alsoSortVA ? 1 : 0);
+    COSMO_LAUNCHED();
+    cudaEvent_t e2 = ev(s);
+
+    // cornerstone leaf tree from the single-root seed (src/tree.cu:126-136)
+    s.csTree.resize(2, s.st);
+    {
+        const uint64_t seed[2] = {0, kKeyEnd};
+        COSMO_CUDA(cudaMemcpyAsync(s.csTree.get(), seed, sizeof(seed), cudaMemcpyHostToDevice, s.st));
+    }
+    int nL = 1;
+    for (int round = 0; round < 64; ++round)
+    {
+        s.counts.resize(nL, s.st);
+        s.ops.resize(nL, s.st);
+        s.opsScan.resize(size_t(nL) + 1, s.st);
+        leaf_count_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.csTree.get(), nL, s.keysA.get(), ds,
+                                                             s.counts.get(), s.ops.get());
+        COSMO_LAUNCHED();
+        const int total = int(scan_exclusive(s, s.ops.get(), s.opsScan.get(), nL, true));
+        if (total == nL) break;
+        s.csTree2.resize(size_t(total) + 1, s.st);
+        leaf_split_kernel<<<iceil(nL + 1, kBlk), kBlk, 0, s.st>>>(s.csTree.get(), nL, s.ops.get(),
+                                                                  s.opsScan.get(), s.csTree2.get());
+        COSMO_LAUNCHED();
+        std::swap(s.csTree, s.csTree2);
+        nL = total;
+    }
+    s.nLeaves = nL;
+    s.layout.resize(size_t(nL) + 1, s.st);
+    scan_exclusive(s, s.counts.get(), s.layout.get(), nL, false);
+
+    // linked octree: pre-order emission, then BFS order by sorting the prefixes
+    s.nodeCount.resize(nL, s.st);
+    s.leafPreStart.resize(size_t(nL) + 1, s.st);
+    node_count_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.csTree.get(), nL, s.nodeCount.get());
+    COSMO_LAUNCHED();
+    const int numNodes = int(scan_exclusive(s, s.nodeCount.get(), s.leafPreStart.get(), nL, true));
+    s.numNodes = numNodes;
+    for (auto* b : {&s.prePrefix, &s.bfsPrefix}) b->resize(numNodes, s.st);
+    for (auto* b : {&s.preLeaf, &s.preSkip, &s.bfsToPre, &s.preToBfs, &s.childOffsets, &s.internalToLeaf})
+        b->resize(numNodes, s.st);
+    s.centers.resize(size_t(3) * numNodes, s.st);
+    s.sizes.resize(size_t(3) * numNodes, s.st);
+    s.preCenter.resize(numNodes, s.st);
+    s.preHalf.resize(numNodes, s.st);
+    s.levelRange.resize(kMaxLevel + 2, s.st);
+    s.leafToInternal.resize(nL, s.st);
+    node_emit_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.csTree.get(), nL, s.leafPreStart.get(), numNodes,
+                                                         s.prePrefix.get(), s.preLeaf.get(), s.preSkip.get());
+    COSMO_LAUNCHED();
+    // sort (prefix, pre-order index); prePrefix is the key ping-pong partner
+    COSMO_CUDA(cudaMemcpyAsync(s.bfsPrefix.get(), s.prePrefix.get(), size_t(numNodes) * 8,
+                               cudaMemcpyDeviceToDevice, s.st));
+    s.nodeKeysTmp.resize(numNodes, s.st);
+    s.nodeValsTmp.resize(numNodes, s.st);
+    radix_sort_u64(s, s.bfsPrefix.get(), s.nodeKeysTmp.get(), s.bfsToPre.get(), s.nodeValsTmp.get(), numNodes,
+                   true);
+    cudaEvent_t e3 = ev(s);
+
+    bfs_link_kernel<<<iceil(numNodes, kBlk), kBlk, 0, s.st>>>(
+        s.bfsPrefix.get(), s.bfsToPre.get(), numNodes, s.preLeaf.get(), s.preToBfs.get(),
+        s.childOffsets.get(), s.internalToLeaf.get(), s.leafToInternal.get(), s.levelRange.get(), s.box.get(),
+        s.centers.get(), s.sizes.get(), s.preCenter.get(), s.preHalf.get());
+    COSMO_LAUNCHED();
+    particle_leaf_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.layout.get(), nL, n, ds, s.particleLeaf.get());
+    COSMO_LAUNCHED();
+    s.hmaxLeaf.resize(nL, s.st);
+    s.hmaxNode.resize(numNodes, s.st);
+    s.hmaxPre.resize(numNodes, s.st);
+    s.jcount.resize(nL, s.st);
+    s.jOffset.resize(size_t(nL) + 1, s.st);
+    s.allLeaves.resize(nL, s.st);
+    iota_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.allLeaves.get(), nL);
+    COSMO_LAUNCHED();
+    cudaEvent_t e4 = ev(s);
+
+    read_scalars(s);
+    s.nAlive = s.hscal->nAlive;
+    s.t.bbox += elapsed_s(e0, e1);
+    s.t.keysSort += elapsed_s(e1, e2);
+    s.t.tree += elapsed_s(e2, e3);
+    s.t.nodes += elapsed_s(e3, e4);
+}
+
+void hmax_leaves(State& s, const int* leaves, int nActive)
+{
+    if (nActive <= 0) return;
+    hmax_leaf_kernel<<<iceil(nActive, kBlk), kBlk, 0, s.st>>>(s.xyzh.get(), s.layout.get(), leaves, nActive,
+                                                             s.hmaxLeaf.get());
+    COSMO_LAUNCHED();
+}
+
+void hmax_upsweep(State& s)
+{
+    int lr[kMaxLevel + 2];
+    COSMO_CUDA(cudaMemcpyAsync(s.hsmall, s.levelRange.get(), sizeof(lr), cudaMemcpyDeviceToHost, s.st));
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    std::copy(s.hsmall, s.hsmall + kMaxLevel + 2, lr);
+    for (int L = kMaxLevel; L >= 0; --L)
+    {
+        const int a = lr[L], b = lr[L + 1];
+        if (b <= a) continue;
+        hmax_level_kernel<<<iceil(b - a, kBlk), kBlk, 0, s.st>>>(a, b, s.childOffsets.get(), s.internalToLeaf.get(),
+                                                                 s.hmaxLeaf.get(), s.hmaxNode.get(),
+                                                                 s.bfsToPre.get(), s.hmaxPre.get());
+        COSMO_LAUNCHED();
+    }
+}
+
+template<bool Sym, bool Per>
+static void walk(State& s, bool fill)
+{
+    const int nL = s.nLeaves;
+    const int blocks = iceil(long(nL) * 32, kBlk);
+    auto args = [&](auto kern) {
+        kern<<<blocks, kBlk, 0, s.st>>>(nL, s.numNodes, s.leafToInternal.get(), s.centers.get(), s.sizes.get(),
+                                        s.hmaxLeaf.get(), s.preCenter.get(), s.preHalf.get(), s.preSkip.get(),
+                                        s.preLeaf.get(), s.hmaxPre.get(), s.box.get(), s.jcount.get(),
+                                        s.jOffset.get(), s.jlist.get(), &s.dscal.get()->err);
+    };
+    if (fill) args(list_walk_kernel<Sym, Per, true>);
+    else args(list_walk_kernel<Sym, Per, false>);
+    COSMO_LAUNCHED();
+}
+
+// include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.
+void build_lists(State& s, bool symmetric)
+{
+    auto run = [&](bool fill) {
+        if (symmetric) { if (s.periodic) walk<true, true>(s, fill); else walk<true, false>(s, fill); }
+        else { if (s.periodic) walk<false, true>(s, fill); else walk<false, false>(s, fill); }
+    };
+    run(false);
+    const uint32_t total = scan_exclusive(s, s.jcount.get(), s.jOffset.get(), s.nLeaves, true);
+    s.jlist.resize(std::max<uint32_t>(total, 1u), s.st);
+    run(true);
+}
+
+} // namespace cosmo

@@ -1,0 +1,116 @@
+"""Seeded synthetic particle sets (csrc/inputs.cpp): the reference driver's lattice and
+jiggle, and the generators of the measured workloads.  Host-only."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .capi import LIBDIR
+
+_L = None
+
+
+def _lib():
+    global _L
+    if _L is None:
+        path = os.path.join(LIBDIR, "libcosmo_inputs.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build with make -C cosmosphere_b200")
+        L = ctypes.CDLL(path)
+        P, I, D, U64, LNG = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_uint64, ctypes.c_long
+        L.cin_lattice_count.argtypes = [I]
+        L.cin_lattice_count.restype = LNG
+        L.cin_lattice.argtypes = [I, P, P, P, P]
+        L.cin_lattice.restype = D
+        L.cin_jiggle_ref.argtypes = [LNG, P, ctypes.c_uint]
+        L.cin_jiggle_ref.restype = LNG
+        L.cin_jiggle_frac.argtypes = [LNG, P, D, D, D, U64]
+        L.cin_jiggle_frac.restype = LNG
+        L.cin_gaussian.argtypes = [LNG, P, D, D, U64]
+        L.cin_uniform.argtypes = [LNG, P, D, D, U64]
+        L.cin_uniform_box.argtypes = [LNG, P, P, P, P, D, D, D, U64]
+        L.cin_uniform_box.restype = D
+        L.cin_plummer.argtypes = [LNG, P, P, P, P, P, P, P, D, D, D, D, D, D, U64]
+        L.cin_plummer.restype = D
+        _L = L
+    return _L
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+class Particles(dict):
+    """x, y, z, h (and optionally vx, vy, vz, u) as float64 arrays, plus n and pmass."""
+
+    @property
+    def n(self):
+        return int(self["x"].size)
+
+
+def lattice(npartx: int) -> Particles:
+    """The reference driver's close-packed lattice (src/main.cu:84-109)."""
+    L = _lib()
+    n = L.cin_lattice_count(npartx)
+    x, y, z, h = (np.empty(n) for _ in range(4))
+    pm = L.cin_lattice(npartx, _p(x), _p(y), _p(z), _p(h))
+    return Particles(x=x, y=y, z=z, h=h, pmass=pm)
+
+
+def jiggle_ref(h: np.ndarray, seed: int = 42) -> int:
+    """The reference driver's jiggle (src/main.cu:47-63), in place."""
+    return int(_lib().cin_jiggle_ref(h.size, _p(h), seed))
+
+
+def jiggle_frac(h: np.ndarray, frac=0.01, lo=0.65, hi=1.35, seed: int = 42) -> int:
+    """round(frac*n) particles picked uniformly, h scaled by U[lo, hi], in place."""
+    return int(_lib().cin_jiggle_frac(h.size, _p(h), frac, lo, hi, seed))
+
+
+def gaussian(n, mean=0.0, sigma=1.0, seed=42) -> np.ndarray:
+    a = np.empty(n)
+    _lib().cin_gaussian(n, _p(a), mean, sigma, seed)
+    return a
+
+
+def uniform(n, lo=0.0, hi=1.0, seed=42) -> np.ndarray:
+    a = np.empty(n)
+    _lib().cin_uniform(n, _p(a), lo, hi, seed)
+    return a
+
+
+def uniform_box(n, hfac=1.2, hlo=0.8, hhi=1.2, seed=42) -> Particles:
+    x, y, z, h = (np.empty(n) for _ in range(4))
+    pm = _lib().cin_uniform_box(n, _p(x), _p(y), _p(z), _p(h), hfac, hlo, hhi, seed)
+    return Particles(x=x, y=y, z=z, h=h, pmass=pm)
+
+
+def plummer(n, rmax=20.0, hfact=1.0, lnsigma=0.3, ulo=1.0, uhi=1.0, vfrac=0.5, seed=42) -> Particles:
+    """Plummer sphere (a=1, M=1, G=1) truncated at rmax; h from the local density times a
+    log-normal factor (lnsigma > 0) or U[ulo, uhi]; |v| = vfrac * circular speed."""
+    a = [np.empty(n) for _ in range(7)]
+    pm = _lib().cin_plummer(n, *(_p(v) for v in a), rmax, hfact, lnsigma, ulo, uhi, vfrac, seed)
+    x, y, z, h, vx, vy, vz = a
+    return Particles(x=x, y=y, z=z, h=h, vx=vx, vy=vy, vz=vz, pmass=pm)
+
+
+def lattice100_workload(npartx: int = 100, seed: int = 42, vsigma=0.1, u=1.0, gamma=5.0 / 3.0,
+                        alpha=1.0, hfact=1.2) -> Particles:
+    """The lattice-with-jiggle density + force workload: the close-packed lattice, 1% of
+    particles with h scaled by U[0.65, 1.35], velocities N(0, vsigma^2) per component,
+    u = 1, gamma = 5/3, alpha_AV = 1.  Thermodynamics use rho = pmass (hfact/h)^3 of the
+    initial h: P = (gamma-1) rho u, pro2 = P/rho^2, cs = sqrt(gamma (gamma-1) u)."""
+    p = lattice(npartx)
+    jiggle_frac(p["h"], 0.01, 0.65, 1.35, seed)
+    n = p.n
+    p["vx"] = gaussian(n, 0.0, vsigma, seed + 1)
+    p["vy"] = gaussian(n, 0.0, vsigma, seed + 2)
+    p["vz"] = gaussian(n, 0.0, vsigma, seed + 3)
+    rho = p["pmass"] * (hfact / p["h"]) ** 3
+    p["pro2"] = (gamma - 1.0) * u / rho
+    p["cs"] = np.full(n, np.sqrt(gamma * (gamma - 1.0) * u))
+    p["alpha"] = np.full(n, alpha)
+    p["u"] = np.full(n, u)
+    return p

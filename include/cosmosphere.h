@@ -1,0 +1,121 @@
+/*
+ * cosmosphere.h -- the C-ABI of libcosmoSPHere for B200 (sm_100a).
+ *
+ * A drop-in for the library Phantom's Fortran links (-lcosmoSPHere): the same symbols,
+ * argument meanings and error behaviour as the reference's include/arrays.hpp:15-61,
+ * src/dens_c_api.cu:47 and :128, src/force_c_api.cu:26 and src/pin_c_api.cu:22-34.
+ *
+ * Conventions (unchanged from the reference):
+ *   - one process-wide state on the current CUDA device; single host thread;
+ *   - every call returns only when its device work is done;
+ *   - errors print a "FATAL:" line on stderr and abort(); nothing returns a code;
+ *   - a slot moves as one host block of ncomp*n doubles, component-major;
+ *   - the device keeps particles in Hilbert order; transfers permute through it.
+ * Kernel choice is fixed when the library is built, as in the reference (KERNEL=cubic
+ * gives libcosmoSPHere.so, KERNEL=quintic gives libcosmoSPHere_quintic.so).
+ */
+#ifndef COSMOSPHERE_H
+#define COSMOSPHERE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Slot ids, shared with Phantom's gpu_arrays ibun_* (include/arrays.hpp:15-25). */
+enum CosmoSlot
+{
+    COSMO_POS       = 1, /* x, y, z */
+    COSMO_HSML      = 2, /* h */
+    COSMO_VEL       = 3, /* vx, vy, vz */
+    COSMO_ACCEL     = 4, /* ax, ay, az */
+    COSMO_DENS_OUT  = 5, /* rho, d(rho)/d(h) */
+    COSMO_GRAD_OUT  = 6, /* div v, xi, d(div v)/dt */
+    COSMO_THERMO    = 7, /* p/rho^2, c_s, alpha_AV, u */
+    COSMO_FORCE_OUT = 8  /* fx, fy, fz, du/dt, vsigmax, div v */
+};
+
+/* Size every particle-length device array for n particles; n <= 0 is a no-op and a
+ * repeated n is free.  Replaces src/arrays_c_api.cu:31 (cosmo_arrays_init). */
+void cosmo_arrays_init(int n);
+
+/* Components of a slot, 0 if unknown.  Replaces src/arrays_c_api.cu:152. */
+int cosmo_slot_ncomp(int slot);
+
+/* Send a slot in the caller's particle order, for the next density solve to sort.
+ * Aborts if n differs from cosmo_arrays_init's or the slot is unknown.
+ * Replaces src/arrays_c_api.cu:158 (cosmo_upload). */
+void cosmo_upload(int slot, const double* host, int n);
+
+/* Send a slot and gather it into the device's Hilbert order; needs a density solve for
+ * this n to have built the ordering, else aborts.  Replaces src/arrays_c_api.cu:164. */
+void cosmo_upload_sorted(int slot, const double* host, int n);
+
+/* Fetch a slot back in the caller's order (scatter through the ordering, then copy).
+ * Replaces src/arrays_c_api.cu:178 (cosmo_download). */
+void cosmo_download(int slot, double* host, int n);
+
+/* Page-lock / release a caller buffer (cudaHostRegister).  Null or zero size is a
+ * no-op; failure is silent.  Replaces src/pin_c_api.cu:22 and :29. */
+void cosmo_pin_host(void* ptr, size_t nbytes);
+void cosmo_unpin_host(void* ptr);
+
+/* Kernel support radius in units of h: 2 (cubic) or 3 (quintic).
+ * Replaces src/dens_c_api.cu:128 (cosmo_kernel_radius). */
+double cosmo_kernel_radius(void);
+
+/* Density / smoothing-length solve with the gradient sweep: Hilbert keys, sort, leaf
+ * tree, octree, j-leaf lists, Newton-Raphson to |dh/h| < tolh, then div v, xi and
+ * d(div v)/dt at the converged h.  box = {xmin,xmax,ymin,ymax,zmin,zmax} is read only
+ * when periodic != 0; hfact <= 0 selects the kernel's default.  Results stay on the
+ * device (HSML, DENS_OUT, GRAD_OUT).  Aborts on a size mismatch, non-convergence within
+ * the iteration cap (100, or COSMO_MAX_ITER) or a kernel support reaching half the
+ * periodic box.  Replaces src/dens_c_api.cu:47 (densityiterate_gpu_c). */
+void densityiterate_gpu_c(int n, double pmass, int periodic, const double* box, double tolh, double hfact);
+
+/* Force pass on the tree of the last density solve: pressure + artificial-viscosity
+ * accelerations, du/dt, vsigmax and div v over the symmetric (gather + scatter) lists.
+ * Uses THERMO (and VEL if re-sent) uploaded with cosmo_upload_sorted.  Aborts without a
+ * density solve for this n.  Replaces src/force_c_api.cu:26 (force_gpu_c). */
+void force_gpu_c(int n, double pmass, double beta, double alphau, int disc_viscosity, int pdv_heating,
+                 int shock_heating);
+
+/* ---- harness hooks (no counterpart in the reference; used by tests and bench) ---- */
+
+/* Set the Newton iteration cap (default 100, as src/density_base.cu:50). */
+void cosmo_x_set_max_iter(int max_iter);
+
+/* Density solve that returns a status instead of aborting: 0 ok, 1 unconverged,
+ * 2 periodic support too large, -1 size mismatch. */
+int cosmo_x_density(int n, double pmass, int periodic, const double* box, double tolh, double hfact, int max_iter,
+                    int with_gradients);
+
+/* Wait for the library's stream. */
+void cosmo_x_sync(void);
+
+/* Make device dev current for the library (before its first call on this thread). */
+void cosmo_x_set_device(int dev);
+
+/* Record mark id (0..15) on the library's stream; seconds between two marks. */
+void cosmo_x_mark(int id);
+double cosmo_x_mark_elapsed(int a, int b);
+
+/* Number of the library's kernel launches so far in this process. */
+unsigned long long cosmo_x_launches(void);
+
+/* Measured FP64 FMA throughput of the current GPU, TFLOP/s. */
+double cosmo_x_fp64_peak(void);
+
+/* Named scalar of the last solve (counts, timings in seconds); NaN if unknown. */
+double cosmo_x_scalar(const char* name);
+
+/* Copy a named device array (Hilbert order / tree / lists) to the host; returns its
+ * length or -1.  dtype: 0 f64, 1 i32, 2 u32, 3 u64, 4 i64.  out == NULL only queries. */
+long cosmo_x_array(const char* name, void* out, int* dtype);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COSMOSPHERE_H */

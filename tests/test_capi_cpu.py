@@ -1,0 +1,61 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol the headers declare,
+and its checks that run before any CUDA call behave as the reference's."""
+import os
+import re
+import subprocess
+import sys
+
+import pytest
+
+from cosmosphere_b200 import capi
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(REPO, "include", "cosmosphere.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(cosmo_\w+|densityiterate_gpu_c|force_gpu_c)\s*\(", txt)))
+
+
+@pytest.mark.parametrize("quintic", [False, True])
+def test_library_exports_every_declared_symbol(quintic):
+    L = capi.load(quintic)
+    names = _declared()
+    assert "densityiterate_gpu_c" in names and "cosmo_download" in names
+    for name in names:
+        assert hasattr(L, name), name
+
+
+def test_exports_list_matches_header():
+    assert sorted(capi.EXPORTS) == _declared()
+
+
+def test_slot_table_and_kernel_radius():
+    c = capi.Cosmo()
+    assert [c.slot_ncomp(s) for s in range(0, 10)] == [0, 3, 1, 3, 3, 2, 3, 4, 6, 0]
+    assert c.kernel_radius() == 2.0
+    assert capi.Cosmo(quintic=True).kernel_radius() == 3.0
+
+
+def test_static_archive_builds(tmp_path):
+    # the archive Phantom links (-lcosmoSPHere)
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "cosmosphere_b200"), "static"], check=True)
+    assert os.path.exists(os.path.join(REPO, "cosmosphere_b200", "lib", "libcosmoSPHere.a"))
+
+
+def _child(code):
+    return subprocess.run([sys.executable, "-c", "import sys; sys.path.insert(0, %r)\n" % REPO + code],
+                          capture_output=True, text=True, timeout=120)
+
+
+@pytest.mark.parametrize("call,msg", [
+    ("c.upload(capi.POS, np.zeros(30), 10)", "FATAL: cosmo_upload(slot=1) with n=10 but the device arrays are sized for 0"),
+    ("c.download(capi.HSML, 10)", "FATAL: cosmo_download(slot=2) with n=10 but the device arrays are sized for 0"),
+    ("c.density(10, 0.1)", "FATAL: densityiterate_gpu_c called with n=10 but the device arrays are sized for 0"),
+    ("c.force(10, 0.1)", "FATAL: force_gpu_c called with n=10 but the device arrays are sized for 0"),
+])
+def test_fatal_before_any_device_work(call, msg):
+    r = _child("import numpy as np\nfrom cosmosphere_b200 import capi\nc = capi.Cosmo()\n" + call)
+    assert r.returncode != 0
+    assert msg in r.stderr

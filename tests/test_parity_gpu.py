@@ -1,0 +1,256 @@
+"""Parity of the CUDA library, called through its C-ABI, with the CPU oracle on the same
+seeded inputs.  The plain FP64 form is required to be bit-exact on everything: keys,
+sort order, leaf tree, octree, node geometry, j-leaf lists, h, rho, gradh, the gradient
+fields and the forces (the specification's bound for the FP64 fields is 1e-10 relative;
+bit equality is the stronger property the library is built to hold)."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from cosmosphere_b200 import capi, inputs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+TREE = ["keys", "order", "csTree", "counts", "layout", "prefixes", "childOffsets", "internalToLeaf",
+        "levelRange", "leafToInternal", "centers", "sizes"]
+FIELDS = ["x", "y", "z", "h", "rho", "gradh", "divv", "xi", "ddivvdt"]
+FORCE = ["fx", "fy", "fz", "f4", "vsigmax", "divvF"]
+
+
+def _vel_acc(p, seed=5):
+    n = p.n
+    if "vx" in p:
+        v = np.stack([p["vx"], p["vy"], p["vz"]])
+    else:
+        v = np.stack([inputs.gaussian(n, 0, 0.1, seed + k) for k in range(3)])
+    a = np.stack([inputs.gaussian(n, 0, 1.0, seed + 10 + k) for k in range(3)])
+    return v, a
+
+
+def _thermo(p, hfact):
+    n = p.n
+    if "pro2" in p:
+        return np.stack([p["pro2"], p["cs"], p["alpha"], p["u"]])
+    rho = p["pmass"] * (hfact / p["h"]) ** 3
+    return np.stack([(2.0 / 3.0) / rho, np.full(n, np.sqrt(10.0 / 9.0)), np.full(n, 1.0), np.full(n, 1.0)])
+
+
+def run_pair(p, *, quintic=False, box=None, force=True, tolh=1e-4, disc=0, beta=2.0, alphau=0.1):
+    n = p.n
+    hfact = 1.0 if quintic else 1.2
+    v, a = _vel_acc(p)
+    c = capi.Cosmo(quintic)
+    c.arrays_init(n)
+    c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+    c.upload(capi.HSML, p["h"])
+    c.upload(capi.VEL, v)
+    c.upload(capi.ACCEL, a)
+    c.density(n, p["pmass"], periodic_box=box, tolh=tolh, hfact=hfact)
+    o = O.Oracle(quintic=quintic)
+    st = o.density(p["x"], p["y"], p["z"], p["h"], p["pmass"], periodic_box=box, tolh=tolh, hfact=hfact,
+                   vel=v, acc=a)
+    assert st == 0
+    if force:
+        th = _thermo(p, hfact)
+        c.upload(capi.THERMO, th, sorted_=True)
+        c.force(n, p["pmass"], beta=beta, alphau=alphau, disc=disc)
+        assert o.force(th, beta=beta, alphau=alphau, disc=disc) == 0
+    return c, o
+
+
+def assert_same(c, o, names):
+    for k in names:
+        g, r = c.array(k), o.array(k)
+        assert g.shape == r.shape, (k, g.shape, r.shape)
+        np.testing.assert_array_equal(g, r, err_msg=k)
+
+
+def assert_lists_same(c, o):
+    assert_same(c, o, ["jcount", "jOffset", "jlist"])
+
+
+def check_all(c, o, force=True):
+    assert c.scalar("nAlive") == o.scalar("nAlive")
+    assert c.scalar("nLeaves") == o.scalar("nLeaves")
+    assert c.scalar("numNodes") == o.scalar("numNodes")
+    assert c.scalar("itersRun") == o.scalar("itersRun")
+    np.testing.assert_array_equal(c.array("activePerIter"), o.array("activePerIter"))
+    assert_same(c, o, TREE)
+    nA = int(o.scalar("nAlive"))
+    np.testing.assert_array_equal(c.array("particleLeaf")[:nA], o.array("particleLeaf")[:nA])
+    assert_same(c, o, FIELDS)
+    if force:
+        assert_same(c, o, FORCE + ["hmax_node"])
+    assert_lists_same(c, o)                       # gather after density; symmetric after force
+    assert c.scalar("pairsDensity") == o.scalar("pairsDensity")
+    assert c.scalar("pairsGrad") == o.scalar("pairsGrad")
+    if force:
+        assert c.scalar("pairsForce") == o.scalar("pairsForce")
+
+
+def test_lattice_jiggle_open():
+    p = inputs.lattice(16)
+    inputs.jiggle_ref(p["h"], 42)
+    c, o = run_pair(p)
+    check_all(c, o)
+
+
+def test_lattice100_workload_small():
+    p = inputs.lattice100_workload(20)
+    c, o = run_pair(p)
+    check_all(c, o)
+
+
+def test_periodic_jittered_lattice():
+    x, y, z = (np.asarray(v) for v in np.meshgrid(*(np.arange(12) / 12.0,) * 3, indexing="ij"))
+    n = x.size
+    rng = np.random.default_rng(11)
+    p = inputs.Particles(x=(x.ravel() + rng.uniform(0, 0.02, n)) % 1.0, y=(y.ravel() + rng.uniform(0, 0.02, n)) % 1.0,
+                         z=(z.ravel() + rng.uniform(0, 0.02, n)) % 1.0, h=np.full(n, 1.2 / 12), pmass=1.0 / n)
+    inputs.jiggle_frac(p["h"], 0.05, 0.65, 1.35, 9)
+    c, o = run_pair(p, box=[0.0, 1.0, 0.0, 1.0, 0.0, 1.0])
+    check_all(c, o)
+
+
+def test_quintic_plummer_lognormal():
+    p = inputs.plummer(12000, lnsigma=0.3, seed=42)
+    c, o = run_pair(p, quintic=True)
+    check_all(c, o)
+
+
+def test_disc_viscosity_and_partial_heating():
+    p = inputs.lattice100_workload(12)
+    c, o = run_pair(p, disc=1, alphau=0.5)
+    check_all(c, o)
+    th = _thermo(p, 1.2)
+    c.upload(capi.THERMO, th, sorted_=True)
+    c.force(p.n, p["pmass"], beta=2.0, alphau=0.5, disc=0, pdv=0, shock=1)
+    o.force(th, beta=2.0, alphau=0.5, disc=0, pdv=0, shock=1)
+    assert_same(c, o, FORCE)
+
+
+def test_dead_particles():
+    p = inputs.lattice(12)
+    dead = np.arange(3, p.n, 41)
+    p["h"][dead] = -1.0
+    p["h"][7] = 0.0
+    c, o = run_pair(p)
+    check_all(c, o)
+    n = p.n
+    h = c.download(capi.HSML, n)[0]
+    np.testing.assert_array_equal(h[dead], -1.0)
+    f = c.download(capi.FORCE_OUT, n)
+    assert np.all(f[:, dead] == 0.0)
+    g = c.download(capi.GRAD_OUT, n)
+    assert np.all(g[1, dead] == 1.0) and np.all(g[0, dead] == 0.0)
+
+
+def test_c_abi_transfers_round_trip():
+    p = inputs.lattice100_workload(14)
+    c, o = run_pair(p)
+    n = p.n
+    pos = c.download(capi.POS, n)
+    np.testing.assert_array_equal(pos, np.stack([p["x"], p["y"], p["z"]]))
+    np.testing.assert_array_equal(c.download(capi.HSML, n)[0], o.unsorted("h"))
+    d = c.download(capi.DENS_OUT, n)
+    np.testing.assert_array_equal(d[0], o.unsorted("rho"))
+    np.testing.assert_array_equal(d[1], o.unsorted("gradh"))
+    g = c.download(capi.GRAD_OUT, n)
+    for k, name in enumerate(("divv", "xi", "ddivvdt")):
+        np.testing.assert_array_equal(g[k], o.unsorted(name))
+    f = c.download(capi.FORCE_OUT, n)
+    for k, name in enumerate(FORCE):
+        np.testing.assert_array_equal(f[k], o.unsorted(name))
+    # upload_sorted then download returns what was sent, in the caller's order
+    v2 = np.stack([inputs.gaussian(n, 0, 1, 77 + k) for k in range(3)])
+    c.upload(capi.VEL, v2, sorted_=True)
+    np.testing.assert_array_equal(c.download(capi.VEL, n), v2)
+    th = c.download(capi.THERMO, n)
+    np.testing.assert_array_equal(th, _thermo(p, 1.2))
+
+
+def test_pinned_host_buffers_and_repeat_solve():
+    p = inputs.lattice100_workload(14)
+    n = p.n
+    c = capi.Cosmo()
+    buf = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]))
+    hb = p["h"].copy()
+    c.pin(buf)
+    c.pin(hb)
+    c.arrays_init(n)
+    outs = []
+    for _ in range(2):
+        c.upload(capi.POS, buf)
+        c.upload(capi.HSML, hb)
+        c.density(n, p["pmass"])
+        outs.append(c.download(capi.DENS_OUT, n))
+    c.unpin(buf)
+    c.unpin(hb)
+    np.testing.assert_array_equal(outs[0], outs[1])
+    # force twice on the same tree: the symmetric list is cached, results identical
+    th = _thermo(p, 1.2)
+    c.upload(capi.THERMO, th, sorted_=True)
+    c.force(n, p["pmass"])
+    f1 = c.download(capi.FORCE_OUT, n)
+    c.force(n, p["pmass"])
+    np.testing.assert_array_equal(f1, c.download(capi.FORCE_OUT, n))
+
+
+def test_resize_between_solves():
+    for npx in (10, 14, 10):
+        p = inputs.lattice(npx)
+        c, o = run_pair(p, force=False)
+        assert_same(c, o, ["h", "rho", "gradh"])
+
+
+def test_lattice50_reference_driver_case():
+    """The reference driver's `lattice 50` (173,850 particles, open boundaries)."""
+    p = inputs.lattice(50)
+    c, o = run_pair(p, force=True)
+    check_all(c, o)
+
+
+def _child(code, env=None):
+    e = dict(os.environ)
+    e.update(env or {})
+    return subprocess.run([sys.executable, "-c", "import sys; sys.path.insert(0, %r)\n" % REPO + code],
+                          capture_output=True, text=True, timeout=300, env=e)
+
+
+PRE = ("import numpy as np\nfrom cosmosphere_b200 import capi, inputs\n"
+       "p = inputs.lattice(10); n = p.n; c = capi.Cosmo(); c.arrays_init(n)\n"
+       "c.upload(capi.POS, np.stack([p['x'], p['y'], p['z']])); c.upload(capi.HSML, p['h'])\n")
+
+
+def test_fatal_unconverged_within_cap():
+    r = _child(PRE + "c.density(n, p['pmass'])\n", env={"COSMO_MAX_ITER": "1"})
+    assert r.returncode != 0
+    assert "FATAL: solveDensH: unconverged=" in r.stderr
+
+
+def test_fatal_force_before_density():
+    r = _child(PRE + "c.force(n, p['pmass'])\n")
+    assert r.returncode != 0
+    assert "FATAL: force_gpu_c called with no GPU density solve for this particle set" in r.stderr
+
+
+def test_fatal_upload_sorted_before_density():
+    r = _child(PRE + "c.upload(capi.THERMO, np.zeros(4 * n), n, sorted_=True)\n")
+    assert r.returncode != 0
+    assert "with no ordering: a density solve must have run first" in r.stderr
+
+
+def test_fatal_periodic_support():
+    code = ("import numpy as np\nfrom cosmosphere_b200 import capi\n"
+            "g = (np.arange(3) + 0.5) / 3; X, Y, Z = np.meshgrid(g, g, g, indexing='ij')\n"
+            "c = capi.Cosmo(); c.arrays_init(27)\n"
+            "c.upload(capi.POS, np.stack([X.ravel(), Y.ravel(), Z.ravel()])); c.upload(capi.HSML, np.full(27, 0.4))\n"
+            "c.density(27, 1 / 27, periodic_box=[0, 1, 0, 1, 0, 1])\n")
+    r = _child(code)
+    assert r.returncode != 0
+    assert "reaches half the periodic box" in r.stderr
