@@ -10,6 +10,7 @@
  */
 #include <algorithm>
 
+#include "pairstream.cuh"
 #include "state.hpp"
 
 namespace cosmo {
@@ -18,24 +19,6 @@ namespace {
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
-
-struct JCursor
-{
-    // Iterates the particles of an i-leaf's j-leaves, in order.
-    const int* list;
-    const uint32_t* layout;
-    uint32_t nj;
-};
-
-// k-th (0-based) set bit of the 64-bit mask (lo | hi << 32), or -1.
-__device__ __forceinline__ int kth_slot(uint32_t lo, uint32_t hi, int k)
-{
-    const int nlo = __popc(lo);
-    if (k < nlo) return int(__fns(lo, 0, k + 1));
-    k -= nlo;
-    if (k < __popc(hi)) return 32 + int(__fns(hi, 0, k + 1));
-    return -1;
-}
 
 template<bool Periodic>
 __global__ void __launch_bounds__(kThreads)
@@ -46,7 +29,9 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
                   double hfact, const DevBox* __restrict__ box, int* __restrict__ nextLeaves,
                   DevScalars* __restrict__ ds)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ int sIdx[kWarpsPerBlock][kRing];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nWarps = (gridDim.x * blockDim.x) >> 5;
     double lx = 0, ly = 0, lz = 0;
@@ -68,25 +53,25 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
             const uint32_t m1 = __ballot_sync(0xffffffffu, act1);
             const int nAct = __popc(m0) + __popc(m1);
             if (nAct == 0) continue;
-            for (int k0 = 0; k0 < nAct; k0 += 32)
+            const int G = (nAct + 31) >> 5;
+            for (int grp = 0; grp < G; ++grp)
             {
-                const int slot = kth_slot(m0, m1, k0 + lane);
+                const int slot = group_slot(m0, m1, nAct, grp, G, lane);
                 const bool mine = slot >= 0;
                 const uint32_t i = g + uint32_t(mine ? slot : 0);
                 const double4 pi = xyzh[i];
                 const double hi = pi.w;
                 const double hinv2 = 1.0 / (hi * hi);
+                const double rs = kRadKernel * hi;
+                const double rmax = warp_max(mine ? rs : 0.0);
+                const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
                 double rhoi = 0.0, gradhi = 0.0;
                 unsigned int gp = 0, gc = 0;
-                for (uint32_t jl = 0; jl < nj; ++jl)
-                {
-                    const int jLeaf = jlist[jb + jl];
-                    const uint32_t q0 = layout[jLeaf], q1 = layout[jLeaf + 1];
-                    for (uint32_t j = q0; j < q1; ++j)
-                    {
-                        const double2 xy = __ldg(reinterpret_cast<const double2*>(xyzh + j));
-                        const double zj = __ldg(reinterpret_cast<const double*>(xyzh + j) + 2);
-                        double dx = pi.x - xy.x, dy = pi.y - xy.y, dz = pi.z - zj;
+                stream_pairs(
+                    sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
+                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+                    [&](const double4& pj, int) {
+                        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                         nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                         const double q2 = pair_r2(dx, dy, dz) * hinv2;
                         ++gc;
@@ -99,8 +84,7 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
                             gradhi += -q * dwk - 3.0 * wk;
                             ++gp;
                         }
-                    }
-                }
+                    });
                 bool stillActive = false;
                 if (mine)
                 {
@@ -190,6 +174,9 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                 double* __restrict__ divv, double* __restrict__ xiOut, double* __restrict__ ddivvdt,
                 double pmass, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
 {
+    __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ int sIdx[kWarpsPerBlock][kRing];
+    const int wib = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -201,32 +188,38 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
     {
         const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
         const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
-        for (uint32_t g = p0; g < p1; g += 32)
+        for (uint32_t g = p0; g < p1; g += 64)
         {
-            const uint32_t i = g + lane;
-            const bool mine = i < p1;
-            const uint32_t ii = mine ? i : p0;
-            const double4 pi = xyzh[ii];
-            const double4 vi = vel4[ii];
-            const double4 ai = acc4[ii];
+            const uint32_t m0 = __ballot_sync(0xffffffffu, g + lane < p1);
+            const uint32_t m1 = __ballot_sync(0xffffffffu, g + 32 + lane < p1);
+            const int nAct = __popc(m0) + __popc(m1);
+            const int G = (nAct + 31) >> 5;
+            for (int grp = 0; grp < G; ++grp)
+            {
+            const int slot = group_slot(m0, m1, nAct, grp, G, lane);
+            const bool mine = slot >= 0;
+            const uint32_t i = g + uint32_t(mine ? slot : 0);
+            const double4 pi = xyzh[i];
+            const double4 vi = vel4[i];
+            const double4 ai = acc4[i];
             const double hi = pi.w;
             const double hinv2 = 1.0 / (hi * hi);
+            const double rs = kRadKernel * hi;
+            const double rmax = warp_max(mine ? rs : 0.0);
+            const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
             double rhoi = 0.0, gradhi = 0.0, divs = 0.0;
             double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, da[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             double rxx = 0, rxy = 0, rxz = 0, ryy = 0, ryz = 0, rzz = 0;
             unsigned int gp = 0;
-            for (uint32_t jl = 0; jl < nj; ++jl)
-            {
-                const int jLeaf = jlist[jb + jl];
-                const uint32_t q0 = layout[jLeaf], q1 = layout[jLeaf + 1];
-                for (uint32_t j = q0; j < q1; ++j)
-                {
-                    const double4 pj = ldg4(xyzh + j);
+            stream_pairs(
+                sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
+                [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+                [&](const double4& pj, int j) {
                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                     const double r2 = pair_r2(dx, dy, dz);
                     const double q2 = r2 * hinv2;
-                    if (!(q2 < kRadK2)) continue;
+                    if (!(q2 < kRadK2)) return;
                     ++gp;
                     const double q = sqrt(q2);
                     double wk, dwk;
@@ -250,8 +243,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                     da[6] += daz * rx; da[7] += daz * ry; da[8] += daz * rz;
                     rxx -= dx * rx; rxy -= dx * ry; rxz -= dx * rz;
                     ryy -= dy * ry; ryz -= dy * rz; rzz -= dz * rz;
-                }
-            }
+                });
             if (!mine) continue;
             pairs += gp;
             const double hi1 = 1.0 / hi;
@@ -311,6 +303,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
             xiOut[i] = xi_limiter(gm);
             ddivvdt[i] = div_a - (gm[0] * gm[0] + gm[4] * gm[4] + gm[8] * gm[8]
                                   + 2.0 * (gm[1] * gm[3] + gm[2] * gm[6] + gm[5] * gm[7]));
+            }
         }
     }
 #pragma unroll

@@ -7,6 +7,7 @@
  */
 #include <algorithm>
 
+#include "pairstream.cuh"
 #include "state.hpp"
 
 namespace cosmo {
@@ -52,6 +53,9 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
              double* __restrict__ vsigmax, double* __restrict__ divvF, double pmass, double beta, int pdv,
              int shock, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
 {
+    __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ int sIdx[kWarpsPerBlock][kRing];
+    const int wib = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -63,11 +67,18 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
     {
         const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
         const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
-        for (uint32_t g = p0; g < p1; g += 32)
+        for (uint32_t g = p0; g < p1; g += 64)
         {
-            const uint32_t i = g + lane;
-            const bool mine = i < p1;
-            const uint32_t ii = mine ? i : p0;
+          const uint32_t m0 = __ballot_sync(0xffffffffu, g + lane < p1);
+          const uint32_t m1 = __ballot_sync(0xffffffffu, g + 32 + lane < p1);
+          const int nAct = __popc(m0) + __popc(m1);
+          const int G = (nAct + 31) >> 5;
+          for (int grp = 0; grp < G; ++grp)
+          {
+            const int slot = group_slot(m0, m1, nAct, grp, G, lane);
+            const bool mine = slot >= 0;
+            const uint32_t i = g + uint32_t(mine ? slot : 0);
+            const uint32_t ii = i;
             const double4 pi = xyzh[ii];
             const double4 vi = vel4[ii];
             const double4 ti = thermo4[ii];
@@ -80,21 +91,20 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
             double itx = 0, ity = 0, itz = 0, jtx = 0, jty = 0, jtz = 0;
             double f4s = 0.0, vsm = 0.0, divs = 0.0;
             unsigned int gp = 0;
-            for (uint32_t jl = 0; jl < nj; ++jl)
-            {
-                const int jLeaf = jlist[jb + jl];
-                const uint32_t q0 = layout[jLeaf], q1 = layout[jLeaf + 1];
-                for (uint32_t j = q0; j < q1; ++j)
-                {
-                    const double4 pj = ldg4(xyzh + j);
+            const double rg = kRadKernel * warp_max(mine ? hi : 0.0);
+            const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, 0.0, rg);
+            stream_pairs(
+                sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
+                [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
+                [&](const double4& pj, int j) {
                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                     const double dr2 = pair_r2(dx, dy, dz);
-                    if (!(dr2 > 0.0)) continue;
+                    if (!(dr2 > 0.0)) return;
                     const double hj = pj.w;
                     {
                         const double rmax2 = kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10);
-                        if (dr2 >= rmax2) continue;
+                        if (dr2 >= rmax2) return;
                     }
                     const double4 aj = ldg4(prepA + j);
                     const double qi2 = dr2 * hsqinvi;
@@ -171,8 +181,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
                         f4s += vsigu * denij * autermj * gkj;
                     }
                     if (took) ++gp;
-                }
-            }
+                });
             if (!mine) continue;
             pairs += gp;
             fx[i] = itx + jtx;
@@ -181,6 +190,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
             f4[i] = f4s;
             vsigmax[i] = vsm;
             divvF[i] = -divs * bi.w;
+          }
         }
     }
 #pragma unroll

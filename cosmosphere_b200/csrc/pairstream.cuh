@@ -1,0 +1,151 @@
+/*
+ * pairstream.cuh -- the j-stream shared by the density, gradient and force kernels.
+ *
+ * A warp owns one group of up to 32 i-particles of one leaf (one per lane).  It walks
+ * the leaf's j-leaf list in ascending order, loading 32 consecutive j particles per
+ * batch with coalesced 128-bit loads.  Each j is tested ONCE, by the lane that loaded
+ * it, against a conservative box around the whole group (the "group filter"); the
+ * survivors are compacted with a ballot, in order, into a per-warp shared-memory ring,
+ * and every lane then evaluates them one by one (broadcast reads).  A j rejected by the
+ * filter cannot be accepted by any lane's exact test, so the accepted pairs -- and the
+ * order in which each lane sums them -- are exactly those of walking the whole list.
+ */
+#pragma once
+
+#include "common.cuh"
+
+namespace cosmo {
+
+constexpr int kRing = 64;     // double4 entries per warp ring (2 KB)
+
+// Conservative box of a group: centre c, half extents e (inflated by the caller's
+// support and a rounding margin), and the periodic lengths.
+struct GroupBox
+{
+    double cx, cy, cz, ex, ey, ez;
+};
+
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Box of [x - r, x + r] over the lanes that own a particle, plus an absolute margin far
+// above the rounding of any coordinate involved (1e-9 of the support, 1e-13 of |c|).
+__device__ __forceinline__ GroupBox group_box(bool mine, double x, double y, double z, double r, double rmax)
+{
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    const double lx = warp_min(mine ? x - r : inf), hx = warp_max(mine ? x + r : -inf);
+    const double ly = warp_min(mine ? y - r : inf), hy = warp_max(mine ? y + r : -inf);
+    const double lz = warp_min(mine ? z - r : inf), hz = warp_max(mine ? z + r : -inf);
+    GroupBox b;
+    b.cx = 0.5 * (lx + hx); b.cy = 0.5 * (ly + hy); b.cz = 0.5 * (lz + hz);
+    const double mx = 1e-9 * rmax + 1e-13 * (fabs(b.cx) + fabs(b.cy) + fabs(b.cz) + 1e-300);
+    b.ex = 0.5 * (hx - lx) + mx; b.ey = 0.5 * (hy - ly) + mx; b.ez = 0.5 * (hz - lz) + mx;
+    return b;
+}
+
+// Per-axis distance of a coordinate from a box centre, at the nearest periodic image.
+template<bool Periodic>
+__device__ __forceinline__ double axis_dist(double x, double c, double L)
+{
+    double d = fabs(x - c);
+    if (Periodic) d = fmin(d, L - d);
+    return d;
+}
+
+// Gather filter: inside the group's box of search spheres.
+template<bool Periodic>
+__device__ __forceinline__ bool in_gather_box(const double4& p, const GroupBox& b, double lx, double ly, double lz)
+{
+    return axis_dist<Periodic>(p.x, b.cx, lx) <= b.ex && axis_dist<Periodic>(p.y, b.cy, ly) <= b.ey &&
+           axis_dist<Periodic>(p.z, b.cz, lz) <= b.ez;
+}
+
+// Symmetric filter: within R*max(hmax_group, h_j) of the box of the group's positions.
+template<bool Periodic>
+__device__ __forceinline__ bool in_sym_box(const double4& p, const GroupBox& b, double rg, double lx, double ly,
+                                           double lz)
+{
+    const double gx = axis_dist<Periodic>(p.x, b.cx, lx) - b.ex;
+    const double gy = axis_dist<Periodic>(p.y, b.cy, ly) - b.ey;
+    const double gz = axis_dist<Periodic>(p.z, b.cz, lz) - b.ez;
+    const double dx = gx > 0.0 ? gx : 0.0, dy = gy > 0.0 ? gy : 0.0, dz = gz > 0.0 ? gz : 0.0;
+    const double r = fmax(rg, kRadKernel * p.w) * (1.0 + 1e-9);
+    return dx * dx + dy * dy + dz * dz <= r * r;
+}
+
+// Stream the j particles of one i-leaf list through the group filter into the ring and
+// hand each survivor (with its index) to consume(pj, j), in ascending j order, on every
+// lane.  filter(pj) is evaluated by the loading lane only.
+template<class Filter, class Consume>
+__device__ __forceinline__ void stream_pairs(double4* ring, int* ringIdx, uint32_t jb, uint32_t nj,
+                                             const int* __restrict__ jlist, const uint32_t* __restrict__ layout,
+                                             const double4* __restrict__ xyzh, Filter filter, Consume consume)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    int head = 0, cnt = 0;
+    auto drain = [&](int count) {
+        for (int k = 0; k < count; ++k)
+        {
+            const int s = (head + k) & (kRing - 1);
+            consume(ring[s], ringIdx[s]);
+        }
+        head = (head + count) & (kRing - 1);
+        cnt -= count;
+        __syncwarp();
+    };
+    for (uint32_t jl = 0; jl < nj; ++jl)
+    {
+        const int jLeaf = jlist[jb + jl];
+        const uint32_t q0 = layout[jLeaf], q1 = layout[jLeaf + 1];
+        for (uint32_t b = q0; b < q1; b += 32)
+        {
+            const uint32_t j = b + lane;
+            bool pass = false;
+            double4 pj;
+            if (j < q1)
+            {
+                pj = ldg4(xyzh + j);
+                pass = filter(pj);
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, pass);
+            if (pass)
+            {
+                const int s = (head + cnt + __popc(m & lt)) & (kRing - 1);
+                ring[s] = pj;
+                ringIdx[s] = int(j);
+            }
+            cnt += __popc(m);
+            __syncwarp();
+            if (cnt >= 32) drain(32);
+        }
+    }
+    if (cnt > 0) drain(cnt);
+}
+
+// Near-equal split of a leaf window's active slots into warp groups: group g of G takes
+// active ranks [g*nAct/G, (g+1)*nAct/G).  Returns the lane's slot in the 64-slot window
+// (or -1) via kth set bit of (lo | hi << 32).
+__device__ __forceinline__ int group_slot(uint32_t lo, uint32_t hi, int nAct, int g, int G, int lane)
+{
+    const int k0 = g * nAct / G, k1 = (g + 1) * nAct / G;
+    int k = k0 + lane;
+    if (k >= k1) return -1;
+    const int nlo = __popc(lo);
+    if (k < nlo) return int(__fns(lo, 0, k + 1));
+    k -= nlo;
+    return 32 + int(__fns(hi, 0, k + 1));
+}
+
+} // namespace cosmo
