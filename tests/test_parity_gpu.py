@@ -254,3 +254,25 @@ def test_fatal_periodic_support():
     r = _child(code)
     assert r.returncode != 0
     assert "reaches half the periodic box" in r.stderr
+
+
+def test_reference_driver_runs_unchanged_on_this_library():
+    """The reference's own standalone driver (src/main.cu, compiled from the reference by
+    oracle/Makefile against libcosmoSPHere) runs on this library; its printed h and rho
+    ranges match the oracle's for the same lattice and jiggle."""
+    drv = os.path.join(REPO, "oracle", "_ref", "ref_driver_b200")
+    if not os.path.exists(drv):
+        pytest.skip("reference driver not built (needs the reference checkout at build time)")
+    r = subprocess.run([drv, "lattice", "20", "no_output", "jiggle"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if "Output" in ln and "range" in ln]
+    assert len(lines) == 4          # h and rho, for the flat and the warp-per-leaf call
+    p = inputs.lattice(20)
+    inputs.jiggle_ref(p["h"], 42)
+    o = O.Oracle()
+    assert o.density(p["x"], p["y"], p["z"], p["h"], p["pmass"], with_gradients=False) == 0
+    h, rho = o.array("h"), o.array("rho")
+    want_h = " Output h   range: [%.6e, %.6e]" % (h.min(), h.max())
+    want_r = " Output rho range: [%.6e, %.6e]" % (rho.min(), rho.max())
+    assert lines[0] == want_h and lines[2] == want_h
+    assert lines[1] == want_r and lines[3] == want_r
