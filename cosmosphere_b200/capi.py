@@ -22,6 +22,7 @@ EXPORTS = [
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
+    "cosmo_hilbert_order_noalloc",
 ]
 
 _DT = {0: np.float64, 1: np.int32, 2: np.uint32, 3: np.uint64, 4: np.int64}
@@ -56,6 +57,8 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_mark_elapsed.restype = D
     L.cosmo_x_launches.restype = ctypes.c_ulonglong
     L.cosmo_x_fp64_peak.restype = D
+    L.cosmo_hilbert_order_noalloc.argtypes = [I, P, P, P, P, I, P, P, P]
+    L.cosmo_hilbert_order_noalloc.restype = I
     return L
 
 
@@ -133,6 +136,14 @@ class Cosmo:
 
     def sync(self):
         self.L.cosmo_x_sync()
+
+    def hilbert_order_noalloc(self, n: int, d_x: int, d_y: int, d_z: int, d_h: int, d_keys: int, d_order: int,
+                              periodic_box=None) -> int:
+        """The allocation-free keys + sort entry point; all pointers are device addresses."""
+        box = _c(periodic_box if periodic_box is not None else np.zeros(6))
+        return int(self.L.cosmo_hilbert_order_noalloc(int(n), d_x, d_y, d_z, d_h,
+                                                      1 if periodic_box is not None else 0, box.ctypes.data,
+                                                      d_keys, d_order))
 
     def set_device(self, dev: int):
         self.L.cosmo_x_set_device(int(dev))

@@ -723,6 +723,83 @@ void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int 
     // eight passes: the result is back in kA / vA
 }
 
+// ---------------------------------------------------------------------------------------
+// Hilbert keys and their stable sort with every buffer supplied by the caller (used by
+// the allocation-free entry point in noalloc.cu).  Same kernels and launch sequence as
+// build_tree's keys + radix_sort_u64; scratch is carved as laid out below.
+// ---------------------------------------------------------------------------------------
+namespace {
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
+constexpr int kRawBboxBlocks = 296;
+}
+
+size_t keysort_scratch_bytes(int n)
+{
+    const size_t tiles = size_t(std::max(1, iceil(n, kSortTile)));
+    size_t b = 0;
+    b += align_up(sizeof(DevBox));
+    b += align_up(size_t(kRawBboxBlocks) * 6 * sizeof(double));
+    b += align_up(kSortPasses * 256 * sizeof(uint32_t));       // histograms
+    b += align_up(kSortPasses * 256 * sizeof(uint32_t));       // bin bases
+    b += align_up(16 * sizeof(unsigned int) + sizeof(int));    // tile tickets + error word
+    b += align_up(size_t(kSortPasses) * tiles * 256 * sizeof(uint32_t));
+    b += align_up(size_t(n) * sizeof(uint64_t));               // key ping-pong partner
+    b += align_up(size_t(n) * sizeof(int));                    // index ping-pong partner
+    return b;
+}
+
+int keysort_raw(int n, const double* x, const double* y, const double* z, const double* h,
+                const double* periodicBox, uint64_t* keysOut, int* orderOut, void* scratch, int numSMs,
+                cudaStream_t st)
+{
+    const int tiles = std::max(1, iceil(n, kSortTile));
+    char* p = static_cast<char*>(scratch);
+    auto take = [&](size_t bytes) { char* q = p; p += align_up(bytes); return q; };
+    DevBox* box = reinterpret_cast<DevBox*>(take(sizeof(DevBox)));
+    double* part = reinterpret_cast<double*>(take(size_t(kRawBboxBlocks) * 6 * sizeof(double)));
+    uint32_t* hist = reinterpret_cast<uint32_t*>(take(kSortPasses * 256 * sizeof(uint32_t)));
+    uint32_t* base = reinterpret_cast<uint32_t*>(take(kSortPasses * 256 * sizeof(uint32_t)));
+    unsigned int* tickets = reinterpret_cast<unsigned int*>(take(16 * sizeof(unsigned int) + sizeof(int)));
+    int* err = reinterpret_cast<int*>(tickets + 16);
+    uint32_t* lookback = reinterpret_cast<uint32_t*>(take(size_t(kSortPasses) * tiles * 256 * sizeof(uint32_t)));
+    uint64_t* kB = reinterpret_cast<uint64_t*>(take(size_t(n) * sizeof(uint64_t)));
+    int* vB = reinterpret_cast<int*>(take(size_t(n) * sizeof(int)));
+
+    // The array keeps the previous call's contents: clear what must start at zero.
+    if (cudaMemsetAsync(hist, 0, kSortPasses * 256 * sizeof(uint32_t), st) != cudaSuccess) return -2;
+    if (cudaMemsetAsync(tickets, 0, 16 * sizeof(unsigned int) + sizeof(int), st) != cudaSuccess) return -2;
+    if (cudaMemsetAsync(lookback, 0, size_t(kSortPasses) * tiles * 256 * sizeof(uint32_t), st) != cudaSuccess)
+        return -2;
+    if (periodicBox)
+        set_box_kernel<<<1, 32, 0, st>>>(periodicBox[0], periodicBox[1], periodicBox[2], periodicBox[3],
+                                         periodicBox[4], periodicBox[5], box);
+    else
+    {
+        const int nb = std::min(std::min(iceil(n, kBlk), 2 * numSMs), kRawBboxBlocks);
+        bbox_partial_kernel<<<nb, kBlk, 0, st>>>(x, y, z, n, part);
+        bbox_final_kernel<<<1, 32, 0, st>>>(part, nb, box);
+    }
+    keys_kernel<<<iceil(n, kBlk), kBlk, 0, st>>>(x, y, z, h, n, box, keysOut);
+    digit_hist_kernel<<<std::min(iceil(n, kBlk), 4 * numSMs), kBlk, 0, st>>>(keysOut, n, hist);
+    digit_base_kernel<<<kSortPasses, 256, 0, st>>>(hist, base);
+    uint64_t* ki = keysOut; uint64_t* ko = kB;
+    int* vi = nullptr; int* vo = vB;
+    for (int pass = 0; pass < kSortPasses; ++pass)
+    {
+        onesweep_kernel<<<tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n, 8 * pass, base + 256 * pass,
+                                                        lookback + size_t(pass) * tiles * 256, &tickets[pass], err);
+        std::swap(ki, ko);
+        vi = vo;
+        vo = (vo == vB) ? orderOut : vB;
+    }
+    if (cudaGetLastError() != cudaSuccess) return -2;
+    int e = 0;
+    if (cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -2;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -2;
+    return e ? -3 : 0;
+}
+
 void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
 {
     const int n = s.ngas;

@@ -81,6 +81,25 @@ void densityiterate_gpu_c(int n, double pmass, int periodic, const double* box, 
 void force_gpu_c(int n, double pmass, double beta, double alphau, int disc_viscosity, int pdv_heating,
                  int shock_heating);
 
+/* Hilbert keys and the stable sort order of n particles, computed without allocating
+ * any device memory.  No counterpart in the reference: it exists for callers that cannot
+ * call cudaMalloc at this point -- a caller that fixes its device-memory budget at start
+ * and treats a later allocation as a failure, or one that keeps its own GPU work in
+ * flight (cudaMalloc/cudaFree synchronise the device).  Inputs d_x, d_y, d_z, d_h and
+ * outputs d_keys (n sorted keys) and d_order (sorted position -> input index) are DEVICE
+ * pointers the caller owns; box6 is a host array read only when periodic != 0.  The
+ * results equal the keys and ordering a density solve of the same particles builds.
+ * Scratch is a fixed 7.06 MiB array inside the library, held by every GPU that loads it
+ * until exit; n must be in [1, 524288], else it returns -1 (with a message on stderr)
+ * and does nothing.  The first call on a device looks up that array's address; make
+ * that first call before any stream capture.  Runs on the legacy default stream and
+ * returns when done: 0 ok, -1 size rejected, -2 CUDA error, -3 device wait gave up.
+ * Every call uses the same array: calls that overlap on the GPU (from several threads
+ * or streams) race and corrupt each other's results. */
+int cosmo_hilbert_order_noalloc(int n, const double* d_x, const double* d_y, const double* d_z,
+                                const double* d_h, int periodic, const double* box6,
+                                unsigned long long* d_keys, int* d_order);
+
 /* ---- harness hooks (no counterpart in the reference; used by tests and bench) ---- */
 
 /* Set the Newton iteration cap (default 100, as src/density_base.cu:50). */

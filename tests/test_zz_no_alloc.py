@@ -1,0 +1,62 @@
+"""The allocation-free entry point, cosmo_hilbert_order_noalloc, against the keys and
+sort order the regular density solve builds for the same particles.
+
+It serves callers that cannot allocate device memory at call time (a fixed device
+budget set at start-up, or GPU work of their own in flight that cudaMalloc's device-wide
+synchronisation would stall).  This file is collected last on purpose."""
+import numpy as np
+import pytest
+
+from cosmosphere_b200 import capi, inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def _reference_order(p, box=None):
+    """Keys and order from the regular entry points (cosmo_upload + densityiterate_gpu_c)."""
+    n = p.n
+    c = capi.Cosmo()
+    c.arrays_init(n)
+    c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+    c.upload(capi.HSML, p["h"])
+    c.density(n, p["pmass"], periodic_box=box)
+    return c, c.array("keys"), c.array("order")
+
+
+def _device(a, torch, dtype):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_noalloc_matches_regular_entry_point_twice(periodic):
+    import torch
+    p = inputs.lattice100_workload(24)
+    if periodic:
+        p["x"], p["y"], p["z"] = (np.mod(p[k] + 0.013, 1.0) for k in "xyz")
+    box = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0] if periodic else None
+    n = p.n
+    c, want_keys, want_order = _reference_order(p, box)
+    dx, dy, dz, dh = (_device(p[k], torch, torch.float64) for k in "xyzh")
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    order = torch.empty(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    for call in range(2):
+        keys.fill_(-1)
+        order.fill_(-1)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        rc = c.hilbert_order_noalloc(n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(), dh.data_ptr(),
+                                     keys.data_ptr(), order.data_ptr(), periodic_box=box)
+        torch.cuda.synchronize()
+        assert rc == 0, (call, rc)
+        if call == 1:                       # after the first call's set-up, nothing more is reserved
+            assert torch.cuda.mem_get_info()[0] == free_before
+        np.testing.assert_array_equal(keys.cpu().numpy().view(np.uint64), want_keys, err_msg=f"call {call}")
+        np.testing.assert_array_equal(order.cpu().numpy(), want_order, err_msg=f"call {call}")
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(capfd):
+    c = capi.Cosmo()
+    assert c.hilbert_order_noalloc((1 << 19) + 1, 0, 0, 0, 0, 0, 0) == -1
+    assert c.hilbert_order_noalloc(0, 0, 0, 0, 0, 0, 0) == -1
+    assert "outside [1, 524288]" in capfd.readouterr().err
