@@ -70,20 +70,24 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
                 stream_pairs(
                     sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
                     [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                    [&](const double4& pj, int) {
-                        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                        const double q2 = pair_r2(dx, dy, dz) * hinv2;
-                        ++gc;
-                        if (q2 < kRadK2)
-                        {
-                            const double q = sqrt(q2);
-                            double wk, dwk;
-                            sph_kernel(q2, q, wk, dwk);
-                            rhoi += wk;
-                            gradhi += -q * dwk - 3.0 * wk;
-                            ++gp;
-                        }
+                    [&](const double4* ring, const int* ringIdx, int head, int count) {
+                        auto q2of = [&](const double4& pj) {
+                            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                            nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                            return pair_r2(dx, dy, dz) * hinv2;
+                        };
+                        gc += count;
+                        two_pass(ring, ringIdx, head, count, mine,
+                                 [&](const double4& pj) { return q2of(pj) < kRadK2; },
+                                 [&](const double4& pj, int) {
+                                     const double q2 = q2of(pj);
+                                     const double q = sqrt(q2);
+                                     double wk, dwk;
+                                     sph_kernel(q2, q, wk, dwk);
+                                     rhoi += wk;
+                                     gradhi += -q * dwk - 3.0 * wk;
+                                     ++gp;
+                                 });
                     });
                 bool stillActive = false;
                 if (mine)
@@ -214,12 +218,18 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
             stream_pairs(
                 sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
                 [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                [&](const double4& pj, int j) {
+                [&](const double4* ring, const int* ringIdx, int head, int count) {
+                  two_pass(ring, ringIdx, head, count, mine,
+                  [&](const double4& pj) {
+                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                    return pair_r2(dx, dy, dz) * hinv2 < kRadK2;
+                  },
+                  [&](const double4& pj, int j) {
                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                     const double r2 = pair_r2(dx, dy, dz);
                     const double q2 = r2 * hinv2;
-                    if (!(q2 < kRadK2)) return;
                     ++gp;
                     const double q = sqrt(q2);
                     double wk, dwk;
@@ -243,6 +253,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                     da[6] += daz * rx; da[7] += daz * ry; da[8] += daz * rz;
                     rxx -= dx * rx; rxy -= dx * ry; rxz -= dx * rz;
                     ryy -= dy * ry; ryz -= dy * rz; rzz -= dz * rz;
+                  });
                 });
             if (!mine) continue;
             pairs += gp;

@@ -96,16 +96,23 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
             stream_pairs(
                 sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
                 [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
-                [&](const double4& pj, int j) {
-                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                [&](const double4* ring, const int* ringIdx, int head, int count) {
+                  auto dr2of = [&](const double4& pj, double& dx, double& dy, double& dz) {
+                    dx = pi.x - pj.x; dy = pi.y - pj.y; dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                    const double dr2 = pair_r2(dx, dy, dz);
-                    if (!(dr2 > 0.0)) return;
+                    return pair_r2(dx, dy, dz);
+                  };
+                  two_pass(ring, ringIdx, head, count, mine,
+                  [&](const double4& pj) {
+                    double dx, dy, dz;
+                    const double dr2 = dr2of(pj, dx, dy, dz);
                     const double hj = pj.w;
-                    {
-                        const double rmax2 = kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10);
-                        if (dr2 >= rmax2) return;
-                    }
+                    return (dr2 > 0.0) && !(dr2 >= kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10));
+                  },
+                  [&](const double4& pj, int j) {
+                    double dx, dy, dz;
+                    const double dr2 = dr2of(pj, dx, dy, dz);
+                    const double hj = pj.w;
                     const double4 aj = ldg4(prepA + j);
                     const double qi2 = dr2 * hsqinvi;
                     const double qj2 = dr2 * aj.x;
@@ -181,6 +188,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
                         f4s += vsigu * denij * autermj * gkj;
                     }
                     if (took) ++gp;
+                  });
                 });
             if (!mine) continue;
             pairs += gp;

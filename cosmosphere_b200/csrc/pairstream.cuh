@@ -85,22 +85,18 @@ __device__ __forceinline__ bool in_sym_box(const double4& p, const GroupBox& b, 
 }
 
 // Stream the j particles of one i-leaf list through the group filter into the ring and
-// hand each survivor (with its index) to consume(pj, j), in ascending j order, on every
-// lane.  filter(pj) is evaluated by the loading lane only.
-template<class Filter, class Consume>
+// hand the survivors to batch(ring, ringIdx, head, count) in runs of up to 32, in
+// ascending j order, on every lane.  filter(pj) is evaluated by the loading lane only.
+template<class Filter, class Batch>
 __device__ __forceinline__ void stream_pairs(double4* ring, int* ringIdx, uint32_t jb, uint32_t nj,
                                              const int* __restrict__ jlist, const uint32_t* __restrict__ layout,
-                                             const double4* __restrict__ xyzh, Filter filter, Consume consume)
+                                             const double4* __restrict__ xyzh, Filter filter, Batch batch)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     int head = 0, cnt = 0;
     auto drain = [&](int count) {
-        for (int k = 0; k < count; ++k)
-        {
-            const int s = (head + k) & (kRing - 1);
-            consume(ring[s], ringIdx[s]);
-        }
+        batch(ring, ringIdx, head, count);
         head = (head + count) & (kRing - 1);
         cnt -= count;
         __syncwarp();
@@ -132,6 +128,32 @@ __device__ __forceinline__ void stream_pairs(double4* ring, int* ringIdx, uint32
         }
     }
     if (cnt > 0) drain(cnt);
+}
+
+// Two passes over one batch of up to 32 ring entries, for a lane's own particle:
+//   A  test(pj) -> bool for every entry, branch-free, collected into a 32-bit mask;
+//   B  for the set bits in ascending order (all lanes in lockstep until every lane's
+//      mask is empty), accept(pj, j) evaluates the pair.
+// The order in which a lane accepts its pairs is the ring order, i.e. ascending j.
+template<class Test, class Accept>
+__device__ __forceinline__ void two_pass(const double4* ring, const int* ringIdx, int head, int count, bool mine,
+                                         Test test, Accept accept)
+{
+    uint32_t acc = 0;
+#pragma unroll 4
+    for (int k = 0; k < count; ++k)
+        acc |= (test(ring[(head + k) & (kRing - 1)]) ? 1u : 0u) << k;
+    if (!mine) acc = 0;
+    while (__any_sync(0xffffffffu, acc != 0))
+    {
+        if (acc)
+        {
+            const int k = __ffs(acc) - 1;
+            acc &= acc - 1;
+            const int s = (head + k) & (kRing - 1);
+            accept(ring[s], ringIdx[s]);
+        }
+    }
 }
 
 // Near-equal split of a leaf window's active slots into warp groups: group g of G takes
