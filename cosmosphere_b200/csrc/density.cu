@@ -30,6 +30,7 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
                   DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ float4 sRingF[kWarpsPerBlock][kRing];
     __shared__ int sIdx[kWarpsPerBlock][kRing];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -67,20 +68,24 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
                 const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
                 double rhoi = 0.0, gradhi = 0.0;
                 unsigned int gp = 0, gc = 0;
+                // float copy of the group relative to the box centre, and the lane's
+                // conservative float threshold (R h + margin)^2, rounded up
+                const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
+                const double rm = rs + fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0);
+                const float tf = __double2float_ru(rm * rm * (1.0 + 1e-6));
+                const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
                 stream_pairs(
-                    sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
+                    sRing[wib], sRingF[wib], sIdx[wib], bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
                     [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                    [&](const double4* ring, const int* ringIdx, int head, int count) {
-                        auto q2of = [&](const double4& pj) {
-                            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                            nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                            return pair_r2(dx, dy, dz) * hinv2;
-                        };
+                    [&](const double4* ring, const float4* ringf, const int* ringIdx, int head, int count) {
                         gc += count;
-                        two_pass(ring, ringIdx, head, count, mine,
-                                 [&](const double4& pj) { return q2of(pj) < kRadK2; },
+                        two_pass(ring, ringf, ringIdx, head, count, mine,
+                                 [&](const float4& pf) { return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= tf; },
                                  [&](const double4& pj, int) {
-                                     const double q2 = q2of(pj);
+                                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                                     const double q2 = pair_r2(dx, dy, dz) * hinv2;
+                                     if (!(q2 < kRadK2)) return;
                                      const double q = sqrt(q2);
                                      double wk, dwk;
                                      sph_kernel(q2, q, wk, dwk);
@@ -179,6 +184,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                 double pmass, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ float4 sRingF[kWarpsPerBlock][kRing];
     __shared__ int sIdx[kWarpsPerBlock][kRing];
     const int wib = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -215,21 +221,22 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
             double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, da[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             double rxx = 0, rxy = 0, rxz = 0, ryy = 0, ryz = 0, rzz = 0;
             unsigned int gp = 0;
+            const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
+            const double rm = rs + fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0);
+            const float tf = __double2float_ru(rm * rm * (1.0 + 1e-6));
+            const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
             stream_pairs(
-                sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
+                sRing[wib], sRingF[wib], sIdx[wib], bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
                 [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                [&](const double4* ring, const int* ringIdx, int head, int count) {
-                  two_pass(ring, ringIdx, head, count, mine,
-                  [&](const double4& pj) {
-                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                    return pair_r2(dx, dy, dz) * hinv2 < kRadK2;
-                  },
+                [&](const double4* ring, const float4* ringf, const int* ringIdx, int head, int count) {
+                  two_pass(ring, ringf, ringIdx, head, count, mine,
+                  [&](const float4& pf) { return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= tf; },
                   [&](const double4& pj, int j) {
                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                     const double r2 = pair_r2(dx, dy, dz);
                     const double q2 = r2 * hinv2;
+                    if (!(q2 < kRadK2)) return;
                     ++gp;
                     const double q = sqrt(q2);
                     double wk, dwk;

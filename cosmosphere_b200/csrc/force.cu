@@ -54,6 +54,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
              int shock, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ float4 sRingF[kWarpsPerBlock][kRing];
     __shared__ int sIdx[kWarpsPerBlock][kRing];
     const int wib = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -93,26 +94,29 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
             unsigned int gp = 0;
             const double rg = kRadKernel * warp_max(mine ? hi : 0.0);
             const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, 0.0, rg);
+            // float prefilter: r_f^2 <= (R max(h_i, h_j) (1 + 1e-5) + margin)^2; the exact
+            // tests (dr2 > 0, dr2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10)) run in the accept pass
+            const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
+            const float mf = __double2float_ru(fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0) +
+                                               1e-6 * rg);
+            const float hif = float(hi);
+            const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
             stream_pairs(
-                sRing[wib], sIdx[wib], jb, nj, jlist, layout, xyzh,
+                sRing[wib], sRingF[wib], sIdx[wib], bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
                 [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
-                [&](const double4* ring, const int* ringIdx, int head, int count) {
-                  auto dr2of = [&](const double4& pj, double& dx, double& dy, double& dz) {
-                    dx = pi.x - pj.x; dy = pi.y - pj.y; dz = pi.z - pj.z;
-                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                    return pair_r2(dx, dy, dz);
-                  };
-                  two_pass(ring, ringIdx, head, count, mine,
-                  [&](const double4& pj) {
-                    double dx, dy, dz;
-                    const double dr2 = dr2of(pj, dx, dy, dz);
-                    const double hj = pj.w;
-                    return (dr2 > 0.0) && !(dr2 >= kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10));
+                [&](const double4* ring, const float4* ringf, const int* ringIdx, int head, int count) {
+                  two_pass(ring, ringf, ringIdx, head, count, mine,
+                  [&](const float4& pf) {
+                    const float r = fmaf(float(kRadKernel) * 1.00001f, fmaxf(hif, pf.w), mf);
+                    return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= r * r;
                   },
                   [&](const double4& pj, int j) {
-                    double dx, dy, dz;
-                    const double dr2 = dr2of(pj, dx, dy, dz);
+                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                    const double dr2 = pair_r2(dx, dy, dz);
+                    if (!(dr2 > 0.0)) return;
                     const double hj = pj.w;
+                    if (dr2 >= kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10)) return;
                     const double4 aj = ldg4(prepA + j);
                     const double qi2 = dr2 * hsqinvi;
                     const double qj2 = dr2 * aj.x;

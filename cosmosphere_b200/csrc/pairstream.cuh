@@ -84,65 +84,118 @@ __device__ __forceinline__ bool in_sym_box(const double4& p, const GroupBox& b, 
     return dx * dx + dy * dy + dz * dz <= r * r;
 }
 
+__device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
 // Stream the j particles of one i-leaf list through the group filter into the ring and
-// hand the survivors to batch(ring, ringIdx, head, count) in runs of up to 32, in
+// hand the survivors to batch(ring, ringf, ringIdx, head, count) in runs of up to 32, in
 // ascending j order, on every lane.  filter(pj) is evaluated by the loading lane only.
+//
+// Up to 32 list entries and their particle ranges are fetched at once, one per lane; a
+// warp prefix sum over the range lengths flattens them, so every load batch is 32
+// consecutive stream positions (each lane finds its particle by a 5-step binary search
+// over the prefix sums), and the next batch's loads are issued before the current batch
+// is filtered and evaluated.
 template<class Filter, class Batch>
-__device__ __forceinline__ void stream_pairs(double4* ring, int* ringIdx, uint32_t jb, uint32_t nj,
-                                             const int* __restrict__ jlist, const uint32_t* __restrict__ layout,
+__device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
+                                             double cz, uint32_t jb, uint32_t nj, const int* __restrict__ jlist,
+                                             const uint32_t* __restrict__ layout,
                                              const double4* __restrict__ xyzh, Filter filter, Batch batch)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     int head = 0, cnt = 0;
     auto drain = [&](int count) {
-        batch(ring, ringIdx, head, count);
+        batch(ring, ringf, ringIdx, head, count);
         head = (head + count) & (kRing - 1);
         cnt -= count;
         __syncwarp();
     };
-    for (uint32_t jl = 0; jl < nj; ++jl)
+    for (uint32_t lb = 0; lb < nj; lb += 32)
     {
-        const int jLeaf = jlist[jb + jl];
-        const uint32_t q0 = layout[jLeaf], q1 = layout[jLeaf + 1];
-        for (uint32_t b = q0; b < q1; b += 32)
+        const int nb = int(min(32u, nj - lb));
+        uint32_t s0 = 0, len = 0;
+        if (lane < nb)
         {
-            const uint32_t j = b + lane;
-            bool pass = false;
-            double4 pj;
-            if (j < q1)
+            const int leaf = jlist[jb + lb + lane];
+            s0 = layout[leaf];
+            len = layout[leaf + 1] - s0;
+        }
+        const uint32_t incl = warp_incl_scan_u32(len);
+        const uint32_t excl = incl - len;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        // particle index of stream position p (p < total)
+        auto locate = [&](uint32_t p) -> uint32_t {
+            int t = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
             {
-                pj = ldg4(xyzh + j);
-                pass = filter(pj);
+                const uint32_t e = __shfl_sync(0xffffffffu, excl, (t + step) & 31);
+                if (t + step < nb && e <= p) t += step;
             }
+            return __shfl_sync(0xffffffffu, s0, t) + (p - __shfl_sync(0xffffffffu, excl, t));
+        };
+        uint32_t j = 0;
+        double4 pj = make_double4(0, 0, 0, 0);
+        if (total > 0)
+        {
+            j = locate(lane);
+            if (uint32_t(lane) < total) pj = ldg4(xyzh + j);
+        }
+        for (uint32_t p0 = 0; p0 < total; p0 += 32)
+        {
+            const bool valid = p0 + lane < total;
+            // prefetch the next batch before working on this one
+            uint32_t jn = 0;
+            double4 pn = make_double4(0, 0, 0, 0);
+            if (p0 + 32 < total)
+            {
+                jn = locate(p0 + 32 + lane);
+                if (p0 + 32 + lane < total) pn = ldg4(xyzh + jn);
+            }
+            const bool pass = valid && filter(pj);
             const uint32_t m = __ballot_sync(0xffffffffu, pass);
             if (pass)
             {
-                const int s = (head + cnt + __popc(m & lt)) & (kRing - 1);
-                ring[s] = pj;
-                ringIdx[s] = int(j);
+                const int slot = (head + cnt + __popc(m & lt)) & (kRing - 1);
+                ring[slot] = pj;
+                ringf[slot] = make_float4(float(pj.x - cx), float(pj.y - cy), float(pj.z - cz), float(pj.w));
+                ringIdx[slot] = int(j);
             }
             cnt += __popc(m);
             __syncwarp();
             if (cnt >= 32) drain(32);
+            j = jn;
+            pj = pn;
         }
     }
     if (cnt > 0) drain(cnt);
 }
 
 // Two passes over one batch of up to 32 ring entries, for a lane's own particle:
-//   A  test(pj) -> bool for every entry, branch-free, collected into a 32-bit mask;
+//   A  test(pf) on the float copy, branch-free, collected into a 32-bit mask.  It is a
+//      CONSERVATIVE prefilter: it may pass a pair the exact test rejects, never the
+//      reverse (see fp32_margin);
 //   B  for the set bits in ascending order (all lanes in lockstep until every lane's
-//      mask is empty), accept(pj, j) evaluates the pair.
+//      mask is empty), accept(pj, j) applies the exact FP64 test and evaluates the pair.
 // The order in which a lane accepts its pairs is the ring order, i.e. ascending j.
 template<class Test, class Accept>
-__device__ __forceinline__ void two_pass(const double4* ring, const int* ringIdx, int head, int count, bool mine,
-                                         Test test, Accept accept)
+__device__ __forceinline__ void two_pass(const double4* ring, const float4* ringf, const int* ringIdx, int head,
+                                         int count, bool mine, Test test, Accept accept)
 {
     uint32_t acc = 0;
-#pragma unroll 4
+#pragma unroll 8
     for (int k = 0; k < count; ++k)
-        acc |= (test(ring[(head + k) & (kRing - 1)]) ? 1u : 0u) << k;
+        acc |= (test(ringf[(head + k) & (kRing - 1)]) ? 1u : 0u) << k;
     if (!mine) acc = 0;
     while (__any_sync(0xffffffffu, acc != 0))
     {
@@ -154,6 +207,36 @@ __device__ __forceinline__ void two_pass(const double4* ring, const int* ringIdx
             accept(ring[s], ringIdx[s]);
         }
     }
+}
+
+// Absolute error bound of a float-relative-coordinate distance for a group.  Relative
+// coordinates are at most A = the box half extent (plus the period when periodic).  Per
+// axis, the two conversions, the subtraction and the periodic fold each round by at most
+// 2A*2^-24, so |d_float - |dx|| <= 6A*2^-24 and the 3-vector error is below
+// sqrt(3)*6A*2^-24 < 11A*2^-24; 16A*2^-24 covers it with room.  Relative rounding of
+// the squares and sums is covered by the caller's (1 + 1e-6) or (1 + 1e-5) factor.
+__device__ __forceinline__ double fp32_margin(const GroupBox& b, double period)
+{
+    const double A = fmax(b.ex, fmax(b.ey, b.ez)) + period;
+    return 16.0 * A * 5.9604644775390625e-8;
+}
+
+// Per-axis float distance, at the nearest periodic image when periodic.
+template<bool Periodic>
+__device__ __forceinline__ float axis_df(float a, float b, float L)
+{
+    float d = fabsf(a - b);
+    if (Periodic) d = fminf(d, L - d);
+    return d;
+}
+
+template<bool Periodic>
+__device__ __forceinline__ float r2_f32(float xi, float yi, float zi, const float4& pf, float Lx, float Ly, float Lz)
+{
+    const float dx = axis_df<Periodic>(xi, pf.x, Lx);
+    const float dy = axis_df<Periodic>(yi, pf.y, Ly);
+    const float dz = axis_df<Periodic>(zi, pf.z, Lz);
+    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
 }
 
 // Near-equal split of a leaf window's active slots into warp groups: group g of G takes
