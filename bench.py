@@ -37,7 +37,7 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-METRIC = "density+force particle-updates/s (lattice 100 + jiggle, plain FP64)"
+METRIC = "density+force particle-updates/s (lattice 100 + jiggle)"
 UNIT = "particle-updates/s"
 FLOP_PER_DENSITY_PAIR = 30.0
 FLOP_PER_NR_UPDATE = 30.0
@@ -155,6 +155,32 @@ def ncu_traffic(kernel: str):
     return None
 
 
+def mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs):
+    """Max / rms errors of the mixed form against the FP64 form, same inputs, same GPU."""
+    from cosmosphere_b200 import capi
+    res = {}
+    for mode in (0, 1):
+        c.set_precision(bool(mode))
+        c.upload(capi.POS, pos, n); c.upload(capi.HSML, hsml, n)
+        c.upload(capi.VEL, vel, n); c.upload(capi.ACCEL, acc, n)
+        c.density(n, p["pmass"], tolh=1e-4, hfact=1.2)
+        c.upload(capi.THERMO, thermo, n, sorted_=True)
+        c.force(n, p["pmass"], beta=2.0, alphau=0.0)
+        res[mode] = {k: c.download(k, n).copy() for k in outs}
+    c.set_precision(False)
+    r0, r1 = res[0], res[1]
+    rel = lambda a, b: np.abs(a - b) / np.abs(b)
+    f0, f1 = r0[capi.FORCE_OUT][:3], r1[capi.FORCE_OUT][:3]
+    amag = np.sqrt((f0 ** 2).sum(0))
+    da = np.sqrt(((f1 - f0) ** 2).sum(0))
+    rms_a = float(np.sqrt((amag ** 2).mean()))
+    eh, er = rel(r1[capi.HSML][0], r0[capi.HSML][0]), rel(r1[capi.DENS_OUT][0], r0[capi.DENS_OUT][0])
+    return {"vs": "plain FP64 form (bit-exact with the FP64 oracle)",
+            "h_max_rel": float(eh.max()), "h_rms_rel": float(np.sqrt((eh ** 2).mean())),
+            "rho_max_rel": float(er.max()), "rho_rms_rel": float(np.sqrt((er ** 2).mean())),
+            "a_max_rel_to_rms_a": float(da.max() / rms_a), "a_rms_rel_to_rms_a": float(np.sqrt((da ** 2).mean()) / rms_a)}
+
+
 def run_reference(args, rank, world, local, dist):
     """The CPU arm: the oracle port of the path, all host threads, a bounded sample."""
     if rank != 0:
@@ -193,6 +219,7 @@ def main():
     ap.add_argument("--npartx", type=int, default=100)
     ap.add_argument("--ref-npartx", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--profile", action="store_true",
                     help="for ncu: set up, run --warmup and --steps device-resident steps, print nothing else")
     args = ap.parse_args()
@@ -219,6 +246,11 @@ def main():
     for a in [pos, hsml, vel, acc, thermo] + list(outs.values()):
         c.pin(a)
     c.arrays_init(n)
+    mixed = args.precision == "mixed"
+    accuracy = None
+    if mixed and not args.profile:
+        accuracy = mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs)
+    c.set_precision(mixed)
 
     def upload_inputs():
         c.upload(capi.POS, pos, n)
@@ -320,7 +352,8 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+            "precision": args.precision, "accuracy_vs_fp64": accuracy,
             "config": {"workload": f"lattice {args.npartx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, "
                                    "cubic, open boundaries",
                        "particles": n, "particles_per_gpu": n, "nr_iterations": len(act),
@@ -328,7 +361,8 @@ def main():
                        "l2": "working set ~0.4 GB > 126 MB L2 (no flush needed)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * t_e2e / args.steps},
-            "roofline": {"kernel": "density_nr_kernel", "bound": "fp64", "achieved": achieved,
+            "roofline": {"kernel": "density_nr_mixed_kernel" if mixed else "density_nr_kernel",
+                         "bound": "fp64", "achieved": achieved,
                          "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                          "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
                          "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",

@@ -22,7 +22,7 @@ EXPORTS = [
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
-    "cosmo_hilbert_order_noalloc",
+    "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
 ]
 
 _DT = {0: np.float64, 1: np.int32, 2: np.uint32, 3: np.uint64, 4: np.int64}
@@ -59,6 +59,8 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_fp64_peak.restype = D
     L.cosmo_hilbert_order_noalloc.argtypes = [I, P, P, P, P, I, P, P, P]
     L.cosmo_hilbert_order_noalloc.restype = I
+    L.cosmo_set_precision.argtypes = [I]
+    L.cosmo_get_precision.restype = I
     return L
 
 
@@ -144,6 +146,12 @@ class Cosmo:
         return int(self.L.cosmo_hilbert_order_noalloc(int(n), d_x, d_y, d_z, d_h,
                                                       1 if periodic_box is not None else 0, box.ctypes.data,
                                                       d_keys, d_order))
+
+    def set_precision(self, mixed: bool):
+        self.L.cosmo_set_precision(1 if mixed else 0)
+
+    def precision(self) -> int:
+        return int(self.L.cosmo_get_precision())
 
     def set_device(self, dev: int):
         self.L.cosmo_x_set_device(int(dev))

@@ -68,6 +68,7 @@ void ensure_init(State& s)
     std::memset(s.hscal, 0, sizeof(DevScalars));
     s.box.resize(1, s.st);
     if (const char* e = std::getenv("COSMO_MAX_ITER")) s.maxIter = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("COSMO_PRECISION")) s.precision = (std::string(e) == "mixed") ? 1 : 0;
 }
 
 // src/gpu_state.cu:21-46: every particle-length array, sized once per count.
@@ -414,6 +415,21 @@ void force_gpu_c(int n, double pmass, double beta, double alphau, int disc_visco
                      s.ngas, s.nLeaves, 1e3 * t.upsweep, 1e3 * t.fjbuild, 1e3 * t.prep, 1e3 * t.fkern, gpu, wall,
                      wall - gpu);
     }
+}
+
+// Select the arithmetic of the pair kernels for the following solves and force passes.
+void cosmo_set_precision(int mode)
+{
+    State& s = state();
+    ensure_init(s);
+    s.precision = (mode == 1) ? 1 : 0;
+}
+
+int cosmo_get_precision(void)
+{
+    State& s = state();
+    ensure_init(s);
+    return s.precision;
 }
 
 // ---------------------------------------------------------------- harness hooks

@@ -81,7 +81,7 @@ density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint3
                         gc += count;
                         two_pass(ring, ringf, ringIdx, head, count, mine,
                                  [&](const float4& pf) { return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= tf; },
-                                 [&](const double4& pj, int) {
+                                 [&](const double4& pj, const float4&, int) {
                                      double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                                      nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                                      const double q2 = pair_r2(dx, dy, dz) * hinv2;
@@ -231,7 +231,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                 [&](const double4* ring, const float4* ringf, const int* ringIdx, int head, int count) {
                   two_pass(ring, ringf, ringIdx, head, count, mine,
                   [&](const float4& pf) { return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= tf; },
-                  [&](const double4& pj, int j) {
+                  [&](const double4& pj, const float4&, int j) {
                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                     const double r2 = pair_r2(dx, dy, dz);
@@ -400,7 +400,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         cudaEvent_t j1 = ev(s);
         COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 2 * sizeof(int), s.st));
         const int grid = grid_for(s, nActiveLeaves);
-        if (s.periodic)
+        if (s.precision == 1)
+            launch_density_mixed(s, nActiveLeaves, pmass, tolh, hfact);
+        else if (s.periodic)
             density_nr_kernel<true><<<grid, kThreads, 0, s.st>>>(
                 s.activeA.get(), nActiveLeaves, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
                 s.xyzh.get(), s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(),
@@ -457,7 +459,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         build_lists(s, false);
         cudaEvent_t g1 = ev(s);
         const int grid = grid_for(s, nL);
-        if (s.periodic)
+        if (s.precision == 1)
+            launch_gradient_mixed(s, pmass);
+        else if (s.periodic)
             gradient_kernel<true><<<grid, kThreads, 0, s.st>>>(
                 nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.vel4.get(),
                 s.acc4.get(), s.rho.get(), s.gradh.get(), s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass,

@@ -110,7 +110,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
                     const float r = fmaf(float(kRadKernel) * 1.00001f, fmaxf(hif, pf.w), mf);
                     return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= r * r;
                   },
-                  [&](const double4& pj, int j) {
+                  [&](const double4& pj, const float4&, int j) {
                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                     const double dr2 = pair_r2(dx, dy, dz);
@@ -253,9 +253,14 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
                                           s.vsigmax.get(), s.divvF.get(), pmass, beta, pdv ? 1 : 0,
                                           shock ? 1 : 0, s.box.get(), ds);
     };
-    if (s.periodic) { if (disc) launch(force_kernel<true, true>); else launch(force_kernel<true, false>); }
-    else { if (disc) launch(force_kernel<false, true>); else launch(force_kernel<false, false>); }
-    COSMO_LAUNCHED();
+    if (s.precision == 1)
+        launch_force_mixed(s, pmass, beta, disc, pdv, shock);
+    else
+    {
+        if (s.periodic) { if (disc) launch(force_kernel<true, true>); else launch(force_kernel<true, false>); }
+        else { if (disc) launch(force_kernel<false, true>); else launch(force_kernel<false, false>); }
+        COSMO_LAUNCHED();
+    }
     if (n > s.nAlive)
     {
         force_dead_kernel<<<iceil(n - s.nAlive, 256), 256, 0, s.st>>>(s.nAlive, n, s.fx.get(), s.fy.get(),

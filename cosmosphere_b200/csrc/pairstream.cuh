@@ -186,7 +186,7 @@ __device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* 
 //      CONSERVATIVE prefilter: it may pass a pair the exact test rejects, never the
 //      reverse (see fp32_margin);
 //   B  for the set bits in ascending order (all lanes in lockstep until every lane's
-//      mask is empty), accept(pj, j) applies the exact FP64 test and evaluates the pair.
+//      mask is empty), accept(pj, pf, j) applies the exact test and evaluates the pair.
 // The order in which a lane accepts its pairs is the ring order, i.e. ascending j.
 template<class Test, class Accept>
 __device__ __forceinline__ void two_pass(const double4* ring, const float4* ringf, const int* ringIdx, int head,
@@ -204,7 +204,7 @@ __device__ __forceinline__ void two_pass(const double4* ring, const float4* ring
             const int k = __ffs(acc) - 1;
             acc &= acc - 1;
             const int s = (head + k) & (kRing - 1);
-            accept(ring[s], ringIdx[s]);
+            accept(ring[s], ringf[s], ringIdx[s]);
         }
     }
 }
@@ -251,6 +251,56 @@ __device__ __forceinline__ int group_slot(uint32_t lo, uint32_t hi, int nAct, in
     if (k < nlo) return int(__fns(lo, 0, k + 1));
     k -= nlo;
     return 32 + int(__fns(hi, 0, k + 1));
+}
+
+// Compensated (Kahan) FP32 accumulation; the exact sum is s - c, formed in FP64.
+struct KahanF
+{
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x)
+    {
+        const float y = x - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return double(s) - double(c); }
+};
+
+// The SPH kernel in FP32 (same polynomials as sph_kernel).
+__device__ __forceinline__ void sph_kernel_f(float q2, float q, float& w, float& dw)
+{
+    if constexpr (kQuintic)
+    {
+        if (q < 1.0f)
+        {
+            const float q4 = q2 * q2;
+            w  = fmaf(-10.0f * q4, q, fmaf(30.0f, q4, fmaf(-60.0f, q2, 66.0f)));
+            dw = q * fmaf(-50.0f * q2, q, fmaf(120.0f, q2, -120.0f));
+        }
+        else if (q < 2.0f)
+        {
+            const float a = q - 3.0f, b = q - 2.0f;
+            const float a2 = a * a, b2 = b * b;
+            w  = fmaf(6.0f, b2 * b2 * b, -(a2 * a2 * a));
+            dw = fmaf(30.0f, b2 * b2, -5.0f * (a2 * a2));
+        }
+        else if (q < 3.0f)
+        {
+            const float a = q - 3.0f, a2 = a * a;
+            w  = -(a2 * a2 * a);
+            dw = -5.0f * (a2 * a2);
+        }
+        else { w = 0.0f; dw = 0.0f; }
+    }
+    else
+    {
+        (void)q2;
+        const float a = fmaxf(2.0f - q, 0.0f), b = fmaxf(1.0f - q, 0.0f);
+        const float a2 = a * a, b2 = b * b;
+        w  = 0.25f * fmaf(-4.0f * b2, b, a2 * a);
+        dw = 0.25f * fmaf(12.0f, b2, -3.0f * a2);
+    }
 }
 
 } // namespace cosmo

@@ -89,6 +89,7 @@ struct State
     double boxHost[6] = {0, 0, 0, 0, 0, 0};
     uint64_t token = 0, jlistToken = 0;
     int itersRun = 0, maxIter = 100;
+    int precision = 0;     // 0 plain FP64 (the drop-in form), 1 mixed FP32/FP64
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;
@@ -97,6 +98,7 @@ struct State
     DBuf<double> ux, uy, uz, uh, uvx, uvy, uvz, uax, uay, uaz;
     // Hilbert-order particle data
     DBuf<double4> xyzh, vel4, acc4, thermo4, prepA, prepB;
+    DBuf<float4> prepAf, prepBf, thermof;       // FP32 force factors (mixed form)
     DBuf<double> rho, gradh, divv, xi, ddivvdt, fx, fy, fz, f4, vsigmax, divvF;
     DBuf<double> xfer;                          // 6n: one slot's worth of host traffic
     DBuf<uint64_t> keysA, keysB;
@@ -143,6 +145,11 @@ uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool
 struct DensResult { int itersRun; int unconverged; int status; };
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh,
                          double hfact, int maxIter, bool withGradients);
+
+// mixed.cu
+void launch_density_mixed(State& s, int nActiveLeaves, double pmass, double tolh, double hfact);
+void launch_gradient_mixed(State& s, double pmass);
+void launch_force_mixed(State& s, double pmass, double beta, bool disc, bool pdv, bool shock);
 
 // force.cu
 void compute_forces(State& s, double pmass, double beta, double alphau, bool disc, bool pdv,

@@ -81,6 +81,16 @@ void densityiterate_gpu_c(int n, double pmass, int periodic, const double* box, 
 void force_gpu_c(int n, double pmass, double beta, double alphau, int disc_viscosity, int pdv_heating,
                  int shock_heating);
 
+/* Arithmetic of the pair kernels for the following density solves and force passes:
+ * COSMO_PRECISION_FP64 (default; the drop-in form, bit-for-bit with the FP64 oracle) or
+ * COSMO_PRECISION_MIXED (FP32 pair arithmetic on leaf-relative coordinates with Kahan-
+ * compensated sums combined in FP64; FP64 keys, tree, Newton-Raphson update and Omega).
+ * The environment variable COSMO_PRECISION=mixed sets the same at start-up.  No
+ * counterpart in the reference, which is FP64 only. */
+enum CosmoPrecision { COSMO_PRECISION_FP64 = 0, COSMO_PRECISION_MIXED = 1 };
+void cosmo_set_precision(int mode);
+int cosmo_get_precision(void);
+
 /* Hilbert keys and the stable sort order of n particles, computed without allocating
  * any device memory.  No counterpart in the reference: it exists for callers that cannot
  * call cudaMalloc at this point -- a caller that fixes its device-memory budget at start
