@@ -23,6 +23,8 @@ EXPORTS = [
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
+    "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_upload",
+    "cosmo_batch_density", "cosmo_batch_download", "cosmo_batch_scalar",
 ]
 
 _DT = {0: np.float64, 1: np.int32, 2: np.uint32, 3: np.uint64, 4: np.int64}
@@ -61,6 +63,16 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_hilbert_order_noalloc.restype = I
     L.cosmo_set_precision.argtypes = [I]
     L.cosmo_get_precision.restype = I
+    L.cosmo_batch_init.argtypes = [I, P]
+    L.cosmo_batch_init.restype = I
+    L.cosmo_batch_set_params.argtypes = [P, P, P]
+    L.cosmo_batch_set_bucket.argtypes = [P]
+    L.cosmo_batch_upload.argtypes = [P, P, P, P]
+    L.cosmo_batch_density.argtypes = [D, D, I]
+    L.cosmo_batch_density.restype = I
+    L.cosmo_batch_download.argtypes = [P, P, P]
+    L.cosmo_batch_scalar.argtypes = [ctypes.c_char_p]
+    L.cosmo_batch_scalar.restype = D
     return L
 
 
@@ -179,3 +191,44 @@ class Cosmo:
         out = np.empty(n, dtype=_DT[dt.value])
         self.L.cosmo_x_array(name.encode(), out.ctypes.data if n else None, ctypes.byref(dt))
         return out
+
+
+class Batch:
+    """The batched form: many independent sets, one segmented sort and forest, one
+    density launch per Newton iteration for all of them."""
+
+    def __init__(self, sets, quintic: bool = False, bucket=None):
+        """sets: list of dicts with x, y, z, h, pmass and optional box (periodic)."""
+        self.L = load(quintic)
+        self.sizes = [int(np.asarray(s["x"]).size) for s in sets]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int32)
+        self.n = int(self.offsets[-1])
+        rc = self.L.cosmo_batch_init(len(sets), self.offsets.ctypes.data)
+        if rc != 0:
+            raise ValueError("cosmo_batch_init rejected the set sizes")
+        pm = np.array([s["pmass"] for s in sets], dtype=np.float64)
+        per = np.array([1 if s.get("box") is not None else 0 for s in sets], dtype=np.int32)
+        box = np.array([s["box"] if s.get("box") is not None else [0.0] * 6 for s in sets], dtype=np.float64)
+        self.L.cosmo_batch_set_params(pm.ctypes.data, per.ctypes.data, box.ctypes.data)
+        if bucket is not None:
+            b = np.ascontiguousarray(np.broadcast_to(np.asarray(bucket, dtype=np.int32), (len(sets),)))
+            self.L.cosmo_batch_set_bucket(b.ctypes.data)
+        self._keep = (pm, per, box)
+        cat = lambda k: np.ascontiguousarray(np.concatenate([np.asarray(s[k], dtype=np.float64) for s in sets]))
+        self.x, self.y, self.z, self.h = cat("x"), cat("y"), cat("z"), cat("h")
+
+    def upload(self):
+        self.L.cosmo_batch_upload(self.x.ctypes.data, self.y.ctypes.data, self.z.ctypes.data, self.h.ctypes.data)
+
+    def density(self, tolh=1e-4, hfact=-1.0, max_iter=100) -> int:
+        return int(self.L.cosmo_batch_density(float(tolh), float(hfact), int(max_iter)))
+
+    def download(self):
+        h, rho, gh = (np.empty(self.n) for _ in range(3))
+        self.L.cosmo_batch_download(h.ctypes.data, rho.ctypes.data, gh.ctypes.data)
+        o = self.offsets
+        split = lambda a: [a[o[k]:o[k + 1]] for k in range(len(self.sizes))]
+        return split(h), split(rho), split(gh)
+
+    def scalar(self, name: str) -> float:
+        return float(self.L.cosmo_batch_scalar(name.encode()))

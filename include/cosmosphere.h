@@ -91,6 +91,29 @@ enum CosmoPrecision { COSMO_PRECISION_FP64 = 0, COSMO_PRECISION_MIXED = 1 };
 void cosmo_set_precision(int mode);
 int cosmo_get_precision(void);
 
+/* ---- batched form: many independent particle sets in one solve (no counterpart in
+ * the reference, which solves one set per call) ----
+ * The sets are concatenated set-major: set s owns entries [offsets[s], offsets[s+1]).
+ * One segmented (set, key) sort, one forest with a tree per set, and one density launch
+ * per Newton-Raphson iteration for all sets; per particle the arithmetic is the
+ * single-set form's (cosmo_set_precision), so each set's h, rho and d(rho)/dh equal those
+ * of solving it alone.  No gradient sweep or force pass in this form.
+ * cosmo_batch_init returns 0, or -1 for bad offsets. */
+int cosmo_batch_init(int nsets, const int* offsets);
+/* Per-set particle mass, periodicity (nonzero: periodic) and box {xmin,xmax,...} (6 per
+ * set, read where periodic); periodic/box6 may be NULL for all-open sets. */
+void cosmo_batch_set_params(const double* pmass, const int* periodic, const double* box6);
+/* Leaf capacity of each set's tree (default 64, the reference's BUCKET_SIZE). */
+void cosmo_batch_set_bucket(const int* bucket_per_set);
+/* Positions and initial h of all sets (host arrays, length offsets[nsets]). */
+void cosmo_batch_upload(const double* x, const double* y, const double* z, const double* h);
+/* Solve every set; 0 ok, 1 some particle unconverged within max_iter (<= 0: 100). */
+int cosmo_batch_density(double tolh, double hfact, int max_iter);
+/* Converged h, rho and d(rho)/dh of all sets, in the upload order. */
+void cosmo_batch_download(double* h, double* rho, double* gradh);
+/* Counters and timings (seconds) of the last batch solve; NaN if unknown. */
+double cosmo_batch_scalar(const char* name);
+
 /* Hilbert keys and the stable sort order of n particles, computed without allocating
  * any device memory.  No counterpart in the reference: it exists for callers that cannot
  * call cudaMalloc at this point -- a caller that fixes its device-memory budget at start
