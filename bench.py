@@ -181,6 +181,77 @@ def mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs):
             "a_max_rel_to_rms_a": float(da.max() / rms_a), "a_rms_rel_to_rms_a": float(np.sqrt((da ** 2).mean()) / rms_a)}
 
 
+def run_ensemble(args):
+    """The batched-ensemble workload: 256 sets (log-uniform 1e4..5e5 particles, periodic
+    uniform boxes and Plummer spheres), density / Newton-Raphson only.  Batched solves
+    (plain and mixed) against 256 sequential plain FP64 single-set solves on the same GPU."""
+    from cosmosphere_b200 import capi, inputs
+    sets = inputs.ensemble_sets(args.nsets)
+    n = sum(p.n for p in sets)
+    c = capi.Cosmo()
+    res = {}
+    outs = {}
+    for mode in ("fp64", "mixed"):
+        c.set_precision(mode == "mixed")
+        b = capi.Batch(sets)
+        b.upload()
+        for _ in range(args.warmup):
+            assert b.density(final_rho=True) == 0
+        t = 0.0
+        upd = 0.0
+        tnr = 0.0
+        for _ in range(args.steps):
+            assert b.density(final_rho=True) == 0
+            t += b.scalar("t_total")
+            tnr += b.scalar("t_nr")
+            upd += b.scalar("updates")
+        # end to end: upload + solve + download through the batch C-ABI
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            b.upload()
+            assert b.density(final_rho=True) == 0
+            out = b.download()
+        we = (time.perf_counter() - w0) / args.steps
+        outs[mode] = out
+        res[mode] = {"value": upd / t, "ms_per_solve": 1e3 * t / args.steps, "e2e_ms_per_solve": 1e3 * we,
+                     "ms_newton_loop_graph": 1e3 * tnr / args.steps, "graph": b.scalar("graph") == 1.0,
+                     "updates_per_solve": upd / args.steps, "iters": b.scalar("itersRun"),
+                     "leaves": b.scalar("nLeaves")}
+    c.set_precision(False)
+    # sequential plain FP64 single-set solves
+    tseq = 0.0
+    useq = 0.0
+    c.mark(4)
+    for p in sets:
+        c.arrays_init(p.n)
+        c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+        c.upload(capi.HSML, p["h"])
+        c.mark(5)
+        assert c.density_status(p.n, p["pmass"], periodic_box=p.get("box"), with_gradients=False) == 0
+        c.mark(6)
+        tseq += c.elapsed(5, 6)
+        useq += float(c.array("activePerIter").sum())
+    h0, r0 = np.concatenate(outs["fp64"][0]), np.concatenate(outs["fp64"][1])
+    h1, r1 = np.concatenate(outs["mixed"][0]), np.concatenate(outs["mixed"][1])
+    live = h0 > 0
+    line = {"metric": f"batched density particle-updates/s ({len(sets)}-set ensemble)",
+            "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["mixed"]["ms_per_solve"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{len(sets)} sets, log-uniform 1e4..5e5 particles, even: periodic uniform box, "
+                                   "odd: Plummer r<20; h = 1.2 x spacing x U[0.8,1.2]; cubic; density/NR loop "
+                                   "as one CUDA graph + rho at the converged h",
+                       "particles": n},
+            "batched_mixed": res["mixed"], "batched_fp64": res["fp64"],
+            "sequential_fp64": {"value": useq / tseq, "ms_total": 1e3 * tseq, "updates": useq,
+                                "how": "one single-set plain FP64 solve per set through the C-ABI, device-timed"},
+            "speedup_mixed_batched_vs_sequential_fp64": (res["mixed"]["value"]) / (useq / tseq),
+            "speedup_mixed_vs_fp64_batched": res["mixed"]["value"] / res["fp64"]["value"],
+            "accuracy_mixed_vs_fp64": {"h_max_rel": float(np.max(np.abs(h1[live] / h0[live] - 1))),
+                                       "rho_max_rel": float(np.max(np.abs(r1[live] / r0[live] - 1)))}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world, local, dist):
     """The CPU arm: the oracle port of the path, all host threads, a bounded sample."""
     if rank != 0:
@@ -220,6 +291,8 @@ def main():
     ap.add_argument("--ref-npartx", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "ensemble"])
+    ap.add_argument("--nsets", type=int, default=256)
     ap.add_argument("--profile", action="store_true",
                     help="for ncu: set up, run --warmup and --steps device-resident steps, print nothing else")
     args = ap.parse_args()
@@ -228,6 +301,9 @@ def main():
     rank, world, local, dist = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, rank, world, local, dist)
+        return
+    if args.workload == "ensemble":
+        run_ensemble(args)
         return
 
     from cosmosphere_b200 import capi

@@ -68,7 +68,7 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_batch_set_params.argtypes = [P, P, P]
     L.cosmo_batch_set_bucket.argtypes = [P]
     L.cosmo_batch_upload.argtypes = [P, P, P, P]
-    L.cosmo_batch_density.argtypes = [D, D, I]
+    L.cosmo_batch_density.argtypes = [D, D, I, I]
     L.cosmo_batch_density.restype = I
     L.cosmo_batch_download.argtypes = [P, P, P]
     L.cosmo_batch_scalar.argtypes = [ctypes.c_char_p]
@@ -220,8 +220,9 @@ class Batch:
     def upload(self):
         self.L.cosmo_batch_upload(self.x.ctypes.data, self.y.ctypes.data, self.z.ctypes.data, self.h.ctypes.data)
 
-    def density(self, tolh=1e-4, hfact=-1.0, max_iter=100) -> int:
-        return int(self.L.cosmo_batch_density(float(tolh), float(hfact), int(max_iter)))
+    def density(self, tolh=1e-4, hfact=-1.0, max_iter=100, graph=True, final_rho=False) -> int:
+        flags = (1 if graph else 0) | (2 if final_rho else 0)
+        return int(self.L.cosmo_batch_density(float(tolh), float(hfact), int(max_iter), flags))
 
     def download(self):
         h, rho, gh = (np.empty(self.n) for _ in range(3))

@@ -22,22 +22,32 @@
 
 namespace cosmo {
 
+// Newton-loop state kept on the device, so the loop body needs no host reads.
+struct LoopState
+{
+    int nActiveLeaves, nActiveParticles, iter, maxIter, nAll, pad[3];
+    long long activePerIter[128];
+};
+
 struct Batch
 {
     State core;                       // stream, device scalars, scratch for sort and scan
     int nsets = 0, n = 0, nLeaves = 0, numNodes = 0, itersRun = 0, unconverged = 0;
     std::vector<int> offs;            // host copy, nsets + 1
     std::vector<long long> activePerIter;
-    double tBuild = 0, tNR = 0, tList = 0;
+    double tBuild = 0, tNR = 0, tList = 0, tTotal = 0;
     unsigned long long pairs = 0;
     DBuf<int> dOffs, setOf, nAliveSet, setLeafStart, setNodeStart, bucket, setPer;
     DBuf<double> ux, uy, uz, uh, pmass, setBox6, rho, gradh, hmaxLeaf;
     DBuf<double4> xyzh, preCenter, preHalf;
-    DBuf<int> converged, orderA, orderB, leafSet, leafSet2, leafPre, preLeaf, preSkip, jlist, activeA, activeB;
+    DBuf<int> converged, orderA, orderB, leafSet, leafSet2, leafPre, preLeaf, preSkip, jlist, activeA, activeB, allLeaves;
     DBuf<uint64_t> keysA, keysB, leafKey, leafKey2;
     DBuf<uint32_t> ops, opsScan, nodeCount, leafPreStart, jcount, jOffset, setHist, setBase;
     DBuf<uint2> leafRange;
     DBuf<DevBox> boxes;
+    DBuf<LoopState> loop;
+    uint32_t listCap = 0;
+    bool graphUsed = false;
 };
 
 namespace {
@@ -317,10 +327,11 @@ __global__ void node_emit_kernel_b(const uint64_t* __restrict__ key, const int* 
 }
 
 __global__ void hmax_leaf_kernel_b(const double4* __restrict__ xyzh, const uint2* __restrict__ range,
-                                   const int* __restrict__ leaves, int nActive, double* __restrict__ hmax)
+                                   const int* __restrict__ leaves, const int* __restrict__ countPtr,
+                                   double* __restrict__ hmax)
 {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= nActive) return;
+    if (t >= *countPtr) return;
     const int l = leaves[t];
     const uint2 r = range[l];
     double hm = 0.0;
@@ -341,7 +352,7 @@ list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ s
                    const double4* __restrict__ preCenter, const double4* __restrict__ preHalf,
                    const int* __restrict__ preSkip, const int* __restrict__ preLeaf, const DevBox* __restrict__ boxes,
                    uint32_t* __restrict__ jcount, const uint32_t* __restrict__ jOffset, int* __restrict__ jlist,
-                   int* err)
+                   uint32_t listCap, int* err)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -356,7 +367,16 @@ list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ s
     const DevBox bx = boxes[s];
     const bool per = bx.periodic != 0;
     uint32_t count = 0, base = 0, cap = 0;
-    if (Fill) { base = jOffset[leaf]; cap = jOffset[leaf + 1] - base; }
+    if (Fill)
+    {
+        base = jOffset[leaf];
+        cap = jOffset[leaf + 1] - base;
+        if (jOffset[leaf + 1] > listCap)   // the preallocated list is too small: report, write nothing
+        {
+            if (lane == 0) atomicOr(err, int(kErrListFull));
+            return;
+        }
+    }
     const uint32_t lt = (1u << lane) - 1u;
     int p = ns;
     while (p < ne)
@@ -565,9 +585,9 @@ __device__ __forceinline__ void group_sums(double4* ring, float4* ringf, int* ri
     else { rhoi = r0; gradhi = g0; }
 }
 
-template<bool Mixed>
+template<bool Mixed, bool EvalAll>
 __global__ void __launch_bounds__(kThreads)
-density_batch_kernel(const int* __restrict__ leaves, int nLeavesActive, const int* __restrict__ leafSet,
+density_batch_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr, const int* __restrict__ leafSet,
                      const uint2* __restrict__ range, const uint32_t* __restrict__ jOffset,
                      const uint32_t* __restrict__ jcount, const int* __restrict__ jlist, double4* __restrict__ xyzh,
                      double* __restrict__ rho, double* __restrict__ gradh, int* __restrict__ converged,
@@ -578,6 +598,7 @@ density_batch_kernel(const int* __restrict__ leaves, int nLeavesActive, const in
     __shared__ float4 sRingF[kWarpsPerBlock][kRing];
     __shared__ int sIdx[kWarpsPerBlock][kRing];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nLeavesActive = *countPtr;
     unsigned long long pairs = 0;
     // dynamic work distribution over the active leaves of every set
     for (;;)
@@ -598,8 +619,8 @@ density_batch_kernel(const int* __restrict__ leaves, int nLeavesActive, const in
         for (uint32_t g = p0; g < p1; g += 64)
         {
             const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            const bool act0 = a0 < p1 && converged[a0] == 0;
-            const bool act1 = a1 < p1 && converged[a1] == 0;
+            const bool act0 = a0 < p1 && (EvalAll || converged[a0] == 0);
+            const bool act1 = a1 < p1 && (EvalAll || converged[a1] == 0);
             const uint32_t m0 = __ballot_sync(0xffffffffu, act0);
             const uint32_t m1 = __ballot_sync(0xffffffffu, act1);
             const int nAct = __popc(m0) + __popc(m1);
@@ -612,6 +633,7 @@ density_batch_kernel(const int* __restrict__ leaves, int nLeavesActive, const in
                 const uint32_t i = g + uint32_t(mine ? slot : 0);
                 const double4 pi = xyzh[i];
                 const double rs = kRadKernel * pi.w;
+                if (EvalAll && !(pi.w > 0.0)) continue;   // (never: live particles only)
                 const double rmax = warp_max(mine ? rs : 0.0);
                 const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
                 double rhoi = 0.0, gradhi = 0.0;
@@ -623,6 +645,19 @@ density_batch_kernel(const int* __restrict__ leaves, int nLeavesActive, const in
                     group_sums<false, Mixed>(sRing[wib], sRingF[wib], sIdx[wib], mine, pi, bx, 0.0, 0.0, 0.0, jb, nj,
                                              jlist, range, xyzh, rhoi, gradhi, gp);
                 bool still = false;
+                if (EvalAll)
+                {
+                    // rho and d(rho)/dh at the converged h (src/density_base.cu:635-643)
+                    if (mine)
+                    {
+                        pairs += gp;
+                        const double hi1 = 1.0 / pi.w;
+                        const double hi31 = hi1 * hi1 * hi1;
+                        rho[i] = rhoi * kCnormk * pmass * hi31;
+                        gradh[i] = gradhi * kCnormk * pmass * (hi31 * hi1);
+                    }
+                    continue;
+                }
                 if (mine)
                 {
                     pairs += gp;
@@ -647,6 +682,33 @@ density_batch_kernel(const int* __restrict__ leaves, int nLeavesActive, const in
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     if (lane == 0) atomicAdd(&ds->pairs[0], pairs);
+}
+
+__global__ void loop_reset_kernel(DevScalars* ds)
+{
+    ds->nextActive = 0;
+    ds->unconverged = 0;
+    ds->workCounter[0] = 0;
+}
+
+__global__ void copy_active_kernel(const int* __restrict__ src, int* __restrict__ dst, const DevScalars* __restrict__ ds,
+                                   int cap)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < cap && t < ds->nextActive) dst[t] = src[t];
+}
+
+// End of one Newton iteration: record it, adopt the next active set, and decide
+// whether the loop goes on (the graph's while condition when run as a graph).
+__global__ void loop_epilogue_kernel(LoopState* ls, const DevScalars* ds, cudaGraphConditionalHandle handle,
+                                     int setCondition)
+{
+    if (ls->iter < 128) ls->activePerIter[ls->iter] = ls->nActiveParticles;
+    ls->iter += 1;
+    ls->nActiveLeaves = ds->nextActive;
+    ls->nActiveParticles = ds->unconverged;
+    const int more = (ls->nActiveParticles > 0 && ls->iter < ls->maxIter && ds->err == 0) ? 1 : 0;
+    if (setCondition) cudaGraphSetConditional(handle, more);
 }
 
 __global__ void iota_kernel_b(int* __restrict__ a, int n)
@@ -779,89 +841,200 @@ static void batch_build(Batch& B)
     B.jOffset.resize(size_t(L) + 1, s.st);
     B.activeA.resize(L, s.st);
     B.activeB.resize(L, s.st);
+    B.allLeaves.resize(L, s.st);
     iota_kernel_b<<<iceil(L, kBlk), kBlk, 0, s.st>>>(B.activeA.get(), L);
+    COSMO_LAUNCHED();
+    iota_kernel_b<<<iceil(L, kBlk), kBlk, 0, s.st>>>(B.allLeaves.get(), L);
     COSMO_LAUNCHED();
     cudaEvent_t e1 = ev(s);
     read_scalars(s);
     B.tBuild = elapsed_s(e0, e1);
 }
 
-static void batch_lists(Batch& B)
+static void walk_lists(Batch& B, bool fill)
 {
     State& s = B.core;
     const int L = B.nLeaves;
     const int blocks = iceil(long(L) * 32, 256);
-    list_walk_kernel_b<false><<<blocks, 256, 0, s.st>>>(L, B.leafSet.get(), B.setNodeStart.get(), B.leafPre.get(),
-                                                       B.hmaxLeaf.get(), B.preCenter.get(), B.preHalf.get(),
-                                                       B.preSkip.get(), B.preLeaf.get(), B.boxes.get(), B.jcount.get(),
-                                                       B.jOffset.get(), B.jlist.get(), &s.dscal.get()->err);
-    COSMO_LAUNCHED();
-    const uint32_t total = scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, true);
-    B.jlist.resize(std::max<uint32_t>(total, 1u), s.st);
-    list_walk_kernel_b<true><<<blocks, 256, 0, s.st>>>(L, B.leafSet.get(), B.setNodeStart.get(), B.leafPre.get(),
-                                                      B.hmaxLeaf.get(), B.preCenter.get(), B.preHalf.get(),
-                                                      B.preSkip.get(), B.preLeaf.get(), B.boxes.get(), B.jcount.get(),
-                                                      B.jOffset.get(), B.jlist.get(), &s.dscal.get()->err);
+    auto go = [&](auto kern) {
+        kern<<<blocks, 256, 0, s.st>>>(L, B.leafSet.get(), B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(),
+                                       B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(),
+                                       B.boxes.get(), B.jcount.get(), B.jOffset.get(), B.jlist.get(), B.listCap,
+                                       &s.dscal.get()->err);
+    };
+    if (fill) go(list_walk_kernel_b<true>);
+    else go(list_walk_kernel_b<false>);
     COSMO_LAUNCHED();
 }
 
-static int batch_solve(Batch& B, double tolh, double hfact, int maxIter)
+// One Newton-Raphson iteration, every count read on the device: hmax of the active
+// leaves, the gather lists of all leaves (count, scan, fill), the density kernel over
+// the active leaves of all sets, the new active set, and the loop bookkeeping.  Run
+// eagerly, or captured once as the body of a graph's while node.
+static void nr_iteration(Batch& B, double tolh, double hfact, cudaGraphConditionalHandle handle, int setCond)
+{
+    State& s = B.core;
+    DevScalars* ds = s.dscal.get();
+    LoopState* ls = B.loop.get();
+    const int L = B.nLeaves;
+    hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.activeA.get(),
+                                                       &ls->nActiveLeaves, B.hmaxLeaf.get());
+    COSMO_LAUNCHED();
+    walk_lists(B, false);
+    scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, false);
+    walk_lists(B, true);
+    loop_reset_kernel<<<1, 1, 0, s.st>>>(ds);
+    COSMO_LAUNCHED();
+    const int grid = s.numSMs * 8;
+    auto go = [&](auto kern) {
+        kern<<<grid, kThreads, 0, s.st>>>(B.activeA.get(), &ls->nActiveLeaves, B.leafSet.get(), B.leafRange.get(),
+                                          B.jOffset.get(), B.jcount.get(), B.jlist.get(), B.xyzh.get(), B.rho.get(),
+                                          B.gradh.get(), B.converged.get(), B.pmass.get(), tolh, hfact, B.boxes.get(),
+                                          B.activeB.get(), ds);
+    };
+    if (s.precision == 1) go(density_batch_kernel<true, false>);
+    else go(density_batch_kernel<false, false>);
+    COSMO_LAUNCHED();
+    copy_active_kernel<<<iceil(L, 256), 256, 0, s.st>>>(B.activeB.get(), B.activeA.get(), ds, L);
+    COSMO_LAUNCHED();
+    loop_epilogue_kernel<<<1, 1, 0, s.st>>>(ls, ds, handle, setCond);
+    COSMO_LAUNCHED();
+}
+
+// rho and d(rho)/dh of every live particle at its final h (one more gather pass).
+static void final_rho(Batch& B)
+{
+    State& s = B.core;
+    DevScalars* ds = s.dscal.get();
+    LoopState* ls = B.loop.get();
+    const int L = B.nLeaves;
+    hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.allLeaves.get(), &ls->nAll,
+                                                       B.hmaxLeaf.get());
+    COSMO_LAUNCHED();
+    walk_lists(B, false);
+    const uint32_t total = scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, true);
+    if (total > B.listCap)
+    {
+        B.listCap = total + total / 4 + 1024;
+        B.jlist.resize(B.listCap, s.st);
+    }
+    walk_lists(B, true);
+    loop_reset_kernel<<<1, 1, 0, s.st>>>(ds);
+    COSMO_LAUNCHED();
+    const int grid = s.numSMs * 8;
+    auto go = [&](auto kern) {
+        kern<<<grid, kThreads, 0, s.st>>>(B.allLeaves.get(), &ls->nAll, B.leafSet.get(), B.leafRange.get(),
+                                          B.jOffset.get(), B.jcount.get(), B.jlist.get(), B.xyzh.get(), B.rho.get(),
+                                          B.gradh.get(), B.converged.get(), B.pmass.get(), 0.0, 0.0, B.boxes.get(),
+                                          B.activeB.get(), ds);
+    };
+    if (s.precision == 1) go(density_batch_kernel<true, true>);
+    else go(density_batch_kernel<false, true>);
+    COSMO_LAUNCHED();
+}
+
+static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int flags, int attempt = 0)
 {
     State& s = B.core;
     if (!(hfact > 0.0)) hfact = kHfactDefault;
+    maxIter = std::max(1, std::min(maxIter, 128));
     ev_reset();
     DevScalars* ds = s.dscal.get();
     COSMO_CUDA(cudaMemsetAsync(B.rho.get(), 0, size_t(B.n) * 8, s.st));
     COSMO_CUDA(cudaMemsetAsync(B.gradh.get(), 0, size_t(B.n) * 8, s.st));
     COSMO_CUDA(cudaMemsetAsync(B.converged.get(), 0, size_t(B.n) * 4, s.st));
     COSMO_CUDA(cudaMemsetAsync(&ds->pairs[0], 0, sizeof(ds->pairs), s.st));
+    cudaEvent_t t0 = ev(s);
     batch_build(B);
-    int nActiveLeaves = B.nLeaves;
-    long long nActiveParticles = 0;
+    const int L = B.nLeaves;
+    long long nAliveTotal = 0;
     {
         std::vector<int> na(B.nsets);
         COSMO_CUDA(cudaMemcpy(na.data(), B.nAliveSet.get(), size_t(B.nsets) * 4, cudaMemcpyDeviceToHost));
-        for (int v : na) nActiveParticles += v;
+        for (int v : na) nAliveTotal += v;
     }
-    B.activePerIter.clear();
-    B.tNR = B.tList = 0.0;
-    B.itersRun = 0;
-    const int grid = s.numSMs * 8;
-    for (int iter = 0; iter < maxIter; ++iter)
+    B.loop.resize(1, s.st);
+    LoopState init{};
+    init.nActiveLeaves = L;
+    init.nActiveParticles = int(nAliveTotal);
+    init.iter = 0;
+    init.maxIter = maxIter;
+    init.nAll = L;
+    COSMO_CUDA(cudaMemcpyAsync(B.loop.get(), &init, sizeof(LoopState), cudaMemcpyHostToDevice, s.st));
+    // Size the list storage from the first iteration's lists (lists grow with h; a build
+    // that outgrows the storage reports it and the solve is repeated with twice as much).
+    hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.activeA.get(),
+                                                       &B.loop.get()->nActiveLeaves, B.hmaxLeaf.get());
+    COSMO_LAUNCHED();
+    walk_lists(B, false);
+    const uint32_t total0 = scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, true);
+    const uint32_t want = (total0 << (1 + attempt)) + 1024;
+    if (B.listCap < want) B.listCap = want;
+    B.jlist.resize(B.listCap, s.st);
+    s.scanTmp.resize(size_t(iceil(L, 4096)) + 1, s.st);
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    cudaEvent_t t1 = ev(s);
+
+    const bool useGraph = (flags & COSMO_BATCH_GRAPH) != 0;
+    B.graphUsed = useGraph;
+    if (useGraph)
     {
-        cudaEvent_t a = ev(s);
-        hmax_leaf_kernel_b<<<iceil(nActiveLeaves, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(),
-                                                                        B.activeA.get(), nActiveLeaves,
-                                                                        B.hmaxLeaf.get());
-        COSMO_LAUNCHED();
-        batch_lists(B);
-        cudaEvent_t b = ev(s);
-        COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 2 * sizeof(int), s.st));
-        COSMO_CUDA(cudaMemsetAsync(&ds->workCounter[0], 0, sizeof(int), s.st));
-        auto go = [&](auto kern) {
-            kern<<<grid, kThreads, 0, s.st>>>(B.activeA.get(), nActiveLeaves, B.leafSet.get(), B.leafRange.get(),
-                                              B.jOffset.get(), B.jcount.get(), B.jlist.get(), B.xyzh.get(),
-                                              B.rho.get(), B.gradh.get(), B.converged.get(), B.pmass.get(), tolh,
-                                              hfact, B.boxes.get(), B.activeB.get(), ds);
-        };
-        if (s.precision == 1) go(density_batch_kernel<true>);
-        else go(density_batch_kernel<false>);
-        COSMO_LAUNCHED();
-        cudaEvent_t c = ev(s);
-        read_scalars(s);
-        B.tList += elapsed_s(a, b);
-        B.tNR += elapsed_s(b, c);
-        B.activePerIter.push_back(nActiveParticles);
-        B.itersRun = iter + 1;
-        nActiveLeaves = s.hscal->nextActive;
-        nActiveParticles = s.hscal->unconverged;
-        std::swap(B.activeA, B.activeB);
-        if (nActiveParticles == 0) break;
+        cudaGraph_t graph = nullptr;
+        COSMO_CUDA(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle handle;
+        COSMO_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        COSMO_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        COSMO_CUDA(cudaStreamBeginCaptureToGraph(s.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        nr_iteration(B, tolh, hfact, handle, 1);
+        COSMO_CUDA(cudaStreamEndCapture(s.st, &body));
+        cudaGraphExec_t exec = nullptr;
+        COSMO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        COSMO_CUDA(cudaGraphLaunch(exec, s.st));
+        COSMO_CUDA(cudaStreamSynchronize(s.st));
+        COSMO_CUDA(cudaGraphExecDestroy(exec));
+        COSMO_CUDA(cudaGraphDestroy(graph));
     }
+    else
+    {
+        LoopState h{};
+        for (int iter = 0; iter < maxIter; ++iter)
+        {
+            nr_iteration(B, tolh, hfact, cudaGraphConditionalHandle(0), 0);
+            COSMO_CUDA(cudaMemcpyAsync(&h, B.loop.get(), 16, cudaMemcpyDeviceToHost, s.st));
+            COSMO_CUDA(cudaStreamSynchronize(s.st));
+            if (h.nActiveParticles == 0) break;
+            read_scalars(s);
+            if (s.hscal->err) break;
+        }
+    }
+    cudaEvent_t t2 = ev(s);
+    read_scalars(s);
+    if ((s.hscal->err & kErrListFull) && attempt < 6)
+    {
+        COSMO_CUDA(cudaMemsetAsync(&ds->err, 0, sizeof(int), s.st));
+        return batch_solve(B, tolh, hfact, maxIter, flags, attempt + 1);
+    }
+    LoopState fin{};
+    COSMO_CUDA(cudaMemcpy(&fin, B.loop.get(), sizeof(LoopState), cudaMemcpyDeviceToHost));
+    B.itersRun = fin.iter;
+    B.unconverged = fin.nActiveParticles;
+    B.activePerIter.assign(fin.activePerIter, fin.activePerIter + std::min(fin.iter, 128));
+    if (flags & COSMO_BATCH_FINAL_RHO) final_rho(B);
+    cudaEvent_t t3 = ev(s);
     check_dev_err(s, "cosmo_batch_density");
+    B.tBuild = elapsed_s(t0, t1);
+    B.tNR = elapsed_s(t1, t2);
+    B.tList = 0.0;
+    B.tTotal = elapsed_s(t0, t3);
     B.pairs = s.hscal->pairs[0];
-    B.unconverged = int(nActiveParticles);
-    return nActiveParticles > 0 ? 1 : 0;
+    return B.unconverged > 0 ? 1 : 0;
 }
 
 } // namespace cosmo
@@ -939,12 +1112,12 @@ void cosmo_batch_upload(const double* x, const double* y, const double* z, const
     COSMO_CUDA(cudaStreamSynchronize(s.st));
 }
 
-int cosmo_batch_density(double tolh, double hfact, int maxIter)
+int cosmo_batch_density(double tolh, double hfact, int maxIter, int flags)
 {
     Batch& B = batch();
     if (B.n < 1) return -1;
     B.core.precision = state().precision;
-    return batch_solve(B, tolh, hfact, maxIter > 0 ? maxIter : 100);
+    return batch_solve(B, tolh, hfact, maxIter > 0 ? maxIter : 100, flags);
 }
 
 void cosmo_batch_download(double* h, double* rho, double* gradh)
@@ -978,6 +1151,9 @@ double cosmo_batch_scalar(const char* name)
         return double(u);
     }
     if (k == "t_build") return B.tBuild;
+    if (k == "t_total") return B.tTotal;
+    if (k == "t_nr") return B.tNR;
+    if (k == "graph") return B.graphUsed ? 1.0 : 0.0;
     if (k == "t_nr") return B.tNR;
     if (k == "t_list") return B.tList;
     return NAN;

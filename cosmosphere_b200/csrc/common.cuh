@@ -253,6 +253,7 @@ enum DevErr : int
     kErrListCap   = 2,      // a j-list fill found more entries than its count pass
     kErrStageWait = 4,      // a TMA staging wait gave up
     kErrQueueWait = 8,      // a persistent-queue wait gave up
+    kErrListFull  = 16,     // a j-list build needed more than the preallocated capacity
 };
 
 } // namespace cosmo

@@ -114,3 +114,22 @@ def lattice100_workload(npartx: int = 100, seed: int = 42, vsigma=0.1, u=1.0, ga
     p["alpha"] = np.full(n, alpha)
     p["u"] = np.full(n, u)
     return p
+
+
+def ensemble_sets(nsets: int = 256, nmin: float = 1e4, nmax: float = 5e5, seed: int = 42):
+    """The batched-ensemble workload: nsets independent sets with sizes log-uniform in
+    [nmin, nmax] (seeded); even sets uniform random in the unit periodic box, odd sets
+    Plummer spheres (a = 1, r < 20); h = 1.2 x the local mean spacing x U[0.8, 1.2]
+    (the spacing from the mean density for the box, from the Plummer density profile
+    for the spheres); pmass = 1/N."""
+    rng = np.random.default_rng(seed)
+    sizes = np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsets))).astype(np.int64)
+    sets = []
+    for k, n in enumerate(sizes):
+        if k % 2 == 0:
+            p = uniform_box(int(n), hfac=1.2, hlo=0.8, hhi=1.2, seed=seed + 1000 + k)
+            p["box"] = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+        else:
+            p = plummer(int(n), rmax=20.0, hfact=1.2, lnsigma=0.0, ulo=0.8, uhi=1.2, seed=seed + 1000 + k)
+        sets.append(p)
+    return sets

@@ -107,8 +107,15 @@ void cosmo_batch_set_params(const double* pmass, const int* periodic, const doub
 void cosmo_batch_set_bucket(const int* bucket_per_set);
 /* Positions and initial h of all sets (host arrays, length offsets[nsets]). */
 void cosmo_batch_upload(const double* x, const double* y, const double* z, const double* h);
-/* Solve every set; 0 ok, 1 some particle unconverged within max_iter (<= 0: 100). */
-int cosmo_batch_density(double tolh, double hfact, int max_iter);
+/* Solve every set; 0 ok, 1 some particle unconverged within max_iter (<= 0: 100; at
+ * most 128).  flags: COSMO_BATCH_GRAPH runs the whole Newton loop as one CUDA graph
+ * whose body (hmax, lists, density, bookkeeping) repeats under a device-side while
+ * condition, with no host round trip per iteration; COSMO_BATCH_FINAL_RHO adds one
+ * gather pass that re-evaluates rho and d(rho)/dh at the converged h (without it they
+ * are the last iteration's, taken at the h before its update, as the reference's
+ * solve without gradients returns them). */
+enum { COSMO_BATCH_GRAPH = 1, COSMO_BATCH_FINAL_RHO = 2 };
+int cosmo_batch_density(double tolh, double hfact, int max_iter, int flags);
 /* Converged h, rho and d(rho)/dh of all sets, in the upload order. */
 void cosmo_batch_download(double* h, double* rho, double* gradh);
 /* Counters and timings (seconds) of the last batch solve; NaN if unknown. */

@@ -89,3 +89,41 @@ def test_bucket_size_does_not_change_plain_results(sets, singles, bucket):
     for k, (hs, d) in enumerate(singles):
         np.testing.assert_allclose(h[k], hs, rtol=1e-12, atol=0, err_msg=f"set {k}")
         np.testing.assert_allclose(rho[k], d[0], rtol=1e-12, atol=0, err_msg=f"set {k}")
+
+
+def test_graph_loop_equals_host_loop(sets):
+    """The Newton loop run as one CUDA graph (device-side while condition) gives the
+    same bits as the same loop driven from the host."""
+    capi.Cosmo().set_precision(False)
+    b = capi.Batch(sets)
+    b.upload()
+    assert b.density(graph=True) == 0
+    g = b.download()
+    assert b.scalar("graph") == 1.0
+    iters_g = b.scalar("itersRun")
+    assert b.density(graph=False) == 0
+    hst = b.download()
+    assert b.scalar("itersRun") == iters_g
+    for a, c in zip(g, hst):
+        for x, y in zip(a, c):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_final_rho_mixed_within_bound(sets):
+    """With rho re-evaluated at the converged h, the mixed form's rho is within 1e-5 of
+    the FP64 form's (without it, rho is one Newton step behind h, and a particle that
+    converges one iteration earlier in one form carries a rho one step apart)."""
+    res = {}
+    for mixed in (False, True):
+        capi.Cosmo().set_precision(mixed)
+        b = capi.Batch(sets)
+        b.upload()
+        assert b.density(final_rho=True) == 0
+        res[mixed] = b.download()
+    capi.Cosmo().set_precision(False)
+    for k in range(len(sets)):
+        h0, r0 = res[False][0][k], res[False][1][k]
+        h1, r1 = res[True][0][k], res[True][1][k]
+        live = h0 > 0
+        assert np.max(np.abs(h1[live] / h0[live] - 1)) <= 1e-5, k
+        assert np.max(np.abs(r1[live] / r0[live] - 1)) <= 1e-5, k
