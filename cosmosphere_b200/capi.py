@@ -25,6 +25,8 @@ EXPORTS = [
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
     "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_upload",
     "cosmo_batch_density", "cosmo_batch_download", "cosmo_batch_scalar",
+    "cosmo_serve_start", "cosmo_serve_submit", "cosmo_serve_continue", "cosmo_serve_wait",
+    "cosmo_serve_request_stat", "cosmo_serve_release", "cosmo_serve_stat", "cosmo_serve_stop",
 ]
 
 _DT = {0: np.float64, 1: np.int32, 2: np.uint32, 3: np.uint64, 4: np.int64}
@@ -73,6 +75,22 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_batch_download.argtypes = [P, P, P]
     L.cosmo_batch_scalar.argtypes = [ctypes.c_char_p]
     L.cosmo_batch_scalar.restype = D
+    LNG = ctypes.c_long
+    L.cosmo_serve_start.argtypes = [I, D]
+    L.cosmo_serve_start.restype = I
+    L.cosmo_serve_submit.argtypes = [I, D, I, P, D, D, P, P, P, P, D, D, I]
+    L.cosmo_serve_submit.restype = LNG
+    L.cosmo_serve_continue.argtypes = [LNG, D, P, I]
+    L.cosmo_serve_continue.restype = LNG
+    L.cosmo_serve_wait.argtypes = [LNG, P, P, P, P]
+    L.cosmo_serve_wait.restype = I
+    L.cosmo_serve_request_stat.argtypes = [LNG, ctypes.c_char_p]
+    L.cosmo_serve_request_stat.restype = D
+    L.cosmo_serve_release.argtypes = [LNG]
+    L.cosmo_serve_release.restype = I
+    L.cosmo_serve_stat.argtypes = [ctypes.c_char_p]
+    L.cosmo_serve_stat.restype = D
+    L.cosmo_serve_stop.restype = I
     return L
 
 
@@ -233,3 +251,59 @@ class Batch:
 
     def scalar(self, name: str) -> float:
         return float(self.L.cosmo_batch_scalar(name.encode()))
+
+
+class Server:
+    """The served form: continuous batching of density + force requests over worker
+    slots, with device-resident sets and an HBM budget."""
+
+    def __init__(self, slots: int = 4, budget_gb: float = 150.0, quintic: bool = False):
+        self.L = load(quintic)
+        if self.L.cosmo_serve_start(int(slots), float(budget_gb)) != 0:
+            raise RuntimeError("cosmo_serve_start failed (already running?)")
+        self.n = {}
+
+    def submit(self, p, thermo, *, box=None, tolh=1e-4, hfact=-1.0, beta=2.0, alphau=0.0, keep=True) -> int:
+        n = int(np.asarray(p["x"]).size)
+        pos = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]), dtype=np.float64)
+        h = np.ascontiguousarray(p["h"], dtype=np.float64)
+        vel = (np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]]), dtype=np.float64)
+               if "vx" in p else None)
+        th = np.ascontiguousarray(thermo, dtype=np.float64)
+        b = _c(box if box is not None else np.zeros(6))
+        rid = int(self.L.cosmo_serve_submit(n, float(p["pmass"]), 1 if box is not None else 0, b.ctypes.data,
+                                            float(tolh), float(hfact), pos.ctypes.data, h.ctypes.data,
+                                            vel.ctypes.data if vel is not None else None, th.ctypes.data,
+                                            float(beta), float(alphau), 1 if keep else 0))
+        if rid < 0:
+            raise RuntimeError("submit rejected")
+        self.n[rid] = n
+        return rid
+
+    def cont(self, set_id: int, dt: float, thermo=None, keep=True) -> int:
+        th = np.ascontiguousarray(thermo, dtype=np.float64) if thermo is not None else None
+        rid = int(self.L.cosmo_serve_continue(int(set_id), float(dt), th.ctypes.data if th is not None else None,
+                                              1 if keep else 0))
+        if rid < 0:
+            raise RuntimeError("continue rejected: set not resident")
+        self.n[rid] = self.n[set_id]
+        return rid
+
+    def wait(self, rid: int):
+        n = self.n[rid]
+        h, dens, grad, force = np.empty(n), np.empty((2, n)), np.empty((3, n)), np.empty((6, n))
+        st = int(self.L.cosmo_serve_wait(int(rid), h.ctypes.data, dens.ctypes.data, grad.ctypes.data,
+                                         force.ctypes.data))
+        return st, {"h": h, "dens": dens, "grad": grad, "force": force}
+
+    def stat(self, rid: int, name: str) -> float:
+        return float(self.L.cosmo_serve_request_stat(int(rid), name.encode()))
+
+    def server_stat(self, name: str) -> float:
+        return float(self.L.cosmo_serve_stat(name.encode()))
+
+    def release(self, set_id: int) -> int:
+        return int(self.L.cosmo_serve_release(int(set_id)))
+
+    def stop(self):
+        self.L.cosmo_serve_stop()

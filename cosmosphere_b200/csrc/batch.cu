@@ -938,7 +938,7 @@ static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int fla
     State& s = B.core;
     if (!(hfact > 0.0)) hfact = kHfactDefault;
     maxIter = std::max(1, std::min(maxIter, 128));
-    ev_reset();
+    ev_reset(s);
     DevScalars* ds = s.dscal.get();
     COSMO_CUDA(cudaMemsetAsync(B.rho.get(), 0, size_t(B.n) * 8, s.st));
     COSMO_CUDA(cudaMemsetAsync(B.gradh.get(), 0, size_t(B.n) * 8, s.st));

@@ -20,7 +20,8 @@
 
 namespace cosmo {
 
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
+std::atomic<long long> g_deviceBytes{0};
 
 // FP64 throughput probe: independent FMA chains per thread, no memory traffic.
 __global__ void fp64_peak_kernel(double* out, int iters, double a, double b)
@@ -71,6 +72,61 @@ void ensure_init(State& s)
     if (const char* e = std::getenv("COSMO_PRECISION")) s.precision = (std::string(e) == "mixed") ? 1 : 0;
 }
 
+size_t state_device_bytes(const State& s)
+{
+    size_t b = 0;
+    auto add = [&](const auto& buf) { b += buf.cap * sizeof(*buf.p); };
+    for (auto* d : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
+                    &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp})
+        add(*d);
+    for (auto* d : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) add(*d);
+    for (auto* d : {&s.prepAf, &s.prepBf, &s.thermof}) add(*d);
+    for (auto* d : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) add(*d);
+    for (auto* d : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
+                    &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
+                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp})
+        add(*d);
+    for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount, &s.jOffset,
+                    &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
+        add(*d);
+    add(s.box);
+    add(s.dscal);
+    return b;
+}
+
+void release_state(State& s)
+{
+    if (!s.st) return;
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    for (auto* b : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
+                    &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp})
+        b->release();
+    for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) b->release();
+    for (auto* b : {&s.prepAf, &s.prepBf, &s.thermof}) b->release();
+    for (auto* b : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) b->release();
+    for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
+                    &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
+                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp})
+        b->release();
+    for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount, &s.jOffset,
+                    &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
+        b->release();
+    s.box.release();
+    s.dscal.release();
+    for (auto& e : s.evPool) COSMO_CUDA(cudaEventDestroy(e));
+    s.evPool.clear();
+    if (s.hscal) COSMO_CUDA(cudaFreeHost(s.hscal));
+    if (s.hsmall) COSMO_CUDA(cudaFreeHost(s.hsmall));
+    s.hscal = nullptr;
+    s.hsmall = nullptr;
+    COSMO_CUDA(cudaStreamDestroy(s.st));
+    s.st = nullptr;
+    s.sizedFor = 0;
+    s.orderFor = 0;
+}
+
 // src/gpu_state.cu:21-46: every particle-length array, sized once per count.
 void size_particle_arrays(State& s, int n)
 {
@@ -104,27 +160,25 @@ void check_dev_err(State& s, const char* where)
               (e & kErrQueueWait) ? "queue wait timeout" : "");
 }
 
-namespace {
+// Each state records its phase timings with its own pool of events (the served form runs
+// several states from several host threads); elapsed times are read right after the
+// synchronisations that follow them, so a ring of 1024 is never overrun.
 constexpr int kEvPool = 1024;
-cudaEvent_t gEv[kEvPool];
-int gEvNext = 0;
-bool gEvInit = false;
-}
 
 cudaEvent_t ev(State& s)
 {
-    if (!gEvInit)
+    if (s.evPool.empty())
     {
-        for (auto& e : gEv) COSMO_CUDA(cudaEventCreate(&e));
-        gEvInit = true;
+        s.evPool.resize(kEvPool);
+        for (auto& e : s.evPool) COSMO_CUDA(cudaEventCreate(&e));
     }
-    cudaEvent_t e = gEv[gEvNext];
-    gEvNext = (gEvNext + 1) % kEvPool;
+    cudaEvent_t e = s.evPool[s.evNext];
+    s.evNext = (s.evNext + 1) % kEvPool;
     COSMO_CUDA(cudaEventRecord(e, s.st));
     return e;
 }
 
-void ev_reset() { gEvNext = 0; }
+void ev_reset(State& s) { s.evNext = 0; }
 
 double elapsed_s(cudaEvent_t a, cudaEvent_t b)
 {
@@ -460,7 +514,7 @@ double cosmo_x_mark_elapsed(int a, int b)
     return ms * 1e-3;
 }
 
-unsigned long long cosmo_x_launches(void) { return g_launches; }
+unsigned long long cosmo_x_launches(void) { return g_launches.load(); }
 
 // Measured FP64 FMA throughput of this GPU in TFLOP/s (2 flops per FMA).
 double cosmo_x_fp64_peak(void)

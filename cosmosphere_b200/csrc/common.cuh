@@ -8,6 +8,7 @@
  */
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -30,7 +31,7 @@ namespace cosmo {
 
 // Every launch site calls this right after <<<...>>>: it checks the launch and counts it
 // (the count is reported by the harness as the number of the library's kernel launches).
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 #define COSMO_LAUNCHED()                                                                   \
     do {                                                                                   \
         ++::cosmo::g_launches;                                                             \

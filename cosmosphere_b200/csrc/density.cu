@@ -375,7 +375,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     if (periodicBox) std::copy(periodicBox, periodicBox + 6, s.boxHost);
     s.activePerIter.clear();
     s.t = Timings{};
-    ev_reset();
+    ev_reset(s);
     DevScalars* ds = s.dscal.get();
     COSMO_CUDA(cudaMemsetAsync(s.rho.get(), 0, size_t(n) * 8, s.st));
     COSMO_CUDA(cudaMemsetAsync(s.gradh.get(), 0, size_t(n) * 8, s.st));

@@ -25,12 +25,27 @@
 
 namespace cosmo {
 
+// Device bytes currently held by every state of the library (admission control of the
+// served form charges requests against it).
+extern std::atomic<long long> g_deviceBytes;
+
 template<class T>
 struct DBuf
 {
     T*     p   = nullptr;
     size_t n   = 0;
     size_t cap = 0;
+
+    void release()
+    {
+        if (p)
+        {
+            COSMO_CUDA(cudaFree(p));
+            g_deviceBytes -= (long long)(cap * sizeof(T));
+        }
+        p = nullptr;
+        n = cap = 0;
+    }
 
     // Grow to hold c elements.  Contents are kept only when keep is set; new memory is
     // zeroed, as the reference's thrust::device_vector value-initialises.
@@ -41,12 +56,14 @@ struct DBuf
             T* q = nullptr;
             const size_t newCap = c + c / 8 + 16;
             COSMO_CUDA(cudaMalloc(&q, newCap * sizeof(T)));
+            g_deviceBytes += (long long)(newCap * sizeof(T));
             COSMO_CUDA(cudaMemsetAsync(q, 0, newCap * sizeof(T), st));
             if (keep && p && n) COSMO_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
             if (p)
             {
                 COSMO_CUDA(cudaStreamSynchronize(st));
                 COSMO_CUDA(cudaFree(p));
+                g_deviceBytes -= (long long)(cap * sizeof(T));
             }
             p = q;
             cap = newCap;
@@ -127,10 +144,14 @@ struct State
     DBuf<DevScalars> dscal;
     DevScalars* hscal = nullptr;                // pinned host mirror
     int* hsmall = nullptr;                      // pinned scratch for small reads (64 ints)
+    std::vector<cudaEvent_t> evPool;            // timing events of this state's stream
+    int evNext = 0;
 };
 
 State& state();
 void ensure_init(State& s);
+void release_state(State& s);        // free every device and pinned buffer and the stream
+size_t state_device_bytes(const State& s);
 void size_particle_arrays(State& s, int n);
 
 // tree.cu
@@ -162,7 +183,7 @@ struct EventPair
 };
 double elapsed_s(cudaEvent_t a, cudaEvent_t b);
 cudaEvent_t ev(State& s);            // record an event on the state's stream (pooled)
-void ev_reset();
+void ev_reset(State& s);
 
 void read_scalars(State& s);         // dscal -> hscal, synchronising the stream
 void check_dev_err(State& s, const char* where);

@@ -121,6 +121,42 @@ void cosmo_batch_download(double* h, double* rho, double* gradh);
 /* Counters and timings (seconds) of the last batch solve; NaN if unknown. */
 double cosmo_batch_scalar(const char* name);
 
+/* ---- served form: a request loop with continuous batching (no counterpart in the
+ * reference) ----
+ * cosmo_serve_start launches `slots` worker threads on the current device with the
+ * current precision; each runs one request at a time on its particle set's own CUDA
+ * stream, so requests overlap on the GPU.  A queued request starts as soon as a slot is
+ * free and, for a new set, the library's device memory plus admitted estimates fit
+ * hbm_budget_gb (idle resident sets are evicted least-recently-used first; a request
+ * larger than the whole budget is rejected).  Returns 0, or -1 if already running. */
+int cosmo_serve_start(int slots, double hbm_budget_gb);
+/* Submit a new set: density solve with gradients, then force.  pos3 (3n), h (n), vel3
+ * (3n, may be NULL), thermo4 (4n: p/rho^2, c_s, alpha, u) are copied at submission,
+ * component-major, caller order.  keep_resident keeps the set on the device for
+ * cosmo_serve_continue.  Returns the request id (also the set id), or -1. */
+long cosmo_serve_submit(int n, double pmass, int periodic, const double* box6, double tolh, double hfact,
+                        const double* pos3, const double* h, const double* vel3, const double* thermo4, double beta,
+                        double alphau, int keep_resident);
+/* Continue a resident set one step: positions advance on the device by v*dt, the
+ * Newton iteration starts from the previous converged h; thermo4 may be NULL (keep).
+ * Returns the request id, or -1 if the set is not resident. */
+long cosmo_serve_continue(long set_id, double dt, const double* thermo4, int keep_resident);
+/* Block until a request finishes and copy its results (caller order) into the given,
+ * non-NULL outputs: h (n), dens (rho, gradh: 2n), grad (div v, xi, d(div v)/dt: 3n),
+ * force (fx, fy, fz, du/dt, vsigmax, div v: 6n).  Returns 1 done, -1 rejected or
+ * unknown, -2 unconverged. */
+int cosmo_serve_wait(long request_id, double* h, double* dens, double* grad, double* force);
+/* Per-request figures in seconds or counts: latency, queue, service, submit, start,
+ * done, updates, iters, slot, n, status. */
+double cosmo_serve_request_stat(long request_id, const char* name);
+/* Drop an idle resident set (0), or -1 if unknown or busy. */
+int cosmo_serve_release(long set_id);
+/* Server figures: device_bytes, budget, resident_sets, max_inflight, completed,
+ * rejected, evicted, queued, slots. */
+double cosmo_serve_stat(const char* name);
+/* Stop the workers (after the running requests) and release every resident set. */
+int cosmo_serve_stop(void);
+
 /* Hilbert keys and the stable sort order of n particles, computed without allocating
  * any device memory.  No counterpart in the reference: it exists for callers that cannot
  * call cudaMalloc at this point -- a caller that fixes its device-memory budget at start
