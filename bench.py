@@ -252,6 +252,160 @@ def run_ensemble(args):
     print(json.dumps(line), flush=True)
 
 
+def _served_fp64_loop(reqs):
+    """The plain FP64 one-request-at-a-time loop through the C-ABI: per request upload,
+    density, thermo, force and download of every output; a continuation drifts its set's
+    positions on the host by v dt (wrapped in a periodic box) and restarts Newton from the
+    set's last h.  Returns per-request service seconds, updates and (h, rho)."""
+    from cosmosphere_b200 import capi
+    c = capi.Cosmo()
+    c.set_precision(False)
+    last = {}
+    serv, upd, res = [], [], []
+    for k, e in enumerate(reqs):
+        j = k if e["kind"] == "new" else e["of"]
+        f = reqs[j]
+        p, n = f["p"], f["n"]
+        if e["kind"] == "new":
+            pos, h = f["pos3"], np.ascontiguousarray(p["h"])
+        else:
+            pos, h = last[j]
+            pos = pos + f["vel3"] * e["dt"]
+            if p.get("box") is not None:
+                pos = np.where(pos >= 1.0, pos - 1.0, np.where(pos < 0.0, pos + 1.0, pos))
+        box = p.get("box")
+        outs = {capi.HSML: np.empty((1, n)), capi.DENS_OUT: np.empty((2, n)), capi.GRAD_OUT: np.empty((3, n)),
+                capi.FORCE_OUT: np.empty((6, n))}
+        t0 = time.perf_counter()
+        c.arrays_init(n)
+        c.upload(capi.POS, pos, n)
+        c.upload(capi.HSML, h, n)
+        c.upload(capi.VEL, f["vel3"], n)
+        c.upload(capi.ACCEL, np.zeros((3, n)), n)
+        c.density(n, p["pmass"], tolh=1e-4, hfact=1.2, periodic_box=box)
+        c.upload(capi.THERMO, f["thermo4"], n, sorted_=True)
+        c.force(n, p["pmass"], beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
+        for slot, buf in outs.items():
+            c.download(slot, n, buf)
+        serv.append(time.perf_counter() - t0)
+        upd.append(float(c.array("activePerIter").sum() + c.scalar("nAlive")))
+        last[j] = (pos, outs[capi.HSML][0].copy())
+        res.append((outs[capi.HSML][0], outs[capi.DENS_OUT][0]))
+    return serv, upd, res
+
+
+def _served_run(reqs, arrivals, slots, budget_gb):
+    """Submit the requests to the served form at their arrival times (seconds after the
+    start); returns per-request latency, updates, (h, rho) and the makespan."""
+    from cosmosphere_b200 import capi
+    srv = capi.Server(slots=slots, budget_gb=budget_gb)
+    rid = []
+    try:
+        t0 = time.perf_counter()
+        for k, e in enumerate(reqs):
+            dly = t0 + arrivals[k] - time.perf_counter()
+            if dly > 0:
+                time.sleep(dly)
+            if e["kind"] == "new":
+                p = e["p"]
+                rid.append(srv.submit({"x": p["x"], "y": p["y"], "z": p["z"], "h": p["h"], "pmass": p["pmass"],
+                                       "vx": p["vx"], "vy": p["vy"], "vz": p["vz"]}, e["thermo4"],
+                                      box=p.get("box"), hfact=1.2, keep=True))
+            else:
+                rid.append(srv.cont(rid[e["of"]], e["dt"]))
+        res, lat, upd, subm, done = [], [], [], [], []
+        for r in rid:
+            st, o = srv.wait(r)
+            if st != 1:
+                raise RuntimeError(f"served request {r} ended with status {st}")
+            res.append((o["h"], o["dens"][0]))
+            lat.append(srv.stat(r, "latency"))
+            upd.append(srv.stat(r, "updates"))
+            subm.append(srv.stat(r, "submit"))
+            done.append(srv.stat(r, "done"))
+        info = {"max_inflight": srv.server_stat("max_inflight"), "evicted": srv.server_stat("evicted"),
+                "rejected": srv.server_stat("rejected"), "resident_sets_at_end": srv.server_stat("resident_sets"),
+                "device_bytes_at_end": srv.server_stat("device_bytes")}
+        makespan = max(done) - min(subm)
+    finally:
+        srv.stop()
+    return lat, upd, res, makespan, info
+
+
+def run_served(args):
+    """The served stream: requests with particle counts log-uniform in [5e3, 2e6] from the
+    lattice / periodic-uniform / Plummer generators, 30% continuing a device-resident set
+    (drift by v dt, dt = 0.1 min(h/c_s), Newton warm-started from the last h), admitted
+    against an HBM budget, mixed precision; against the plain FP64 one-request-at-a-time
+    loop through the C-ABI."""
+    from cosmosphere_b200 import capi, inputs
+    tg = time.perf_counter()
+    reqs = inputs.served_requests(args.nreq, seed=42)
+    tg = time.perf_counter() - tg
+    c = capi.Cosmo()
+    # warm-up: the CUDA context and the FP64 loop's buffers at the largest size
+    big = max((e for e in reqs if e["kind"] == "new"), key=lambda e: e["n"])
+    _served_fp64_loop([big])
+    serv, upd64, res64 = _served_fp64_loop(reqs)
+    total_upd = float(np.sum(upd64))
+    cap64 = total_upd / float(np.sum(serv))
+    # Poisson arrivals at `load` x the FP64 loop's request rate
+    rate = args.serve_load * len(reqs) / float(np.sum(serv))
+    rng = np.random.default_rng(7)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    arrivals -= arrivals[0]
+    # the FP64 loop's latencies under the same arrivals (one request at a time, FIFO)
+    lat64, free = [], 0.0
+    for a, s_ in zip(arrivals, serv):
+        start = max(a, free)
+        free = start + s_
+        lat64.append(free - a)
+    make64 = free - arrivals[0]
+    c.set_precision(True)
+    _served_run([big], [0.0], args.slots, args.budget_gb)       # warm-up of the slots' states
+    lat, upd, res, makespan, info = _served_run(reqs, arrivals, args.slots, args.budget_gb)
+    # saturated: every request at t = 0
+    lat_b, upd_b, _, make_b, info_b = _served_run(reqs, np.zeros(len(reqs)), args.slots, args.budget_gb)
+    c.set_precision(False)
+    eh = max(float(np.max(np.abs(a[0] / b[0] - 1.0))) for a, b in zip(res, res64))
+    er = max(float(np.max(np.abs(a[1] / b[1] - 1.0))) for a, b in zip(res, res64))
+    nnew = sum(1 for e in reqs if e["kind"] == "new")
+    bytes_in = sum(8 * e["n"] * 11 for e in reqs if e["kind"] == "new")
+    bytes_out = sum(8 * 12 * reqs[k if e["kind"] == "new" else e["of"]]["n"] for k, e in enumerate(reqs))
+    pct = lambda a, q: float(np.percentile(np.asarray(a) * 1e3, q))
+    thr_stream = float(np.sum(upd)) / makespan
+    thr_sat = float(np.sum(upd_b)) / make_b
+    line = {"metric": "served density+force particle-updates/s (Poisson stream, 5e3..2e6 particles)",
+            "value": thr_sat, "unit": UNIT, "n_gpus": 1, "steps": len(reqs), "warmup": 1,
+            "ms_per_step": 1e3 * make_b / len(reqs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{len(reqs)} requests ({nnew} new sets, {len(reqs) - nnew} continuations), "
+                                   "counts log-uniform 5e3..2e6 from lattice+jiggle / periodic uniform box / "
+                                   "Plummer (cubic), density(NR+gradients)+force, dt = 0.1 min(h/c_s)",
+                       "particles_new": int(sum(e["n"] for e in reqs if e["kind"] == "new")),
+                       "slots": args.slots, "hbm_budget_gb": args.budget_gb,
+                       "offered_load": f"Poisson at {args.serve_load} x the FP64 loop's request rate "
+                                       f"({rate:.1f} req/s)",
+                       "input_generation_s": tg},
+            "e2e": {"value": thr_sat, "unit": UNIT, "h2d_bytes_per_step": bytes_in / len(reqs),
+                    "d2h_bytes_per_step": bytes_out / len(reqs),
+                    "how": "every request through the served C-ABI from host buffers: copy at submission, "
+                           "H2D, solve, D2H of all outputs"},
+            "served_mixed": {"stream": {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "max_ms": pct(lat, 100),
+                                        "throughput": thr_stream, "makespan_s": makespan, **info},
+                             "saturated": {"throughput": thr_sat, "makespan_s": make_b, "p50_ms": pct(lat_b, 50),
+                                           "p99_ms": pct(lat_b, 99), **info_b}},
+            "fp64_loop": {"stream": {"p50_ms": pct(lat64, 50), "p99_ms": pct(lat64, 99), "max_ms": pct(lat64, 100),
+                                     "throughput": total_upd / make64, "makespan_s": make64},
+                          "capacity": cap64, "service_p50_ms": pct(serv, 50), "service_p99_ms": pct(serv, 99),
+                          "how": "plain FP64, one request at a time through the C-ABI, wall-timed per request; "
+                                 "stream latencies from the same arrivals, FIFO"},
+            "speedup_saturated_vs_fp64_loop": thr_sat / cap64,
+            "accuracy_mixed_vs_fp64": {"h_max_rel": eh, "rho_max_rel": er},
+            "roofline": None, "cpu_baseline": None, "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world, local, dist):
     """The CPU arm: the oracle port of the path, all host threads, a bounded sample."""
     if rank != 0:
@@ -291,7 +445,12 @@ def main():
     ap.add_argument("--ref-npartx", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "ensemble"])
+    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "ensemble", "served"])
+    ap.add_argument("--nreq", type=int, default=64, help="served: requests in the stream")
+    ap.add_argument("--slots", type=int, default=4, help="served: worker slots")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="served: HBM budget")
+    ap.add_argument("--serve-load", type=float, default=0.9,
+                    help="served: Poisson rate as a multiple of the FP64 loop's request rate")
     ap.add_argument("--nsets", type=int, default=256)
     ap.add_argument("--profile", action="store_true",
                     help="for ncu: set up, run --warmup and --steps device-resident steps, print nothing else")
@@ -304,6 +463,9 @@ def main():
         return
     if args.workload == "ensemble":
         run_ensemble(args)
+        return
+    if args.workload == "served":
+        run_served(args)
         return
 
     from cosmosphere_b200 import capi

@@ -950,7 +950,8 @@ static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int fla
     long long nAliveTotal = 0;
     {
         std::vector<int> na(B.nsets);
-        COSMO_CUDA(cudaMemcpy(na.data(), B.nAliveSet.get(), size_t(B.nsets) * 4, cudaMemcpyDeviceToHost));
+        COSMO_CUDA(cudaMemcpyAsync(na.data(), B.nAliveSet.get(), size_t(B.nsets) * 4, cudaMemcpyDeviceToHost, s.st));
+        COSMO_CUDA(cudaStreamSynchronize(s.st));
         for (int v : na) nAliveTotal += v;
     }
     B.loop.resize(1, s.st);
@@ -1022,7 +1023,8 @@ static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int fla
         return batch_solve(B, tolh, hfact, maxIter, flags, attempt + 1);
     }
     LoopState fin{};
-    COSMO_CUDA(cudaMemcpy(&fin, B.loop.get(), sizeof(LoopState), cudaMemcpyDeviceToHost));
+    COSMO_CUDA(cudaMemcpyAsync(&fin, B.loop.get(), sizeof(LoopState), cudaMemcpyDeviceToHost, s.st));
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
     B.itersRun = fin.iter;
     B.unconverged = fin.nActiveParticles;
     B.activePerIter.assign(fin.activePerIter, fin.activePerIter + std::min(fin.iter, 128));

@@ -12,7 +12,9 @@
 #include <chrono>
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "state.hpp"
 #include "../../include/cosmosphere.h"
@@ -22,6 +24,37 @@ namespace cosmo {
 
 std::atomic<unsigned long long> g_launches{0};
 std::atomic<long long> g_deviceBytes{0};
+
+cudaMemPool_t device_pool()
+{
+    static std::mutex m;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    COSMO_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fatal("device_pool: device ordinal out of range");
+    std::lock_guard<std::mutex> lk(m);
+    if (!pools[dev])
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        COSMO_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        uint64_t keep = UINT64_MAX;   // freed blocks stay cached for the next state
+        COSMO_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pools[dev];
+}
+
+namespace {
+
+// Page-locked scalar blocks of released states, reused by new ones: freeing page-locked
+// memory waits for the whole device, which would stall every other state's work.
+std::mutex g_pinnedMutex;
+std::vector<std::pair<DevScalars*, int*>> g_pinnedFree;
+
+}
 
 // FP64 throughput probe: independent FMA chains per thread, no memory traffic.
 __global__ void fp64_peak_kernel(double* out, int iters, double a, double b)
@@ -64,8 +97,20 @@ void ensure_init(State& s)
     COSMO_CUDA(cudaDeviceGetAttribute(&s.numSMs, cudaDevAttrMultiProcessorCount, s.device));
     COSMO_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
     s.dscal.resize(1, s.st);
-    COSMO_CUDA(cudaMallocHost(&s.hscal, sizeof(DevScalars)));
-    COSMO_CUDA(cudaMallocHost(&s.hsmall, 64 * sizeof(int)));
+    {
+        std::lock_guard<std::mutex> lk(g_pinnedMutex);
+        if (!g_pinnedFree.empty())
+        {
+            s.hscal = g_pinnedFree.back().first;
+            s.hsmall = g_pinnedFree.back().second;
+            g_pinnedFree.pop_back();
+        }
+    }
+    if (!s.hscal)
+    {
+        COSMO_CUDA(cudaMallocHost(&s.hscal, sizeof(DevScalars)));
+        COSMO_CUDA(cudaMallocHost(&s.hsmall, 64 * sizeof(int)));
+    }
     std::memset(s.hscal, 0, sizeof(DevScalars));
     s.box.resize(1, s.st);
     if (const char* e = std::getenv("COSMO_MAX_ITER")) s.maxIter = std::max(1, std::atoi(e));
@@ -85,10 +130,11 @@ size_t state_device_bytes(const State& s)
     for (auto* d : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) add(*d);
     for (auto* d : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
-                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp})
+                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext})
         add(*d);
-    for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount, &s.jOffset,
-                    &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
+    add(s.items);
+    for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
+                    &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
         add(*d);
     add(s.box);
     add(s.dscal);
@@ -102,23 +148,27 @@ void release_state(State& s)
     for (auto* b : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
                     &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp})
-        b->release();
-    for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) b->release();
-    for (auto* b : {&s.prepAf, &s.prepBf, &s.thermof}) b->release();
-    for (auto* b : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) b->release();
+        b->release(s.st);
+    for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) b->release(s.st);
+    for (auto* b : {&s.prepAf, &s.prepBf, &s.thermof}) b->release(s.st);
+    for (auto* b : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) b->release(s.st);
     for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
-                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp})
-        b->release();
-    for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount, &s.jOffset,
-                    &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
-        b->release();
-    s.box.release();
-    s.dscal.release();
+                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext})
+        b->release(s.st);
+    s.items.release(s.st);
+    for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
+                    &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
+        b->release(s.st);
+    s.box.release(s.st);
+    s.dscal.release(s.st);
     for (auto& e : s.evPool) COSMO_CUDA(cudaEventDestroy(e));
     s.evPool.clear();
-    if (s.hscal) COSMO_CUDA(cudaFreeHost(s.hscal));
-    if (s.hsmall) COSMO_CUDA(cudaFreeHost(s.hsmall));
+    if (s.hscal)
+    {
+        std::lock_guard<std::mutex> lk(g_pinnedMutex);
+        g_pinnedFree.emplace_back(s.hscal, s.hsmall);
+    }
     s.hscal = nullptr;
     s.hsmall = nullptr;
     COSMO_CUDA(cudaStreamDestroy(s.st));

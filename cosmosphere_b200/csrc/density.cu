@@ -20,127 +20,219 @@ namespace {
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
-template<bool Periodic>
-__global__ void __launch_bounds__(kThreads)
-density_nr_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint32_t* __restrict__ layout,
-                  const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
-                  const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
-                  double* __restrict__ gradh, int* __restrict__ converged, double pmass, double tolh,
-                  double hfact, const DevBox* __restrict__ box, int* __restrict__ nextLeaves,
-                  DevScalars* __restrict__ ds)
-{
-    __shared__ double4 sRing[kWarpsPerBlock][kRing];
-    __shared__ float4 sRingF[kWarpsPerBlock][kRing];
-    __shared__ int sIdx[kWarpsPerBlock][kRing];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nWarps = (gridDim.x * blockDim.x) >> 5;
-    double lx = 0, ly = 0, lz = 0;
-    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
-    unsigned long long pairs = 0, cand = 0;
+constexpr int kRec = 256;                       // pair records per warp
 
-    for (int w = warpGlobal; w < nLeavesActive; w += nWarps)
+// Zero the per-iteration counters of the Newton work queue and the leaf re-queue flags.
+__global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restrict__ leafNext, int nL)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0)
+    {
+        ds->nextActive = 0;
+        ds->unconverged = 0;
+        ds->workCounter[0] = 0;
+        ds->itemsHeavy = 0;
+        ds->itemsLight = 0;
+    }
+    for (int l = t; l < nL; l += gridDim.x * blockDim.x) leafNext[l] = 0;
+}
+
+// Work items of one Newton iteration: every group of a leaf's 64-slot window of
+// unconverged particles is one item (leaf, window << 16 | group << 8 | groups, the two
+// halves of the window's active mask).  Groups hold up to 32 particles; a leaf whose
+// gather list streams more than kSplitStream particles is cut into smaller groups, about
+// kSplitWork / stream particles each, so that no single warp carries the iteration's
+// tail.  Cut items are queued from the front of the buffer and run first, whole groups
+// from the back.  The items of a window hold at most its active particles, so cap = the
+// particle count always suffices.
+constexpr uint32_t kSplitStream = 4096;
+constexpr uint32_t kSplitWork = 32u * 4096u;
+
+__global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
+                                  const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
+                                  int4* __restrict__ items, int cap, DevScalars* __restrict__ ds)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nWarps = (gridDim.x * blockDim.x) >> 5;
+    for (int w = warp; w < nActive; w += nWarps)
     {
         const int leaf = leaves[w];
         const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
-        const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
-        bool leafActive = false;
+        const uint32_t S = jstream[leaf];
+        const int gsize = S <= kSplitStream ? 32 : max(1, int(kSplitWork / S));
         for (uint32_t g = p0; g < p1; g += 64)
         {
             const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            const bool act0 = a0 < p1 && converged[a0] == 0;
-            const bool act1 = a1 < p1 && converged[a1] == 0;
-            const uint32_t m0 = __ballot_sync(0xffffffffu, act0);
-            const uint32_t m1 = __ballot_sync(0xffffffffu, act1);
+            const uint32_t m0 = __ballot_sync(0xffffffffu, a0 < p1 && converged[a0] == 0);
+            const uint32_t m1 = __ballot_sync(0xffffffffu, a1 < p1 && converged[a1] == 0);
             const int nAct = __popc(m0) + __popc(m1);
             if (nAct == 0) continue;
-            const int G = (nAct + 31) >> 5;
-            for (int grp = 0; grp < G; ++grp)
+            const int whole = (nAct + 31) >> 5;
+            const int G = max(whole, (nAct + gsize - 1) / gsize);
+            const bool split = G > whole;
+            int base = 0;
+            if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            const int wnd = int((g - p0) >> 6);
+            for (int k = lane; k < G; k += 32)
             {
-                const int slot = group_slot(m0, m1, nAct, grp, G, lane);
-                const bool mine = slot >= 0;
-                const uint32_t i = g + uint32_t(mine ? slot : 0);
-                const double4 pi = xyzh[i];
-                const double hi = pi.w;
-                const double hinv2 = 1.0 / (hi * hi);
-                const double rs = kRadKernel * hi;
-                const double rmax = warp_max(mine ? rs : 0.0);
-                const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-                double rhoi = 0.0, gradhi = 0.0;
-                unsigned int gp = 0, gc = 0;
-                // float copy of the group relative to the box centre, and the lane's
-                // conservative float threshold (R h + margin)^2, rounded up
-                const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
-                const double rm = rs + fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0);
-                const float tf = __double2float_ru(rm * rm * (1.0 + 1e-6));
-                const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
-                stream_pairs(
-                    sRing[wib], sRingF[wib], sIdx[wib], bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
-                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                    [&](const double4* ring, const float4* ringf, const int* ringIdx, int head, int count) {
-                        gc += count;
-                        two_pass(ring, ringf, ringIdx, head, count, mine,
-                                 [&](const float4& pf) { return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= tf; },
-                                 [&](const double4& pj, const float4&, int) {
-                                     double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                                     const double q2 = pair_r2(dx, dy, dz) * hinv2;
-                                     if (!(q2 < kRadK2)) return;
-                                     const double q = sqrt(q2);
-                                     double wk, dwk;
-                                     sph_kernel(q2, q, wk, dwk);
-                                     rhoi += wk;
-                                     gradhi += -q * dwk - 3.0 * wk;
-                                     ++gp;
-                                 });
-                    });
-                bool stillActive = false;
-                if (mine)
-                {
-                    pairs += gp;
-                    cand += gc;
-                    // Newton-Raphson step, src/density_base.cu:294-333
-                    const double hi1 = 1.0 / hi;
-                    const double hi31 = hi1 * hi1 * hi1;
-                    const double hi41 = hi31 * hi1;
-                    const double rho_i = rhoi * kCnormk * pmass * hi31;
-                    const double grad_i = gradhi * kCnormk * pmass * hi41;
-                    if (!(rho_i > 0.0))
-                    {
-                        rho[i] = 0.0;
-                        gradh[i] = 0.0;
-                        converged[i] = 0;
-                        stillActive = true;
-                    }
-                    else
-                    {
-                        const double rhoh_i = pmass * (hfact * hi1) * (hfact * hi1) * (hfact * hi1);
-                        const double funci = rhoh_i - rho_i;
-                        const double dhdrhoi = -hi / (3.0 * rhoh_i);
-                        const double omegai = 1.0 - dhdrhoi * grad_i;
-                        const double safe = (omegai > 0.0) ? omegai : fabs(omegai + 1e-300);
-                        const double hraw = hi - funci * dhdrhoi / safe;
-                        double hnew;
-                        if (hraw > 1.2 * hi) hnew = 1.2 * hi;
-                        else if (hraw < 0.8 * hi) hnew = 0.8 * hi;
-                        else hnew = hraw;
-                        rho[i] = rho_i;
-                        gradh[i] = grad_i;
-                        reinterpret_cast<double*>(xyzh + i)[3] = hnew;
-                        const int conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
-                        converged[i] = conv;
-                        stillActive = !conv;
-                    }
-                }
-                const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
-                if (still)
-                {
-                    leafActive = true;
-                    if (lane == 0) atomicAdd(&ds->unconverged, __popc(still));
-                }
+                const int idx = split ? base + k : cap - 1 - (base + k);
+                if (idx >= 0 && idx < cap) items[idx] = make_int4(leaf, (wnd << 16) | (k << 8) | G, int(m0), int(m1));
             }
         }
-        if (leafActive && lane == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
+    }
+}
+
+// One Newton iteration over the work items, taken dynamically (a persistent grid).
+//
+// A warp owns one group of a leaf.  Candidates stream through the group filter into the
+// ring (stream_pairs); every batch of up to 32 is then tested with j on the lanes: for each
+// group particle in turn, all lanes apply the exact FP64 test q^2 = r^2/h_i^2 < R^2 to their
+// candidate, and the accepted pairs are appended, particle-major, to the warp's record
+// buffer -- so each particle's records are contiguous and in ascending j.  The records are
+// then evaluated with one pair per lane (W, -q dW/dq - 3W), and each particle's owner lane
+// adds its own records in order.  Every lane works in all three phases whatever the
+// group's size or spatial spread, and each particle's sums still run over j in ascending
+// Hilbert index, the oracle's order, so the results agree with it bit for bit.
+template<bool Periodic>
+__global__ void __launch_bounds__(kThreads)
+density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
+                  const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
+                  const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
+                  double* __restrict__ gradh, int* __restrict__ converged, double pmass, double tolh,
+                  double hfact, const DevBox* __restrict__ box, int* __restrict__ leafNext,
+                  int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
+{
+    __shared__ double4 sRing[kWarpsPerBlock][kRing];
+    __shared__ double4 sGrp[kWarpsPerBlock][32];
+    __shared__ double sRecA[kWarpsPerBlock][kRec];
+    __shared__ double sRecB[kWarpsPerBlock][kRec];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
+    unsigned long long pairs = 0, cand = 0;
+    double* recA = sRecA[wib];
+    double* recB = sRecB[wib];
+
+    for (;;)
+    {
+        int w = 0;
+        if (lane == 0) w = atomicAdd(&ds->workCounter[0], 1);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= nItems) break;
+        const int4 it = items[w < nHeavy ? w : cap - 1 - (w - nHeavy)];
+        const int leaf = it.x;
+        const int wnd = it.y >> 16, grp = (it.y >> 8) & 255, G = it.y & 255;
+        const uint32_t m0 = uint32_t(it.z), m1 = uint32_t(it.w);
+        const int nAct = __popc(m0) + __popc(m1);
+        const int ng = (grp + 1) * nAct / G - grp * nAct / G;
+        const uint32_t g0 = layout[leaf] + 64u * uint32_t(wnd);
+        const int slot = group_slot(m0, m1, nAct, grp, G, lane);
+        const bool mine = slot >= 0;
+        const uint32_t i = g0 + uint32_t(mine ? slot : 0);
+        const double4 pi = xyzh[i];
+        const double hi = pi.w;
+        const double hinv2 = 1.0 / (hi * hi);
+        const double rs = kRadKernel * hi;
+        const double rmax = warp_max(mine ? rs : 0.0);
+        const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
+        if (mine) sGrp[wib][lane] = make_double4(pi.x, pi.y, pi.z, hinv2);
+        __syncwarp();
+        double rhoi = 0.0, gradhi = 0.0;
+        unsigned int gp = 0, gc = 0;
+        const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
+        stream_pairs<false, false>(
+            sRing[wib], nullptr, nullptr, bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
+            [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+            [&](const double4* ring, const float4*, const int*, int head, int count) {
+                gc += count;
+                const double4 pj = ring[(head + (lane < count ? lane : 0)) & (kRing - 1)];
+                int nrec = 0, segStart = 0, segCount = 0;
+                auto flush = [&]() {
+                    __syncwarp();
+                    for (int r = lane; r < nrec; r += 32)
+                    {
+                        const double q2 = recA[r];
+                        const double q = sqrt(q2);
+                        double wk, dwk;
+                        sph_kernel(q2, q, wk, dwk);
+                        recA[r] = wk;
+                        recB[r] = -q * dwk - 3.0 * wk;
+                    }
+                    __syncwarp();
+                    for (int t = 0; t < segCount; ++t)
+                    {
+                        rhoi += recA[segStart + t];
+                        gradhi += recB[segStart + t];
+                    }
+                    gp += segCount;
+                    segCount = 0;
+                    nrec = 0;
+                    __syncwarp();
+                };
+                for (int ii = 0; ii < ng; ++ii)
+                {
+                    const double4 g = sGrp[wib][ii];
+                    double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                    const double q2 = pair_r2(dx, dy, dz) * g.w;
+                    const bool acc = lane < count && q2 < kRadK2;
+                    const uint32_t m = __ballot_sync(0xffffffffu, acc);
+                    const int c = __popc(m);
+                    if (nrec + c > kRec) flush();
+                    if (acc) recA[nrec + __popc(m & lt)] = q2;
+                    if (lane == ii) { segStart = nrec; segCount = c; }
+                    nrec += c;
+                }
+                if (nrec > 0) flush();
+            });
+        bool stillActive = false;
+        if (mine)
+        {
+            pairs += gp;
+            cand += gc;
+            // Newton-Raphson step, src/density_base.cu:294-333
+            const double hi1 = 1.0 / hi;
+            const double hi31 = hi1 * hi1 * hi1;
+            const double hi41 = hi31 * hi1;
+            const double rho_i = rhoi * kCnormk * pmass * hi31;
+            const double grad_i = gradhi * kCnormk * pmass * hi41;
+            if (!(rho_i > 0.0))
+            {
+                rho[i] = 0.0;
+                gradh[i] = 0.0;
+                converged[i] = 0;
+                stillActive = true;
+            }
+            else
+            {
+                const double rhoh_i = pmass * (hfact * hi1) * (hfact * hi1) * (hfact * hi1);
+                const double funci = rhoh_i - rho_i;
+                const double dhdrhoi = -hi / (3.0 * rhoh_i);
+                const double omegai = 1.0 - dhdrhoi * grad_i;
+                const double safe = (omegai > 0.0) ? omegai : fabs(omegai + 1e-300);
+                const double hraw = hi - funci * dhdrhoi / safe;
+                double hnew;
+                if (hraw > 1.2 * hi) hnew = 1.2 * hi;
+                else if (hraw < 0.8 * hi) hnew = 0.8 * hi;
+                else hnew = hraw;
+                rho[i] = rho_i;
+                gradh[i] = grad_i;
+                reinterpret_cast<double*>(xyzh + i)[3] = hnew;
+                const int conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
+                converged[i] = conv;
+                stillActive = !conv;
+            }
+        }
+        const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
+        if (still && lane == 0)
+        {
+            atomicAdd(&ds->unconverged, __popc(still));
+            if (atomicExch(&leafNext[leaf], 1) == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -361,6 +453,15 @@ int grid_for(const State& s, int work)
     return std::max(1, std::min(maxBlocks, iceil(work, kWarpsPerBlock)));
 }
 
+// A persistent grid: as many blocks of the kernel as fit on the device at once.
+template<class K>
+int persistent_grid(const State& s, K kernel)
+{
+    int perSM = 0;
+    COSMO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, 0));
+    return std::max(1, perSM) * s.numSMs;
+}
+
 } // namespace
 
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh, double hfact,
@@ -387,6 +488,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     const int nL = s.nLeaves;
     s.activeA.resize(nL, s.st);
     s.activeB.resize(nL, s.st);
+    s.leafNext.resize(nL, s.st);
+    const int itemCap = std::max(s.nAlive, 1);
+    s.items.resize(itemCap, s.st);
     COSMO_CUDA(cudaMemcpyAsync(s.activeA.get(), s.allLeaves.get(), size_t(nL) * 4, cudaMemcpyDeviceToDevice, s.st));
     int nActiveLeaves = nL;
     long long nActiveParticles = s.nAlive;
@@ -398,21 +502,27 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         hmax_leaves(s, s.activeA.get(), nActiveLeaves);
         build_lists(s, false);
         cudaEvent_t j1 = ev(s);
-        COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 2 * sizeof(int), s.st));
-        const int grid = grid_for(s, nActiveLeaves);
         if (s.precision == 1)
+        {
+            COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 2 * sizeof(int), s.st));
             launch_density_mixed(s, nActiveLeaves, pmass, tolh, hfact);
-        else if (s.periodic)
-            density_nr_kernel<true><<<grid, kThreads, 0, s.st>>>(
-                s.activeA.get(), nActiveLeaves, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
-                s.xyzh.get(), s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(),
-                s.activeB.get(), ds);
+        }
         else
-            density_nr_kernel<false><<<grid, kThreads, 0, s.st>>>(
-                s.activeA.get(), nActiveLeaves, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
-                s.xyzh.get(), s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(),
+        {
+            begin_iteration_kernel<<<std::min(iceil(nL, 256), 4 * s.numSMs), 256, 0, s.st>>>(ds, s.leafNext.get(),
+                                                                                            nL);
+            COSMO_LAUNCHED();
+            plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
+                s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(), s.items.get(),
+                itemCap, ds);
+            COSMO_LAUNCHED();
+            auto nr = s.periodic ? density_nr_kernel<true> : density_nr_kernel<false>;
+            nr<<<persistent_grid(s, nr), kThreads, 0, s.st>>>(
+                s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+                s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.leafNext.get(),
                 s.activeB.get(), ds);
-        COSMO_LAUNCHED();
+            COSMO_LAUNCHED();
+        }
         cudaEvent_t j2 = ev(s);
         read_scalars(s);
         s.t.jbuild += elapsed_s(j0, j1);

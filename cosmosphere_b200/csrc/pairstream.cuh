@@ -105,7 +105,7 @@ __device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v)
 // consecutive stream positions (each lane finds its particle by a 5-step binary search
 // over the prefix sums), and the next batch's loads are issued before the current batch
 // is filtered and evaluated.
-template<class Filter, class Batch>
+template<bool Float = true, bool Index = true, class Filter, class Batch>
 __device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
                                              double cz, uint32_t jb, uint32_t nj, const int* __restrict__ jlist,
                                              const uint32_t* __restrict__ layout,
@@ -168,8 +168,9 @@ __device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* 
             {
                 const int slot = (head + cnt + __popc(m & lt)) & (kRing - 1);
                 ring[slot] = pj;
-                ringf[slot] = make_float4(float(pj.x - cx), float(pj.y - cy), float(pj.z - cz), float(pj.w));
-                ringIdx[slot] = int(j);
+                if constexpr (Float)
+                    ringf[slot] = make_float4(float(pj.x - cx), float(pj.y - cy), float(pj.z - cz), float(pj.w));
+                if constexpr (Index) ringIdx[slot] = int(j);
             }
             cnt += __popc(m);
             __syncwarp();

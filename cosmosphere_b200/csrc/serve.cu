@@ -38,15 +38,33 @@ namespace cosmo {
 
 namespace {
 
+struct DevBox3
+{
+    double lo[3], hi[3];
+};
+
+// Drift x += v dt; in a periodic box a coordinate that leaves [lo, hi) is wrapped back
+// by one box length.
+__device__ __forceinline__ double drift(double x, double v, double dt, int periodic, double lo, double hi)
+{
+    double y = x + v * dt;
+    if (periodic)
+    {
+        if (y >= hi) y = y - (hi - lo);
+        else if (y < lo) y = y + (hi - lo);
+    }
+    return y;
+}
+
 __global__ void advance_kernel(double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
                                const double* __restrict__ vx, const double* __restrict__ vy,
-                               const double* __restrict__ vz, int n, double dt)
+                               const double* __restrict__ vz, int n, double dt, int periodic, DevBox3 box)
 {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    x[i] += vx[i] * dt;
-    y[i] += vy[i] * dt;
-    z[i] += vz[i] * dt;
+    x[i] = drift(x[i], vx[i], dt, periodic, box.lo[0], box.hi[0]);
+    y[i] = drift(y[i], vy[i], dt, periodic, box.lo[1], box.hi[1]);
+    z[i] = drift(z[i], vz[i], dt, periodic, box.lo[2], box.hi[2]);
 }
 
 // Previous converged h (Hilbert order) back to the caller's order: the warm start.
@@ -118,6 +136,7 @@ struct Request
     int status = 0;                             // 0 pending, 1 done, -1 rejected, -2 unconverged
     int itersRun = 0;
     int slot = -1;
+    int pendingConts = 0;                       // continuations submitted before admission
 };
 
 struct ResidentSet
@@ -172,7 +191,9 @@ Request* pick(Server& S, std::vector<std::unique_ptr<ResidentSet>>& evict)
             auto si = S.sets.find(r->setId);
             if (si == S.sets.end())
             {
-                r->status = -1;   // its set was released
+                auto oi = S.reqs.find(r->setId);
+                if (oi != S.reqs.end() && oi->second->status == 0) continue;   // set not admitted yet
+                r->status = -1;   // its set was released, rejected or failed
                 S.queue.erase(it);
                 S.cvDone.notify_all();
                 return pick(S, evict);
@@ -225,6 +246,7 @@ Request* pick(Server& S, std::vector<std::unique_ptr<ResidentSet>>& evict)
         rs->alphau = r->alphau;
         std::copy(r->box, r->box + 6, rs->box);
         rs->busy = true;
+        rs->queued = r->pendingConts;
         S.sets[r->id] = std::move(rs);
         S.queue.erase(it);
         return r;
@@ -257,8 +279,9 @@ int run_request(Server& S, Request* r, ResidentSet* rs)
     }
     else
     {
+        const DevBox3 b3 = {{rs->box[0], rs->box[2], rs->box[4]}, {rs->box[1], rs->box[3], rs->box[5]}};
         advance_kernel<<<iceil(n, 256), 256, 0, st.st>>>(st.ux.get(), st.uy.get(), st.uz.get(), st.uvx.get(),
-                                                         st.uvy.get(), st.uvz.get(), n, r->dt);
+                                                         st.uvy.get(), st.uvz.get(), n, r->dt, rs->periodic, b3);
         COSMO_LAUNCHED();
         warm_h_kernel<<<iceil(n, 256), 256, 0, st.st>>>(st.orderA.get(), n, st.xyzh.get(), st.uh.get());
         COSMO_LAUNCHED();
@@ -411,18 +434,27 @@ long cosmo_serve_continue(long set_id, double dt, const double* thermo4, int kee
     Server& S = server();
     std::lock_guard<std::mutex> lk(S.m);
     if (!S.running) return -1;
+    // the set is resident, or its first request is still waiting for admission
     auto si = S.sets.find(set_id);
-    if (si == S.sets.end()) return -1;
+    Request* origin = nullptr;
+    if (si == S.sets.end())
+    {
+        auto oi = S.reqs.find(set_id);
+        if (oi == S.reqs.end() || !oi->second->isNew || oi->second->status != 0 || !oi->second->keep) return -1;
+        if (std::find(S.queue.begin(), S.queue.end(), oi->second.get()) == S.queue.end()) return -1;
+        origin = oi->second.get();
+    }
     auto r = std::make_unique<Request>();
     r->isNew = false;
     r->keep = keep_resident != 0;
     r->setId = set_id;
-    r->n = si->second->n;
+    r->n = origin ? origin->n : si->second->n;
     r->dt = dt;
     if (thermo4) r->thermo.assign(thermo4, thermo4 + 4 * size_t(r->n));
     r->id = S.nextId++;
     r->tSubmit = now_s();
-    si->second->queued += 1;
+    if (origin) origin->pendingConts += 1;
+    else si->second->queued += 1;
     Request* raw = r.get();
     S.reqs[r->id] = std::move(r);
     S.queue.push_back(raw);

@@ -29,6 +29,11 @@ namespace cosmo {
 // served form charges requests against it).
 extern std::atomic<long long> g_deviceBytes;
 
+// The library's stream-ordered memory pool on the current device (created on first use,
+// release threshold unlimited): buffers are taken and returned in stream order, so growing
+// or dropping one state's buffers never synchronises the device under other states' work.
+cudaMemPool_t device_pool();
+
 template<class T>
 struct DBuf
 {
@@ -36,36 +41,36 @@ struct DBuf
     size_t n   = 0;
     size_t cap = 0;
 
-    void release()
+    // Return the buffer to the pool after the work already queued on st.
+    void release(cudaStream_t st = nullptr)
     {
         if (p)
         {
-            COSMO_CUDA(cudaFree(p));
+            COSMO_CUDA(cudaFreeAsync(p, st));
             g_deviceBytes -= (long long)(cap * sizeof(T));
         }
         p = nullptr;
         n = cap = 0;
     }
 
-    // Grow to hold c elements.  Contents are kept only when keep is set; new memory is
-    // zeroed, as the reference's thrust::device_vector value-initialises.
+    // Grow to hold c elements, in st's order.  Contents are kept only when keep is set;
+    // new memory is zeroed, as the reference's thrust::device_vector value-initialises.
     void resize(size_t c, cudaStream_t st, bool keep = false)
     {
         if (c > cap)
         {
-            T* q = nullptr;
+            void* q = nullptr;
             const size_t newCap = c + c / 8 + 16;
-            COSMO_CUDA(cudaMalloc(&q, newCap * sizeof(T)));
+            COSMO_CUDA(cudaMallocFromPoolAsync(&q, newCap * sizeof(T), device_pool(), st));
             g_deviceBytes += (long long)(newCap * sizeof(T));
             COSMO_CUDA(cudaMemsetAsync(q, 0, newCap * sizeof(T), st));
             if (keep && p && n) COSMO_CUDA(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
             if (p)
             {
-                COSMO_CUDA(cudaStreamSynchronize(st));
-                COSMO_CUDA(cudaFree(p));
+                COSMO_CUDA(cudaFreeAsync(p, st));
                 g_deviceBytes -= (long long)(cap * sizeof(T));
             }
-            p = q;
+            p = static_cast<T*>(q);
             cap = newCap;
         }
         n = c;
@@ -83,7 +88,8 @@ struct DevScalars
     int workCounter[4];          // dynamic work distribution for persistent kernels
     unsigned long long pairs[4]; // accepted pairs: density, gradient, force, candidates
     unsigned int sortTiles[16];  // onesweep tile tickets, one per digit pass
-    int pad[8];
+    int itemsHeavy, itemsLight;  // Newton work items of the current iteration (split, whole)
+    int pad[6];
 };
 
 struct Timings
@@ -133,7 +139,10 @@ struct State
     DBuf<double4> preCenter, preHalf;           // pre-order copies for the walk
     DBuf<double> hmaxLeaf, hmaxNode, hmaxPre;
     DBuf<uint32_t> jcount, jOffset;
+    DBuf<uint32_t> jstream;                     // particles in each leaf's gather list
     DBuf<int> jlist;
+    DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
+    DBuf<int> leafNext;                         // leaf already queued for the next iteration
     DBuf<int> activeA, activeB, allLeaves;
 
     // scratch

@@ -350,7 +350,8 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const double4* __restrict__ preHalf, const int* __restrict__ preSkip,
                  const int* __restrict__ preLeaf, const double* __restrict__ hmaxPre,
                  const DevBox* __restrict__ box, uint32_t* __restrict__ jcount,
-                 const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err)
+                 const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err,
+                 const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -368,7 +369,7 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
     double lx = 0, ly = 0, lz = 0;
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
 
-    uint32_t count = 0, base = 0, cap = 0;
+    uint32_t count = 0, base = 0, cap = 0, stream = 0;
     if (Fill) { base = jOffset[leaf]; cap = jOffset[leaf + 1] - base; }
     const uint32_t lt = (1u << lane) - 1u;
 
@@ -425,6 +426,8 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                     else atomicOr(err, int(kErrListCap));
                 }
             }
+            else if (jstream != nullptr && ((emitMask >> lane) & 1u))
+                stream += layout[pl + 1] - layout[pl];
             count += __popc(emitMask);
             if (r >= 32) { next = p + 32; break; }
             int rskip = __shfl_sync(0xffffffffu, skip, r);
@@ -435,10 +438,19 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
         }
         p = next;
     }
+    if (!Fill && jstream != nullptr)
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) stream += __shfl_xor_sync(0xffffffffu, stream, o);
+    }
     if (lane == 0)
     {
         if (Fill) { if (count != cap) atomicOr(err, int(kErrListCap)); }
-        else jcount[leaf] = count;
+        else
+        {
+            jcount[leaf] = count;
+            if (jstream != nullptr) jstream[leaf] = stream;
+        }
     }
 }
 
@@ -674,6 +686,7 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
     s.hmaxNode.resize(numNodes, s.st);
     s.hmaxPre.resize(numNodes, s.st);
     s.jcount.resize(nL, s.st);
+    s.jstream.resize(nL, s.st);
     s.jOffset.resize(size_t(nL) + 1, s.st);
     s.allLeaves.resize(nL, s.st);
     iota_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.allLeaves.get(), nL);
@@ -722,7 +735,8 @@ static void walk(State& s, bool fill)
         kern<<<blocks, kBlk, 0, s.st>>>(nL, s.numNodes, s.leafToInternal.get(), s.centers.get(), s.sizes.get(),
                                         s.hmaxLeaf.get(), s.preCenter.get(), s.preHalf.get(), s.preSkip.get(),
                                         s.preLeaf.get(), s.hmaxPre.get(), s.box.get(), s.jcount.get(),
-                                        s.jOffset.get(), s.jlist.get(), &s.dscal.get()->err);
+                                        s.jOffset.get(), s.jlist.get(), &s.dscal.get()->err, s.layout.get(),
+                                        (!fill && !Sym) ? s.jstream.get() : nullptr);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);

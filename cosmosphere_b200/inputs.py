@@ -133,3 +133,57 @@ def ensemble_sets(nsets: int = 256, nmin: float = 1e4, nmax: float = 5e5, seed: 
             p = plummer(int(n), rmax=20.0, hfact=1.2, lnsigma=0.0, ulo=0.8, uhi=1.2, seed=seed + 1000 + k)
         sets.append(p)
     return sets
+
+
+def _thermo(p, u, gamma=5.0 / 3.0, alpha=1.0, hfact=1.2):
+    """pro2, cs, alpha, u of an ideal gas at internal energy u, with rho estimated from
+    the initial h: rho = pmass (hfact/h)^3."""
+    n = p.n
+    rho = p["pmass"] * (hfact / p["h"]) ** 3
+    uu = np.broadcast_to(np.asarray(u, dtype=np.float64), (n,))
+    return np.ascontiguousarray(np.stack([(gamma - 1.0) * uu / rho, np.sqrt(gamma * (gamma - 1.0) * uu),
+                                          np.full(n, alpha), uu]))
+
+
+def served_requests(nreq: int = 96, nmin: float = 5e3, nmax: float = 2e6, pcont: float = 0.3, seed: int = 42):
+    """The served-stream request list: particle counts log-uniform in [nmin, nmax]
+    (seeded), each new set drawn from the lattice-with-jiggle, periodic-uniform-box or
+    Plummer generator; with probability pcont a request instead continues an earlier set
+    by one step of dt = 0.1 min(h/c_s) over that set's initial h.
+
+    Each entry is a dict: kind "new" with the particle set p (x, y, z, h, vx, vy, vz,
+    pmass, optional box), pos3 (3, n), vel3 (3, n) and thermo4 (4, n) component-major;
+    or kind "cont" with "of" (the index of the set's first request) and dt."""
+    rng = np.random.default_rng(seed)
+    out = []
+    firsts = []
+    for k in range(nreq):
+        if firsts and rng.uniform() < pcont:
+            j = int(rng.choice(firsts))
+            out.append({"kind": "cont", "of": j, "dt": out[j]["dt"]})
+            continue
+        n = int(np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        g = int(rng.integers(3))
+        s = seed + 7919 * (k + 1)
+        if g == 0:
+            npx = max(4, int(round((n / 1.403) ** (1.0 / 3.0))))
+            p = lattice100_workload(npx, seed=s)
+            th = np.ascontiguousarray(np.stack([p["pro2"], p["cs"], p["alpha"], p["u"]]))
+            gen = f"lattice {npx} + jiggle"
+        elif g == 1:
+            p = uniform_box(n, hfac=1.2, hlo=0.8, hhi=1.2, seed=s)
+            p["box"] = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+            p["vx"], p["vy"], p["vz"] = (gaussian(n, 0.0, 0.1, s + a) for a in (1, 2, 3))
+            th = _thermo(p, 1.0)
+            gen = "periodic uniform box"
+        else:
+            p = plummer(n, rmax=20.0, hfact=1.2, lnsigma=0.3, vfrac=0.5, seed=s)
+            th = _thermo(p, 0.05)
+            gen = "Plummer"
+        dt = 0.1 * float(np.min(p["h"] / th[1]))
+        out.append({"kind": "new", "p": p, "gen": gen, "n": p.n, "dt": dt,
+                    "pos3": np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]])),
+                    "vel3": np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]])),
+                    "thermo4": th})
+        firsts.append(k)
+    return out

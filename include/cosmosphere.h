@@ -137,9 +137,11 @@ int cosmo_serve_start(int slots, double hbm_budget_gb);
 long cosmo_serve_submit(int n, double pmass, int periodic, const double* box6, double tolh, double hfact,
                         const double* pos3, const double* h, const double* vel3, const double* thermo4, double beta,
                         double alphau, int keep_resident);
-/* Continue a resident set one step: positions advance on the device by v*dt, the
- * Newton iteration starts from the previous converged h; thermo4 may be NULL (keep).
- * Returns the request id, or -1 if the set is not resident. */
+/* Continue a set one step: positions advance on the device by v*dt (wrapped into a
+ * periodic box), the Newton iteration starts from the previous converged h; thermo4 may
+ * be NULL (keep).  The set may be resident or still queued for admission (its first
+ * request submitted with keep_resident); continuations of one set run in submission
+ * order.  Returns the request id, or -1 if the set is unknown or was dropped. */
 long cosmo_serve_continue(long set_id, double dt, const double* thermo4, int keep_resident);
 /* Block until a request finishes and copy its results (caller order) into the given,
  * non-NULL outputs: h (n), dens (rho, gradh: 2n), grad (div v, xi, d(div v)/dt: 3n),

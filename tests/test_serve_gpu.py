@@ -164,3 +164,53 @@ def test_lru_eviction_of_idle_resident_sets():
         assert S.wait(S.cont(ids[2], 1e-4))[0] == 1
     finally:
         S.stop()
+
+
+def drift_wrap(x, v, dt, box):
+    """Host drift of the served continuation: x + v dt, wrapped into a periodic box."""
+    y = x + v * dt
+    if box is not None:
+        lo, hi = box[0], box[1]
+        y = np.where(y >= hi, y - (hi - lo), np.where(y < lo, y + (hi - lo), y))
+    return y
+
+
+def test_continuations_queued_before_admission(reqs):
+    """Continuations may be submitted while their set's first request still waits in the
+    queue; they run after it, in order, and equal the same steps done through the C-ABI
+    (periodic box: drifted coordinates wrap)."""
+    p, box = reqs[2]
+    n = p.n
+    th = thermo_for(p)
+    S = capi.Server(slots=1)
+    try:
+        blocker = S.submit(reqs[0][0], thermo_for(reqs[0][0]), keep=False)
+        r0 = S.submit(p, th, box=box, keep=True)
+        dt = 0.05
+        r1 = S.cont(r0, dt)
+        r2 = S.cont(r0, dt)
+        out = [S.wait(r) for r in (blocker, r0, r1, r2)]
+        assert S.stat(r1, "start") >= S.stat(r0, "done") and S.stat(r2, "start") >= S.stat(r1, "done")
+    finally:
+        S.stop()
+    assert all(st == 1 for st, _ in out)
+    c = capi.Cosmo()
+    pos = np.stack([p["x"], p["y"], p["z"]])
+    vel = np.stack([p["vx"], p["vy"], p["vz"]])
+    h = p["h"]
+    for k in range(3):
+        if k:
+            pos = drift_wrap(pos, vel, dt, box)
+        c.arrays_init(n)
+        c.upload(capi.POS, pos)
+        c.upload(capi.HSML, h)
+        c.upload(capi.VEL, vel)
+        c.upload(capi.ACCEL, np.zeros((3, n)))
+        c.density(n, p["pmass"], periodic_box=box)
+        c.upload(capi.THERMO, th, sorted_=True)
+        c.force(n, p["pmass"], beta=2.0, alphau=0.0)
+        h = c.download(capi.HSML, n)[0]
+        got = out[k + 1][1]
+        np.testing.assert_array_equal(got["h"], h, err_msg=f"step {k}")
+        np.testing.assert_array_equal(got["force"], c.download(capi.FORCE_OUT, n), err_msg=f"step {k}")
+    assert np.all((pos >= 0.0) & (pos < 1.0))
