@@ -21,6 +21,7 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
 constexpr int kRec = 256;                       // pair records per warp
+constexpr double kListMargin = 1.15;            // gather-radius widening of the Newton lists
 
 // Zero the per-iteration counters of the Newton work queue and the leaf re-queue flags.
 __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restrict__ leafNext, int nL)
@@ -30,6 +31,7 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
     {
         ds->nextActive = 0;
         ds->unconverged = 0;
+        ds->listStale = 0;
         ds->workCounter[0] = 0;
         ds->itemsHeavy = 0;
         ds->itemsLight = 0;
@@ -96,13 +98,13 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
 // group's size or spatial spread, and each particle's sums still run over j in ascending
 // Hilbert index, the oracle's order, so the results agree with it bit for bit.
 template<bool Periodic>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 6)
 density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                   const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
                   double* __restrict__ gradh, int* __restrict__ converged, double pmass, double tolh,
-                  double hfact, const DevBox* __restrict__ box, int* __restrict__ leafNext,
-                  int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
+                  double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
+                  int* __restrict__ leafNext, int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
     __shared__ double4 sGrp[kWarpsPerBlock][32];
@@ -173,19 +175,29 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
                     nrec = 0;
                     __syncwarp();
                 };
-                for (int ii = 0; ii < ng; ++ii)
+                // four group particles per step: independent FP64 chains for the scheduler
+                for (int i0 = 0; i0 < ng; i0 += 4)
                 {
-                    const double4 g = sGrp[wib][ii];
-                    double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
-                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                    const double q2 = pair_r2(dx, dy, dz) * g.w;
-                    const bool acc = lane < count && q2 < kRadK2;
-                    const uint32_t m = __ballot_sync(0xffffffffu, acc);
-                    const int c = __popc(m);
-                    if (nrec + c > kRec) flush();
-                    if (acc) recA[nrec + __popc(m & lt)] = q2;
-                    if (lane == ii) { segStart = nrec; segCount = c; }
-                    nrec += c;
+                    if (nrec + 4 * 32 > kRec) flush();
+                    double q2u[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                    {
+                        const double4 g = sGrp[wib][min(i0 + u, 31)];
+                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                        q2u[u] = pair_r2(dx, dy, dz) * g.w;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                    {
+                        const bool acc = lane < count && i0 + u < ng && q2u[u] < kRadK2;
+                        const uint32_t m = __ballot_sync(0xffffffffu, acc);
+                        const int c = __popc(m);
+                        if (acc) recA[nrec + __popc(m & lt)] = q2u[u];
+                        if (lane == i0 + u) { segStart = nrec; segCount = c; }
+                        nrec += c;
+                    }
                 }
                 if (nrec > 0) flush();
             });
@@ -225,6 +237,7 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
                 const int conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
                 converged[i] = conv;
                 stillActive = !conv;
+                if (!conv && hnew > listH[leaf]) ds->listStale = 1;
             }
         }
         const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
@@ -495,16 +508,26 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     int nActiveLeaves = nL;
     long long nActiveParticles = s.nAlive;
 
+    // The gather lists are built with a widened radius and reused while every active h
+    // stays inside it: a superset list in ascending leaf order offers the same accepted
+    // pairs in the same order, so the sums do not change.  hmaxLeaf is still refreshed
+    // for the active leaves every iteration, as the reference does, so the exact lists of
+    // the last iteration can be rebuilt afterwards.
+    bool listsValid = false, listsWidened = false;
     cudaEvent_t e3 = ev(s);
     for (int iter = 0; iter < maxIter; ++iter)
     {
         cudaEvent_t j0 = ev(s);
         hmax_leaves(s, s.activeA.get(), nActiveLeaves);
-        build_lists(s, false);
+        if (!listsValid)
+        {
+            build_lists(s, false, kListMargin);
+            listsValid = listsWidened = true;
+        }
         cudaEvent_t j1 = ev(s);
         if (s.precision == 1)
         {
-            COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 2 * sizeof(int), s.st));
+            COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 3 * sizeof(int), s.st));
             launch_density_mixed(s, nActiveLeaves, pmass, tolh, hfact);
         }
         else
@@ -519,8 +542,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
             auto nr = s.periodic ? density_nr_kernel<true> : density_nr_kernel<false>;
             nr<<<persistent_grid(s, nr), kThreads, 0, s.st>>>(
                 s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-                s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.leafNext.get(),
-                s.activeB.get(), ds);
+                s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
+                s.leafNext.get(), s.activeB.get(), ds);
             COSMO_LAUNCHED();
         }
         cudaEvent_t j2 = ev(s);
@@ -531,10 +554,19 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         s.itersRun = iter + 1;
         nActiveLeaves = s.hscal->nextActive;
         nActiveParticles = s.hscal->unconverged;
+        if (s.hscal->listStale) listsValid = false;
         std::swap(s.activeA, s.activeB);
         if (nActiveParticles == 0) break;
     }
     (void)e3;
+    if (listsWidened && !withGradients)
+    {
+        cudaEvent_t j0 = ev(s);
+        build_lists(s, false);
+        cudaEvent_t j1 = ev(s);
+        COSMO_CUDA(cudaEventSynchronize(j1));
+        s.t.jbuild += elapsed_s(j0, j1);
+    }
     check_dev_err(s, "solveDensH");
     res.itersRun = s.itersRun;
     res.unconverged = int(nActiveParticles);

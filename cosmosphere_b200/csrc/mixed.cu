@@ -32,8 +32,8 @@ density_nr_mixed_kernel(const int* __restrict__ leaves, int nLeavesActive, const
                         const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                         const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
                         double* __restrict__ gradh, int* __restrict__ converged, double pmass, double tolh,
-                        double hfact, const DevBox* __restrict__ box, int* __restrict__ nextLeaves,
-                        DevScalars* __restrict__ ds)
+                        double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
+                        int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
     __shared__ float4 sRingF[kWarpsPerBlock][kRing];
@@ -132,6 +132,7 @@ density_nr_mixed_kernel(const int* __restrict__ leaves, int nLeavesActive, const
                         const int conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
                         converged[i] = conv;
                         stillActive = !conv;
+                        if (!conv && hnew > listH[leaf]) ds->listStale = 1;
                     }
                 }
                 const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
@@ -517,8 +518,8 @@ void launch_density_mixed(State& s, int nActiveLeaves, double pmass, double tolh
     auto go = [&](auto kern) {
         kern<<<grid, kThreads, 0, s.st>>>(s.activeA.get(), nActiveLeaves, s.layout.get(), s.jOffset.get(),
                                           s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.rho.get(), s.gradh.get(),
-                                          s.converged.get(), pmass, tolh, hfact, s.box.get(), s.activeB.get(),
-                                          s.dscal.get());
+                                          s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
+                                          s.activeB.get(), s.dscal.get());
     };
     if (s.periodic) go(density_nr_mixed_kernel<true>);
     else go(density_nr_mixed_kernel<false>);

@@ -85,11 +85,13 @@ struct DevScalars
     int err;                     // DevErr bits
     int nextActive;              // active-leaf appends of the current NR iteration
     int unconverged;             // particles left unconverged by the current iteration
+    int listStale;               // an updated h outgrew the gather radius its leaf's list has
+    int pad0;
     int workCounter[4];          // dynamic work distribution for persistent kernels
     unsigned long long pairs[4]; // accepted pairs: density, gradient, force, candidates
     unsigned int sortTiles[16];  // onesweep tile tickets, one per digit pass
     int itemsHeavy, itemsLight;  // Newton work items of the current iteration (split, whole)
-    int pad[6];
+    int pad[4];
 };
 
 struct Timings
@@ -140,6 +142,7 @@ struct State
     DBuf<double> hmaxLeaf, hmaxNode, hmaxPre;
     DBuf<uint32_t> jcount, jOffset;
     DBuf<uint32_t> jstream;                     // particles in each leaf's gather list
+    DBuf<double> listH;                         // h each leaf's gather list covers
     DBuf<int> jlist;
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
     DBuf<int> leafNext;                         // leaf already queued for the next iteration
@@ -166,7 +169,10 @@ void size_particle_arrays(State& s, int n);
 // tree.cu
 void build_tree(State& s, const double* periodicBox, bool alsoSortVA);
 void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
-void build_lists(State& s, bool symmetric);
+// Gather (symmetric = false) or symmetric j-leaf lists for all leaves.  margin > 1 widens
+// the gather radius to R * hmax * margin, so the lists stay valid while h grows by up to
+// that factor; listH records the h each leaf's list covers.
+void build_lists(State& s, bool symmetric, double margin = 1.0);
 void hmax_upsweep(State& s);
 void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int n, bool iotaValues);
 uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool readTotal);

@@ -351,7 +351,8 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const int* __restrict__ preLeaf, const double* __restrict__ hmaxPre,
                  const DevBox* __restrict__ box, uint32_t* __restrict__ jcount,
                  const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err,
-                 const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream)
+                 const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
+                 double* __restrict__ listH)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -361,6 +362,7 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
     const double isx = sizes[3 * iNode], isy = sizes[3 * iNode + 1], isz = sizes[3 * iNode + 2];
     double hmax = hmaxLeaf[leaf];
     if (!isfinite(hmax) || hmax <= 0.0) hmax = 0.0;
+    hmax *= margin;
     const double radHi = kRadKernel * hmax;
     // gather: the i-box inflated by radHi; symmetric: the raw i-box
     const double ax = Symmetric ? isx : isx + radHi;
@@ -450,6 +452,7 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
         {
             jcount[leaf] = count;
             if (jstream != nullptr) jstream[leaf] = stream;
+            if (listH != nullptr) listH[leaf] = hmax;
         }
     }
 }
@@ -687,6 +690,7 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
     s.hmaxPre.resize(numNodes, s.st);
     s.jcount.resize(nL, s.st);
     s.jstream.resize(nL, s.st);
+    s.listH.resize(nL, s.st);
     s.jOffset.resize(size_t(nL) + 1, s.st);
     s.allLeaves.resize(nL, s.st);
     iota_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.allLeaves.get(), nL);
@@ -727,7 +731,7 @@ void hmax_upsweep(State& s)
 }
 
 template<bool Sym, bool Per>
-static void walk(State& s, bool fill)
+static void walk(State& s, bool fill, double margin)
 {
     const int nL = s.nLeaves;
     const int blocks = iceil(long(nL) * 32, kBlk);
@@ -736,7 +740,8 @@ static void walk(State& s, bool fill)
                                         s.hmaxLeaf.get(), s.preCenter.get(), s.preHalf.get(), s.preSkip.get(),
                                         s.preLeaf.get(), s.hmaxPre.get(), s.box.get(), s.jcount.get(),
                                         s.jOffset.get(), s.jlist.get(), &s.dscal.get()->err, s.layout.get(),
-                                        (!fill && !Sym) ? s.jstream.get() : nullptr);
+                                        (!fill && !Sym) ? s.jstream.get() : nullptr, margin,
+                                        (!fill && !Sym) ? s.listH.get() : nullptr);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
@@ -744,11 +749,11 @@ static void walk(State& s, bool fill)
 }
 
 // include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.
-void build_lists(State& s, bool symmetric)
+void build_lists(State& s, bool symmetric, double margin)
 {
     auto run = [&](bool fill) {
-        if (symmetric) { if (s.periodic) walk<true, true>(s, fill); else walk<true, false>(s, fill); }
-        else { if (s.periodic) walk<false, true>(s, fill); else walk<false, false>(s, fill); }
+        if (symmetric) { if (s.periodic) walk<true, true>(s, fill, margin); else walk<true, false>(s, fill, margin); }
+        else { if (s.periodic) walk<false, true>(s, fill, margin); else walk<false, false>(s, fill, margin); }
     };
     run(false);
     const uint32_t total = scan_exclusive(s, s.jcount.get(), s.jOffset.get(), s.nLeaves, true);
