@@ -12,6 +12,9 @@
 
 #include "pairstream.cuh"
 #include "state.hpp"
+#include "workitems.cuh"
+#include "densengine.cuh"
+#include "rows.cuh"
 
 namespace cosmo {
 
@@ -20,85 +23,52 @@ namespace {
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
-constexpr int kRec = 256;                       // pair records per warp
 constexpr double kListMargin = 1.15;            // gather-radius widening of the Newton lists
 
-// Zero the per-iteration counters of the Newton work queue and the leaf re-queue flags.
-__global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restrict__ leafNext, int nL)
+// Newton-Raphson step of one particle from its un-normalised sums (src/density_base.cu:
+// 294-333): rho, d(rho)/dh, the new h (clamped to +-20%) and whether |dh/h| < tolh.
+// Returns true while the particle stays unconverged.
+__device__ __forceinline__ bool newton_step(double rhoi, double gradhi, double hi, double pmass, double hfact,
+                                           double tolh, double& rhoOut, double& gradOut, double& hOut, int& conv)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t == 0)
+    const double hi1 = 1.0 / hi;
+    const double hi31 = hi1 * hi1 * hi1;
+    const double hi41 = hi31 * hi1;
+    const double rho_i = rhoi * kCnormk * pmass * hi31;
+    const double grad_i = gradhi * kCnormk * pmass * hi41;
+    if (!(rho_i > 0.0))
     {
-        ds->nextActive = 0;
-        ds->unconverged = 0;
-        ds->listStale = 0;
-        ds->workCounter[0] = 0;
-        ds->itemsHeavy = 0;
-        ds->itemsLight = 0;
+        rhoOut = 0.0;
+        gradOut = 0.0;
+        hOut = hi;
+        conv = 0;
+        return true;
     }
-    for (int l = t; l < nL; l += gridDim.x * blockDim.x) leafNext[l] = 0;
+    const double rhoh_i = pmass * (hfact * hi1) * (hfact * hi1) * (hfact * hi1);
+    const double funci = rhoh_i - rho_i;
+    const double dhdrhoi = -hi / (3.0 * rhoh_i);
+    const double omegai = 1.0 - dhdrhoi * grad_i;
+    const double safe = (omegai > 0.0) ? omegai : fabs(omegai + 1e-300);
+    const double hraw = hi - funci * dhdrhoi / safe;
+    double hnew;
+    if (hraw > 1.2 * hi) hnew = 1.2 * hi;
+    else if (hraw < 0.8 * hi) hnew = 0.8 * hi;
+    else hnew = hraw;
+    rhoOut = rho_i;
+    gradOut = grad_i;
+    hOut = hnew;
+    conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
+    return !conv;
 }
 
-// Work items of one Newton iteration: every group of a leaf's 64-slot window of
-// unconverged particles is one item (leaf, window << 16 | group << 8 | groups, the two
-// halves of the window's active mask).  Groups hold up to 32 particles; a leaf whose
-// gather list streams more than kSplitStream particles is cut into smaller groups, about
-// kSplitWork / stream particles each, so that no single warp carries the iteration's
-// tail.  Cut items are queued from the front of the buffer and run first, whole groups
-// from the back.  The items of a window hold at most its active particles, so cap = the
-// particle count always suffices.
-constexpr uint32_t kSplitStream = 4096;
-constexpr uint32_t kSplitWork = 32u * 4096u;
-
-__global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
-                                  const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
-                                  int4* __restrict__ items, int cap, DevScalars* __restrict__ ds)
-{
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nWarps = (gridDim.x * blockDim.x) >> 5;
-    for (int w = warp; w < nActive; w += nWarps)
-    {
-        const int leaf = leaves[w];
-        const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
-        const uint32_t S = jstream[leaf];
-        const int gsize = S <= kSplitStream ? 32 : max(1, int(kSplitWork / S));
-        for (uint32_t g = p0; g < p1; g += 64)
-        {
-            const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            const uint32_t m0 = __ballot_sync(0xffffffffu, a0 < p1 && converged[a0] == 0);
-            const uint32_t m1 = __ballot_sync(0xffffffffu, a1 < p1 && converged[a1] == 0);
-            const int nAct = __popc(m0) + __popc(m1);
-            if (nAct == 0) continue;
-            const int whole = (nAct + 31) >> 5;
-            const int G = max(whole, (nAct + gsize - 1) / gsize);
-            const bool split = G > whole;
-            int base = 0;
-            if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            const int wnd = int((g - p0) >> 6);
-            for (int k = lane; k < G; k += 32)
-            {
-                const int idx = split ? base + k : cap - 1 - (base + k);
-                if (idx >= 0 && idx < cap) items[idx] = make_int4(leaf, (wnd << 16) | (k << 8) | G, int(m0), int(m1));
-            }
-        }
-    }
-}
-
-// One Newton iteration over the work items, taken dynamically (a persistent grid).
-//
-// A warp owns one group of a leaf.  Candidates stream through the group filter into the
-// ring (stream_pairs); every batch of up to 32 is then tested with j on the lanes: for each
-// group particle in turn, all lanes apply the exact FP64 test q^2 = r^2/h_i^2 < R^2 to their
-// candidate, and the accepted pairs are appended, particle-major, to the warp's record
-// buffer -- so each particle's records are contiguous and in ascending j.  The records are
-// then evaluated with one pair per lane (W, -q dW/dq - 3W), and each particle's owner lane
-// adds its own records in order.  Every lane works in all three phases whatever the
-// group's size or spatial spread, and each particle's sums still run over j in ascending
-// Hilbert index, the oracle's order, so the results agree with it bit for bit.
-template<bool Periodic>
-__global__ void __launch_bounds__(kThreads, 6)
+// One Newton iteration over the work items, taken dynamically by a persistent grid of
+// warps: each item's group sums come from density_group (plain FP64, bit for bit the
+// oracle's; or mixed), then the FP64 Newton-Raphson step of src/density_base.cu:294-333.
+// A warp whose group keeps an unconverged particle queues the leaf for the next
+// iteration (once per leaf), and flags the lists stale when an updated h outgrows the
+// radius its leaf's list covers.
+template<bool Periodic, bool Mixed>
+__global__ void __launch_bounds__(kThreads, Mixed ? 8 : 6)
 density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                   const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
@@ -106,139 +76,41 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
                   double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
                   int* __restrict__ leafNext, int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
 {
-    __shared__ double4 sRing[kWarpsPerBlock][kRing];
-    __shared__ double4 sGrp[kWarpsPerBlock][32];
-    __shared__ double sRecA[kWarpsPerBlock][kRec];
-    __shared__ double sRecB[kWarpsPerBlock][kRec];
+    __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
     double lx = 0, ly = 0, lz = 0;
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     unsigned long long pairs = 0, cand = 0;
-    double* recA = sRecA[wib];
-    double* recB = sRecB[wib];
 
     for (;;)
     {
-        int w = 0;
-        if (lane == 0) w = atomicAdd(&ds->workCounter[0], 1);
-        w = __shfl_sync(0xffffffffu, w, 0);
-        if (w >= nItems) break;
-        const int4 it = items[w < nHeavy ? w : cap - 1 - (w - nHeavy)];
-        const int leaf = it.x;
-        const int wnd = it.y >> 16, grp = (it.y >> 8) & 255, G = it.y & 255;
-        const uint32_t m0 = uint32_t(it.z), m1 = uint32_t(it.w);
-        const int nAct = __popc(m0) + __popc(m1);
-        const int ng = (grp + 1) * nAct / G - grp * nAct / G;
-        const uint32_t g0 = layout[leaf] + 64u * uint32_t(wnd);
-        const int slot = group_slot(m0, m1, nAct, grp, G, lane);
+        const int w = next_item(ds, nHeavy, nItems, cap);
+        if (w < 0) break;
+        const Item d = decode_item(items[w], layout);
+        const int leaf = d.leaf;
+        const int slot = group_slot(d.m0, d.m1, d.nAct, d.grp, d.G, lane);
         const bool mine = slot >= 0;
-        const uint32_t i = g0 + uint32_t(mine ? slot : 0);
+        const uint32_t i = d.g0 + uint32_t(mine ? slot : 0);
         const double4 pi = xyzh[i];
         const double hi = pi.w;
-        const double hinv2 = 1.0 / (hi * hi);
-        const double rs = kRadKernel * hi;
-        const double rmax = warp_max(mine ? rs : 0.0);
-        const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-        if (mine) sGrp[wib][lane] = make_double4(pi.x, pi.y, pi.z, hinv2);
-        __syncwarp();
-        double rhoi = 0.0, gradhi = 0.0;
-        unsigned int gp = 0, gc = 0;
-        const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
-        stream_pairs<false, false>(
-            sRing[wib], nullptr, nullptr, bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
-            [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-            [&](const double4* ring, const float4*, const int*, int head, int count) {
-                gc += count;
-                const double4 pj = ring[(head + (lane < count ? lane : 0)) & (kRing - 1)];
-                int nrec = 0, segStart = 0, segCount = 0;
-                auto flush = [&]() {
-                    __syncwarp();
-                    for (int r = lane; r < nrec; r += 32)
-                    {
-                        const double q2 = recA[r];
-                        const double q = sqrt(q2);
-                        double wk, dwk;
-                        sph_kernel(q2, q, wk, dwk);
-                        recA[r] = wk;
-                        recB[r] = -q * dwk - 3.0 * wk;
-                    }
-                    __syncwarp();
-                    for (int t = 0; t < segCount; ++t)
-                    {
-                        rhoi += recA[segStart + t];
-                        gradhi += recB[segStart + t];
-                    }
-                    gp += segCount;
-                    segCount = 0;
-                    nrec = 0;
-                    __syncwarp();
-                };
-                // four group particles per step: independent FP64 chains for the scheduler
-                for (int i0 = 0; i0 < ng; i0 += 4)
-                {
-                    if (nrec + 4 * 32 > kRec) flush();
-                    double q2u[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                    {
-                        const double4 g = sGrp[wib][min(i0 + u, 31)];
-                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
-                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                        q2u[u] = pair_r2(dx, dy, dz) * g.w;
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                    {
-                        const bool acc = lane < count && i0 + u < ng && q2u[u] < kRadK2;
-                        const uint32_t m = __ballot_sync(0xffffffffu, acc);
-                        const int c = __popc(m);
-                        if (acc) recA[nrec + __popc(m & lt)] = q2u[u];
-                        if (lane == i0 + u) { segStart = nrec; segCount = c; }
-                        nrec += c;
-                    }
-                }
-                if (nrec > 0) flush();
-            });
+        double rhoi, gradhi;
+        unsigned int gp, gc;
+        density_group<Periodic, Mixed>(sScr[wib], mine, d.ng, pi, lx, ly, lz, jOffset[leaf], jcount[leaf], jlist,
+                                       LayoutRanges{layout}, xyzh, rhoi, gradhi, gp, gc);
         bool stillActive = false;
         if (mine)
         {
             pairs += gp;
             cand += gc;
-            // Newton-Raphson step, src/density_base.cu:294-333
-            const double hi1 = 1.0 / hi;
-            const double hi31 = hi1 * hi1 * hi1;
-            const double hi41 = hi31 * hi1;
-            const double rho_i = rhoi * kCnormk * pmass * hi31;
-            const double grad_i = gradhi * kCnormk * pmass * hi41;
-            if (!(rho_i > 0.0))
-            {
-                rho[i] = 0.0;
-                gradh[i] = 0.0;
-                converged[i] = 0;
-                stillActive = true;
-            }
-            else
-            {
-                const double rhoh_i = pmass * (hfact * hi1) * (hfact * hi1) * (hfact * hi1);
-                const double funci = rhoh_i - rho_i;
-                const double dhdrhoi = -hi / (3.0 * rhoh_i);
-                const double omegai = 1.0 - dhdrhoi * grad_i;
-                const double safe = (omegai > 0.0) ? omegai : fabs(omegai + 1e-300);
-                const double hraw = hi - funci * dhdrhoi / safe;
-                double hnew;
-                if (hraw > 1.2 * hi) hnew = 1.2 * hi;
-                else if (hraw < 0.8 * hi) hnew = 0.8 * hi;
-                else hnew = hraw;
-                rho[i] = rho_i;
-                gradh[i] = grad_i;
-                reinterpret_cast<double*>(xyzh + i)[3] = hnew;
-                const int conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
-                converged[i] = conv;
-                stillActive = !conv;
-                if (!conv && hnew > listH[leaf]) ds->listStale = 1;
-            }
+            double ro, go, ho;
+            int conv;
+            stillActive = newton_step(rhoi, gradhi, hi, pmass, hfact, tolh, ro, go, ho, conv);
+            rho[i] = ro;
+            gradh[i] = go;
+            reinterpret_cast<double*>(xyzh + i)[3] = ho;
+            converged[i] = conv;
+            if (stillActive && ho > listH[leaf]) ds->listStale = 1;
         }
         const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
         if (still && lane == 0)
@@ -277,8 +149,201 @@ __device__ inline double xi_limiter(const double g[9])
     return (fac + trS > 2.220446049250313e-16) ? fac / (fac + trS) : 1.0;
 }
 
-// Post-convergence sweep (src/density_base.cu:529-714): rho, gradh at the converged h,
-// div v, the xi limiter and d(div v)/dt, for every live particle.
+// The sums of the post-convergence sweep for one particle (src/density_base.cu:529-714),
+// added pair by pair in ascending j, and the finish: rho, gradh at the converged h, div v,
+// the xi limiter and d(div v)/dt.
+struct GradSums
+{
+    double rhoi = 0.0, gradhi = 0.0, divs = 0.0;
+    double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, da[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double rxx = 0, rxy = 0, rxz = 0, ryy = 0, ryz = 0, rzz = 0;
+    unsigned int gp = 0;
+
+    // One pair: separation (dx, dy, dz) at the nearest image, r^2 and q^2 = r^2 / h_i^2.
+    __device__ __forceinline__ void add(double dx, double dy, double dz, double r2, double q2, const double4& vi,
+                                        const double4& ai, const double4& vj, const double4& aj, double pm)
+    {
+        ++gp;
+        const double q = sqrt(q2);
+        double wk, dwk;
+        sph_kernel(q2, q, wk, dwk);
+        rhoi += wk;
+        gradhi += -q * dwk - 3.0 * wk;
+        const double rij = sqrt(r2);
+        const double rij1 = 1.0 / (rij + 2.220446049250313e-16);
+        const double rg = rij1 * dwk;
+        const double rx = dx * rg * pm, ry = dy * rg * pm, rz = dz * rg * pm;
+        const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+        divs += dvx * rx + dvy * ry + dvz * rz;
+        dv[0] += dvx * rx; dv[1] += dvx * ry; dv[2] += dvx * rz;
+        dv[3] += dvy * rx; dv[4] += dvy * ry; dv[5] += dvy * rz;
+        dv[6] += dvz * rx; dv[7] += dvz * ry; dv[8] += dvz * rz;
+        const double dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
+        da[0] += dax * rx; da[1] += dax * ry; da[2] += dax * rz;
+        da[3] += day * rx; da[4] += day * ry; da[5] += day * rz;
+        da[6] += daz * rx; da[7] += daz * ry; da[8] += daz * rz;
+        rxx -= dx * rx; rxy -= dx * ry; rxz -= dx * rz;
+        ryy -= dy * ry; ryz -= dy * rz; rzz -= dz * rz;
+    }
+
+    __device__ __forceinline__ void finish(uint32_t i, double hi, double pm, double* __restrict__ rho,
+                                           double* __restrict__ gradh, double* __restrict__ divv,
+                                           double* __restrict__ xiOut, double* __restrict__ ddivvdt) const
+    {
+        const double hi1 = 1.0 / hi;
+        const double hi31 = hi1 * hi1 * hi1;
+        const double hi41 = hi31 * hi1;
+        const double rho_i = rhoi * kCnormk * pm * hi31;
+        const double grad_i = gradhi * kCnormk * pm * hi41;
+        rho[i] = rho_i;
+        gradh[i] = grad_i;
+        if (!(rho_i > 0.0))
+        {
+            divv[i] = 0.0; ddivvdt[i] = 0.0; xiOut[i] = 1.0;
+            return;
+        }
+        const double omega = 1.0 + (hi / (3.0 * rho_i)) * grad_i;
+        const double omega_inv = (omega > 0.0) ? (1.0 / omega) : 1.0;
+        const double term = kCnormk * omega_inv * hi41 / rho_i;
+        const double denom = rxx * ryy * rzz + 2.0 * rxy * rxz * ryz - rxx * ryz * ryz - ryy * rxz * rxz
+                             - rzz * rxy * rxy;
+        const double rm0 = ryy * rzz - ryz * ryz;
+        const double rm1 = rxz * ryz - rzz * rxy;
+        const double rm2 = rxy * ryz - rxz * ryy;
+        const double rm3 = rzz * rxx - rxz * rxz;
+        const double rm4 = rxy * rxz - rxx * ryz;
+        const double rm5 = rxx * ryy - rxy * rxy;
+        divv[i] = -divs * term;
+        double gm[9], div_a;
+        if (fabs(denom) > 2.2250738585072014e-308)
+        {
+            const double dd = 1.0 / denom;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                const double sx = dv[3 * r], sy = dv[3 * r + 1], sz = dv[3 * r + 2];
+                gm[3 * r]     = -(sx * rm0 + sy * rm1 + sz * rm2) * dd;
+                gm[3 * r + 1] = -(sx * rm1 + sy * rm3 + sz * rm4) * dd;
+                gm[3 * r + 2] = -(sx * rm2 + sy * rm4 + sz * rm5) * dd;
+            }
+            double diag = 0.0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                const double sx = da[3 * r], sy = da[3 * r + 1], sz = da[3 * r + 2];
+                const double gx = (sx * rm0 + sy * rm1 + sz * rm2) * dd;
+                const double gy = (sx * rm1 + sy * rm3 + sz * rm4) * dd;
+                const double gz = (sx * rm2 + sy * rm4 + sz * rm5) * dd;
+                diag += (r == 0) ? gx : ((r == 1) ? gy : gz);
+            }
+            div_a = -diag;
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) gm[c] = -dv[c] * term;
+            div_a = -term * (da[0] + da[4] + da[8]);
+        }
+        xiOut[i] = xi_limiter(gm);
+        ddivvdt[i] = div_a - (gm[0] * gm[0] + gm[4] * gm[4] + gm[8] * gm[8]
+                              + 2.0 * (gm[1] * gm[3] + gm[2] * gm[6] + gm[5] * gm[7]));
+    }
+};
+
+// Post-convergence sweep, first pass: every live particle's gather row at its converged
+// h -- the j with q^2 = r^2 / h_i^2 < R^2 (the exact test of the sweep), ascending.
+template<bool Periodic>
+__global__ void __launch_bounds__(kThreads)
+gather_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
+                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
+                   const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
+                   int* __restrict__ nbl, int* __restrict__ nblCount, DevScalars* __restrict__ ds)
+{
+    __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
+    for (;;)
+    {
+        const int w = next_item(ds, nHeavy, nItems, cap);
+        if (w < 0) break;
+        const Item d = decode_item(items[w], layout);
+        const int slot = group_slot(d.m0, d.m1, d.nAct, d.grp, d.G, lane);
+        const bool mine = slot >= 0;
+        const uint32_t i = d.g0 + uint32_t(mine ? slot : 0);
+        const double4 pi = xyzh[i];
+        const double hinv2 = 1.0 / (pi.w * pi.w);
+        const double rs = kRadKernel * pi.w;
+        const double rmax = warp_max(mine ? rs : 0.0);
+        const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
+        int rowLen = 0;
+        rows_group(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), bx, jOffset[d.leaf], jcount[d.leaf],
+                   jlist, LayoutRanges{layout}, xyzh,
+                   [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+                   [&](const double4& g, const double4& pj) {
+                       double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                       return pair_r2(dx, dy, dz) * g.w < kRadK2;
+                   },
+                   mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
+        if (mine) nblCount[i] = rowLen;
+    }
+}
+
+// Post-convergence sweep, second pass: one lane per live particle over its row, the
+// exact test and the sums in the row's (ascending) order -- the same pairs and order as
+// the group sweep, so the results agree with it bit for bit.  Overflowed rows are left
+// to gradient_kernel.
+template<bool Periodic>
+__global__ void __launch_bounds__(kThreads)
+gradient_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict__ nblCount,
+                    const double4* __restrict__ xyzh, const double4* __restrict__ vel4,
+                    const double4* __restrict__ acc4, double* __restrict__ rho, double* __restrict__ gradh,
+                    double* __restrict__ divv, double* __restrict__ xiOut, double* __restrict__ ddivvdt,
+                    double pmass, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
+{
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    unsigned long long pairs = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nAlive; i += gridDim.x * blockDim.x)
+    {
+        const int cnt = nblCount[i];
+        if (unsigned(cnt) > unsigned(kNbl)) continue;
+        const double4 pi = xyzh[i];
+        const double4 vi = vel4[i];
+        const double4 ai = acc4[i];
+        const double hi = pi.w;
+        const double hinv2 = 1.0 / (hi * hi);
+        const int* row = nbl + size_t(i) * kNbl;
+        GradSums g;
+        auto pair = [&](int j) {
+            const double4 pj = ldg4(xyzh + j);
+            double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+            const double r2 = pair_r2(dx, dy, dz);
+            const double q2 = r2 * hinv2;
+            if (!(q2 < kRadK2)) return;
+            g.add(dx, dy, dz, r2, q2, vi, ai, ldg4(vel4 + j), ldg4(acc4 + j), pmass);
+        };
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4)
+        {
+            const int4 q = *reinterpret_cast<const int4*>(row + k);
+            pair(q.x); pair(q.y); pair(q.z); pair(q.w);
+        }
+        for (; k < cnt; ++k) pair(row[k]);
+        pairs += g.gp;
+        g.finish(uint32_t(i), hi, pmass, rho, gradh, divv, xiOut, ddivvdt);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&ds->pairs[1], pairs);
+}
+
+// Post-convergence sweep over the group path (src/density_base.cu:529-714) for the
+// particles whose rows overflowed (nblCount > kNbl), or for all live ones when nblCount is
+// null: rho, gradh at the converged h, div v, the xi limiter and d(div v)/dt.
 template<bool Periodic>
 __global__ void __launch_bounds__(kThreads)
 gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __restrict__ jOffset,
@@ -286,7 +351,8 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                 const double4* __restrict__ xyzh, const double4* __restrict__ vel4,
                 const double4* __restrict__ acc4, double* __restrict__ rho, double* __restrict__ gradh,
                 double* __restrict__ divv, double* __restrict__ xiOut, double* __restrict__ ddivvdt,
-                double pmass, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
+                double pmass, const DevBox* __restrict__ box, const int* __restrict__ nblCount,
+                DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
     __shared__ float4 sRingF[kWarpsPerBlock][kRing];
@@ -299,14 +365,15 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     unsigned long long pairs = 0;
     const double pm = pmass;
+    auto wanted = [&](uint32_t a) { return nblCount == nullptr || unsigned(nblCount[a]) > unsigned(kNbl); };
     for (int leaf = warpGlobal; leaf < nL; leaf += nWarps)
     {
         const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
         const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
         for (uint32_t g = p0; g < p1; g += 64)
         {
-            const uint32_t m0 = __ballot_sync(0xffffffffu, g + lane < p1);
-            const uint32_t m1 = __ballot_sync(0xffffffffu, g + 32 + lane < p1);
+            const uint32_t m0 = __ballot_sync(0xffffffffu, g + lane < p1 && wanted(g + lane));
+            const uint32_t m1 = __ballot_sync(0xffffffffu, g + 32 + lane < p1 && wanted(g + 32 + lane));
             const int nAct = __popc(m0) + __popc(m1);
             const int G = (nAct + 31) >> 5;
             for (int grp = 0; grp < G; ++grp)
@@ -322,10 +389,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
             const double rs = kRadKernel * hi;
             const double rmax = warp_max(mine ? rs : 0.0);
             const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-            double rhoi = 0.0, gradhi = 0.0, divs = 0.0;
-            double dv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, da[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            double rxx = 0, rxy = 0, rxz = 0, ryy = 0, ryz = 0, rzz = 0;
-            unsigned int gp = 0;
+            GradSums gs;
             const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
             const double rm = rs + fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0);
             const float tf = __double2float_ru(rm * rm * (1.0 + 1e-6));
@@ -342,90 +406,12 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
                     const double r2 = pair_r2(dx, dy, dz);
                     const double q2 = r2 * hinv2;
                     if (!(q2 < kRadK2)) return;
-                    ++gp;
-                    const double q = sqrt(q2);
-                    double wk, dwk;
-                    sph_kernel(q2, q, wk, dwk);
-                    rhoi += wk;
-                    gradhi += -q * dwk - 3.0 * wk;
-                    const double rij = sqrt(r2);
-                    const double rij1 = 1.0 / (rij + 2.220446049250313e-16);
-                    const double rg = rij1 * dwk;
-                    const double rx = dx * rg * pm, ry = dy * rg * pm, rz = dz * rg * pm;
-                    const double4 vj = ldg4(vel4 + j);
-                    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
-                    divs += dvx * rx + dvy * ry + dvz * rz;
-                    dv[0] += dvx * rx; dv[1] += dvx * ry; dv[2] += dvx * rz;
-                    dv[3] += dvy * rx; dv[4] += dvy * ry; dv[5] += dvy * rz;
-                    dv[6] += dvz * rx; dv[7] += dvz * ry; dv[8] += dvz * rz;
-                    const double4 aj = ldg4(acc4 + j);
-                    const double dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
-                    da[0] += dax * rx; da[1] += dax * ry; da[2] += dax * rz;
-                    da[3] += day * rx; da[4] += day * ry; da[5] += day * rz;
-                    da[6] += daz * rx; da[7] += daz * ry; da[8] += daz * rz;
-                    rxx -= dx * rx; rxy -= dx * ry; rxz -= dx * rz;
-                    ryy -= dy * ry; ryz -= dy * rz; rzz -= dz * rz;
+                    gs.add(dx, dy, dz, r2, q2, vi, ai, ldg4(vel4 + j), ldg4(acc4 + j), pm);
                   });
                 });
             if (!mine) continue;
-            pairs += gp;
-            const double hi1 = 1.0 / hi;
-            const double hi31 = hi1 * hi1 * hi1;
-            const double hi41 = hi31 * hi1;
-            const double rho_i = rhoi * kCnormk * pm * hi31;
-            const double grad_i = gradhi * kCnormk * pm * hi41;
-            rho[i] = rho_i;
-            gradh[i] = grad_i;
-            if (!(rho_i > 0.0))
-            {
-                divv[i] = 0.0; ddivvdt[i] = 0.0; xiOut[i] = 1.0;
-                continue;
-            }
-            const double omega = 1.0 + (hi / (3.0 * rho_i)) * grad_i;
-            const double omega_inv = (omega > 0.0) ? (1.0 / omega) : 1.0;
-            const double term = kCnormk * omega_inv * hi41 / rho_i;
-            const double denom = rxx * ryy * rzz + 2.0 * rxy * rxz * ryz - rxx * ryz * ryz - ryy * rxz * rxz
-                                 - rzz * rxy * rxy;
-            const double rm0 = ryy * rzz - ryz * ryz;
-            const double rm1 = rxz * ryz - rzz * rxy;
-            const double rm2 = rxy * ryz - rxz * ryy;
-            const double rm3 = rzz * rxx - rxz * rxz;
-            const double rm4 = rxy * rxz - rxx * ryz;
-            const double rm5 = rxx * ryy - rxy * rxy;
-            divv[i] = -divs * term;
-            double gm[9], div_a;
-            if (fabs(denom) > 2.2250738585072014e-308)
-            {
-                const double dd = 1.0 / denom;
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-                {
-                    const double sx = dv[3 * r], sy = dv[3 * r + 1], sz = dv[3 * r + 2];
-                    gm[3 * r]     = -(sx * rm0 + sy * rm1 + sz * rm2) * dd;
-                    gm[3 * r + 1] = -(sx * rm1 + sy * rm3 + sz * rm4) * dd;
-                    gm[3 * r + 2] = -(sx * rm2 + sy * rm4 + sz * rm5) * dd;
-                }
-                double diag = 0.0;
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-                {
-                    const double sx = da[3 * r], sy = da[3 * r + 1], sz = da[3 * r + 2];
-                    const double gx = (sx * rm0 + sy * rm1 + sz * rm2) * dd;
-                    const double gy = (sx * rm1 + sy * rm3 + sz * rm4) * dd;
-                    const double gz = (sx * rm2 + sy * rm4 + sz * rm5) * dd;
-                    diag += (r == 0) ? gx : ((r == 1) ? gy : gz);
-                }
-                div_a = -diag;
-            }
-            else
-            {
-#pragma unroll
-                for (int c = 0; c < 9; ++c) gm[c] = -dv[c] * term;
-                div_a = -term * (da[0] + da[4] + da[8]);
-            }
-            xiOut[i] = xi_limiter(gm);
-            ddivvdt[i] = div_a - (gm[0] * gm[0] + gm[4] * gm[4] + gm[8] * gm[8]
-                                  + 2.0 * (gm[1] * gm[3] + gm[2] * gm[6] + gm[5] * gm[7]));
+            pairs += gs.gp;
+            gs.finish(i, hi, pm, rho, gradh, divv, xiOut, ddivvdt);
             }
         }
     }
@@ -466,15 +452,6 @@ int grid_for(const State& s, int work)
     return std::max(1, std::min(maxBlocks, iceil(work, kWarpsPerBlock)));
 }
 
-// A persistent grid: as many blocks of the kernel as fit on the device at once.
-template<class K>
-int persistent_grid(const State& s, K kernel)
-{
-    int perSM = 0;
-    COSMO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, 0));
-    return std::max(1, perSM) * s.numSMs;
-}
-
 } // namespace
 
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh, double hfact,
@@ -504,6 +481,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.leafNext.resize(nL, s.st);
     const int itemCap = std::max(s.nAlive, 1);
     s.items.resize(itemCap, s.st);
+
     COSMO_CUDA(cudaMemcpyAsync(s.activeA.get(), s.allLeaves.get(), size_t(nL) * 4, cudaMemcpyDeviceToDevice, s.st));
     int nActiveLeaves = nL;
     long long nActiveParticles = s.nAlive;
@@ -525,12 +503,6 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
             listsValid = listsWidened = true;
         }
         cudaEvent_t j1 = ev(s);
-        if (s.precision == 1)
-        {
-            COSMO_CUDA(cudaMemsetAsync(&ds->nextActive, 0, 3 * sizeof(int), s.st));
-            launch_density_mixed(s, nActiveLeaves, pmass, tolh, hfact);
-        }
-        else
         {
             begin_iteration_kernel<<<std::min(iceil(nL, 256), 4 * s.numSMs), 256, 0, s.st>>>(ds, s.leafNext.get(),
                                                                                             nL);
@@ -539,8 +511,10 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(), s.items.get(),
                 itemCap, ds);
             COSMO_LAUNCHED();
-            auto nr = s.periodic ? density_nr_kernel<true> : density_nr_kernel<false>;
-            nr<<<persistent_grid(s, nr), kThreads, 0, s.st>>>(
+            const bool mx = s.precision == 1;
+            auto nr = mx ? (s.periodic ? density_nr_kernel<true, true> : density_nr_kernel<false, true>)
+                         : (s.periodic ? density_nr_kernel<true, false> : density_nr_kernel<false, false>);
+            nr<<<persistent_grid(s, nr, kThreads), kThreads, 0, s.st>>>(
                 s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
                 s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
                 s.leafNext.get(), s.activeB.get(), ds);
@@ -603,16 +577,35 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         const int grid = grid_for(s, nL);
         if (s.precision == 1)
             launch_gradient_mixed(s, pmass);
-        else if (s.periodic)
-            gradient_kernel<true><<<grid, kThreads, 0, s.st>>>(
-                nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.vel4.get(),
-                s.acc4.get(), s.rho.get(), s.gradh.get(), s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass,
-                s.box.get(), ds);
         else
-            gradient_kernel<false><<<grid, kThreads, 0, s.st>>>(
-                nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.vel4.get(),
-                s.acc4.get(), s.rho.get(), s.gradh.get(), s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass,
-                s.box.get(), ds);
+        {
+            // rows at the converged h, then one lane per particle over its row; the group
+            // sweep covers only the rows that overflowed
+            const int nA = std::max(s.nAlive, 1);
+            s.items.resize(nA, s.st);
+            s.nbl.resize(size_t(nA) * kNbl, s.st);
+            s.nblCount.resize(nA, s.st);
+            begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
+            COSMO_LAUNCHED();
+            plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
+                                                            s.items.get(), nA, ds);
+            COSMO_LAUNCHED();
+            auto rows = s.periodic ? gather_rows_kernel<true> : gather_rows_kernel<false>;
+            rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
+                s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+                s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
+            COSMO_LAUNCHED();
+            auto gr = s.periodic ? gradient_row_kernel<true> : gradient_row_kernel<false>;
+            gr<<<std::max(1, std::min(iceil(s.nAlive, kThreads), 8 * s.numSMs)), kThreads, 0, s.st>>>(
+                s.nAlive, s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.vel4.get(), s.acc4.get(), s.rho.get(),
+                s.gradh.get(), s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass, s.box.get(), ds);
+            COSMO_LAUNCHED();
+            auto gk = s.periodic ? gradient_kernel<true> : gradient_kernel<false>;
+            gk<<<grid, kThreads, 0, s.st>>>(nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
+                                            s.xyzh.get(), s.vel4.get(), s.acc4.get(), s.rho.get(), s.gradh.get(),
+                                            s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass, s.box.get(),
+                                            s.nblCount.get(), ds);
+        }
         COSMO_LAUNCHED();
         if (n > s.nAlive)
         {

@@ -8,7 +8,9 @@
 #include <algorithm>
 
 #include "pairstream.cuh"
+#include "rows.cuh"
 #include "state.hpp"
+#include "workitems.cuh"
 
 namespace cosmo {
 
@@ -43,6 +45,130 @@ __global__ void force_prep_kernel(const double4* __restrict__ xyzh, const double
                             kCnormk * oinv * h4 / rho);
 }
 
+// The i-side quantities of one particle and its force sums.
+struct ForceAcc
+{
+    double4 p, v, t, a, b;      // xyzh, vel4, thermo4, prepA, prepB of i
+    double itx = 0, ity = 0, itz = 0, jtx = 0, jty = 0, jtz = 0;
+    double f4s = 0.0, vsm = 0.0, divs = 0.0;
+    unsigned int gp = 0;
+
+    __device__ __forceinline__ void load(uint32_t i, const double4* __restrict__ xyzh,
+                                         const double4* __restrict__ vel4, const double4* __restrict__ thermo4,
+                                         const double4* __restrict__ prepA, const double4* __restrict__ prepB)
+    {
+        p = xyzh[i]; v = vel4[i]; t = thermo4[i]; a = prepA[i]; b = prepB[i];
+    }
+
+    // One pair with j (src/force.cu:232-383): the exact tests dr^2 > 0 and
+    // dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10), then the i-side and j-side terms.
+    template<bool Periodic, bool Disc>
+    __device__ __forceinline__ void add(const double4& pj, int j, const double4* __restrict__ vel4,
+                                        const double4* __restrict__ thermo4, const double4* __restrict__ prepA,
+                                        const double4* __restrict__ prepB, double lx, double ly, double lz,
+                                        double pm, double beta, int pdv, int shock)
+    {
+        double dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
+        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+        const double dr2 = pair_r2(dx, dy, dz);
+        if (!(dr2 > 0.0)) return;
+        const double hi = p.w, hj = pj.w;
+        if (dr2 >= kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10)) return;
+        const double pro2i = t.x, vwavei = t.y, alphai = t.z, eni = t.w;
+        const double hsqinvi = a.x, hinvi = a.y, rhoi = a.z, rho1i = a.w;
+        const double grkfaci = b.x, pri = b.y, autermi = b.z;
+        const double4 aj = ldg4(prepA + j);
+        const double qi2 = dr2 * hsqinvi;
+        const double qj2 = dr2 * aj.x;
+        const double dr = sqrt(dr2);
+        const double rij1 = 1.0 / dr;
+        const double rx = dx * rij1, ry = dy * rij1, rz = dz * rij1;
+        const double4 vj = ldg4(vel4 + j);
+        const double dvx = v.x - vj.x, dvy = v.y - vj.y, dvz = v.z - vj.z;
+        const double projv = dvx * rx + dvy * ry + dvz * rz;
+        const double4 tj = ldg4(thermo4 + j);
+        const double4 bj = ldg4(prepB + j);
+        const double rhoj = aj.z, rho1j = aj.w, pro2j = tj.x;
+        const double vwavej = tj.y, alphaj = tj.z, enj = tj.w;
+        const double prj = bj.y, autermj = bj.z;
+        const double vsigi = fmax(vwavei - beta * projv, 0.0);
+        const double vsigavi = fmax(alphai * vwavei - beta * projv, 0.0);
+        const double vsigj = fmax(vwavej - beta * projv, 0.0);
+        const double vsigavj = fmax(alphaj * vwavej - beta * projv, 0.0);
+        const double pvs = fmax(vsigi, vsigj);
+        double qr2i = 0.0, qr2j = 0.0;
+        const double denij = eni - enj;
+        const double vsigu = sqrt(fabs(pri - prj) * (2.0 / (rhoi + rhoj)));
+        if (Disc)
+        {
+            const double hori = hi * rij1, horj = hj * rij1;
+            if (projv < 0.0)
+            {
+                qr2i = -0.5 * rho1i * (alphai * vwavei - beta * projv) * hori * projv;
+                qr2j = -0.5 * rho1j * (alphaj * vwavej - beta * projv) * horj * projv;
+            }
+            else
+            {
+                qr2i = -0.5 * rho1i * alphai * vwavei * hori * projv;
+                qr2j = -0.5 * rho1j * alphaj * vwavej * horj * projv;
+            }
+        }
+        else if (projv < 0.0)
+        {
+            qr2i = -0.5 * rho1i * vsigavi * projv;
+            qr2j = -0.5 * rho1j * vsigavj * projv;
+        }
+        bool took = false;
+        if (qi2 < kRadK2)
+        {
+            took = true;
+            vsm = fmax(vsm, pvs);
+            double wk, dwk;
+            const double q = dr * hinvi;
+            sph_kernel(qi2, q, wk, dwk);
+            divs += pm * dwk * projv;
+            const double gki = dwk * grkfaci;
+            const double gpi = pm * (pro2i + qr2i) * gki;
+            itx += -gpi * rx; ity += -gpi * ry; itz += -gpi * rz;
+            const double pdvi = pm * pro2i * projv * gki;
+            const double dissi = Disc ? -0.5 * pm * rho1i * alphai * vwavei * (hi * rij1) * projv * projv * gki
+                                      : pm * qr2i * projv * gki;
+            const double condi = vsigu * denij * autermi * gki;
+            if (pdv) f4s += pdvi;
+            if (shock) f4s += dissi;
+            f4s += condi;
+        }
+        if (qj2 < kRadK2)
+        {
+            took = true;
+            vsm = fmax(vsm, pvs);
+            double wk, dwk;
+            const double q = dr * aj.y;
+            sph_kernel(qj2, q, wk, dwk);
+            const double gkj = dwk * bj.x;
+            const double gpj = pm * (pro2j + qr2j) * gkj;
+            jtx -= gpj * rx; jty -= gpj * ry; jtz -= gpj * rz;
+            f4s += vsigu * denij * autermj * gkj;
+        }
+        if (took) ++gp;
+    }
+
+    __device__ __forceinline__ void store(uint32_t i, double* __restrict__ fx, double* __restrict__ fy,
+                                          double* __restrict__ fz, double* __restrict__ f4,
+                                          double* __restrict__ vsigmax, double* __restrict__ divvF) const
+    {
+        fx[i] = itx + jtx;
+        fy[i] = ity + jty;
+        fz[i] = itz + jtz;
+        f4[i] = f4s;
+        vsigmax[i] = vsm;
+        divvF[i] = -divs * b.w;
+    }
+};
+
+// Force pass over the group path (one warp per i-leaf, the symmetric list streamed in
+// ascending j) for the particles whose rows overflowed (nblCount > kNbl), or for all when
+// nblCount is null.
 template<bool Periodic, bool Disc>
 __global__ void __launch_bounds__(kThreads)
 force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __restrict__ jOffset,
@@ -51,7 +177,8 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
              const double4* __restrict__ prepA, const double4* __restrict__ prepB, double* __restrict__ fx,
              double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ f4,
              double* __restrict__ vsigmax, double* __restrict__ divvF, double pmass, double beta, int pdv,
-             int shock, const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
+             int shock, const DevBox* __restrict__ box, const int* __restrict__ nblCount,
+             DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
     __shared__ float4 sRingF[kWarpsPerBlock][kRing];
@@ -64,14 +191,15 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     unsigned long long pairs = 0;
     const double pm = pmass;
+    auto wanted = [&](uint32_t a) { return nblCount == nullptr || !row_ok(nblCount, a); };
     for (int leaf = warpGlobal; leaf < nL; leaf += nWarps)
     {
         const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
         const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
         for (uint32_t g = p0; g < p1; g += 64)
         {
-          const uint32_t m0 = __ballot_sync(0xffffffffu, g + lane < p1);
-          const uint32_t m1 = __ballot_sync(0xffffffffu, g + 32 + lane < p1);
+          const uint32_t m0 = __ballot_sync(0xffffffffu, g + lane < p1 && wanted(g + lane));
+          const uint32_t m1 = __ballot_sync(0xffffffffu, g + 32 + lane < p1 && wanted(g + 32 + lane));
           const int nAct = __popc(m0) + __popc(m1);
           const int G = (nAct + 31) >> 5;
           for (int grp = 0; grp < G; ++grp)
@@ -79,24 +207,14 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
             const int slot = group_slot(m0, m1, nAct, grp, G, lane);
             const bool mine = slot >= 0;
             const uint32_t i = g + uint32_t(mine ? slot : 0);
-            const uint32_t ii = i;
-            const double4 pi = xyzh[ii];
-            const double4 vi = vel4[ii];
-            const double4 ti = thermo4[ii];
-            const double4 ai = prepA[ii];
-            const double4 bi = prepB[ii];
-            const double hi = pi.w;
-            const double pro2i = ti.x, vwavei = ti.y, alphai = ti.z, eni = ti.w;
-            const double hsqinvi = ai.x, hinvi = ai.y, rhoi = ai.z, rho1i = ai.w;
-            const double grkfaci = bi.x, pri = bi.y, autermi = bi.z;
-            double itx = 0, ity = 0, itz = 0, jtx = 0, jty = 0, jtz = 0;
-            double f4s = 0.0, vsm = 0.0, divs = 0.0;
-            unsigned int gp = 0;
+            ForceAcc A;
+            A.load(i, xyzh, vel4, thermo4, prepA, prepB);
+            const double hi = A.p.w;
             const double rg = kRadKernel * warp_max(mine ? hi : 0.0);
-            const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, 0.0, rg);
+            const GroupBox bx = group_box(mine, A.p.x, A.p.y, A.p.z, 0.0, rg);
             // float prefilter: r_f^2 <= (R max(h_i, h_j) (1 + 1e-5) + margin)^2; the exact
-            // tests (dr2 > 0, dr2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10)) run in the accept pass
-            const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
+            // tests run in the accept pass
+            const float xf = float(A.p.x - bx.cx), yf = float(A.p.y - bx.cy), zf = float(A.p.z - bx.cz);
             const float mf = __double2float_ru(fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0) +
                                                1e-6 * rg);
             const float hif = float(hi);
@@ -111,103 +229,99 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
                     return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= r * r;
                   },
                   [&](const double4& pj, const float4&, int j) {
-                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                    const double dr2 = pair_r2(dx, dy, dz);
-                    if (!(dr2 > 0.0)) return;
-                    const double hj = pj.w;
-                    if (dr2 >= kRadK2 * fmax(hi * hi, hj * hj) * (1.0 + 1e-10)) return;
-                    const double4 aj = ldg4(prepA + j);
-                    const double qi2 = dr2 * hsqinvi;
-                    const double qj2 = dr2 * aj.x;
-                    const double dr = sqrt(dr2);
-                    const double rij1 = 1.0 / dr;
-                    const double rx = dx * rij1, ry = dy * rij1, rz = dz * rij1;
-                    const double4 vj = ldg4(vel4 + j);
-                    const double dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
-                    const double projv = dvx * rx + dvy * ry + dvz * rz;
-                    const double4 tj = ldg4(thermo4 + j);
-                    const double4 bj = ldg4(prepB + j);
-                    const double rhoj = aj.z, rho1j = aj.w, pro2j = tj.x;
-                    const double vwavej = tj.y, alphaj = tj.z, enj = tj.w;
-                    const double prj = bj.y, autermj = bj.z;
-                    const double vsigi = fmax(vwavei - beta * projv, 0.0);
-                    const double vsigavi = fmax(alphai * vwavei - beta * projv, 0.0);
-                    const double vsigj = fmax(vwavej - beta * projv, 0.0);
-                    const double vsigavj = fmax(alphaj * vwavej - beta * projv, 0.0);
-                    const double pvs = fmax(vsigi, vsigj);
-                    double qr2i = 0.0, qr2j = 0.0;
-                    const double denij = eni - enj;
-                    const double vsigu = sqrt(fabs(pri - prj) * (2.0 / (rhoi + rhoj)));
-                    if (Disc)
-                    {
-                        const double hori = hi * rij1, horj = hj * rij1;
-                        if (projv < 0.0)
-                        {
-                            qr2i = -0.5 * rho1i * (alphai * vwavei - beta * projv) * hori * projv;
-                            qr2j = -0.5 * rho1j * (alphaj * vwavej - beta * projv) * horj * projv;
-                        }
-                        else
-                        {
-                            qr2i = -0.5 * rho1i * alphai * vwavei * hori * projv;
-                            qr2j = -0.5 * rho1j * alphaj * vwavej * horj * projv;
-                        }
-                    }
-                    else if (projv < 0.0)
-                    {
-                        qr2i = -0.5 * rho1i * vsigavi * projv;
-                        qr2j = -0.5 * rho1j * vsigavj * projv;
-                    }
-                    bool took = false;
-                    if (qi2 < kRadK2)
-                    {
-                        took = true;
-                        vsm = fmax(vsm, pvs);
-                        double wk, dwk;
-                        const double q = dr * hinvi;
-                        sph_kernel(qi2, q, wk, dwk);
-                        divs += pm * dwk * projv;
-                        const double gki = dwk * grkfaci;
-                        const double gpi = pm * (pro2i + qr2i) * gki;
-                        itx += -gpi * rx; ity += -gpi * ry; itz += -gpi * rz;
-                        const double pdvi = pm * pro2i * projv * gki;
-                        const double dissi = Disc
-                            ? -0.5 * pm * rho1i * alphai * vwavei * (hi * rij1) * projv * projv * gki
-                            : pm * qr2i * projv * gki;
-                        const double condi = vsigu * denij * autermi * gki;
-                        if (pdv) f4s += pdvi;
-                        if (shock) f4s += dissi;
-                        f4s += condi;
-                    }
-                    if (qj2 < kRadK2)
-                    {
-                        took = true;
-                        vsm = fmax(vsm, pvs);
-                        double wk, dwk;
-                        const double q = dr * aj.y;
-                        sph_kernel(qj2, q, wk, dwk);
-                        const double gkj = dwk * bj.x;
-                        const double gpj = pm * (pro2j + qr2j) * gkj;
-                        jtx -= gpj * rx; jty -= gpj * ry; jtz -= gpj * rz;
-                        f4s += vsigu * denij * autermj * gkj;
-                    }
-                    if (took) ++gp;
+                    A.add<Periodic, Disc>(pj, j, vel4, thermo4, prepA, prepB, lx, ly, lz, pm, beta, pdv, shock);
                   });
                 });
             if (!mine) continue;
-            pairs += gp;
-            fx[i] = itx + jtx;
-            fy[i] = ity + jty;
-            fz[i] = itz + jtz;
-            f4[i] = f4s;
-            vsigmax[i] = vsm;
-            divvF[i] = -divs * bi.w;
+            pairs += A.gp;
+            A.store(i, fx, fy, fz, f4, vsigmax, divvF);
           }
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     if (lane == 0) atomicAdd(&ds->pairs[2], pairs);
+}
+
+// Symmetric rows: every live particle's j with dr^2 > 0 and
+// dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10) (the force pass's exact tests), ascending.
+template<bool Periodic>
+__global__ void __launch_bounds__(kThreads)
+sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
+                const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
+                const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
+                int* __restrict__ nbl, int* __restrict__ nblCount, DevScalars* __restrict__ ds)
+{
+    __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
+    for (;;)
+    {
+        const int w = next_item(ds, nHeavy, nItems, cap);
+        if (w < 0) break;
+        const Item d = decode_item(items[w], layout);
+        const int slot = group_slot(d.m0, d.m1, d.nAct, d.grp, d.G, lane);
+        const bool mine = slot >= 0;
+        const uint32_t i = d.g0 + uint32_t(mine ? slot : 0);
+        const double4 pi = xyzh[i];
+        const double rg = kRadKernel * warp_max(mine ? pi.w : 0.0);
+        const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, 0.0, rg);
+        int rowLen = 0;
+        rows_group(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, pi.w * pi.w), bx, jOffset[d.leaf],
+                   jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
+                   [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
+                   [&](const double4& g, const double4& pj) {
+                       double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                       const double dr2 = pair_r2(dx, dy, dz);
+                       return dr2 > 0.0 && !(dr2 >= kRadK2 * fmax(g.w, pj.w * pj.w) * (1.0 + 1e-10));
+                   },
+                   mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
+        if (mine) nblCount[i] = rowLen;
+    }
+}
+
+// Force pass over the rows: one lane per live particle, its row's pairs in ascending j --
+// the group pass's pairs and order, so the results agree with it bit for bit.
+template<bool Periodic, bool Disc>
+__global__ void __launch_bounds__(kThreads)
+force_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict__ nblCount,
+                 const double4* __restrict__ xyzh, const double4* __restrict__ vel4,
+                 const double4* __restrict__ thermo4, const double4* __restrict__ prepA,
+                 const double4* __restrict__ prepB, double* __restrict__ fx, double* __restrict__ fy,
+                 double* __restrict__ fz, double* __restrict__ f4, double* __restrict__ vsigmax,
+                 double* __restrict__ divvF, double pmass, double beta, int pdv, int shock,
+                 const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
+{
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    unsigned long long pairs = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nAlive; i += gridDim.x * blockDim.x)
+    {
+        if (!row_ok(nblCount, uint32_t(i))) continue;
+        const int cnt = nblCount[i];
+        ForceAcc A;
+        A.load(uint32_t(i), xyzh, vel4, thermo4, prepA, prepB);
+        const int* row = nbl + size_t(i) * kNbl;
+        auto pair = [&](int j) {
+            A.add<Periodic, Disc>(ldg4(xyzh + j), j, vel4, thermo4, prepA, prepB, lx, ly, lz, pmass, beta, pdv,
+                                  shock);
+        };
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4)
+        {
+            const int4 q = *reinterpret_cast<const int4*>(row + k);
+            pair(q.x); pair(q.y); pair(q.z); pair(q.w);
+        }
+        for (; k < cnt; ++k) pair(row[k]);
+        pairs += A.gp;
+        A.store(uint32_t(i), fx, fy, fz, f4, vsigmax, divvF);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&ds->pairs[2], pairs);
 }
 
 // Dead particles: no force (src/force.cu:191-200).
@@ -251,12 +365,41 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
                                           s.xyzh.get(), s.vel4.get(), s.thermo4.get(), s.prepA.get(),
                                           s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(),
                                           s.vsigmax.get(), s.divvF.get(), pmass, beta, pdv ? 1 : 0,
-                                          shock ? 1 : 0, s.box.get(), ds);
+                                          shock ? 1 : 0, s.box.get(), s.nblCount.get(), ds);
+    };
+    auto launchRows = [&](auto kern) {
+        kern<<<std::max(1, std::min(iceil(s.nAlive, kThreads), 8 * s.numSMs)), kThreads, 0, s.st>>>(
+            s.nAlive, s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.vel4.get(), s.thermo4.get(), s.prepA.get(),
+            s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(), s.vsigmax.get(), s.divvF.get(), pmass,
+            beta, pdv ? 1 : 0, shock ? 1 : 0, s.box.get(), ds);
     };
     if (s.precision == 1)
         launch_force_mixed(s, pmass, beta, disc, pdv, shock);
-    else
+    else if (nL > 0)
     {
+        // symmetric rows (cached with the symmetric lists), then one lane per particle over
+        // its row; the group pass covers only the rows that overflowed
+        if (s.rowsToken != s.token)
+        {
+            const int nA = std::max(s.nAlive, 1);
+            s.items.resize(nA, s.st);
+            s.nbl.resize(size_t(nA) * kNbl, s.st);
+            s.nblCount.resize(nA, s.st);
+            begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
+            COSMO_LAUNCHED();
+            plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
+                                                            s.items.get(), nA, ds);
+            COSMO_LAUNCHED();
+            auto rows = s.periodic ? sym_rows_kernel<true> : sym_rows_kernel<false>;
+            rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
+                s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+                s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
+            COSMO_LAUNCHED();
+            s.rowsToken = s.token;
+        }
+        if (s.periodic) { if (disc) launchRows(force_row_kernel<true, true>); else launchRows(force_row_kernel<true, false>); }
+        else { if (disc) launchRows(force_row_kernel<false, true>); else launchRows(force_row_kernel<false, false>); }
+        COSMO_LAUNCHED();
         if (s.periodic) { if (disc) launch(force_kernel<true, true>); else launch(force_kernel<true, false>); }
         else { if (disc) launch(force_kernel<false, true>); else launch(force_kernel<false, false>); }
         COSMO_LAUNCHED();

@@ -26,137 +26,8 @@ constexpr int kThreads = 32 * kWarpsPerBlock;
 // q = sqrt(q2) for the FP32 path (q2 >= 0); exact 0 for the self pair.
 __device__ __forceinline__ float sqrt_f(float q2) { return q2 > 0.0f ? q2 * rsqrtf(q2) : 0.0f; }
 
-template<bool Periodic>
-__global__ void __launch_bounds__(kThreads)
-density_nr_mixed_kernel(const int* __restrict__ leaves, int nLeavesActive, const uint32_t* __restrict__ layout,
-                        const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
-                        const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
-                        double* __restrict__ gradh, int* __restrict__ converged, double pmass, double tolh,
-                        double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
-                        int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
-{
-    __shared__ double4 sRing[kWarpsPerBlock][kRing];
-    __shared__ float4 sRingF[kWarpsPerBlock][kRing];
-    __shared__ int sIdx[kWarpsPerBlock][kRing];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nWarps = (gridDim.x * blockDim.x) >> 5;
-    double lx = 0, ly = 0, lz = 0;
-    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
-    const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
-    unsigned long long pairs = 0, cand = 0;
-
-    for (int w = warpGlobal; w < nLeavesActive; w += nWarps)
-    {
-        const int leaf = leaves[w];
-        const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
-        const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
-        bool leafActive = false;
-        for (uint32_t g = p0; g < p1; g += 64)
-        {
-            const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            const bool act0 = a0 < p1 && converged[a0] == 0;
-            const bool act1 = a1 < p1 && converged[a1] == 0;
-            const uint32_t m0 = __ballot_sync(0xffffffffu, act0);
-            const uint32_t m1 = __ballot_sync(0xffffffffu, act1);
-            const int nAct = __popc(m0) + __popc(m1);
-            if (nAct == 0) continue;
-            const int G = (nAct + 31) >> 5;
-            for (int grp = 0; grp < G; ++grp)
-            {
-                const int slot = group_slot(m0, m1, nAct, grp, G, lane);
-                const bool mine = slot >= 0;
-                const uint32_t i = g + uint32_t(mine ? slot : 0);
-                const double4 pi = xyzh[i];
-                const double hi = pi.w;
-                const double rs = kRadKernel * hi;
-                const double rmax = warp_max(mine ? rs : 0.0);
-                const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-                const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
-                const float hinv2f = float(1.0 / (hi * hi));
-                KahanF sr, sg;
-                unsigned int gp = 0, gc = 0;
-                stream_pairs(
-                    sRing[wib], sRingF[wib], sIdx[wib], bx.cx, bx.cy, bx.cz, jb, nj, jlist, layout, xyzh,
-                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                    [&](const double4* ring, const float4* ringf, const int* ringIdx, int head, int count) {
-                        gc += count;
-                        two_pass(ring, ringf, ringIdx, head, count, mine,
-                                 [&](const float4& pf) {
-                                     return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) * hinv2f < float(kRadK2);
-                                 },
-                                 [&](const double4&, const float4& pf, int) {
-                                     const float q2 = r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) * hinv2f;
-                                     const float q = sqrt_f(q2);
-                                     float wk, dwk;
-                                     sph_kernel_f(q2, q, wk, dwk);
-                                     sr.add(wk);
-                                     sg.add(fmaf(-q, dwk, -3.0f * wk));
-                                     ++gp;
-                                 });
-                    });
-                bool stillActive = false;
-                if (mine)
-                {
-                    pairs += gp;
-                    cand += gc;
-                    // FP64 Newton-Raphson step on the FP64-combined sums
-                    const double rhoi = sr.value(), gradhi = sg.value();
-                    const double hi1 = 1.0 / hi;
-                    const double hi31 = hi1 * hi1 * hi1;
-                    const double hi41 = hi31 * hi1;
-                    const double rho_i = rhoi * kCnormk * pmass * hi31;
-                    const double grad_i = gradhi * kCnormk * pmass * hi41;
-                    if (!(rho_i > 0.0))
-                    {
-                        rho[i] = 0.0;
-                        gradh[i] = 0.0;
-                        converged[i] = 0;
-                        stillActive = true;
-                    }
-                    else
-                    {
-                        const double rhoh_i = pmass * (hfact * hi1) * (hfact * hi1) * (hfact * hi1);
-                        const double funci = rhoh_i - rho_i;
-                        const double dhdrhoi = -hi / (3.0 * rhoh_i);
-                        const double omegai = 1.0 - dhdrhoi * grad_i;
-                        const double safe = (omegai > 0.0) ? omegai : fabs(omegai + 1e-300);
-                        const double hraw = hi - funci * dhdrhoi / safe;
-                        double hnew;
-                        if (hraw > 1.2 * hi) hnew = 1.2 * hi;
-                        else if (hraw < 0.8 * hi) hnew = 0.8 * hi;
-                        else hnew = hraw;
-                        rho[i] = rho_i;
-                        gradh[i] = grad_i;
-                        reinterpret_cast<double*>(xyzh + i)[3] = hnew;
-                        const int conv = (fabs((hnew - hi) / hi) < tolh) ? 1 : 0;
-                        converged[i] = conv;
-                        stillActive = !conv;
-                        if (!conv && hnew > listH[leaf]) ds->listStale = 1;
-                    }
-                }
-                const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
-                if (still)
-                {
-                    leafActive = true;
-                    if (lane == 0) atomicAdd(&ds->unconverged, __popc(still));
-                }
-            }
-        }
-        if (leafActive && lane == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-    {
-        pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
-        cand += __shfl_xor_sync(0xffffffffu, cand, o);
-    }
-    if (lane == 0)
-    {
-        atomicAdd(&ds->pairs[0], pairs);
-        atomicAdd(&ds->pairs[3], cand);
-    }
-}
+// The Newton iteration's mixed form is density_nr_kernel<Periodic, true> (density.cu,
+// densengine.cuh); the gradient sweep and the force pass follow.
 
 __device__ inline double xi_limiter_m(const double g[9])
 {
@@ -511,20 +382,6 @@ int grid_for(const State& s, int work)
 }
 
 } // namespace
-
-void launch_density_mixed(State& s, int nActiveLeaves, double pmass, double tolh, double hfact)
-{
-    const int grid = grid_for(s, nActiveLeaves);
-    auto go = [&](auto kern) {
-        kern<<<grid, kThreads, 0, s.st>>>(s.activeA.get(), nActiveLeaves, s.layout.get(), s.jOffset.get(),
-                                          s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.rho.get(), s.gradh.get(),
-                                          s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
-                                          s.activeB.get(), s.dscal.get());
-    };
-    if (s.periodic) go(density_nr_mixed_kernel<true>);
-    else go(density_nr_mixed_kernel<false>);
-    COSMO_LAUNCHED();
-}
 
 void launch_gradient_mixed(State& s, double pmass)
 {

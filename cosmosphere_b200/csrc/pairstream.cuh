@@ -96,20 +96,49 @@ __device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v)
     return v;
 }
 
+// The particle range of a j-leaf: layout[leaf] .. layout[leaf + 1] for a single set,
+// or a table of (begin, end) pairs for a forest.
+struct LayoutRanges
+{
+    const uint32_t* __restrict__ layout;
+    __device__ __forceinline__ uint2 operator()(int leaf) const { return make_uint2(layout[leaf], layout[leaf + 1]); }
+};
+
+struct TableRanges
+{
+    const uint2* __restrict__ range;
+    __device__ __forceinline__ uint2 operator()(int leaf) const { return range[leaf]; }
+};
+
+// Signed offset of x from c at the nearest periodic image (L > 0), or plain (L == 0).
+__device__ __forceinline__ double image_offset(double x, double c, double L)
+{
+    double d = x - c;
+    if (L > 0.0)
+    {
+        if (d > 0.5 * L) d -= L;
+        else if (d < -0.5 * L) d += L;
+    }
+    return d;
+}
+
 // Stream the j particles of one i-leaf list through the group filter into the ring and
 // hand the survivors to batch(ring, ringf, ringIdx, head, count) in runs of up to 32, in
 // ascending j order, on every lane.  filter(pj) is evaluated by the loading lane only.
+// The ring keeps what the caller asks for: the FP64 xyzh (Dbl), an FP32 copy relative to
+// the group box centre at the nearest periodic image when lx, ly, lz > 0 (Float), and
+// the particle index (Index).
 //
 // Up to 32 list entries and their particle ranges are fetched at once, one per lane; a
 // warp prefix sum over the range lengths flattens them, so every load batch is 32
 // consecutive stream positions (each lane finds its particle by a 5-step binary search
 // over the prefix sums), and the next batch's loads are issued before the current batch
 // is filtered and evaluated.
-template<bool Float = true, bool Index = true, class Filter, class Batch>
-__device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
-                                             double cz, uint32_t jb, uint32_t nj, const int* __restrict__ jlist,
-                                             const uint32_t* __restrict__ layout,
-                                             const double4* __restrict__ xyzh, Filter filter, Batch batch)
+template<bool Dbl, bool Float, bool Index, class Ranges, class Filter, class Batch>
+__device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
+                                              double cz, double lx, double ly, double lz, uint32_t jb, uint32_t nj,
+                                              const int* __restrict__ jlist, Ranges ranges,
+                                              const double4* __restrict__ xyzh, Filter filter, Batch batch)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -126,9 +155,9 @@ __device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* 
         uint32_t s0 = 0, len = 0;
         if (lane < nb)
         {
-            const int leaf = jlist[jb + lb + lane];
-            s0 = layout[leaf];
-            len = layout[leaf + 1] - s0;
+            const uint2 r = ranges(jlist[jb + lb + lane]);
+            s0 = r.x;
+            len = r.y - r.x;
         }
         const uint32_t incl = warp_incl_scan_u32(len);
         const uint32_t excl = incl - len;
@@ -167,9 +196,10 @@ __device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* 
             if (pass)
             {
                 const int slot = (head + cnt + __popc(m & lt)) & (kRing - 1);
-                ring[slot] = pj;
+                if constexpr (Dbl) ring[slot] = pj;
                 if constexpr (Float)
-                    ringf[slot] = make_float4(float(pj.x - cx), float(pj.y - cy), float(pj.z - cz), float(pj.w));
+                    ringf[slot] = make_float4(float(image_offset(pj.x, cx, lx)), float(image_offset(pj.y, cy, ly)),
+                                              float(image_offset(pj.z, cz, lz)), float(pj.w));
                 if constexpr (Index) ringIdx[slot] = int(j);
             }
             cnt += __popc(m);
@@ -180,6 +210,18 @@ __device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* 
         }
     }
     if (cnt > 0) drain(cnt);
+}
+
+// stream_ranges over a single set's leaves, FP32 copies relative to the box centre
+// without periodic shift (the pair tests fold the images themselves).
+template<bool Float = true, bool Index = true, class Filter, class Batch>
+__device__ __forceinline__ void stream_pairs(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
+                                             double cz, uint32_t jb, uint32_t nj, const int* __restrict__ jlist,
+                                             const uint32_t* __restrict__ layout,
+                                             const double4* __restrict__ xyzh, Filter filter, Batch batch)
+{
+    stream_ranges<true, Float, Index>(ring, ringf, ringIdx, cx, cy, cz, 0.0, 0.0, 0.0, jb, nj, jlist,
+                                      LayoutRanges{layout}, xyzh, filter, batch);
 }
 
 // Two passes over one batch of up to 32 ring entries, for a lane's own particle:

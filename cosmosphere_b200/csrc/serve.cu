@@ -117,9 +117,9 @@ double now_s()
 }
 
 // Device bytes a new set of n particles is charged at admission (particle arrays, FP32
-// copies, tree and lists; about 500 B/particle measured on the lattice and Plummer sets),
+// copies, tree, lists and neighbour rows; about 1 KB/particle measured on the lattice and Plummer sets),
 // until its real footprint is known.
-constexpr long long kBytesPerParticle = 600;
+constexpr long long kBytesPerParticle = 1200;
 constexpr long long kBytesFixed = 1ll << 20;
 
 struct Request

@@ -91,7 +91,8 @@ struct DevScalars
     unsigned long long pairs[4]; // accepted pairs: density, gradient, force, candidates
     unsigned int sortTiles[16];  // onesweep tile tickets, one per digit pass
     int itemsHeavy, itemsLight;  // Newton work items of the current iteration (split, whole)
-    int pad[4];
+    int listParticles;           // particles of the current pass on their neighbour lists
+    int pad[3];
 };
 
 struct Timings
@@ -112,7 +113,7 @@ struct State
     double pmass = 0.0, hfact = 0.0;
     int periodic = 0;
     double boxHost[6] = {0, 0, 0, 0, 0, 0};
-    uint64_t token = 0, jlistToken = 0;
+    uint64_t token = 0, jlistToken = 0, rowsToken = 0;
     int itersRun = 0, maxIter = 100;
     int precision = 0;     // 0 plain FP64 (the drop-in form), 1 mixed FP32/FP64
     std::vector<long long> activePerIter;
@@ -145,6 +146,10 @@ struct State
     DBuf<double> listH;                         // h each leaf's gather list covers
     DBuf<int> jlist;
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
+    DBuf<int> nbl;                              // per-particle neighbour lists, kNbl per row
+    DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed; < 0: none)
+    DBuf<double> nblH;                          // largest h each row stays complete for
+    DBuf<int> listItems;                        // particles of a pass that use their rows
     DBuf<int> leafNext;                         // leaf already queued for the next iteration
     DBuf<int> activeA, activeB, allLeaves;
 
@@ -183,7 +188,6 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                          double hfact, int maxIter, bool withGradients);
 
 // mixed.cu
-void launch_density_mixed(State& s, int nActiveLeaves, double pmass, double tolh, double hfact);
 void launch_gradient_mixed(State& s, double pmass);
 void launch_force_mixed(State& s, double pmass, double beta, bool disc, bool pdv, bool shock);
 

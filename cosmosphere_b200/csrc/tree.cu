@@ -740,7 +740,7 @@ static void walk(State& s, bool fill, double margin)
                                         s.hmaxLeaf.get(), s.preCenter.get(), s.preHalf.get(), s.preSkip.get(),
                                         s.preLeaf.get(), s.hmaxPre.get(), s.box.get(), s.jcount.get(),
                                         s.jOffset.get(), s.jlist.get(), &s.dscal.get()->err, s.layout.get(),
-                                        (!fill && !Sym) ? s.jstream.get() : nullptr, margin,
+                                        !fill ? s.jstream.get() : nullptr, margin,
                                         (!fill && !Sym) ? s.listH.get() : nullptr);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);

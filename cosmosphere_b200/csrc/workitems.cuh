@@ -1,0 +1,153 @@
+/*
+ * workitems.cuh -- the dynamic work queue of the pair kernels.
+ *
+ * A pass over the leaves is cut into work items, one per group of up to 32 active
+ * particles of a leaf's 64-slot window; leaves whose j-stream is long are cut into smaller
+ * groups so that no single warp carries a pass's tail.  A persistent grid of warps takes
+ * items from a global counter.
+ */
+#pragma once
+
+#include "pairstream.cuh"
+#include "state.hpp"
+
+namespace cosmo {
+
+namespace {
+
+// Zero the per-iteration counters of the Newton work queue and the leaf re-queue flags.
+__global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restrict__ leafNext, int nL)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0)
+    {
+        ds->nextActive = 0;
+        ds->unconverged = 0;
+        ds->listStale = 0;
+        ds->workCounter[0] = 0;
+        ds->itemsHeavy = 0;
+        ds->itemsLight = 0;
+        ds->listParticles = 0;
+    }
+    for (int l = t; l < nL; l += gridDim.x * blockDim.x) leafNext[l] = 0;
+}
+
+// Work items of one pass: every group of a leaf's 64-slot window of active particles
+// (unconverged ones in a Newton iteration; all when converged is null, and all leaves
+// when leaves is null) is one item (leaf, window << 16 | group << 8 | groups, the two
+// halves of the window's active mask).  Groups hold up to 32 particles; a leaf whose
+// gather list streams more than kSplitStream particles is cut into smaller groups, about
+// kSplitWork / stream particles each, so that no single warp carries the iteration's
+// tail.  Cut items are queued from the front of the buffer and run first, whole groups
+// from the back.  The items of a window hold at most its active particles, so cap = the
+// particle count always suffices.
+//
+// With rows given (nblCount, nblH of the per-particle neighbour lists, K entries a row),
+// an active particle whose row is complete for its current h -- no overflow, h <= nblH --
+// goes to listItems instead (ds->listParticles of them) and out of the groups.
+constexpr uint32_t kSplitStream = 4096;
+constexpr uint32_t kSplitWork = 32u * 4096u;
+
+__global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
+                                  const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
+                                  int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
+                                  const int* __restrict__ nblCount = nullptr, const double* __restrict__ nblH = nullptr,
+                                  const double4* __restrict__ xyzh = nullptr, int K = 0,
+                                  int* __restrict__ listItems = nullptr)
+{
+    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
+    auto rowOK = [&](uint32_t a) {
+        return listItems != nullptr && unsigned(nblCount[a]) <= unsigned(K) && xyzh[a].w <= nblH[a];
+    };
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nWarps = (gridDim.x * blockDim.x) >> 5;
+    for (int w = warp; w < nActive; w += nWarps)
+    {
+        const int leaf = leaves ? leaves[w] : w;
+        const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
+        const uint32_t S = jstream[leaf];
+        const int gsize = S <= kSplitStream ? 32 : max(1, int(kSplitWork / S));
+        for (uint32_t g = p0; g < p1; g += 64)
+        {
+            const uint32_t a0 = g + lane, a1 = g + 32 + lane;
+            const bool act0 = a0 < p1 && (!converged || converged[a0] == 0);
+            const bool act1 = a1 < p1 && (!converged || converged[a1] == 0);
+            const bool row0 = act0 && rowOK(a0), row1 = act1 && rowOK(a1);
+            if (listItems != nullptr)
+            {
+                const uint32_t r0 = __ballot_sync(0xffffffffu, row0), r1 = __ballot_sync(0xffffffffu, row1);
+                if (r0 | r1)
+                {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(&ds->listParticles, __popc(r0) + __popc(r1));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (row0) listItems[base + __popc(r0 & lt)] = int(a0);
+                    if (row1) listItems[base + __popc(r0) + __popc(r1 & lt)] = int(a1);
+                }
+            }
+            const uint32_t m0 = __ballot_sync(0xffffffffu, act0 && !row0);
+            const uint32_t m1 = __ballot_sync(0xffffffffu, act1 && !row1);
+            const int nAct = __popc(m0) + __popc(m1);
+            if (nAct == 0) continue;
+            const int whole = (nAct + 31) >> 5;
+            const int G = max(whole, (nAct + gsize - 1) / gsize);
+            const bool split = G > whole;
+            int base = 0;
+            if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            const int wnd = int((g - p0) >> 6);
+            for (int k = lane; k < G; k += 32)
+            {
+                const int idx = split ? base + k : cap - 1 - (base + k);
+                if (idx >= 0 && idx < cap) items[idx] = make_int4(leaf, (wnd << 16) | (k << 8) | G, int(m0), int(m1));
+            }
+        }
+    }
+}
+
+// A persistent grid: as many blocks of the kernel as fit on the device at once.
+template<class K>
+int persistent_grid(const State& s, K kernel, int threads)
+{
+    int perSM = 0;
+    COSMO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, threads, 0));
+    return std::max(1, perSM) * s.numSMs;
+}
+
+// Decode of a work item: the group's particles are the active ranks
+// [grp * nAct / G, (grp + 1) * nAct / G) of the window starting at g0.
+struct Item
+{
+    int leaf, grp, G, nAct, ng;
+    uint32_t g0, m0, m1;
+};
+
+__device__ __forceinline__ Item decode_item(const int4& it, const uint32_t* __restrict__ layout)
+{
+    Item d;
+    d.leaf = it.x;
+    const int wnd = it.y >> 16;
+    d.grp = (it.y >> 8) & 255;
+    d.G = it.y & 255;
+    d.m0 = uint32_t(it.z);
+    d.m1 = uint32_t(it.w);
+    d.nAct = __popc(d.m0) + __popc(d.m1);
+    d.ng = (d.grp + 1) * d.nAct / d.G - d.grp * d.nAct / d.G;
+    d.g0 = layout[d.leaf] + 64u * uint32_t(wnd);
+    return d;
+}
+
+// Next item index of this warp (lane 0 takes it), or -1 when the queue is empty.  Cut
+// items sit at the front of the buffer, whole ones at the back.
+__device__ __forceinline__ int next_item(DevScalars* ds, int nHeavy, int nItems, int cap)
+{
+    int w = 0;
+    if ((threadIdx.x & 31) == 0) w = atomicAdd(&ds->workCounter[0], 1);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= nItems) return -1;
+    return w < nHeavy ? w : cap - 1 - (w - nHeavy);
+}
+
+} // namespace
+} // namespace cosmo
