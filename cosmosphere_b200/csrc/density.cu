@@ -575,26 +575,26 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         build_lists(s, false);
         cudaEvent_t g1 = ev(s);
         const int grid = grid_for(s, nL);
+        // rows at the converged h, then one lane per particle over its row; the group
+        // sweep covers only the rows that overflowed
+        const int nA = std::max(s.nAlive, 1);
+        s.items.resize(nA, s.st);
+        s.nbl.resize(size_t(nA) * kNbl, s.st);
+        s.nblCount.resize(nA, s.st);
+        begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
+        COSMO_LAUNCHED();
+        plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
+                                                        s.items.get(), nA, ds);
+        COSMO_LAUNCHED();
+        auto rows = s.periodic ? gather_rows_kernel<true> : gather_rows_kernel<false>;
+        rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
+            s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+            s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
+        COSMO_LAUNCHED();
         if (s.precision == 1)
             launch_gradient_mixed(s, pmass);
         else
         {
-            // rows at the converged h, then one lane per particle over its row; the group
-            // sweep covers only the rows that overflowed
-            const int nA = std::max(s.nAlive, 1);
-            s.items.resize(nA, s.st);
-            s.nbl.resize(size_t(nA) * kNbl, s.st);
-            s.nblCount.resize(nA, s.st);
-            begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
-            COSMO_LAUNCHED();
-            plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
-                                                            s.items.get(), nA, ds);
-            COSMO_LAUNCHED();
-            auto rows = s.periodic ? gather_rows_kernel<true> : gather_rows_kernel<false>;
-            rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
-                s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-                s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
-            COSMO_LAUNCHED();
             auto gr = s.periodic ? gradient_row_kernel<true> : gradient_row_kernel<false>;
             gr<<<std::max(1, std::min(iceil(s.nAlive, kThreads), 8 * s.numSMs)), kThreads, 0, s.st>>>(
                 s.nAlive, s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.vel4.get(), s.acc4.get(), s.rho.get(),

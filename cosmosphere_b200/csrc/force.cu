@@ -373,9 +373,7 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
             s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(), s.vsigmax.get(), s.divvF.get(), pmass,
             beta, pdv ? 1 : 0, shock ? 1 : 0, s.box.get(), ds);
     };
-    if (s.precision == 1)
-        launch_force_mixed(s, pmass, beta, disc, pdv, shock);
-    else if (nL > 0)
+    if (nL > 0)
     {
         // symmetric rows (cached with the symmetric lists), then one lane per particle over
         // its row; the group pass covers only the rows that overflowed
@@ -397,6 +395,11 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
             COSMO_LAUNCHED();
             s.rowsToken = s.token;
         }
+    }
+    if (s.precision == 1)
+        launch_force_mixed(s, pmass, beta, disc, pdv, shock);
+    else if (nL > 0)
+    {
         if (s.periodic) { if (disc) launchRows(force_row_kernel<true, true>); else launchRows(force_row_kernel<true, false>); }
         else { if (disc) launchRows(force_row_kernel<false, true>); else launchRows(force_row_kernel<false, false>); }
         COSMO_LAUNCHED();
