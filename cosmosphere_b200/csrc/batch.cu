@@ -15,9 +15,11 @@
 #include <cstring>
 #include <string>
 
+#include "densengine.cuh"
 #include "pairstream.cuh"
 #include "sort.cuh"
 #include "state.hpp"
+#include "workitems.cuh"
 #include "../../include/cosmosphere.h"
 
 namespace cosmo {
@@ -42,7 +44,9 @@ struct Batch
     DBuf<double4> xyzh, preCenter, preHalf;
     DBuf<int> converged, orderA, orderB, leafSet, leafSet2, leafPre, preLeaf, preSkip, jlist, activeA, activeB, allLeaves;
     DBuf<uint64_t> keysA, keysB, leafKey, leafKey2;
-    DBuf<uint32_t> ops, opsScan, nodeCount, leafPreStart, jcount, jOffset, setHist, setBase;
+    DBuf<uint32_t> ops, opsScan, nodeCount, leafPreStart, jcount, jOffset, setHist, setBase, jstream;
+    DBuf<int4> items;                 // Newton work items (leaf, window|group|G, m0, m1)
+    DBuf<int> leafNext;               // leaf already queued for the next iteration
     DBuf<uint2> leafRange;
     DBuf<DevBox> boxes;
     DBuf<LoopState> loop;
@@ -347,16 +351,19 @@ __global__ void hmax_leaf_kernel_b(const double4* __restrict__ xyzh, const uint2
 // window scan, include/tree.cuh:228-389 accept test).
 template<bool Fill>
 __global__ void __launch_bounds__(256)
-list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ setNodeStart,
+list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ countPtr, const int* __restrict__ set,
+                   const int* __restrict__ setNodeStart,
                    const int* __restrict__ leafPre, const double* __restrict__ hmaxLeaf,
                    const double4* __restrict__ preCenter, const double4* __restrict__ preHalf,
                    const int* __restrict__ preSkip, const int* __restrict__ preLeaf, const DevBox* __restrict__ boxes,
                    uint32_t* __restrict__ jcount, const uint32_t* __restrict__ jOffset, int* __restrict__ jlist,
-                   uint32_t listCap, int* err)
+                   uint32_t listCap, int* err, const uint2* __restrict__ range, uint32_t* __restrict__ jstream)
 {
     const int lane = threadIdx.x & 31;
-    const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    if (leaf >= L) return;
+    const int nAct = *countPtr;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nAct; t += (gridDim.x * blockDim.x) >> 5)
+    {
+    const int leaf = leaves[t];
     const int s = set[leaf];
     const int ns = setNodeStart[s], ne = setNodeStart[s + 1];
     const double4 ic = preCenter[leafPre[leaf]], is = preHalf[leafPre[leaf]];
@@ -366,7 +373,7 @@ list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ s
     const double ax = is.x + radHi, ay = is.y + radHi, az = is.z + radHi;
     const DevBox bx = boxes[s];
     const bool per = bx.periodic != 0;
-    uint32_t count = 0, base = 0, cap = 0;
+    uint32_t count = 0, base = 0, cap = 0, stream = 0;
     if (Fill)
     {
         base = jOffset[leaf];
@@ -374,7 +381,7 @@ list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ s
         if (jOffset[leaf + 1] > listCap)   // the preallocated list is too small: report, write nothing
         {
             if (lane == 0) atomicOr(err, int(kErrListFull));
-            return;
+            continue;
         }
     }
     const uint32_t lt = (1u << lane) - 1u;
@@ -419,6 +426,7 @@ list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ s
                 if (slot < cap) jlist[base + slot] = pl;
                 else atomicOr(err, int(kErrListCap));
             }
+            if (!Fill && ((emitMask >> lane) & 1u)) stream += range[pl].y - range[pl].x;
             count += __popc(emitMask);
             if (r >= 32) { next = p + 32; break; }
             int rskip = __shfl_sync(0xffffffffu, skip, r);
@@ -429,10 +437,20 @@ list_walk_kernel_b(int L, const int* __restrict__ set, const int* __restrict__ s
         }
         p = next;
     }
+    if (!Fill)
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) stream += __shfl_xor_sync(0xffffffffu, stream, o);
+    }
     if (lane == 0)
     {
         if (Fill) { if (count != cap) atomicOr(err, int(kErrListCap)); }
-        else jcount[leaf] = count;
+        else
+        {
+            jcount[leaf] = count;
+            jstream[leaf] = stream;
+        }
+    }
     }
 }
 
@@ -466,229 +484,96 @@ __device__ __forceinline__ bool nr_step_b(double rhoi, double gradhi, double hi,
     return !conv;
 }
 
-// Sums of one group of i particles over its leaf's list: plain (FP32 prefilter + exact
-// FP64 accept, as the single-set kernel) or mixed (FP32 with Kahan sums).
-template<bool Periodic, bool Mixed>
-__device__ __forceinline__ void group_sums(double4* ring, float4* ringf, int* ringIdx, bool mine, const double4& pi,
-                                           const GroupBox& bx, double lx, double ly, double lz, uint32_t jb,
-                                           uint32_t nj, const int* __restrict__ jlist, const uint2* __restrict__ range,
-                                           const double4* __restrict__ xyzh, double& rhoi, double& gradhi,
-                                           unsigned int& gp)
-{
-    const double hi = pi.w;
-    const double hinv2 = 1.0 / (hi * hi);
-    const float xf = float(pi.x - bx.cx), yf = float(pi.y - bx.cy), zf = float(pi.z - bx.cz);
-    const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
-    const double rs = kRadKernel * hi;
-    const double rm = rs + fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0);
-    const float tf = __double2float_ru(rm * rm * (1.0 + 1e-6));
-    const float hinv2f = float(hinv2);
-    double r0 = 0.0, g0 = 0.0;
-    KahanF sr, sg;
-    // the j stream walks list ranges: reuse stream_pairs with a range-table view
-    const int lane = threadIdx.x & 31;
-    const uint32_t lt = (1u << lane) - 1u;
-    int head = 0, cnt = 0;
-    auto drain = [&](int count) {
-        two_pass(ring, ringf, ringIdx, head, count, mine,
-                 [&](const float4& pf) {
-                     const float r2 = r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz);
-                     return Mixed ? (r2 * hinv2f < float(kRadK2)) : (r2 <= tf);
-                 },
-                 [&](const double4& pj, const float4& pf, int) {
-                     if (Mixed)
-                     {
-                         const float q2 = r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) * hinv2f;
-                         const float q = q2 > 0.0f ? q2 * rsqrtf(q2) : 0.0f;
-                         float wk, dwk;
-                         sph_kernel_f(q2, q, wk, dwk);
-                         sr.add(wk);
-                         sg.add(fmaf(-q, dwk, -3.0f * wk));
-                         ++gp;
-                     }
-                     else
-                     {
-                         double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                         nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                         const double q2 = pair_r2(dx, dy, dz) * hinv2;
-                         if (!(q2 < kRadK2)) return;
-                         const double q = sqrt(q2);
-                         double wk, dwk;
-                         sph_kernel(q2, q, wk, dwk);
-                         r0 += wk;
-                         g0 += -q * dwk - 3.0 * wk;
-                         ++gp;
-                     }
-                 });
-        head = (head + count) & (kRing - 1);
-        cnt -= count;
-        __syncwarp();
-    };
-    for (uint32_t lb = 0; lb < nj; lb += 32)
-    {
-        const int nb = int(min(32u, nj - lb));
-        uint32_t s0 = 0, len = 0;
-        if (lane < nb)
-        {
-            const uint2 r = range[jlist[jb + lb + lane]];
-            s0 = r.x;
-            len = r.y - r.x;
-        }
-        const uint32_t incl = warp_incl_scan_u32(len);
-        const uint32_t excl = incl - len;
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        auto locate = [&](uint32_t p) -> uint32_t {
-            int t = 0;
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1)
-            {
-                const uint32_t e = __shfl_sync(0xffffffffu, excl, (t + step) & 31);
-                if (t + step < nb && e <= p) t += step;
-            }
-            return __shfl_sync(0xffffffffu, s0, t) + (p - __shfl_sync(0xffffffffu, excl, t));
-        };
-        uint32_t j = 0;
-        double4 pj = make_double4(0, 0, 0, 0);
-        if (total > 0)
-        {
-            j = locate(lane);
-            if (uint32_t(lane) < total) pj = ldg4(xyzh + j);
-        }
-        for (uint32_t p0 = 0; p0 < total; p0 += 32)
-        {
-            const bool valid = p0 + lane < total;
-            uint32_t jn = 0;
-            double4 pn = make_double4(0, 0, 0, 0);
-            if (p0 + 32 < total)
-            {
-                jn = locate(p0 + 32 + lane);
-                if (p0 + 32 + lane < total) pn = ldg4(xyzh + jn);
-            }
-            const bool pass = valid && in_gather_box<Periodic>(pj, bx, lx, ly, lz);
-            const uint32_t m = __ballot_sync(0xffffffffu, pass);
-            if (pass)
-            {
-                const int slot = (head + cnt + __popc(m & lt)) & (kRing - 1);
-                ring[slot] = pj;
-                ringf[slot] = make_float4(float(pj.x - bx.cx), float(pj.y - bx.cy), float(pj.z - bx.cz), float(pj.w));
-                ringIdx[slot] = int(j);
-            }
-            cnt += __popc(m);
-            __syncwarp();
-            if (cnt >= 32) drain(32);
-            j = jn;
-            pj = pn;
-        }
-    }
-    if (cnt > 0) drain(cnt);
-    if (Mixed) { rhoi = sr.value(); gradhi = sg.value(); }
-    else { rhoi = r0; gradhi = g0; }
-}
-
+// One Newton iteration (or, EvalAll, rho at the final h) over the work items of every
+// set, taken dynamically by a persistent grid.  Each item carries its leaf; the leaf its
+// set's mass, periodicity and box.  A cut item scans its set's tree for its own box
+// instead of streaming the leaf's whole list.
 template<bool Mixed, bool EvalAll>
 __global__ void __launch_bounds__(kThreads)
-density_batch_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr, const int* __restrict__ leafSet,
+density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restrict__ leafSet,
                      const uint2* __restrict__ range, const uint32_t* __restrict__ jOffset,
                      const uint32_t* __restrict__ jcount, const int* __restrict__ jlist, double4* __restrict__ xyzh,
                      double* __restrict__ rho, double* __restrict__ gradh, int* __restrict__ converged,
                      const double* __restrict__ pmassSet, double tolh, double hfact, const DevBox* __restrict__ boxes,
-                     int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
+                     int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
+                     const int* __restrict__ setNodeStart, const int* __restrict__ leafPre,
+                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds)
 {
-    __shared__ double4 sRing[kWarpsPerBlock][kRing];
-    __shared__ float4 sRingF[kWarpsPerBlock][kRing];
-    __shared__ int sIdx[kWarpsPerBlock][kRing];
+    __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int nLeavesActive = *countPtr;
+    const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     unsigned long long pairs = 0;
-    // dynamic work distribution over the active leaves of every set
     for (;;)
     {
-        int w = 0;
-        if (lane == 0) w = atomicAdd(&ds->workCounter[0], 1);
-        w = __shfl_sync(0xffffffffu, w, 0);
-        if (w >= nLeavesActive) break;
-        const int leaf = leaves[w];
+        const int w = next_item(ds, nHeavy, nItems, cap);
+        if (w < 0) break;
+        const int4 it = items[w];
+        const int leaf = it.x;
+        const Item d = decode_item(it, range[leaf].x);
         const int s = leafSet[leaf];
         const double pmass = pmassSet[s];
         const DevBox bxs = boxes[s];
         const bool per = bxs.periodic != 0;
-        const uint2 r = range[leaf];
-        const uint32_t p0 = r.x, p1 = r.y;
-        const uint32_t jb = jOffset[leaf], nj = jcount[leaf];
-        bool leafActive = false;
-        for (uint32_t g = p0; g < p1; g += 64)
+        const int slot = group_slot(d.m0, d.m1, d.nAct, d.grp, d.G, lane);
+        const bool mine = slot >= 0;
+        const uint32_t i = d.g0 + uint32_t(mine ? slot : 0);
+        const double4 pi = xyzh[i];
+        double rhoi = 0.0, gradhi = 0.0;
+        unsigned int gp = 0, gc = 0;
+        auto src = list_source(jlist, jOffset[leaf], jcount[leaf], TableRanges{range}, xyzh);
+        if (w < nHeavy)
         {
-            const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            const bool act0 = a0 < p1 && (EvalAll || converged[a0] == 0);
-            const bool act1 = a1 < p1 && (EvalAll || converged[a1] == 0);
-            const uint32_t m0 = __ballot_sync(0xffffffffu, act0);
-            const uint32_t m1 = __ballot_sync(0xffffffffu, act1);
-            const int nAct = __popc(m0) + __popc(m1);
-            if (nAct == 0) continue;
-            const int G = (nAct + 31) >> 5;
-            for (int grp = 0; grp < G; ++grp)
-            {
-                const int slot = group_slot(m0, m1, nAct, grp, G, lane);
-                const bool mine = slot >= 0;
-                const uint32_t i = g + uint32_t(mine ? slot : 0);
-                const double4 pi = xyzh[i];
-                const double rs = kRadKernel * pi.w;
-                if (EvalAll && !(pi.w > 0.0)) continue;   // (never: live particles only)
-                const double rmax = warp_max(mine ? rs : 0.0);
-                const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-                double rhoi = 0.0, gradhi = 0.0;
-                unsigned int gp = 0;
-                if (per)
-                    group_sums<true, Mixed>(sRing[wib], sRingF[wib], sIdx[wib], mine, pi, bx, bxs.len[0], bxs.len[1],
-                                            bxs.len[2], jb, nj, jlist, range, xyzh, rhoi, gradhi, gp);
-                else
-                    group_sums<false, Mixed>(sRing[wib], sRingF[wib], sIdx[wib], mine, pi, bx, 0.0, 0.0, 0.0, jb, nj,
-                                             jlist, range, xyzh, rhoi, gradhi, gp);
-                bool still = false;
-                if (EvalAll)
-                {
-                    // rho and d(rho)/dh at the converged h (src/density_base.cu:635-643)
-                    if (mine)
-                    {
-                        pairs += gp;
-                        const double hi1 = 1.0 / pi.w;
-                        const double hi31 = hi1 * hi1 * hi1;
-                        rho[i] = rhoi * kCnormk * pmass * hi31;
-                        gradh[i] = gradhi * kCnormk * pmass * (hi31 * hi1);
-                    }
-                    continue;
-                }
-                if (mine)
-                {
-                    pairs += gp;
-                    double ro, go, ho;
-                    int conv;
-                    still = nr_step_b(rhoi, gradhi, pi.w, pmass, hfact, tolh, ro, go, ho, conv);
-                    rho[i] = ro;
-                    gradh[i] = go;
-                    reinterpret_cast<double*>(xyzh + i)[3] = ho;
-                    converged[i] = conv;
-                }
-                const uint32_t stillMask = __ballot_sync(0xffffffffu, still);
-                if (stillMask)
-                {
-                    leafActive = true;
-                    if (lane == 0) atomicAdd(&ds->unconverged, __popc(stillMask));
-                }
-            }
+            const double4 c = tree.center[leafPre[leaf]], h = tree.half[leafPre[leaf]];
+            double hm = hmaxLeaf[leaf];
+            if (!isfinite(hm) || hm <= 0.0) hm = 0.0;
+            const double ext = kRadKernel * hm;
+            src.walk = true;
+            src.tree = tree;
+            src.tree.n0 = setNodeStart[s];
+            src.tree.n1 = setNodeStart[s + 1];
+            src.rc = make_double3(c.x, c.y, c.z);
+            src.re = make_double3(h.x + ext, h.y + ext, h.z + ext);
         }
-        if (leafActive && lane == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
+        if (per)
+            density_group<true, Mixed>(sScr[wib], mine, d.ng, pi, bxs.len[0], bxs.len[1], bxs.len[2], src, rhoi,
+                                       gradhi, gp, gc);
+        else
+            density_group<false, Mixed>(sScr[wib], mine, d.ng, pi, 0.0, 0.0, 0.0, src, rhoi, gradhi, gp, gc);
+        if (EvalAll)
+        {
+            // rho and d(rho)/dh at the converged h (src/density_base.cu:635-643)
+            if (mine)
+            {
+                pairs += gp;
+                const double hi1 = 1.0 / pi.w;
+                const double hi31 = hi1 * hi1 * hi1;
+                rho[i] = rhoi * kCnormk * pmass * hi31;
+                gradh[i] = gradhi * kCnormk * pmass * (hi31 * hi1);
+            }
+            continue;
+        }
+        bool still = false;
+        if (mine)
+        {
+            pairs += gp;
+            double ro, go, ho;
+            int conv;
+            still = nr_step_b(rhoi, gradhi, pi.w, pmass, hfact, tolh, ro, go, ho, conv);
+            rho[i] = ro;
+            gradh[i] = go;
+            reinterpret_cast<double*>(xyzh + i)[3] = ho;
+            converged[i] = conv;
+        }
+        const uint32_t stillMask = __ballot_sync(0xffffffffu, still);
+        if (stillMask && lane == 0)
+        {
+            atomicAdd(&ds->unconverged, __popc(stillMask));
+            if (atomicExch(&leafNext[leaf], 1) == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     if (lane == 0) atomicAdd(&ds->pairs[0], pairs);
-}
-
-__global__ void loop_reset_kernel(DevScalars* ds)
-{
-    ds->nextActive = 0;
-    ds->unconverged = 0;
-    ds->workCounter[0] = 0;
 }
 
 __global__ void copy_active_kernel(const int* __restrict__ src, int* __restrict__ dst, const DevScalars* __restrict__ ds,
@@ -838,6 +723,9 @@ static void batch_build(Batch& B)
     COSMO_LAUNCHED();
     B.hmaxLeaf.resize(L, s.st);
     B.jcount.resize(L, s.st);
+    B.jstream.resize(L, s.st);
+    B.leafNext.resize(L, s.st);
+    B.items.resize(std::max(B.n, 1), s.st);
     B.jOffset.resize(size_t(L) + 1, s.st);
     B.activeA.resize(L, s.st);
     B.activeB.resize(L, s.st);
@@ -851,19 +739,49 @@ static void batch_build(Batch& B)
     B.tBuild = elapsed_s(e0, e1);
 }
 
-static void walk_lists(Batch& B, bool fill)
+// The gather lists of the given leaves (count on the device); the counts of all other
+// leaves are zero, so the scan sizes the list storage for these leaves only.
+static void walk_lists(Batch& B, bool fill, const int* leaves, const int* countPtr)
 {
     State& s = B.core;
     const int L = B.nLeaves;
-    const int blocks = iceil(long(L) * 32, 256);
+    if (!fill) COSMO_CUDA(cudaMemsetAsync(B.jcount.get(), 0, size_t(L) * sizeof(uint32_t), s.st));
+    const int blocks = std::max(1, std::min(iceil(long(L) * 32, 256), 16 * s.numSMs));
     auto go = [&](auto kern) {
-        kern<<<blocks, 256, 0, s.st>>>(L, B.leafSet.get(), B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(),
+        kern<<<blocks, 256, 0, s.st>>>(leaves, countPtr, B.leafSet.get(), B.setNodeStart.get(), B.leafPre.get(),
+                                       B.hmaxLeaf.get(),
                                        B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(),
                                        B.boxes.get(), B.jcount.get(), B.jOffset.get(), B.jlist.get(), B.listCap,
-                                       &s.dscal.get()->err);
+                                       &s.dscal.get()->err, B.leafRange.get(), B.jstream.get());
     };
     if (fill) go(list_walk_kernel_b<true>);
     else go(list_walk_kernel_b<false>);
+    COSMO_LAUNCHED();
+}
+
+// Work items of the given leaves (count on the device), then the density kernel over
+// them: a Newton iteration, or (evalAll) rho at the final h of every live particle.
+static void run_items(Batch& B, const int* leaves, const int* countPtr, bool evalAll, double tolh, double hfact)
+{
+    State& s = B.core;
+    DevScalars* ds = s.dscal.get();
+    const int L = B.nLeaves;
+    const int cap = std::max(B.n, 1);
+    begin_iteration_kernel<<<std::min(iceil(L, 256), 4 * s.numSMs), 256, 0, s.st>>>(ds, B.leafNext.get(), L);
+    COSMO_LAUNCHED();
+    plan_items_table_kernel<<<s.numSMs * 8, kThreads, 0, s.st>>>(leaves, countPtr, B.leafRange.get(),
+                                                                  evalAll ? nullptr : B.converged.get(),
+                                                                  B.jstream.get(), B.items.get(), cap, ds);
+    COSMO_LAUNCHED();
+    const PreorderTree tree{B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(), 0, 0};
+    auto go = [&](auto kern) {
+        kern<<<persistent_grid(s, kern, kThreads), kThreads, 0, s.st>>>(
+            B.items.get(), cap, B.leafSet.get(), B.leafRange.get(), B.jOffset.get(), B.jcount.get(), B.jlist.get(),
+            B.xyzh.get(), B.rho.get(), B.gradh.get(), B.converged.get(), B.pmass.get(), tolh, hfact, B.boxes.get(),
+            B.leafNext.get(), B.activeB.get(), tree, B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(), ds);
+    };
+    if (evalAll) { if (s.precision == 1) go(density_batch_kernel<true, true>); else go(density_batch_kernel<false, true>); }
+    else { if (s.precision == 1) go(density_batch_kernel<true, false>); else go(density_batch_kernel<false, false>); }
     COSMO_LAUNCHED();
 }
 
@@ -880,21 +798,10 @@ static void nr_iteration(Batch& B, double tolh, double hfact, cudaGraphCondition
     hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.activeA.get(),
                                                        &ls->nActiveLeaves, B.hmaxLeaf.get());
     COSMO_LAUNCHED();
-    walk_lists(B, false);
+    walk_lists(B, false, B.activeA.get(), &ls->nActiveLeaves);
     scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, false);
-    walk_lists(B, true);
-    loop_reset_kernel<<<1, 1, 0, s.st>>>(ds);
-    COSMO_LAUNCHED();
-    const int grid = s.numSMs * 8;
-    auto go = [&](auto kern) {
-        kern<<<grid, kThreads, 0, s.st>>>(B.activeA.get(), &ls->nActiveLeaves, B.leafSet.get(), B.leafRange.get(),
-                                          B.jOffset.get(), B.jcount.get(), B.jlist.get(), B.xyzh.get(), B.rho.get(),
-                                          B.gradh.get(), B.converged.get(), B.pmass.get(), tolh, hfact, B.boxes.get(),
-                                          B.activeB.get(), ds);
-    };
-    if (s.precision == 1) go(density_batch_kernel<true, false>);
-    else go(density_batch_kernel<false, false>);
-    COSMO_LAUNCHED();
+    walk_lists(B, true, B.activeA.get(), &ls->nActiveLeaves);
+    run_items(B, B.activeA.get(), &ls->nActiveLeaves, false, tolh, hfact);
     copy_active_kernel<<<iceil(L, 256), 256, 0, s.st>>>(B.activeB.get(), B.activeA.get(), ds, L);
     COSMO_LAUNCHED();
     loop_epilogue_kernel<<<1, 1, 0, s.st>>>(ls, ds, handle, setCond);
@@ -911,26 +818,15 @@ static void final_rho(Batch& B)
     hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.allLeaves.get(), &ls->nAll,
                                                        B.hmaxLeaf.get());
     COSMO_LAUNCHED();
-    walk_lists(B, false);
+    walk_lists(B, false, B.allLeaves.get(), &ls->nAll);
     const uint32_t total = scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, true);
     if (total > B.listCap)
     {
         B.listCap = total + total / 4 + 1024;
         B.jlist.resize(B.listCap, s.st);
     }
-    walk_lists(B, true);
-    loop_reset_kernel<<<1, 1, 0, s.st>>>(ds);
-    COSMO_LAUNCHED();
-    const int grid = s.numSMs * 8;
-    auto go = [&](auto kern) {
-        kern<<<grid, kThreads, 0, s.st>>>(B.allLeaves.get(), &ls->nAll, B.leafSet.get(), B.leafRange.get(),
-                                          B.jOffset.get(), B.jcount.get(), B.jlist.get(), B.xyzh.get(), B.rho.get(),
-                                          B.gradh.get(), B.converged.get(), B.pmass.get(), 0.0, 0.0, B.boxes.get(),
-                                          B.activeB.get(), ds);
-    };
-    if (s.precision == 1) go(density_batch_kernel<true, true>);
-    else go(density_batch_kernel<false, true>);
-    COSMO_LAUNCHED();
+    walk_lists(B, true, B.allLeaves.get(), &ls->nAll);
+    run_items(B, B.allLeaves.get(), &ls->nAll, true, 0.0, 0.0);
 }
 
 static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int flags, int attempt = 0)
@@ -967,7 +863,7 @@ static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int fla
     hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.activeA.get(),
                                                        &B.loop.get()->nActiveLeaves, B.hmaxLeaf.get());
     COSMO_LAUNCHED();
-    walk_lists(B, false);
+    walk_lists(B, false, B.activeA.get(), &B.loop.get()->nActiveLeaves);
     const uint32_t total0 = scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, true);
     const uint32_t want = (total0 << (1 + attempt)) + 1024;
     if (B.listCap < want) B.listCap = want;

@@ -42,10 +42,8 @@ __device__ __forceinline__ float sqrt_q(float q2) { return q2 > 0.0f ? q2 * rsqr
 // -q dW/dq - 3W over accepted j), gp the accepted pairs and gc the candidates offered.
 template<bool Periodic, bool Mixed, class Ranges>
 __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int ng, const double4& pi, double lx,
-                                              double ly, double lz, uint32_t jb, uint32_t nj,
-                                              const int* __restrict__ jlist, Ranges ranges,
-                                              const double4* __restrict__ xyzh, double& rhoi, double& gradhi,
-                                              unsigned int& gp, unsigned int& gc)
+                                              double ly, double lz, const GroupSource<Ranges>& src, double& rhoi,
+                                              double& gradhi, unsigned int& gp, unsigned int& gc)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -65,8 +63,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         if (mine) grp[lane] = make_double4(pi.x, pi.y, pi.z, hinv2);
         __syncwarp();
         double sr = 0.0, sg = 0.0;
-        stream_ranges<true, false, false>(
-            ring, nullptr, nullptr, bx.cx, bx.cy, bx.cz, 0.0, 0.0, 0.0, jb, nj, jlist, ranges, xyzh,
+        src.template stream<true, false, false, Periodic>(
+            ring, nullptr, nullptr, bx, 0.0, 0.0, 0.0, lx, ly, lz,
             [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
             [&](const double4* rg, const float4*, const int*, int head, int count) {
                 gc += count;
@@ -144,8 +142,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         __syncwarp();
         const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
         KahanF kr, kg;
-        stream_ranges<false, true, false>(
-            nullptr, ringf, nullptr, bx.cx, bx.cy, bx.cz, sx, sy, sz, jb, nj, jlist, ranges, xyzh,
+        src.template stream<false, true, false, Periodic>(
+            nullptr, ringf, nullptr, bx, sx, sy, sz, lx, ly, lz,
             [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
             [&](const double4*, const float4* rf, const int*, int head, int count) {
                 gc += count;

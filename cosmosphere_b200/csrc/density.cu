@@ -74,7 +74,9 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
                   const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
                   double* __restrict__ gradh, int* __restrict__ converged, double pmass, double tolh,
                   double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
-                  int* __restrict__ leafNext, int* __restrict__ nextLeaves, DevScalars* __restrict__ ds)
+                  int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
+                  const int* __restrict__ leafToInternal, const double* __restrict__ centers,
+                  const double* __restrict__ sizes, DevScalars* __restrict__ ds)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -96,8 +98,19 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
         const double hi = pi.w;
         double rhoi, gradhi;
         unsigned int gp, gc;
-        density_group<Periodic, Mixed>(sScr[wib], mine, d.ng, pi, lx, ly, lz, jOffset[leaf], jcount[leaf], jlist,
-                                       LayoutRanges{layout}, xyzh, rhoi, gradhi, gp, gc);
+        // a cut group (its leaf's list streams far more than it needs) scans the tree for
+        // its own box instead, within the region its leaf's list covers
+        auto src = list_source(jlist, jOffset[leaf], jcount[leaf], LayoutRanges{layout}, xyzh);
+        if (w < nHeavy)
+        {
+            const int in = leafToInternal[leaf];
+            const double ext = kRadKernel * listH[leaf];
+            src.walk = true;
+            src.tree = tree;
+            src.rc = make_double3(centers[3 * in], centers[3 * in + 1], centers[3 * in + 2]);
+            src.re = make_double3(sizes[3 * in] + ext, sizes[3 * in + 1] + ext, sizes[3 * in + 2] + ext);
+        }
+        density_group<Periodic, Mixed>(sScr[wib], mine, d.ng, pi, lx, ly, lz, src, rhoi, gradhi, gp, gc);
         bool stillActive = false;
         if (mine)
         {
@@ -517,7 +530,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
             nr<<<persistent_grid(s, nr, kThreads), kThreads, 0, s.st>>>(
                 s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
                 s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
-                s.leafNext.get(), s.activeB.get(), ds);
+                s.leafNext.get(), s.activeB.get(),
+                PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
+                s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds);
             COSMO_LAUNCHED();
         }
         cudaEvent_t j2 = ev(s);

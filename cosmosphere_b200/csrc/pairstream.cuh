@@ -122,43 +122,40 @@ __device__ __forceinline__ double image_offset(double x, double c, double L)
     return d;
 }
 
-// Stream the j particles of one i-leaf list through the group filter into the ring and
-// hand the survivors to batch(ring, ringf, ringIdx, head, count) in runs of up to 32, in
-// ascending j order, on every lane.  filter(pj) is evaluated by the loading lane only.
-// The ring keeps what the caller asks for: the FP64 xyzh (Dbl), an FP32 copy relative to
-// the group box centre at the nearest periodic image when lx, ly, lz > 0 (Float), and
-// the particle index (Index).
-//
-// Up to 32 list entries and their particle ranges are fetched at once, one per lane; a
-// warp prefix sum over the range lengths flattens them, so every load batch is 32
-// consecutive stream positions (each lane finds its particle by a 5-step binary search
-// over the prefix sums), and the next batch's loads are issued before the current batch
-// is filtered and evaluated.
-template<bool Dbl, bool Float, bool Index, class Ranges, class Filter, class Batch>
-__device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
-                                              double cz, double lx, double ly, double lz, uint32_t jb, uint32_t nj,
-                                              const int* __restrict__ jlist, Ranges ranges,
-                                              const double4* __restrict__ xyzh, Filter filter, Batch batch)
+// The warp's candidate ring: j particles that pass the group filter are compacted into
+// it, in order, and handed to batch(ring, ringf, ringIdx, head, count) in runs of up to 32
+// on every lane.  The ring keeps what the caller asks for: the FP64 xyzh (Dbl), an FP32
+// copy relative to the group box centre at the nearest periodic image when lx, ly, lz > 0
+// (Float), and the particle index (Index).
+template<bool Dbl, bool Float, bool Index>
+struct CandidateRing
 {
-    const int lane = threadIdx.x & 31;
-    const uint32_t lt = (1u << lane) - 1u;
+    double4* ring;
+    float4* ringf;
+    int* ringIdx;
+    double cx, cy, cz, lx, ly, lz;
     int head = 0, cnt = 0;
-    auto drain = [&](int count) {
+
+    template<class Batch>
+    __device__ __forceinline__ void drain(int count, Batch& batch)
+    {
         batch(ring, ringf, ringIdx, head, count);
         head = (head + count) & (kRing - 1);
         cnt -= count;
         __syncwarp();
-    };
-    for (uint32_t lb = 0; lb < nj; lb += 32)
+    }
+
+    // Stream the particle ranges held one per lane (s0, len; lanes >= nb hold none), in
+    // lane order.  A warp prefix sum over the lengths flattens them, so every load batch is
+    // 32 consecutive stream positions (each lane finds its particle by a 5-step binary
+    // search over the prefix sums), and the next batch's loads are issued before the
+    // current batch is filtered.  filter(pj) is evaluated by the loading lane only.
+    template<class Filter, class Batch>
+    __device__ __forceinline__ void feed(uint32_t s0, uint32_t len, int nb, const double4* __restrict__ xyzh,
+                                         Filter& filter, Batch& batch)
     {
-        const int nb = int(min(32u, nj - lb));
-        uint32_t s0 = 0, len = 0;
-        if (lane < nb)
-        {
-            const uint2 r = ranges(jlist[jb + lb + lane]);
-            s0 = r.x;
-            len = r.y - r.x;
-        }
+        const int lane = threadIdx.x & 31;
+        const uint32_t lt = (1u << lane) - 1u;
         const uint32_t incl = warp_incl_scan_u32(len);
         const uint32_t excl = incl - len;
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
@@ -183,7 +180,6 @@ __device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int*
         for (uint32_t p0 = 0; p0 < total; p0 += 32)
         {
             const bool valid = p0 + lane < total;
-            // prefetch the next batch before working on this one
             uint32_t jn = 0;
             double4 pn = make_double4(0, 0, 0, 0);
             if (p0 + 32 < total)
@@ -204,12 +200,166 @@ __device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int*
             }
             cnt += __popc(m);
             __syncwarp();
-            if (cnt >= 32) drain(32);
+            if (cnt >= 32) drain(32, batch);
             j = jn;
             pj = pn;
         }
     }
-    if (cnt > 0) drain(cnt);
+
+    template<class Batch>
+    __device__ __forceinline__ void finish(Batch& batch)
+    {
+        if (cnt > 0) drain(cnt, batch);
+    }
+};
+
+// Stream the j particles of one i-leaf list (entries jb .. jb + nj of jlist, in order)
+// through the group filter into the ring, 32 list entries at a time.
+template<bool Dbl, bool Float, bool Index, class Ranges, class Filter, class Batch>
+__device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
+                                              double cz, double lx, double ly, double lz, uint32_t jb, uint32_t nj,
+                                              const int* __restrict__ jlist, Ranges ranges,
+                                              const double4* __restrict__ xyzh, Filter filter, Batch batch)
+{
+    const int lane = threadIdx.x & 31;
+    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, lx, ly, lz};
+    for (uint32_t lb = 0; lb < nj; lb += 32)
+    {
+        const int nb = int(min(32u, nj - lb));
+        uint32_t s0 = 0, len = 0;
+        if (lane < nb)
+        {
+            const uint2 r = ranges(jlist[jb + lb + lane]);
+            s0 = r.x;
+            len = r.y - r.x;
+        }
+        cr.feed(s0, len, nb, xyzh, filter, batch);
+    }
+    cr.finish(batch);
+}
+
+// The pre-order node arrays of a tree (or of one set's range [n0, n1) of a forest) for
+// stream_walk.
+struct PreorderTree
+{
+    const double4* __restrict__ center;
+    const double4* __restrict__ half;
+    const int* __restrict__ skip;
+    const int* __restrict__ leaf;
+    int n0, n1;
+};
+
+// Stream the j particles of every leaf whose cell overlaps the box (c, e) -- and the
+// region (rc, re), when re.x >= 0 -- through the group filter into the ring, found by a
+// stackless pre-order scan of the tree 32 nodes at a time (the scan of list_walk_kernel):
+// leaves come out in ascending order, so the stream is in ascending j as a list's is.
+// Used for groups whose leaf list is far longer than their own search region needs.
+template<bool Dbl, bool Float, bool Index, bool Periodic, class Ranges, class Filter, class Batch>
+__device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
+                                            double cz, double sx, double sy, double sz, const PreorderTree& t,
+                                            double3 c, double3 e, double3 rc, double3 re, double lx, double ly,
+                                            double lz, Ranges ranges, const double4* __restrict__ xyzh,
+                                            Filter filter, Batch batch)
+{
+    const int lane = threadIdx.x & 31;
+    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz};
+    auto fold = [&](double d, double L) { return Periodic ? fmin(d, L - d) : d; };
+    int p = t.n0;
+    while (p < t.n1)
+    {
+        const int idx = p + lane;
+        const bool valid = idx < t.n1;
+        bool accept = false;
+        int skip = 1, pl = -1;
+        if (valid)
+        {
+            const double4 nc = t.center[idx];
+            const double4 nh = t.half[idx];
+            accept = fold(fabs(c.x - nc.x), lx) <= e.x + nh.x && fold(fabs(c.y - nc.y), ly) <= e.y + nh.y &&
+                     fold(fabs(c.z - nc.z), lz) <= e.z + nh.z;
+            if (re.x >= 0.0)
+                accept = accept && fold(fabs(rc.x - nc.x), lx) <= re.x + nh.x &&
+                         fold(fabs(rc.y - nc.y), ly) <= re.y + nh.y && fold(fabs(rc.z - nc.z), lz) <= re.z + nh.z;
+            skip = t.skip[idx];
+            pl = t.leaf[idx];
+        }
+        const uint32_t validMask = __ballot_sync(0xffffffffu, valid);
+        const uint32_t rejMask = __ballot_sync(0xffffffffu, valid && !accept);
+        // the reached, accepted leaves of this window, in lane (pre-) order
+        uint32_t emit = 0;
+        int pos = 0, next = p + 32;
+        for (;;)
+        {
+            const uint32_t fromPos = (pos >= 32) ? 0u : (0xffffffffu << pos);
+            const uint32_t rej = rejMask & fromPos;
+            const int r = rej ? (__ffs(rej) - 1) : 32;
+            const uint32_t runMask = validMask & fromPos & ((r >= 32) ? 0xffffffffu : ((1u << r) - 1u));
+            emit |= runMask;
+            if (r >= 32) { next = p + 32; break; }
+            int rskip = __shfl_sync(0xffffffffu, skip, r);
+            if (rskip < 1) rskip = 1;   // a subtree holds its root: the scan always advances
+            const int target = p + r + rskip;
+            if (target >= p + 32 || target >= t.n1) { next = target; break; }
+            pos = target - p;
+        }
+        emit &= __ballot_sync(0xffffffffu, pl >= 0);
+        if (emit)
+        {
+            // compact the emitted leaves onto the low lanes, keeping their order
+            const bool mineLeaf = (emit >> lane) & 1u;
+            const int nb = __popc(emit);
+            uint2 r = make_uint2(0, 0);
+            if (mineLeaf) r = ranges(pl);
+            // lane k takes the k-th emitted leaf's range
+            const unsigned src = __fns(emit, 0, lane + 1);
+            const int sl = src < 32u ? int(src) : 0;
+            const uint32_t rx = __shfl_sync(0xffffffffu, r.x, sl);
+            const uint32_t ry = __shfl_sync(0xffffffffu, r.y, sl);
+            const uint32_t s0 = lane < nb ? rx : 0u, len = lane < nb ? ry - rx : 0u;
+            cr.feed(s0, len, nb, xyzh, filter, batch);
+        }
+        p = next;
+    }
+    cr.finish(batch);
+}
+
+// Where a group's candidates come from: its leaf's j-leaf list (entries jb .. jb + nj of
+// jlist), or, when walk is set, a pre-order scan of the tree for the leaves overlapping
+// the group's own box, within the leaf list's region (rc, re).
+template<class Ranges>
+struct GroupSource
+{
+    const int* __restrict__ jlist;
+    uint32_t jb, nj;
+    Ranges ranges;
+    const double4* __restrict__ xyzh;
+    bool walk;
+    PreorderTree tree;
+    double3 rc, re;
+
+    template<bool Dbl, bool Float, bool Index, bool Periodic, class Filter, class Batch>
+    __device__ __forceinline__ void stream(double4* ring, float4* ringf, int* ringIdx, const GroupBox& bx, double sx,
+                                           double sy, double sz, double lx, double ly, double lz, Filter filter,
+                                           Batch batch) const
+    {
+        if (walk)
+            stream_walk<Dbl, Float, Index, Periodic>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, tree,
+                                                     make_double3(bx.cx, bx.cy, bx.cz),
+                                                     make_double3(bx.ex, bx.ey, bx.ez), rc, re, lx, ly, lz, ranges,
+                                                     xyzh, filter, batch);
+        else
+            stream_ranges<Dbl, Float, Index>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, jb, nj, jlist,
+                                             ranges, xyzh, filter, batch);
+    }
+};
+
+template<class Ranges>
+__device__ __forceinline__ GroupSource<Ranges> list_source(const int* jlist, uint32_t jb, uint32_t nj, Ranges ranges,
+                                                           const double4* xyzh)
+{
+    GroupSource<Ranges> g{jlist, jb, nj, ranges, xyzh, false, PreorderTree{nullptr, nullptr, nullptr, nullptr, 0, 0},
+                          make_double3(0, 0, 0), make_double3(-1, -1, -1)};
+    return g;
 }
 
 // stream_ranges over a single set's leaves, FP32 copies relative to the box centre

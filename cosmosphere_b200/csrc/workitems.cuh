@@ -48,12 +48,12 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
 constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
 
-__global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
-                                  const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
-                                  int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
-                                  const int* __restrict__ nblCount = nullptr, const double* __restrict__ nblH = nullptr,
-                                  const double4* __restrict__ xyzh = nullptr, int K = 0,
-                                  int* __restrict__ listItems = nullptr)
+template<class Ranges>
+__device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int nActive, Ranges ranges,
+                                           const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
+                                           int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
+                                           const int* __restrict__ nblCount, const double* __restrict__ nblH,
+                                           const double4* __restrict__ xyzh, int K, int* __restrict__ listItems)
 {
     const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
     auto rowOK = [&](uint32_t a) {
@@ -65,7 +65,8 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
     for (int w = warp; w < nActive; w += nWarps)
     {
         const int leaf = leaves ? leaves[w] : w;
-        const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
+        const uint2 rg = ranges(leaf);
+        const uint32_t p0 = rg.x, p1 = rg.y;
         const uint32_t S = jstream[leaf];
         const int gsize = S <= kSplitStream ? 32 : max(1, int(kSplitWork / S));
         for (uint32_t g = p0; g < p1; g += 64)
@@ -106,6 +107,27 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
     }
 }
 
+__global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
+                                  const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
+                                  int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
+                                  const int* __restrict__ nblCount = nullptr, const double* __restrict__ nblH = nullptr,
+                                  const double4* __restrict__ xyzh = nullptr, int K = 0,
+                                  int* __restrict__ listItems = nullptr)
+{
+    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, items, cap, ds, nblCount, nblH, xyzh, K,
+               listItems);
+}
+
+// The same over a forest's range table, the active count read on the device.
+__global__ void plan_items_table_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr,
+                                        const uint2* __restrict__ range, const int* __restrict__ converged,
+                                        const uint32_t* __restrict__ jstream, int4* __restrict__ items, int cap,
+                                        DevScalars* __restrict__ ds)
+{
+    plan_items(leaves, *countPtr, TableRanges{range}, converged, jstream, items, cap, ds, nullptr, nullptr, nullptr,
+               0, nullptr);
+}
+
 // A persistent grid: as many blocks of the kernel as fit on the device at once.
 template<class K>
 int persistent_grid(const State& s, K kernel, int threads)
@@ -123,7 +145,7 @@ struct Item
     uint32_t g0, m0, m1;
 };
 
-__device__ __forceinline__ Item decode_item(const int4& it, const uint32_t* __restrict__ layout)
+__device__ __forceinline__ Item decode_item(const int4& it, uint32_t leafBegin)
 {
     Item d;
     d.leaf = it.x;
@@ -134,8 +156,13 @@ __device__ __forceinline__ Item decode_item(const int4& it, const uint32_t* __re
     d.m1 = uint32_t(it.w);
     d.nAct = __popc(d.m0) + __popc(d.m1);
     d.ng = (d.grp + 1) * d.nAct / d.G - d.grp * d.nAct / d.G;
-    d.g0 = layout[d.leaf] + 64u * uint32_t(wnd);
+    d.g0 = leafBegin + 64u * uint32_t(wnd);
     return d;
+}
+
+__device__ __forceinline__ Item decode_item(const int4& it, const uint32_t* __restrict__ layout)
+{
+    return decode_item(it, layout[it.x]);
 }
 
 // Next item index of this warp (lane 0 takes it), or -1 when the queue is empty.  Cut
