@@ -155,7 +155,7 @@ def ncu_traffic(kernel: str):
     return None
 
 
-def mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs):
+def mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs, hfact=1.2):
     """Max / rms errors of the mixed form against the FP64 form, same inputs, same GPU."""
     from cosmosphere_b200 import capi
     res = {}
@@ -163,7 +163,7 @@ def mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs):
         c.set_precision(bool(mode))
         c.upload(capi.POS, pos, n); c.upload(capi.HSML, hsml, n)
         c.upload(capi.VEL, vel, n); c.upload(capi.ACCEL, acc, n)
-        c.density(n, p["pmass"], tolh=1e-4, hfact=1.2)
+        c.density(n, p["pmass"], tolh=1e-4, hfact=hfact)
         c.upload(capi.THERMO, thermo, n, sorted_=True)
         c.force(n, p["pmass"], beta=2.0, alphau=0.0)
         res[mode] = {k: c.download(k, n).copy() for k in outs}
@@ -444,8 +444,10 @@ def main():
     ap.add_argument("--npartx", type=int, default=100)
     ap.add_argument("--ref-npartx", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "ensemble", "served"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                    help="both: plain FP64 (the headline value) and mixed in one run")
+    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "plummer", "ensemble", "served"])
+    ap.add_argument("--plummer-n", type=int, default=2000000)
     ap.add_argument("--nreq", type=int, default=64, help="served: requests in the stream")
     ap.add_argument("--slots", type=int, default=4, help="served: worker slots")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="served: HBM budget")
@@ -468,10 +470,32 @@ def main():
         run_served(args)
         return
 
+    if args.workload == "plummer":
+        run_particles(args, rank, world, local, dist, plummer_workload(args.plummer_n), quintic=True,
+                      metric="density+force particle-updates/s (Plummer 2M, quintic)",
+                      label=f"Plummer a=1 r<20, {args.plummer_n} particles, h = (m/rho)^(1/3) x lognormal(0.3), "
+                            "|v| = 0.5 v_circ, u = 0.05, quintic, hfact 1.0, density(NR+gradients)+force, open")
+        return
+    run_particles(args, rank, world, local, dist, workload(args.npartx), quintic=False, metric=METRIC,
+                  label=f"lattice {args.npartx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, cubic, "
+                        "open boundaries")
+
+
+def plummer_workload(n, seed=42):
+    """The clustered deep-tree workload: a Plummer sphere (a = 1, r < 20) of n particles,
+    h = hfact (m / rho_Plummer)^(1/3) x lognormal(0.3) with hfact 1.0, velocities isotropic
+    at 0.5 x the circular speed, u = 0.05, gamma = 5/3, alpha_AV = 1 (quintic kernel)."""
+    from cosmosphere_b200 import inputs
+    p = inputs.plummer(n, rmax=20.0, hfact=1.0, lnsigma=0.3, vfrac=0.5, seed=seed)
+    th = inputs._thermo(p, 0.05, hfact=1.0)
+    p["pro2"], p["cs"], p["alpha"], p["u"] = th[0], th[1], th[2], th[3]
+    p["hfact"] = 1.0
+    return p
+
+
+def measure(args, c, p, mixed, hfact, dist, local, profile=False):
+    """Device-resident and end-to-end timing of density + force steps of one precision."""
     from cosmosphere_b200 import capi
-    c = capi.Cosmo()
-    c.set_device(local)
-    p = workload(args.npartx)
     n = p.n
     pm = p["pmass"]
     pos = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]))
@@ -484,10 +508,6 @@ def main():
     for a in [pos, hsml, vel, acc, thermo] + list(outs.values()):
         c.pin(a)
     c.arrays_init(n)
-    mixed = args.precision == "mixed"
-    accuracy = None
-    if mixed and not args.profile:
-        accuracy = mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs)
     c.set_precision(mixed)
 
     def upload_inputs():
@@ -497,12 +517,12 @@ def main():
         c.upload(capi.ACCEL, acc, n)
 
     def step_resident():
-        c.density(n, pm, tolh=1e-4, hfact=1.2)
+        c.density(n, pm, tolh=1e-4, hfact=hfact)
         c.force(n, pm, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
 
     def step_e2e():
         upload_inputs()
-        c.density(n, pm, tolh=1e-4, hfact=1.2)
+        c.density(n, pm, tolh=1e-4, hfact=hfact)
         c.upload(capi.THERMO, thermo, n, sorted_=True)
         c.force(n, pm, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
         for slot, buf in outs.items():
@@ -510,26 +530,20 @@ def main():
 
     # inputs resident; THERMO gathered into Hilbert order once (every step sorts the same input)
     upload_inputs()
-    c.density(n, pm, tolh=1e-4, hfact=1.2)
+    c.density(n, pm, tolh=1e-4, hfact=hfact)
     c.upload(capi.THERMO, thermo, n, sorted_=True)
-
-    # ---------------- device-resident timing
     for _ in range(args.warmup):
         step_resident()
-    if args.profile:
+    if profile:
         for _ in range(args.steps):
             step_resident()
         c.sync()
-        print(json.dumps({"profile_steps": args.steps, "particles": n,
-                          "nr_iterations": len(c.array("activePerIter"))}), flush=True)
-        return
-    clocks = ClockSampler(local)
-    time.sleep(0.3)
+        return {"nr_iterations": len(c.array("activePerIter"))}
     barrier(dist, local)
     c.sync()
     launches0 = c.launches()
     upd_step = 0.0
-    t_nr = t_fk = 0.0
+    t_nr = t_fk = t_gk = 0.0
     pairs = nr_upd = 0.0
     nr_launches = 0
     c.mark(0)
@@ -540,19 +554,17 @@ def main():
         nr_upd += float(act.sum())
         nr_launches += len(act)
         t_nr += c.scalar("t_nrkern")
+        t_gk += c.scalar("t_gradkern")
         t_fk += c.scalar("t_fkern")
         pairs += c.scalar("pairsDensity")
     c.mark(1)
     t_dev = c.elapsed(0, 1)
     c.sync()
     barrier(dist, local)
-    clk = clocks.stop()
     launches = c.launches() - launches0
     t_max = max_over_ranks(dist, local, t_dev)
     upd_total = sum_over_ranks(dist, local, upd_step * args.steps)
-    value = upd_total / t_max
-
-    # ---------------- end to end through the C-ABI
+    # end to end through the C-ABI
     for _ in range(args.warmup):
         step_e2e()
     barrier(dist, local)
@@ -566,55 +578,97 @@ def main():
     t_e2e_wall = time.perf_counter() - w0
     barrier(dist, local)
     t_e2e = max_over_ranks(dist, local, max(t_e2e_dev, t_e2e_wall))
-    e2e_value = upd_total / t_e2e
-    h2d = 8 * n * (3 + 1 + 3 + 3 + 4)
-    d2h = 8 * n * (1 + 2 + 3 + 6)
+    res = {"value": upd_total / t_max, "ms_per_step": 1e3 * t_max / args.steps,
+           "e2e_value": upd_total / t_e2e, "e2e_ms_per_step": 1e3 * t_e2e / args.steps,
+           "updates_per_step": upd_step, "nr_iterations": len(act), "launches": launches,
+           "kernel_ms_per_step": {"density_nr": 1e3 * t_nr / args.steps, "gradient": 1e3 * t_gk / args.steps,
+                                  "force": 1e3 * t_fk / args.steps},
+           "t_nr": t_nr, "nr_upd": nr_upd, "pairs": pairs, "nr_launches": nr_launches,
+           "h2d": 8 * n * (3 + 1 + 3 + 3 + 4), "d2h": 8 * n * (1 + 2 + 3 + 6)}
+    c.set_precision(False)
+    for a in [pos, hsml, vel, acc, thermo] + list(outs.values()):
+        c.unpin(a)
+    return res
 
-    # ---------------- roofline of the Newton density kernel (dominant launch)
+
+def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
+    """One set of particles: the plain FP64 form (the headline value) and the mixed form,
+    with the mixed form's error against FP64 on the same inputs."""
+    from cosmosphere_b200 import capi
+    c = capi.Cosmo(quintic=quintic)
+    c.set_device(local)
+    n = p.n
+    hfact = p.get("hfact", 1.2)
+    if args.profile:
+        r = measure(args, c, p, args.precision == "mixed", hfact, dist, local, profile=True)
+        print(json.dumps({"profile_steps": args.steps, "particles": n, **r}), flush=True)
+        return
+    accuracy = None
+    if args.precision in ("mixed", "both"):
+        pos = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]))
+        hsml = np.ascontiguousarray(p["h"])
+        vel = np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]]))
+        acc = np.zeros((3, n))
+        thermo = np.ascontiguousarray(np.stack([p["pro2"], p["cs"], p["alpha"], p["u"]]))
+        outs = {capi.HSML: np.empty((1, n)), capi.DENS_OUT: np.empty((2, n)), capi.GRAD_OUT: np.empty((3, n)),
+                capi.FORCE_OUT: np.empty((6, n))}
+        c.arrays_init(n)
+        accuracy = mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs, hfact)
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    plain = measure(args, c, p, False, hfact, dist, local) if args.precision in ("fp64", "both") else None
+    mixed = measure(args, c, p, True, hfact, dist, local) if args.precision in ("mixed", "both") else None
+    clk = clocks.stop()
+    head = plain if plain is not None else mixed
+    # roofline of the Newton density kernel (the largest single kernel of the step)
     fp64_peak = c.fp64_peak_tflops()
-    flops = FLOP_PER_DENSITY_PAIR * pairs + FLOP_PER_NR_UPDATE * nr_upd
-    achieved = flops / t_nr / 1e12
+    flops = FLOP_PER_DENSITY_PAIR * head["pairs"] + FLOP_PER_NR_UPDATE * head["nr_upd"]
+    achieved = flops / head["t_nr"] / 1e12
     peaks, src = measured_peaks()
-    hbm_achieved = BYTES_PER_DENSITY_UPDATE * nr_upd / t_nr / 1e9
-    traffic = ncu_traffic("density_nr_kernel")
-
+    hbm_achieved = BYTES_PER_DENSITY_UPDATE * head["nr_upd"] / head["t_nr"] / 1e9
+    kname = "density_nr_kernel"
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not quintic:
         cp = workload(args.ref_npartx)
         u, dt, cores = cpu_oracle_step(cp)
         cpu = {"value": u / dt, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"lattice-{args.ref_npartx} instance of the same generator ({cp.n} particles), "
                          "one density+force step of the CPU oracle (FP64, OpenMP)"}
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-            "precision": args.precision, "accuracy_vs_fp64": accuracy,
-            "config": {"workload": f"lattice {args.npartx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, "
-                                   "cubic, open boundaries",
-                       "particles": n, "particles_per_gpu": n, "nr_iterations": len(act),
-                       "updates_per_step": upd_step, "parallelism": f"replicas x{world}",
-                       "l2": "working set ~0.4 GB > 126 MB L2 (no flush needed)"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": 1e3 * t_e2e / args.steps},
-            "roofline": {"kernel": "density_nr_mixed_kernel" if mixed else "density_nr_kernel",
-                         "bound": "fp64", "achieved": achieved,
-                         "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
-                         "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
-                         "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
-                         "traffic": traffic,
-                         "hbm": {"achieved": hbm_achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                                 "frac": hbm_achieved / peaks.get("hbm_gbs"), "source": src,
-                                 "byte_convention": "56 B per particle-update"},
-                         "launch_ms": 1e3 * t_nr / max(1, nr_launches)},
-            "kernel_ms_per_step": {"density_nr": 1e3 * t_nr / args.steps, "force": 1e3 * t_fk / args.steps},
-            "cpu_baseline": cpu,
-            "clocks": clk,
-            "gpu_launches": launches,
-        }
-        print(json.dumps(line), flush=True)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    strip = lambda r: None if r is None else {k: v for k, v in r.items()
+                                              if k not in ("t_nr", "nr_upd", "pairs", "nr_launches", "h2d", "d2h")}
+    line = {
+        "metric": metric, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if plain is not None else "f32+f64", "data": "synthetic",
+        "precision": "fp64" if plain is not None else "mixed",
+        "config": {"workload": label, "particles": n, "particles_per_gpu": n,
+                   "nr_iterations": head["nr_iterations"], "updates_per_step": head["updates_per_step"],
+                   "parallelism": f"replicas x{world}", "l2": "working set above the 126 MB L2 (no flush needed)"},
+        "e2e": {"value": head["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
+                "d2h_bytes_per_step": head["d2h"], "ms_per_step": head["e2e_ms_per_step"]},
+        "roofline": {"kernel": kname, "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak,
+                     "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
+                     "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
+                     "traffic": ncu_traffic(kname),
+                     "hbm": {"achieved": hbm_achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                             "frac": hbm_achieved / peaks.get("hbm_gbs"), "source": src,
+                             "byte_convention": "56 B per particle-update"},
+                     "launch_ms": 1e3 * head["t_nr"] / max(1, head["nr_launches"])},
+        "kernel_ms_per_step": head["kernel_ms_per_step"],
+        "plain_fp64": strip(plain),
+        "mixed": None if mixed is None else {**strip(mixed),
+                                             "speedup_vs_plain": (mixed["value"] / plain["value"]) if plain else None,
+                                             "accuracy_vs_fp64": accuracy},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": head["launches"],
+    }
+    print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 

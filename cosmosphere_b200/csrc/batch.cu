@@ -771,7 +771,8 @@ static void run_items(Batch& B, const int* leaves, const int* countPtr, bool eva
     COSMO_LAUNCHED();
     plan_items_table_kernel<<<s.numSMs * 8, kThreads, 0, s.st>>>(leaves, countPtr, B.leafRange.get(),
                                                                   evalAll ? nullptr : B.converged.get(),
-                                                                  B.jstream.get(), B.items.get(), cap, ds);
+                                                                  B.jstream.get(), B.xyzh.get(), B.items.get(), cap,
+                                                                  ds);
     COSMO_LAUNCHED();
     const PreorderTree tree{B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(), 0, 0};
     auto go = [&](auto kern) {

@@ -69,6 +69,34 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
             [&](const double4* rg, const float4*, const int*, int head, int count) {
                 gc += count;
                 const double4 pj = rg[(head + (lane < count ? lane : 0)) & (kRing - 1)];
+                if (ng == 1)
+                {
+                    // a single particle (a cut group): every lane evaluates its own pair and
+                    // the sums fold the lanes in order through shuffles, a rejected lane
+                    // adding +0 (which leaves a sum started at +0 unchanged)
+                    const double4 g = grp[0];
+                    double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                    const double q2 = pair_r2(dx, dy, dz) * g.w;
+                    const bool acc = lane < count && q2 < kRadK2;
+                    double wv = 0.0, tv = 0.0;
+                    if (acc)
+                    {
+                        const double q = sqrt(q2);
+                        double wk, dwk;
+                        sph_kernel(q2, q, wk, dwk);
+                        wv = wk;
+                        tv = -q * dwk - 3.0 * wk;
+                    }
+                    gp += __popc(__ballot_sync(0xffffffffu, acc));
+#pragma unroll
+                    for (int k = 0; k < 32; ++k)
+                    {
+                        sr += __shfl_sync(0xffffffffu, wv, k);
+                        sg += __shfl_sync(0xffffffffu, tv, k);
+                    }
+                    return;
+                }
                 int nrec = 0, segStart = 0, segCount = 0;
                 auto flush = [&]() {
                     __syncwarp();
@@ -141,13 +169,37 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         gh[lane] = mine ? float(hinv2) : 0.0f;
         __syncwarp();
         const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
-        KahanF kr, kg;
+        KahanF kr, kg, lr, lg;
         src.template stream<false, true, false, Periodic>(
             nullptr, ringf, nullptr, bx, sx, sy, sz, lx, ly, lz,
             [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
             [&](const double4*, const float4* rf, const int*, int head, int count) {
                 gc += count;
                 const float4 pf = rf[(head + (lane < count ? lane : 0)) & (kRing - 1)];
+                if (ng == 1)
+                {
+                    // a single particle (a cut group): every lane keeps its own compensated
+                    // partial sums, combined in FP64 after the stream
+                    float dx = gx[0] - pf.x, dy = gy[0] - pf.y, dz = gz[0] - pf.z;
+                    if (Periodic && !shifted)
+                    {
+                        dx = axis_df<true>(gx[0], pf.x, Lx);
+                        dy = axis_df<true>(gy[0], pf.y, Ly);
+                        dz = axis_df<true>(gz[0], pf.z, Lz);
+                    }
+                    const float q2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) * gh[0];
+                    const bool acc = lane < count && q2 < float(kRadK2);
+                    if (acc)
+                    {
+                        const float q = sqrt_q(q2);
+                        float wk, dwk;
+                        sph_kernel_f(q2, q, wk, dwk);
+                        lr.add(wk);
+                        lg.add(fmaf(-q, dwk, -3.0f * wk));
+                    }
+                    gp += __popc(__ballot_sync(0xffffffffu, acc));
+                    return;
+                }
                 int nrec = 0, segStart = 0, segCount = 0;
                 auto flush = [&]() {
                     __syncwarp();
@@ -221,6 +273,18 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
             });
         rhoi = kr.value();
         gradhi = kg.value();
+        if (ng == 1)
+        {
+            double a = lr.value(), b = lg.value();
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                a += __shfl_xor_sync(0xffffffffu, a, o);
+                b += __shfl_xor_sync(0xffffffffu, b, o);
+            }
+            rhoi = a;
+            gradhi = b;
+        }
     }
 }
 

@@ -68,7 +68,7 @@ __device__ __forceinline__ bool newton_step(double rhoi, double gradhi, double h
 // iteration (once per leaf), and flags the lists stale when an updated h outgrows the
 // radius its leaf's list covers.
 template<bool Periodic, bool Mixed>
-__global__ void __launch_bounds__(kThreads, Mixed ? 8 : 6)
+__global__ void __launch_bounds__(kThreads, Mixed ? 6 : 5)
 density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                   const int* __restrict__ jlist, double4* __restrict__ xyzh, double* __restrict__ rho,
@@ -521,8 +521,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                                                                                             nL);
             COSMO_LAUNCHED();
             plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
-                s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(), s.items.get(),
-                itemCap, ds);
+                s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(), s.xyzh.get(),
+                s.items.get(), itemCap, ds);
             COSMO_LAUNCHED();
             const bool mx = s.precision == 1;
             auto nr = mx ? (s.periodic ? density_nr_kernel<true, true> : density_nr_kernel<false, true>)
@@ -599,7 +599,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
         COSMO_LAUNCHED();
         plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
-                                                        s.items.get(), nA, ds);
+                                                        s.xyzh.get(), s.items.get(), nA, ds);
         COSMO_LAUNCHED();
         auto rows = s.periodic ? gather_rows_kernel<true> : gather_rows_kernel<false>;
         rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(

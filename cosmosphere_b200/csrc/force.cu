@@ -386,7 +386,7 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
             begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
             COSMO_LAUNCHED();
             plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
-                                                            s.items.get(), nA, ds);
+                                                            s.xyzh.get(), s.items.get(), nA, ds);
             COSMO_LAUNCHED();
             auto rows = s.periodic ? sym_rows_kernel<true> : sym_rows_kernel<false>;
             rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(

@@ -91,8 +91,7 @@ struct DevScalars
     unsigned long long pairs[4]; // accepted pairs: density, gradient, force, candidates
     unsigned int sortTiles[16];  // onesweep tile tickets, one per digit pass
     int itemsHeavy, itemsLight;  // Newton work items of the current iteration (split, whole)
-    int listParticles;           // particles of the current pass on their neighbour lists
-    int pad[3];
+    int pad[4];
 };
 
 struct Timings
@@ -146,10 +145,8 @@ struct State
     DBuf<double> listH;                         // h each leaf's gather list covers
     DBuf<int> jlist;
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
-    DBuf<int> nbl;                              // per-particle neighbour lists, kNbl per row
-    DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed; < 0: none)
-    DBuf<double> nblH;                          // largest h each row stays complete for
-    DBuf<int> listItems;                        // particles of a pass that use their rows
+    DBuf<int> nbl;                              // neighbour rows, kNbl entries per particle
+    DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed)
     DBuf<int> leafNext;                         // leaf already queued for the next iteration
     DBuf<int> activeA, activeB, allLeaves;
 

@@ -27,39 +27,30 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
         ds->workCounter[0] = 0;
         ds->itemsHeavy = 0;
         ds->itemsLight = 0;
-        ds->listParticles = 0;
     }
     for (int l = t; l < nL; l += gridDim.x * blockDim.x) leafNext[l] = 0;
 }
 
-// Work items of one pass: every group of a leaf's 64-slot window of active particles
-// (unconverged ones in a Newton iteration; all when converged is null, and all leaves
-// when leaves is null) is one item (leaf, window << 16 | group << 8 | groups, the two
-// halves of the window's active mask).  Groups hold up to 32 particles; a leaf whose
-// gather list streams more than kSplitStream particles is cut into smaller groups, about
-// kSplitWork / stream particles each, so that no single warp carries the iteration's
-// tail.  Cut items are queued from the front of the buffer and run first, whole groups
-// from the back.  The items of a window hold at most its active particles, so cap = the
+// Work items of one pass.  The active particles (unconverged ones in a Newton iteration;
+// all when converged is null, of all leaves when leaves is null) of each 64-slot window of
+// a leaf are grouped, and each group of up to 32 is one item: (leaf, window << 16 | 1, the
+// two halves of the group's member mask).  A leaf whose gather list streams more than
+// kSplitStream particles is cut into smaller groups, about kSplitWork / stream particles
+// each, so that no single warp carries the pass's tail; cut items are queued from the
+// front of the buffer and run first (their warps scan the tree for their own box), whole
+// groups from the back.  A window's items hold at most its active particles, so cap = the
 // particle count always suffices.
-//
-// With rows given (nblCount, nblH of the per-particle neighbour lists, K entries a row),
-// an active particle whose row is complete for its current h -- no overflow, h <= nblH --
-// goes to listItems instead (ds->listParticles of them) and out of the groups.
 constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
 
 template<class Ranges>
 __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int nActive, Ranges ranges,
                                            const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
-                                           int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
-                                           const int* __restrict__ nblCount, const double* __restrict__ nblH,
-                                           const double4* __restrict__ xyzh, int K, int* __restrict__ listItems)
+                                           const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
+                                           DevScalars* __restrict__ ds)
 {
-    const uint32_t lt = (1u << (threadIdx.x & 31)) - 1u;
-    auto rowOK = [&](uint32_t a) {
-        return listItems != nullptr && unsigned(nblCount[a]) <= unsigned(K) && xyzh[a].w <= nblH[a];
-    };
     const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nWarps = (gridDim.x * blockDim.x) >> 5;
     for (int w = warp; w < nActive; w += nWarps)
@@ -74,34 +65,25 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
             const uint32_t a0 = g + lane, a1 = g + 32 + lane;
             const bool act0 = a0 < p1 && (!converged || converged[a0] == 0);
             const bool act1 = a1 < p1 && (!converged || converged[a1] == 0);
-            const bool row0 = act0 && rowOK(a0), row1 = act1 && rowOK(a1);
-            if (listItems != nullptr)
-            {
-                const uint32_t r0 = __ballot_sync(0xffffffffu, row0), r1 = __ballot_sync(0xffffffffu, row1);
-                if (r0 | r1)
-                {
-                    int base = 0;
-                    if (lane == 0) base = atomicAdd(&ds->listParticles, __popc(r0) + __popc(r1));
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    if (row0) listItems[base + __popc(r0 & lt)] = int(a0);
-                    if (row1) listItems[base + __popc(r0) + __popc(r1 & lt)] = int(a1);
-                }
-            }
-            const uint32_t m0 = __ballot_sync(0xffffffffu, act0 && !row0);
-            const uint32_t m1 = __ballot_sync(0xffffffffu, act1 && !row1);
-            const int nAct = __popc(m0) + __popc(m1);
-            if (nAct == 0) continue;
-            const int whole = (nAct + 31) >> 5;
-            const int G = max(whole, (nAct + gsize - 1) / gsize);
+            const uint32_t c0 = __ballot_sync(0xffffffffu, act0), c1 = __ballot_sync(0xffffffffu, act1);
+            const int nC = __popc(c0) + __popc(c1);
+            if (nC == 0) continue;
+            const int wnd = int((g - p0) >> 6);
+            const int whole = (nC + 31) >> 5;
+            const int G = max(whole, (nC + gsize - 1) / gsize);
             const bool split = G > whole;
             int base = 0;
             if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
             base = __shfl_sync(0xffffffffu, base, 0);
-            const int wnd = int((g - p0) >> 6);
-            for (int k = lane; k < G; k += 32)
+            // group k takes the active ranks [k nC / G, (k + 1) nC / G)
+            const int r0 = __popc(c0 & lt), r1 = __popc(c0) + __popc(c1 & lt);
+            for (int k = 0; k < G; ++k)
             {
+                const int lo = k * nC / G, hi = (k + 1) * nC / G;
+                const uint32_t i0 = __ballot_sync(0xffffffffu, act0 && r0 >= lo && r0 < hi);
+                const uint32_t i1 = __ballot_sync(0xffffffffu, act1 && r1 >= lo && r1 < hi);
                 const int idx = split ? base + k : cap - 1 - (base + k);
-                if (idx >= 0 && idx < cap) items[idx] = make_int4(leaf, (wnd << 16) | (k << 8) | G, int(m0), int(m1));
+                if (lane == 0 && idx >= 0 && idx < cap) items[idx] = make_int4(leaf, (wnd << 16) | 1, int(i0), int(i1));
             }
         }
     }
@@ -109,23 +91,19 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
 
 __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
                                   const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
-                                  int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
-                                  const int* __restrict__ nblCount = nullptr, const double* __restrict__ nblH = nullptr,
-                                  const double4* __restrict__ xyzh = nullptr, int K = 0,
-                                  int* __restrict__ listItems = nullptr)
+                                  const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
+                                  DevScalars* __restrict__ ds)
 {
-    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, items, cap, ds, nblCount, nblH, xyzh, K,
-               listItems);
+    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds);
 }
 
 // The same over a forest's range table, the active count read on the device.
 __global__ void plan_items_table_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr,
                                         const uint2* __restrict__ range, const int* __restrict__ converged,
-                                        const uint32_t* __restrict__ jstream, int4* __restrict__ items, int cap,
-                                        DevScalars* __restrict__ ds)
+                                        const uint32_t* __restrict__ jstream, const double4* __restrict__ xyzh,
+                                        int4* __restrict__ items, int cap, DevScalars* __restrict__ ds)
 {
-    plan_items(leaves, *countPtr, TableRanges{range}, converged, jstream, items, cap, ds, nullptr, nullptr, nullptr,
-               0, nullptr);
+    plan_items(leaves, *countPtr, TableRanges{range}, converged, jstream, xyzh, items, cap, ds);
 }
 
 // A persistent grid: as many blocks of the kernel as fit on the device at once.
