@@ -181,14 +181,20 @@ def mixed_accuracy(c, p, n, pos, hsml, vel, acc, thermo, outs, hfact=1.2):
             "a_max_rel_to_rms_a": float(da.max() / rms_a), "a_rms_rel_to_rms_a": float(np.sqrt((da ** 2).mean()) / rms_a)}
 
 
-def run_ensemble(args):
+def run_ensemble(args, rank, world, local, dist):
     """The batched-ensemble workload: 256 sets (log-uniform 1e4..5e5 particles, periodic
     uniform boxes and Plummer spheres), density / Newton-Raphson only.  Batched solves
-    (plain and mixed) against 256 sequential plain FP64 single-set solves on the same GPU."""
-    from cosmosphere_b200 import capi, inputs
-    sets = inputs.ensemble_sets(args.nsets)
-    n = sum(p.n for p in sets)
+    (plain and mixed) against 256 sequential plain FP64 single-set solves on the same GPU.
+    On N GPUs the sets are packed onto the ranks by particle count (no exchange step);
+    each rank times its own share and the job's time is the slowest rank's."""
+    from cosmosphere_b200 import capi, inputs, shard
+    sizes = inputs.ensemble_sizes(args.nsets)
+    shares = shard.pack_sets(sizes, world)
+    mine = shares[rank]
+    sets = inputs.ensemble_sets(args.nsets, only=mine)
+    n_all = int(sizes.sum())
     c = capi.Cosmo()
+    c.set_device(local)
     res = {}
     outs = {}
     for mode in ("fp64", "mixed"):
@@ -200,28 +206,34 @@ def run_ensemble(args):
         t = 0.0
         upd = 0.0
         tnr = 0.0
+        barrier(dist, local)
         for _ in range(args.steps):
             assert b.density(final_rho=True) == 0
             t += b.scalar("t_total")
             tnr += b.scalar("t_nr")
             upd += b.scalar("updates")
+        t_max = shard.reduce_scalar(dist, t, "max", device=f"cuda:{local}" if dist else None)
+        upd_all = shard.reduce_scalar(dist, upd, "sum", device=f"cuda:{local}" if dist else None)
         # end to end: upload + solve + download through the batch C-ABI
+        barrier(dist, local)
         w0 = time.perf_counter()
         for _ in range(args.steps):
             b.upload()
             assert b.density(final_rho=True) == 0
             out = b.download()
-        we = (time.perf_counter() - w0) / args.steps
+        we = shard.reduce_scalar(dist, (time.perf_counter() - w0) / args.steps, "max",
+                                 device=f"cuda:{local}" if dist else None)
         outs[mode] = out
-        res[mode] = {"value": upd / t, "ms_per_solve": 1e3 * t / args.steps, "e2e_ms_per_solve": 1e3 * we,
+        res[mode] = {"value": upd_all / t_max, "ms_per_solve": 1e3 * t_max / args.steps, "e2e_ms_per_solve": 1e3 * we,
+                     "e2e_value": upd_all / args.steps / we,
                      "ms_newton_loop_graph": 1e3 * tnr / args.steps, "graph": b.scalar("graph") == 1.0,
-                     "updates_per_solve": upd / args.steps, "iters": b.scalar("itersRun"),
-                     "leaves": b.scalar("nLeaves")}
+                     "updates_per_solve": upd_all / args.steps, "iters": b.scalar("itersRun"),
+                     "leaves_rank0": b.scalar("nLeaves")}
     c.set_precision(False)
     # sequential plain FP64 single-set solves
     tseq = 0.0
     useq = 0.0
-    c.mark(4)
+    barrier(dist, local)
     for p in sets:
         c.arrays_init(p.n)
         c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
@@ -231,25 +243,38 @@ def run_ensemble(args):
         c.mark(6)
         tseq += c.elapsed(5, 6)
         useq += float(c.array("activePerIter").sum())
+    tseq = shard.reduce_scalar(dist, tseq, "max", device=f"cuda:{local}" if dist else None)
+    useq = shard.reduce_scalar(dist, useq, "sum", device=f"cuda:{local}" if dist else None)
     h0, r0 = np.concatenate(outs["fp64"][0]), np.concatenate(outs["fp64"][1])
     h1, r1 = np.concatenate(outs["mixed"][0]), np.concatenate(outs["mixed"][1])
     live = h0 > 0
-    line = {"metric": f"batched density particle-updates/s ({len(sets)}-set ensemble)",
-            "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": res["mixed"]["ms_per_solve"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"{len(sets)} sets, log-uniform 1e4..5e5 particles, even: periodic uniform box, "
-                                   "odd: Plummer r<20; h = 1.2 x spacing x U[0.8,1.2]; cubic; density/NR loop "
-                                   "as one CUDA graph + rho at the converged h",
-                       "particles": n},
-            "batched_mixed": res["mixed"], "batched_fp64": res["fp64"],
-            "sequential_fp64": {"value": useq / tseq, "ms_total": 1e3 * tseq, "updates": useq,
-                                "how": "one single-set plain FP64 solve per set through the C-ABI, device-timed"},
-            "speedup_mixed_batched_vs_sequential_fp64": (res["mixed"]["value"]) / (useq / tseq),
-            "speedup_mixed_vs_fp64_batched": res["mixed"]["value"] / res["fp64"]["value"],
-            "accuracy_mixed_vs_fp64": {"h_max_rel": float(np.max(np.abs(h1[live] / h0[live] - 1))),
-                                       "rho_max_rel": float(np.max(np.abs(r1[live] / r0[live] - 1)))}}
-    print(json.dumps(line), flush=True)
+    eh = shard.reduce_scalar(dist, float(np.max(np.abs(h1[live] / h0[live] - 1))), "max",
+                             device=f"cuda:{local}" if dist else None)
+    er = shard.reduce_scalar(dist, float(np.max(np.abs(r1[live] / r0[live] - 1))), "max",
+                             device=f"cuda:{local}" if dist else None)
+    if rank == 0:
+        line = {"metric": f"batched density particle-updates/s ({args.nsets}-set ensemble)",
+                "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": res["mixed"]["ms_per_solve"], "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+                "config": {"workload": f"{args.nsets} sets, log-uniform 1e4..5e5 particles, even: periodic uniform "
+                                       "box, odd: Plummer r<20; h = 1.2 x spacing x U[0.8,1.2]; cubic; density/NR "
+                                       "loop as one CUDA graph + rho at the converged h",
+                           "particles": n_all,
+                           "parallelism": f"sets packed on {world} GPU(s), largest first onto the least-loaded "
+                                          f"(imbalance {shard.imbalance(sizes, shares):.3f})"},
+                "e2e": {"value": res["mixed"]["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": 8 * 4 * n_all,
+                        "d2h_bytes_per_step": 8 * 3 * n_all},
+                "batched_mixed": res["mixed"], "batched_fp64": res["fp64"],
+                "sequential_fp64": {"value": useq / tseq, "ms_total": 1e3 * tseq, "updates": useq,
+                                    "how": "one single-set plain FP64 solve per set through the C-ABI, device-timed"},
+                "speedup_mixed_batched_vs_sequential_fp64": (res["mixed"]["value"]) / (useq / tseq),
+                "speedup_mixed_vs_fp64_batched": res["mixed"]["value"] / res["fp64"]["value"],
+                "accuracy_mixed_vs_fp64": {"h_max_rel": eh, "rho_max_rel": er},
+                "roofline": None, "cpu_baseline": None, "gpu_launches": None}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def _served_fp64_loop(reqs):
@@ -332,23 +357,39 @@ def _served_run(reqs, arrivals, slots, budget_gb):
     return lat, upd, res, makespan, info
 
 
-def run_served(args):
+def run_served(args, rank, world, local, dist):
     """The served stream: requests with particle counts log-uniform in [5e3, 2e6] from the
     lattice / periodic-uniform / Plummer generators, 30% continuing a device-resident set
     (drift by v dt, dt = 0.1 min(h/c_s), Newton warm-started from the last h), admitted
     against an HBM budget, mixed precision; against the plain FP64 one-request-at-a-time
     loop through the C-ABI."""
-    from cosmosphere_b200 import capi, inputs
+    from cosmosphere_b200 import capi, inputs, shard
+    # on N GPUs each rank serves its share of the stream (new sets packed by particle
+    # count, continuations with their set); latencies are gathered, the job's makespan is
+    # the slowest rank's
+    skeleton = inputs.served_requests(args.nreq, seed=42, only=[])
+    owner = shard.pack_requests(skeleton, world)
+    mine = [k for k in range(len(skeleton)) if owner[k] == rank]
     tg = time.perf_counter()
-    reqs = inputs.served_requests(args.nreq, seed=42)
+    full = inputs.served_requests(args.nreq, seed=42, only=mine)
     tg = time.perf_counter() - tg
+    local_of = {k: i for i, k in enumerate(mine)}
+    reqs = []
+    for k in mine:
+        e = dict(full[k])
+        if e["kind"] == "cont":
+            e["of"] = local_of[e["of"]]
+        reqs.append(e)
+    dev = f"cuda:{local}" if dist else None
     c = capi.Cosmo()
+    c.set_device(local)
     # warm-up: the CUDA context and the FP64 loop's buffers at the largest size
     big = max((e for e in reqs if e["kind"] == "new"), key=lambda e: e["n"])
     _served_fp64_loop([big])
     serv, upd64, res64 = _served_fp64_loop(reqs)
     total_upd = float(np.sum(upd64))
-    cap64 = total_upd / float(np.sum(serv))
+    sum_local_serv = float(np.sum(serv))
+    cap64 = total_upd / sum_local_serv
     # Poisson arrivals at `load` x the FP64 loop's request rate
     rate = args.serve_load * len(reqs) / float(np.sum(serv))
     rng = np.random.default_rng(7)
@@ -362,33 +403,50 @@ def run_served(args):
         lat64.append(free - a)
     make64 = free - arrivals[0]
     c.set_precision(True)
-    _served_run([big], [0.0], args.slots, args.budget_gb)       # warm-up of the slots' states
+    # warm-up: one saturated pass of the whole stream, so the device memory pool and the
+    # pinned scalar blocks hold what the stream needs (a long-running server's state)
+    _served_run(reqs, np.zeros(len(reqs)), args.slots, args.budget_gb)
     lat, upd, res, makespan, info = _served_run(reqs, arrivals, args.slots, args.budget_gb)
     # saturated: every request at t = 0
     lat_b, upd_b, _, make_b, info_b = _served_run(reqs, np.zeros(len(reqs)), args.slots, args.budget_gb)
     c.set_precision(False)
-    eh = max(float(np.max(np.abs(a[0] / b[0] - 1.0))) for a, b in zip(res, res64))
-    er = max(float(np.max(np.abs(a[1] / b[1] - 1.0))) for a, b in zip(res, res64))
-    nnew = sum(1 for e in reqs if e["kind"] == "new")
-    bytes_in = sum(8 * e["n"] * 11 for e in reqs if e["kind"] == "new")
-    bytes_out = sum(8 * 12 * reqs[k if e["kind"] == "new" else e["of"]]["n"] for k, e in enumerate(reqs))
+    red = lambda v, op: shard.reduce_scalar(dist, v, op, device=dev)
+    eh = red(max(float(np.max(np.abs(a[0] / b[0] - 1.0))) for a, b in zip(res, res64)), "max")
+    er = red(max(float(np.max(np.abs(a[1] / b[1] - 1.0))) for a, b in zip(res, res64)), "max")
+    nnew = int(red(sum(1 for e in reqs if e["kind"] == "new"), "sum"))
+    nall = int(red(len(reqs), "sum"))
+    bytes_in = red(sum(8 * e["n"] * 11 for e in reqs if e["kind"] == "new"), "sum")
+    bytes_out = red(sum(8 * 12 * reqs[k if e["kind"] == "new" else e["of"]]["n"] for k, e in enumerate(reqs)), "sum")
+    pnew = int(red(sum(e["n"] for e in reqs if e["kind"] == "new"), "sum"))
+    lat, lat_b, lat64 = (shard.gather_floats(dist, v, world) for v in (lat, lat_b, lat64))
+    serv = shard.gather_floats(dist, serv, world)
     pct = lambda a, q: float(np.percentile(np.asarray(a) * 1e3, q))
-    thr_stream = float(np.sum(upd)) / makespan
-    thr_sat = float(np.sum(upd_b)) / make_b
+    thr_stream = red(float(np.sum(upd)), "sum") / red(makespan, "max")
+    thr_sat = red(float(np.sum(upd_b)), "sum") / red(make_b, "max")
+    makespan, make_b, make64 = red(makespan, "max"), red(make_b, "max"), red(make64, "max")
+    total_upd = red(total_upd, "sum")
+    cap64 = total_upd / red(sum_local_serv, "max")
+    rate = red(rate, "sum")
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     line = {"metric": "served density+force particle-updates/s (Poisson stream, 5e3..2e6 particles)",
-            "value": thr_sat, "unit": UNIT, "n_gpus": 1, "steps": len(reqs), "warmup": 1,
-            "ms_per_step": 1e3 * make_b / len(reqs), "higher_is_better": True, "scaling": "weak",
+            "value": thr_sat, "unit": UNIT, "n_gpus": world, "steps": nall, "warmup": 1,
+            "ms_per_step": 1e3 * make_b / nall, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"{len(reqs)} requests ({nnew} new sets, {len(reqs) - nnew} continuations), "
+            "config": {"workload": f"{nall} requests ({nnew} new sets, {nall - nnew} continuations), "
                                    "counts log-uniform 5e3..2e6 from lattice+jiggle / periodic uniform box / "
                                    "Plummer (cubic), density(NR+gradients)+force, dt = 0.1 min(h/c_s)",
-                       "particles_new": int(sum(e["n"] for e in reqs if e["kind"] == "new")),
+                       "particles_new": pnew,
                        "slots": args.slots, "hbm_budget_gb": args.budget_gb,
                        "offered_load": f"Poisson at {args.serve_load} x the FP64 loop's request rate "
-                                       f"({rate:.1f} req/s)",
+                                       f"({rate:.1f} req/s over all GPUs)",
+                       "parallelism": f"requests packed on {world} GPU(s) by particle count, continuations "
+                                      "with their set",
                        "input_generation_s": tg},
-            "e2e": {"value": thr_sat, "unit": UNIT, "h2d_bytes_per_step": bytes_in / len(reqs),
-                    "d2h_bytes_per_step": bytes_out / len(reqs),
+            "e2e": {"value": thr_sat, "unit": UNIT, "h2d_bytes_per_step": bytes_in / nall,
+                    "d2h_bytes_per_step": bytes_out / nall,
                     "how": "every request through the served C-ABI from host buffers: copy at submission, "
                            "H2D, solve, D2H of all outputs"},
             "served_mixed": {"stream": {"p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "max_ms": pct(lat, 100),
@@ -404,6 +462,8 @@ def run_served(args):
             "accuracy_mixed_vs_fp64": {"h_max_rel": eh, "rho_max_rel": er},
             "roofline": None, "cpu_baseline": None, "gpu_launches": None}
     print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_reference(args, rank, world, local, dist):
@@ -464,10 +524,10 @@ def main():
         run_reference(args, rank, world, local, dist)
         return
     if args.workload == "ensemble":
-        run_ensemble(args)
+        run_ensemble(args, rank, world, local, dist)
         return
     if args.workload == "served":
-        run_served(args)
+        run_served(args, rank, world, local, dist)
         return
 
     if args.workload == "plummer":

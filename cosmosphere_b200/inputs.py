@@ -116,16 +116,25 @@ def lattice100_workload(npartx: int = 100, seed: int = 42, vsigma=0.1, u=1.0, ga
     return p
 
 
-def ensemble_sets(nsets: int = 256, nmin: float = 1e4, nmax: float = 5e5, seed: int = 42):
+def ensemble_sizes(nsets: int = 256, nmin: float = 1e4, nmax: float = 5e5, seed: int = 42) -> np.ndarray:
+    """Particle counts of the batched-ensemble sets: log-uniform in [nmin, nmax], seeded."""
+    rng = np.random.default_rng(seed)
+    return np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsets))).astype(np.int64)
+
+
+def ensemble_sets(nsets: int = 256, nmin: float = 1e4, nmax: float = 5e5, seed: int = 42, only=None):
     """The batched-ensemble workload: nsets independent sets with sizes log-uniform in
     [nmin, nmax] (seeded); even sets uniform random in the unit periodic box, odd sets
     Plummer spheres (a = 1, r < 20); h = 1.2 x the local mean spacing x U[0.8, 1.2]
     (the spacing from the mean density for the box, from the Plummer density profile
-    for the spheres); pmass = 1/N."""
-    rng = np.random.default_rng(seed)
-    sizes = np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nsets))).astype(np.int64)
+    for the spheres); pmass = 1/N.  With only (set indices), just those sets, each the
+    same as in the full ensemble."""
+    sizes = ensemble_sizes(nsets, nmin, nmax, seed)
+    keep = set(range(nsets)) if only is None else set(int(k) for k in only)
     sets = []
     for k, n in enumerate(sizes):
+        if k not in keep:
+            continue
         if k % 2 == 0:
             p = uniform_box(int(n), hfac=1.2, hlo=0.8, hhi=1.2, seed=seed + 1000 + k)
             p["box"] = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
@@ -145,26 +154,34 @@ def _thermo(p, u, gamma=5.0 / 3.0, alpha=1.0, hfact=1.2):
                                           np.full(n, alpha), uu]))
 
 
-def served_requests(nreq: int = 96, nmin: float = 5e3, nmax: float = 2e6, pcont: float = 0.3, seed: int = 42):
+def served_requests(nreq: int = 96, nmin: float = 5e3, nmax: float = 2e6, pcont: float = 0.3, seed: int = 42,
+                    only=None):
     """The served-stream request list: particle counts log-uniform in [nmin, nmax]
     (seeded), each new set drawn from the lattice-with-jiggle, periodic-uniform-box or
     Plummer generator; with probability pcont a request instead continues an earlier set
     by one step of dt = 0.1 min(h/c_s) over that set's initial h.
 
-    Each entry is a dict: kind "new" with the particle set p (x, y, z, h, vx, vy, vz,
-    pmass, optional box), pos3 (3, n), vel3 (3, n) and thermo4 (4, n) component-major;
-    or kind "cont" with "of" (the index of the set's first request) and dt."""
+    Each entry is a dict: kind "new" with n and, when generated, the particle set p (x,
+    y, z, h, vx, vy, vz, pmass, optional box), pos3 (3, n), vel3 (3, n), thermo4 (4, n)
+    component-major and dt; or kind "cont" with "of" (the index of the set's first
+    request) and, when its set is generated, dt.  With only (request indices), just the
+    sets of those requests are generated (each the same as in the full stream)."""
     rng = np.random.default_rng(seed)
     out = []
     firsts = []
     for k in range(nreq):
         if firsts and rng.uniform() < pcont:
-            j = int(rng.choice(firsts))
-            out.append({"kind": "cont", "of": j, "dt": out[j]["dt"]})
+            out.append({"kind": "cont", "of": int(rng.choice(firsts))})
             continue
         n = int(np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
         g = int(rng.integers(3))
-        s = seed + 7919 * (k + 1)
+        out.append({"kind": "new", "n": n, "gen_id": g, "seed": seed + 7919 * (k + 1)})
+        firsts.append(k)
+    keep = set(range(nreq)) if only is None else set(int(k) for k in only)
+    for k, e in enumerate(out):
+        if e["kind"] != "new" or k not in keep:
+            continue
+        n, g, s = e["n"], e["gen_id"], e["seed"]
         if g == 0:
             npx = max(4, int(round((n / 1.403) ** (1.0 / 3.0))))
             p = lattice100_workload(npx, seed=s)
@@ -180,10 +197,11 @@ def served_requests(nreq: int = 96, nmin: float = 5e3, nmax: float = 2e6, pcont:
             p = plummer(n, rmax=20.0, hfact=1.2, lnsigma=0.3, vfrac=0.5, seed=s)
             th = _thermo(p, 0.05)
             gen = "Plummer"
-        dt = 0.1 * float(np.min(p["h"] / th[1]))
-        out.append({"kind": "new", "p": p, "gen": gen, "n": p.n, "dt": dt,
-                    "pos3": np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]])),
-                    "vel3": np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]])),
-                    "thermo4": th})
-        firsts.append(k)
+        e.update({"p": p, "gen": gen, "n": p.n, "dt": 0.1 * float(np.min(p["h"] / th[1])),
+                  "pos3": np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]])),
+                  "vel3": np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]])),
+                  "thermo4": th})
+    for e in out:
+        if e["kind"] == "cont" and "dt" in out[e["of"]]:
+            e["dt"] = out[e["of"]]["dt"]
     return out
