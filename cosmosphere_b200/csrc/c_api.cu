@@ -694,6 +694,15 @@ long cosmo_x_array(const char* name, void* out, int* dtype)
     if (k == "sizes") return put(s.sizes.get(), 3 * nN, 8, 0);
     if (k == "hmax_leaf") return put(s.hmaxLeaf.get(), nL, 8, 0);
     if (k == "hmax_node") return put(s.hmaxNode.get(), nN, 8, 0);
+    // the reference's state holds the gather lists after a density solve and the
+    // symmetric ones after a force pass; this library builds the symmetric ones with the
+    // gradient sweep, so the gather view is rebuilt (exactly) when asked for before a force
+    if ((k == "jcount" || k == "jOffset" || k == "jlist") && s.listsSym && !s.forceSinceSolve && nL > 0)
+    {
+        build_lists(s, false);
+        s.jlistToken = 0;
+        COSMO_CUDA(cudaStreamSynchronize(s.st));
+    }
     if (k == "jcount") return put(s.jcount.get(), nL, 4, 2);
     if (k == "jOffset") return put(s.jOffset.get(), nL + 1, 4, 2);
     if (k == "jlist")

@@ -263,51 +263,10 @@ struct GradSums
     }
 };
 
-// Post-convergence sweep, first pass: every live particle's gather row at its converged
-// h -- the j with q^2 = r^2 / h_i^2 < R^2 (the exact test of the sweep), ascending.
-template<bool Periodic>
-__global__ void __launch_bounds__(kThreads)
-gather_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
-                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
-                   const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
-                   int* __restrict__ nbl, int* __restrict__ nblCount, DevScalars* __restrict__ ds)
-{
-    __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double lx = 0, ly = 0, lz = 0;
-    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
-    const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
-    for (;;)
-    {
-        const int w = next_item(ds, nHeavy, nItems, cap);
-        if (w < 0) break;
-        const Item d = decode_item(items[w], layout);
-        const int slot = group_slot(d.m0, d.m1, d.nAct, d.grp, d.G, lane);
-        const bool mine = slot >= 0;
-        const uint32_t i = d.g0 + uint32_t(mine ? slot : 0);
-        const double4 pi = xyzh[i];
-        const double hinv2 = 1.0 / (pi.w * pi.w);
-        const double rs = kRadKernel * pi.w;
-        const double rmax = warp_max(mine ? rs : 0.0);
-        const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-        int rowLen = 0;
-        rows_group(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), bx, jOffset[d.leaf], jcount[d.leaf],
-                   jlist, LayoutRanges{layout}, xyzh,
-                   [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                   [&](const double4& g, const double4& pj) {
-                       double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
-                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                       return pair_r2(dx, dy, dz) * g.w < kRadK2;
-                   },
-                   mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
-        if (mine) nblCount[i] = rowLen;
-    }
-}
-
-// Post-convergence sweep, second pass: one lane per live particle over its row, the
-// exact test and the sums in the row's (ascending) order -- the same pairs and order as
-// the group sweep, so the results agree with it bit for bit.  Overflowed rows are left
-// to gradient_kernel.
+// Post-convergence sweep over the symmetric rows: one lane per live particle over its row
+// (at the converged h a superset of the gather pairs, ascending), the sweep's exact test
+// and the sums in the row's order -- the same pairs and order as the group sweep, so the
+// results agree with it bit for bit.  Overflowed rows are left to gradient_kernel.
 template<bool Periodic>
 __global__ void __launch_bounds__(kThreads)
 gradient_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict__ nblCount,
@@ -583,29 +542,17 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
             return res;
         }
     }
+    bool symBuilt = false;
     if (withGradients)
     {
+        // hmax of every leaf at the converged h, then the symmetric lists and rows of the
+        // force pass: at the converged h they hold every pair of the gather sweep too
         cudaEvent_t g0 = ev(s);
         hmax_leaves(s, s.allLeaves.get(), nL);
-        build_lists(s, false);
+        build_symmetric(s);
+        symBuilt = true;
         cudaEvent_t g1 = ev(s);
         const int grid = grid_for(s, nL);
-        // rows at the converged h, then one lane per particle over its row; the group
-        // sweep covers only the rows that overflowed
-        const int nA = std::max(s.nAlive, 1);
-        s.items.resize(nA, s.st);
-        s.nbl.resize(size_t(nA) * kNbl, s.st);
-        s.nblCount.resize(nA, s.st);
-        begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
-        COSMO_LAUNCHED();
-        plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
-                                                        s.xyzh.get(), s.items.get(), nA, ds);
-        COSMO_LAUNCHED();
-        auto rows = s.periodic ? gather_rows_kernel<true> : gather_rows_kernel<false>;
-        rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
-            s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-            s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
-        COSMO_LAUNCHED();
         if (s.precision == 1)
             launch_gradient_mixed(s, pmass);
         else
@@ -635,6 +582,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     }
     check_dev_err(s, "solveDensH");
     ++s.token;
+    s.forceSinceSolve = false;
+    if (symBuilt) s.jlistToken = s.rowsToken = s.token;
     return res;
 }
 

@@ -243,8 +243,9 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
     if (lane == 0) atomicAdd(&ds->pairs[2], pairs);
 }
 
-// Symmetric rows: every live particle's j with dr^2 > 0 and
-// dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10) (the force pass's exact tests), ascending.
+// Symmetric rows: every live particle's j with dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10),
+// ascending -- the force pass's pairs (which also need dr^2 > 0, tested where the row is
+// used) and, at the converged h, every pair of the gather sweep (i itself included).
 template<bool Periodic>
 __global__ void __launch_bounds__(kThreads)
 sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
@@ -276,7 +277,7 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        const double dr2 = pair_r2(dx, dy, dz);
-                       return dr2 > 0.0 && !(dr2 >= kRadK2 * fmax(g.w, pj.w * pj.w) * (1.0 + 1e-10));
+                       return !(dr2 >= kRadK2 * fmax(g.w, pj.w * pj.w) * (1.0 + 1e-10));
                    },
                    mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
         if (mine) nblCount[i] = rowLen;
@@ -335,23 +336,46 @@ __global__ void force_dead_kernel(int nAlive, int n, double* fx, double* fy, dou
 
 } // namespace
 
+void build_symmetric(State& s)
+{
+    DevScalars* ds = s.dscal.get();
+    const int nL = s.nLeaves;
+    hmax_upsweep(s);
+    build_lists(s, true);
+    if (nL <= 0) return;
+    const int grid = std::max(1, std::min(s.numSMs * 8, iceil(nL, kWarpsPerBlock)));
+    const int nA = std::max(s.nAlive, 1);
+    s.items.resize(nA, s.st);
+    s.nbl.resize(size_t(nA) * kNbl, s.st);
+    s.nblCount.resize(nA, s.st);
+    begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
+    COSMO_LAUNCHED();
+    plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
+                                                    s.xyzh.get(), s.items.get(), nA, ds);
+    COSMO_LAUNCHED();
+    auto rows = s.periodic ? sym_rows_kernel<true> : sym_rows_kernel<false>;
+    rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
+        s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+        s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
+    COSMO_LAUNCHED();
+}
+
 void compute_forces(State& s, double pmass, double beta, double alphau, bool disc, bool pdv, bool shock)
 {
     const int n = s.ngas;
     DevScalars* ds = s.dscal.get();
     COSMO_CUDA(cudaMemsetAsync(&ds->pairs[2], 0, sizeof(unsigned long long), s.st));
     cudaEvent_t e0 = ev(s);
-    // The symmetric list is cached per tree (src/force.cu:19-24).
-    if (s.jlistToken != s.token)
+    s.forceSinceSolve = true;
+    // The symmetric lists and rows are cached per tree (src/force.cu:19-24); the density
+    // solve's gradient sweep has normally built them already.
+    if (s.jlistToken != s.token || s.rowsToken != s.token || !s.listsSym)
     {
-        hmax_upsweep(s);
-        cudaEvent_t e1 = ev(s);
-        build_lists(s, true);
-        s.jlistToken = s.token;
+        build_symmetric(s);
+        s.jlistToken = s.rowsToken = s.token;
         cudaEvent_t e2 = ev(s);
         COSMO_CUDA(cudaStreamSynchronize(s.st));
-        s.t.upsweep += elapsed_s(e0, e1);
-        s.t.fjbuild += elapsed_s(e1, e2);
+        s.t.fjbuild += elapsed_s(e0, e2);
     }
     cudaEvent_t p0 = ev(s);
     force_prep_kernel<<<iceil(n, 256), 256, 0, s.st>>>(s.xyzh.get(), s.gradh.get(), s.thermo4.get(), n, pmass,
@@ -373,29 +397,8 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
             s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(), s.vsigmax.get(), s.divvF.get(), pmass,
             beta, pdv ? 1 : 0, shock ? 1 : 0, s.box.get(), ds);
     };
-    if (nL > 0)
-    {
-        // symmetric rows (cached with the symmetric lists), then one lane per particle over
-        // its row; the group pass covers only the rows that overflowed
-        if (s.rowsToken != s.token)
-        {
-            const int nA = std::max(s.nAlive, 1);
-            s.items.resize(nA, s.st);
-            s.nbl.resize(size_t(nA) * kNbl, s.st);
-            s.nblCount.resize(nA, s.st);
-            begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
-            COSMO_LAUNCHED();
-            plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
-                                                            s.xyzh.get(), s.items.get(), nA, ds);
-            COSMO_LAUNCHED();
-            auto rows = s.periodic ? sym_rows_kernel<true> : sym_rows_kernel<false>;
-            rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
-                s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-                s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
-            COSMO_LAUNCHED();
-            s.rowsToken = s.token;
-        }
-    }
+    // one lane per particle over its symmetric row; the group pass covers only the rows
+    // that overflowed
     if (s.precision == 1)
         launch_force_mixed(s, pmass, beta, disc, pdv, shock);
     else if (nL > 0)

@@ -218,8 +218,9 @@ gradient_mixed_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_
     if (lane == 0) atomicAdd(&ds->pairs[1], pairs);
 }
 
-// Mixed sweep over the gather rows: one lane per particle; the separation is formed in
-// FP64 at the nearest image and rounded to FP32, the pair terms are the group path's.
+// Mixed sweep over the symmetric rows: one lane per particle, the gather pairs selected
+// by the FP64 test; the separation is formed in FP64 at the nearest image and rounded to
+// FP32, the pair terms are the group path's.
 template<bool Periodic>
 __global__ void __launch_bounds__(kThreads)
 gradient_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict__ nblCount,
@@ -242,10 +243,12 @@ gradient_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __
         const float hinv2f = float(1.0 / (pi.w * pi.w));
         const int* row = nbl + size_t(i) * kNbl;
         GradSumsF gs;
+        const double hinv2 = 1.0 / (pi.w * pi.w);
         auto pair = [&](int j) {
             const double4 pj = ldg4(xyzh + j);
             double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+            if (!(pair_r2(dx, dy, dz) * hinv2 < kRadK2)) return;   // the gather pairs of the row
             const float fx = float(dx), fy = float(dy), fz = float(dz);
             const float r2 = fmaf(fz, fz, fmaf(fy, fy, fx * fx));
             gs.add(fx, fy, fz, r2, r2 * hinv2f, vi, ai, ldg4(vel4 + j), ldg4(acc4 + j), pmf);

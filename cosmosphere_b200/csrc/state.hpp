@@ -113,6 +113,8 @@ struct State
     int periodic = 0;
     double boxHost[6] = {0, 0, 0, 0, 0, 0};
     uint64_t token = 0, jlistToken = 0, rowsToken = 0;
+    bool listsSym = false;                      // the lists held are the symmetric ones
+    bool forceSinceSolve = false;               // a force pass ran on the current tree
     int itersRun = 0, maxIter = 100;
     int precision = 0;     // 0 plain FP64 (the drop-in form), 1 mixed FP32/FP64
     std::vector<long long> activePerIter;
@@ -175,6 +177,9 @@ void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
 // the gather radius to R * hmax * margin, so the lists stay valid while h grows by up to
 // that factor; listH records the h each leaf's list covers.
 void build_lists(State& s, bool symmetric, double margin = 1.0);
+// The symmetric lists and the symmetric neighbour rows of the current tree and h (the
+// force pass's pairs; every gather pair of the converged h is among them).
+void build_symmetric(State& s);
 void hmax_upsweep(State& s);
 void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int n, bool iotaValues);
 uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool readTotal);

@@ -759,6 +759,7 @@ void build_lists(State& s, bool symmetric, double margin)
     const uint32_t total = scan_exclusive(s, s.jcount.get(), s.jOffset.get(), s.nLeaves, true);
     s.jlist.resize(std::max<uint32_t>(total, 1u), s.st);
     run(true);
+    s.listsSym = symmetric;
 }
 
 } // namespace cosmo
