@@ -123,14 +123,15 @@ size_t state_device_bytes(const State& s)
     auto add = [&](const auto& buf) { b += buf.cap * sizeof(*buf.p); };
     for (auto* d : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
-                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH})
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH})
         add(*d);
     for (auto* d : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) add(*d);
     for (auto* d : {&s.prepAf, &s.prepBf, &s.thermof}) add(*d);
     for (auto* d : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) add(*d);
     for (auto* d : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
-                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount})
+                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
+                    &s.rowItems})
         add(*d);
     add(s.items);
     for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
@@ -147,14 +148,15 @@ void release_state(State& s)
     COSMO_CUDA(cudaStreamSynchronize(s.st));
     for (auto* b : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
-                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH})
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH})
         b->release(s.st);
     for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) b->release(s.st);
     for (auto* b : {&s.prepAf, &s.prepBf, &s.thermof}) b->release(s.st);
     for (auto* b : {&s.keysA, &s.keysB, &s.csTree, &s.csTree2, &s.prePrefix, &s.bfsPrefix, &s.nodeKeysTmp}) b->release(s.st);
     for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
-                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount})
+                    &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
+                    &s.rowItems})
         b->release(s.st);
     s.items.release(s.st);
     for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
@@ -614,6 +616,7 @@ double cosmo_x_scalar(const char* name)
     if (k == "token") return double(s.token);
     if (k == "hfact") return s.hfact;
     if (k == "maxIter") return s.maxIter;
+    if (k == "settling0") return double(s.settling0);
     if (s.hscal)
     {
         read_scalars(s);

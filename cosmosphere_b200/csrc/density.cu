@@ -24,6 +24,12 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
 constexpr double kListMargin = 1.15;            // gather-radius widening of the Newton lists
+// Newton rows: each still-active particle's j within kRowMargin of its support at its h
+// after the first update, built when at least 80% of the particles are settling (moved
+// by less than kSettle in that update), for the iterations after it; where fewer settle,
+// too many rows would go stale before they are used.
+constexpr double kRowMargin = 1.1;
+constexpr double kSettle = 0.15;
 
 // Newton-Raphson step of one particle from its un-normalised sums (src/density_base.cu:
 // 294-333): rho, d(rho)/dh, the new h (clamped to +-20%) and whether |dh/h| < tolh.
@@ -111,7 +117,7 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
             src.re = make_double3(sizes[3 * in] + ext, sizes[3 * in + 1] + ext, sizes[3 * in + 2] + ext);
         }
         density_group<Periodic, Mixed>(sScr[wib], mine, d.ng, pi, lx, ly, lz, src, rhoi, gradhi, gp, gc);
-        bool stillActive = false;
+        bool stillActive = false, settle = false;
         if (mine)
         {
             pairs += gp;
@@ -124,10 +130,13 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
             reinterpret_cast<double*>(xyzh + i)[3] = ho;
             converged[i] = conv;
             if (stillActive && ho > listH[leaf]) ds->listStale = 1;
+            settle = stillActive && fabs(ho - hi) < kSettle * hi;
         }
         const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
+        const uint32_t settled = __ballot_sync(0xffffffffu, settle);
         if (still && lane == 0)
         {
+            atomicAdd(&ds->settling, __popc(settled));
             atomicAdd(&ds->unconverged, __popc(still));
             if (atomicExch(&leafNext[leaf], 1) == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
         }
@@ -143,6 +152,150 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
         atomicAdd(&ds->pairs[0], pairs);
         atomicAdd(&ds->pairs[3], cand);
     }
+}
+
+// Newton rows of the still-active particles at their current h (ascending j).  A row is
+// complete while the particle's h stays within kRowMargin of the h it was built at and
+// within the radius its leaf's list covers; rowH records that bound.
+
+template<bool Periodic>
+__global__ void __launch_bounds__(kThreads)
+newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
+                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
+                   const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
+                   const double* __restrict__ listH, int* __restrict__ nbl, int* __restrict__ nblCount,
+                   double* __restrict__ rowH, DevScalars* __restrict__ ds)
+{
+    __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
+    const double wide2 = kRadK2 * (kRowMargin * kRowMargin);
+    for (;;)
+    {
+        const int w = next_item(ds, nHeavy, nItems, cap);
+        if (w < 0) break;
+        const Item d = decode_item(items[w], layout);
+        const int slot = group_slot(d.m0, d.m1, d.nAct, d.grp, d.G, lane);
+        const bool mine = slot >= 0;
+        const uint32_t i = d.g0 + uint32_t(mine ? slot : 0);
+        if (w < nHeavy)
+        {
+            // a cut group's leaf streams far more than a row holds: it keeps the group path
+            if (mine) nblCount[i] = kNbl + 1;
+            continue;
+        }
+        const double4 pi = xyzh[i];
+        const double hinv2 = 1.0 / (pi.w * pi.w);
+        const double rs = kRadKernel * kRowMargin * pi.w;
+        const double rmax = warp_max(mine ? rs : 0.0);
+        const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
+        int rowLen = 0;
+        rows_group(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), bx, jOffset[d.leaf],
+                   jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
+                   [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+                   [&](const double4& g, const double4& pj) {
+                       double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                       return pair_r2(dx, dy, dz) * g.w < wide2;
+                   },
+                   mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
+        if (mine)
+        {
+            nblCount[i] = rowLen;
+            rowH[i] = fmin(kRowMargin * pi.w, listH[d.leaf]) * (1.0 - 1e-12);
+        }
+    }
+}
+
+// One Newton iteration for the particles whose rows are complete for their h: one lane
+// per particle over its row (ascending j), the exact test and the sums in the row's
+// order -- the group path's pairs and order, so the plain results agree with it bit for
+// bit; mixed: the mixed pair arithmetic on FP64 separations rounded to FP32, Kahan sums.
+template<bool Periodic, bool Mixed>
+__global__ void __launch_bounds__(kThreads)
+density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl, const int* __restrict__ nblCount,
+                   double4* __restrict__ xyzh, double* __restrict__ rho, double* __restrict__ gradh,
+                   int* __restrict__ converged, double pmass, double tolh, double hfact,
+                   const DevBox* __restrict__ box, const double* __restrict__ listH,
+                   const int* __restrict__ particleLeaf, int* __restrict__ leafNext, int* __restrict__ nextLeaves,
+                   DevScalars* __restrict__ ds)
+{
+    const int n = ds->rowParticles;
+    const int lane = threadIdx.x & 31;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    unsigned long long pairs = 0;
+    for (int t0 = blockIdx.x * blockDim.x; t0 < n; t0 += gridDim.x * blockDim.x)
+    {
+        const int t = t0 + threadIdx.x;
+        bool stillActive = false;
+        int leaf = 0;
+        if (t < n)
+        {
+            const int i = rowItems[t];
+            const double4 pi = xyzh[i];
+            const double hi = pi.w;
+            const double hinv2 = 1.0 / (hi * hi);
+            const float hinv2f = float(hinv2);
+            const int cnt = nblCount[i];
+            const int* row = nbl + size_t(i) * kNbl;
+            double sr = 0.0, sg = 0.0;
+            KahanF kr, kg;
+            unsigned int gp = 0;
+            auto pair = [&](int j) {
+                const double4 pj = ldg4(xyzh + j);
+                double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                const double q2 = pair_r2(dx, dy, dz) * hinv2;
+                if (!(q2 < kRadK2)) return;
+                ++gp;
+                if constexpr (!Mixed)
+                {
+                    const double q = sqrt(q2);
+                    double wk, dwk;
+                    sph_kernel(q2, q, wk, dwk);
+                    sr += wk;
+                    sg += -q * dwk - 3.0 * wk;
+                }
+                else
+                {
+                    const float fx = float(dx), fy = float(dy), fz = float(dz);
+                    const float q2f = fmaf(fz, fz, fmaf(fy, fy, fx * fx)) * hinv2f;
+                    const float q = sqrt_q(q2f);
+                    float wk, dwk;
+                    sph_kernel_f(q2f, q, wk, dwk);
+                    kr.add(wk);
+                    kg.add(fmaf(-q, dwk, -3.0f * wk));
+                }
+            };
+            int k = 0;
+            for (; k + 4 <= cnt; k += 4)
+            {
+                const int4 q = *reinterpret_cast<const int4*>(row + k);
+                pair(q.x); pair(q.y); pair(q.z); pair(q.w);
+            }
+            for (; k < cnt; ++k) pair(row[k]);
+            if constexpr (Mixed) { sr = kr.value(); sg = kg.value(); }
+            pairs += gp;
+            double ro, go, ho;
+            int conv;
+            stillActive = newton_step(sr, sg, hi, pmass, hfact, tolh, ro, go, ho, conv);
+            rho[i] = ro;
+            gradh[i] = go;
+            reinterpret_cast<double*>(xyzh + i)[3] = ho;
+            converged[i] = conv;
+            leaf = particleLeaf[i];
+            if (stillActive && ho > listH[leaf]) ds->listStale = 1;
+        }
+        const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
+        if (still && lane == 0) atomicAdd(&ds->unconverged, __popc(still));
+        if (stillActive && atomicExch(&leafNext[leaf], 1) == 0) nextLeaves[atomicAdd(&ds->nextActive, 1)] = leaf;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    if (lane == 0) atomicAdd(&ds->pairs[0], pairs);
 }
 
 // Cullen & Dehnen xi limiter from the velocity gradient (src/density_base.cu:511-527):
@@ -453,6 +606,10 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.leafNext.resize(nL, s.st);
     const int itemCap = std::max(s.nAlive, 1);
     s.items.resize(itemCap, s.st);
+    s.rowItems.resize(itemCap, s.st);
+    s.nbl.resize(size_t(itemCap) * kNbl, s.st);
+    s.nblCount.resize(itemCap, s.st);
+    s.nblH.resize(itemCap, s.st);
 
     COSMO_CUDA(cudaMemcpyAsync(s.activeA.get(), s.allLeaves.get(), size_t(nL) * 4, cudaMemcpyDeviceToDevice, s.st));
     int nActiveLeaves = nL;
@@ -463,7 +620,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     // pairs in the same order, so the sums do not change.  hmaxLeaf is still refreshed
     // for the active leaves every iteration, as the reference does, so the exact lists of
     // the last iteration can be rebuilt afterwards.
-    bool listsValid = false, listsWidened = false;
+    bool listsValid = false, listsWidened = false, rowsReady = false;
+    int settling0 = 0;
     cudaEvent_t e3 = ev(s);
     for (int iter = 0; iter < maxIter; ++iter)
     {
@@ -476,12 +634,30 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         }
         cudaEvent_t j1 = ev(s);
         {
-            begin_iteration_kernel<<<std::min(iceil(nL, 256), 4 * s.numSMs), 256, 0, s.st>>>(ds, s.leafNext.get(),
-                                                                                            nL);
+            const int bgrid = std::min(iceil(nL, 256), 4 * s.numSMs);
+            if (iter == 1 && nActiveParticles > 0 && 5 * (long long)settling0 >= 4 * (long long)s.activePerIter[0])
+            {
+                // rows of the still-active particles at their h after the first update
+                begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
+                COSMO_LAUNCHED();
+                plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
+                    s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(),
+                    s.xyzh.get(), s.items.get(), itemCap, ds);
+                COSMO_LAUNCHED();
+                auto nrows = s.periodic ? newton_rows_kernel<true> : newton_rows_kernel<false>;
+                nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
+                    s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
+                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nbl.get(), s.nblCount.get(), s.nblH.get(), ds);
+                COSMO_LAUNCHED();
+                rowsReady = true;
+            }
+            begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
             COSMO_LAUNCHED();
             plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
                 s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(), s.xyzh.get(),
-                s.items.get(), itemCap, ds);
+                s.items.get(), itemCap, ds,
+                rowsReady ? RowSplit{s.nblCount.get(), s.nblH.get(), kNbl, s.rowItems.get()}
+                          : RowSplit{nullptr, nullptr, 0, nullptr});
             COSMO_LAUNCHED();
             const bool mx = s.precision == 1;
             auto nr = mx ? (s.periodic ? density_nr_kernel<true, true> : density_nr_kernel<false, true>)
@@ -493,6 +669,16 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
                 s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds);
             COSMO_LAUNCHED();
+            if (rowsReady)
+            {
+                auto rk = mx ? (s.periodic ? density_row_kernel<true, true> : density_row_kernel<false, true>)
+                             : (s.periodic ? density_row_kernel<true, false> : density_row_kernel<false, false>);
+                rk<<<std::max(1, std::min(iceil(int(nActiveParticles), kThreads), 8 * s.numSMs)), kThreads, 0,
+                     s.st>>>(s.rowItems.get(), s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.rho.get(),
+                             s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
+                             s.particleLeaf.get(), s.leafNext.get(), s.activeB.get(), ds);
+                COSMO_LAUNCHED();
+            }
         }
         cudaEvent_t j2 = ev(s);
         read_scalars(s);
@@ -502,6 +688,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         s.itersRun = iter + 1;
         nActiveLeaves = s.hscal->nextActive;
         nActiveParticles = s.hscal->unconverged;
+        if (iter == 0) settling0 = s.settling0 = s.hscal->settling;
         if (s.hscal->listStale) listsValid = false;
         std::swap(s.activeA, s.activeB);
         if (nActiveParticles == 0) break;

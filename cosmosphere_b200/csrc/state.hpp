@@ -91,7 +91,9 @@ struct DevScalars
     unsigned long long pairs[4]; // accepted pairs: density, gradient, force, candidates
     unsigned int sortTiles[16];  // onesweep tile tickets, one per digit pass
     int itemsHeavy, itemsLight;  // Newton work items of the current iteration (split, whole)
-    int pad[4];
+    int rowParticles;            // particles of the current iteration on their neighbour rows
+    int settling;                // unconverged particles whose h moved by less than kSettle
+    int pad[2];
 };
 
 struct Timings
@@ -116,6 +118,7 @@ struct State
     bool listsSym = false;                      // the lists held are the symmetric ones
     bool forceSinceSolve = false;               // a force pass ran on the current tree
     int itersRun = 0, maxIter = 100;
+    long long settling0 = 0;                    // settling particles after the first Newton update
     int precision = 0;     // 0 plain FP64 (the drop-in form), 1 mixed FP32/FP64
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
@@ -149,6 +152,8 @@ struct State
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
     DBuf<int> nbl;                              // neighbour rows, kNbl entries per particle
     DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed)
+    DBuf<double> nblH;                          // largest h a Newton row stays complete for
+    DBuf<int> rowItems;                         // particles of a Newton iteration on their rows
     DBuf<int> leafNext;                         // leaf already queued for the next iteration
     DBuf<int> activeA, activeB, allLeaves;
 

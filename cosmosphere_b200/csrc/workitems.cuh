@@ -27,6 +27,8 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
         ds->workCounter[0] = 0;
         ds->itemsHeavy = 0;
         ds->itemsLight = 0;
+        ds->rowParticles = 0;
+        ds->settling = 0;
     }
     for (int l = t; l < nL; l += gridDim.x * blockDim.x) leafNext[l] = 0;
 }
@@ -43,11 +45,23 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
 constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
 
+// Row classification (optional): with rowCount given, an active particle whose
+// neighbour row is complete for its current h (count <= K and h <= rowH) goes to
+// rowItems (ds->rowParticles of them) instead of a group.
+struct RowSplit
+{
+    const int* __restrict__ rowCount;
+    const double* __restrict__ rowH;
+    int K;
+    int* __restrict__ rowItems;
+};
+
 template<class Ranges>
 __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int nActive, Ranges ranges,
                                            const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
                                            const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
-                                           DevScalars* __restrict__ ds)
+                                           DevScalars* __restrict__ ds, RowSplit rs = RowSplit{nullptr, nullptr, 0,
+                                                                                              nullptr})
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -63,8 +77,26 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
         for (uint32_t g = p0; g < p1; g += 64)
         {
             const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            const bool act0 = a0 < p1 && (!converged || converged[a0] == 0);
-            const bool act1 = a1 < p1 && (!converged || converged[a1] == 0);
+            bool act0 = a0 < p1 && (!converged || converged[a0] == 0);
+            bool act1 = a1 < p1 && (!converged || converged[a1] == 0);
+            if (rs.rowCount != nullptr)
+            {
+                auto rowOK = [&](uint32_t a) {
+                    return unsigned(rs.rowCount[a]) <= unsigned(rs.K) && xyzh[a].w <= rs.rowH[a];
+                };
+                const bool row0 = act0 && rowOK(a0), row1 = act1 && rowOK(a1);
+                const uint32_t q0 = __ballot_sync(0xffffffffu, row0), q1 = __ballot_sync(0xffffffffu, row1);
+                if (q0 | q1)
+                {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(&ds->rowParticles, __popc(q0) + __popc(q1));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (row0) rs.rowItems[base + __popc(q0 & lt)] = int(a0);
+                    if (row1) rs.rowItems[base + __popc(q0) + __popc(q1 & lt)] = int(a1);
+                }
+                act0 = act0 && !row0;
+                act1 = act1 && !row1;
+            }
             const uint32_t c0 = __ballot_sync(0xffffffffu, act0), c1 = __ballot_sync(0xffffffffu, act1);
             const int nC = __popc(c0) + __popc(c1);
             if (nC == 0) continue;
@@ -92,9 +124,10 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
 __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, const uint32_t* __restrict__ layout,
                                   const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
                                   const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
-                                  DevScalars* __restrict__ ds)
+                                  DevScalars* __restrict__ ds,
+                                  RowSplit rs = RowSplit{nullptr, nullptr, 0, nullptr})
 {
-    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds);
+    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, rs);
 }
 
 // The same over a forest's range table, the active count read on the device.
