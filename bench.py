@@ -506,7 +506,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: plain FP64 (the headline value) and mixed in one run")
-    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "plummer", "ensemble", "served"])
+    ap.add_argument("--workload", default="lattice100", choices=["lattice100", "plummer", "ensemble", "served", "file"])
+    ap.add_argument("--input-file", default=None, help="file: a particle file in the reference's Fortran layout")
+    ap.add_argument("--jiggle", action="store_true", help="file: perturb h of ~1%% of the particles first")
     ap.add_argument("--plummer-n", type=int, default=2000000)
     ap.add_argument("--nreq", type=int, default=64, help="served: requests in the stream")
     ap.add_argument("--slots", type=int, default=4, help="served: worker slots")
@@ -530,6 +532,9 @@ def main():
         run_served(args, rank, world, local, dist)
         return
 
+    if args.workload == "file":
+        run_file(args, rank, world, local, dist)
+        return
     if args.workload == "plummer":
         run_particles(args, rank, world, local, dist, plummer_workload(args.plummer_n), quintic=True,
                       metric="density+force particle-updates/s (Plummer 2M, quintic)",
@@ -539,6 +544,63 @@ def main():
     run_particles(args, rank, world, local, dist, workload(args.npartx), quintic=False, metric=METRIC,
                   label=f"lattice {args.npartx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, cubic, "
                         "open boundaries")
+
+
+def run_file(args, rank, world, local, dist):
+    """A particle file in the reference's Fortran record layout (a dump with x, y, z, h
+    and pmass): density / Newton-Raphson solves through the C-ABI, plain FP64 and mixed,
+    in particle-updates/s (Newton updates), as the reference's standalone driver times it.
+    With --jiggle, h of ~1% of the particles is perturbed first as that driver does."""
+    from cosmosphere_b200 import capi, dumpio, inputs
+    if not args.input_file:
+        raise SystemExit("--workload file needs --input-file PATH")
+    p = dumpio.read_particles(args.input_file)
+    if args.jiggle:
+        inputs.jiggle_ref(p["h"], 42)
+    n = p.n
+    c = capi.Cosmo()
+    c.set_device(local)
+    pos = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]))
+    h0 = np.ascontiguousarray(p["h"])
+    hout = np.empty(n)
+    res = {}
+    for mode in ("fp64", "mixed"):
+        c.set_precision(mode == "mixed")
+        c.arrays_init(n)
+        for _ in range(args.warmup):
+            c.upload(capi.POS, pos, n); c.upload(capi.HSML, h0, n)
+            c.density(n, p["pmass"])
+        t = upd = 0.0
+        barrier(dist, local)
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            c.upload(capi.POS, pos, n); c.upload(capi.HSML, h0, n)
+            c.mark(0)
+            c.density(n, p["pmass"])
+            c.mark(1)
+            c.download(capi.HSML, n, hout)
+            t += c.elapsed(0, 1)
+            upd += float(c.array("activePerIter").sum())
+        we = time.perf_counter() - w0
+        res[mode] = {"value": sum_over_ranks(dist, local, upd) / max_over_ranks(dist, local, t),
+                     "e2e_value": sum_over_ranks(dist, local, upd) / max_over_ranks(dist, local, we),
+                     "ms_per_solve": 1e3 * t / args.steps, "iters": len(c.array("activePerIter"))}
+    c.set_precision(False)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "density particle-updates/s (particle file)", "value": res["fp64"]["value"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["fp64"]["ms_per_solve"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": os.path.basename(args.input_file),
+            "config": {"workload": f"{args.input_file}: {n} particles, pmass {p['pmass']:.6e}"
+                                   + (", jiggled" if args.jiggle else "") + "; density/NR only",
+                       "particles": n, "parallelism": f"replicas x{world}"},
+            "e2e": {"value": res["fp64"]["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": 32 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "plain_fp64": res["fp64"], "mixed": res["mixed"],
+            "roofline": None, "cpu_baseline": None, "gpu_launches": None}), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def plummer_workload(n, seed=42):

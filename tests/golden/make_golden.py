@@ -9,6 +9,9 @@ oracle/Makefile's `ref` target, then records:
                             and their constants (radkernel, radk2, cnormk, hfact_default)
   ref_driver_lattice8.npz   what the reference driver uploads for `lattice 8`, with and
                             without its jiggle: n, pmass, x, y, z, h
+  ref_io.npz                a particle file written by cosmosphere_b200.dumpio (its bytes),
+                            what the reference's reader (include/io.hpp) parses from it, and
+                            the reference's h.txt text for the same h
 """
 import ctypes
 import os
@@ -50,6 +53,29 @@ def main(ref="/root/reference"):
         rec[f"{tag}_x"], rec[f"{tag}_y"], rec[f"{tag}_z"] = pos[:n], pos[n:2 * n], pos[2 * n:]
         rec[f"{tag}_h"] = raw[2 + 3 * n:2 + 4 * n]
     np.savez(os.path.join(HERE, "ref_driver_lattice8.npz"), **rec)
+
+    sys.path.insert(0, REPO)
+    from cosmosphere_b200 import dumpio, inputs
+    p = inputs.lattice(5)
+    inputs.jiggle_ref(p["h"], 42)
+    fpath = os.path.join(ORACLE, "_ref", "io_case.dat")
+    dumpio.write_particles(fpath, p["x"], p["y"], p["z"], p["h"], p["pmass"])
+    L = ctypes.CDLL(os.path.join(ORACLE, "_ref", "libref_io.so"))
+    n, pm, err = ctypes.c_int(0), ctypes.c_double(0), ctypes.create_string_buffer(256)
+    assert L.ref_read_particles(fpath.encode(), ctypes.byref(n), ctypes.byref(pm), None, err, 256) == 0, err.value
+    xyzh = np.empty(4 * n.value)
+    L.ref_read_particles(fpath.encode(), ctypes.byref(n), ctypes.byref(pm), xyzh.ctypes.data_as(ctypes.c_void_p),
+                         err, 256)
+    hpath = os.path.join(ORACLE, "_ref", "io_case_h.txt")
+    h = np.ascontiguousarray(xyzh[3 * n.value:])
+    assert L.ref_write_h(hpath.encode(), n, h.ctypes.data_as(ctypes.c_void_p)) == 0
+    with open(fpath, "rb") as f:
+        fbytes = np.frombuffer(f.read(), dtype=np.uint8)
+    with open(hpath, "rb") as f:
+        htext = np.frombuffer(f.read(), dtype=np.uint8)
+    np.savez(os.path.join(HERE, "ref_io.npz"), file_bytes=fbytes, n=n.value, pmass=pm.value,
+             x=xyzh[:n.value], y=xyzh[n.value:2 * n.value], z=xyzh[2 * n.value:3 * n.value], h=h,
+             h_txt=htext)
     print("wrote", os.listdir(HERE))
 
 

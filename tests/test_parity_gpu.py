@@ -276,3 +276,30 @@ def test_reference_driver_runs_unchanged_on_this_library():
     want_r = " Output rho range: [%.6e, %.6e]" % (rho.min(), rho.max())
     assert lines[0] == want_h and lines[2] == want_h
     assert lines[1] == want_r and lines[3] == want_r
+
+
+def test_reference_driver_reads_a_particle_file(tmp_path):
+    """A particle file written by cosmosphere_b200.dumpio, read by the reference's own
+    driver (its include/io.hpp reader) and solved on this library, gives the h.txt that
+    this library's solve of the same particles, written by dumpio.write_h, gives."""
+    drv = os.path.join(REPO, "oracle", "_ref", "ref_driver_b200")
+    if not os.path.exists(drv):
+        pytest.skip("reference driver not built (needs the reference checkout at build time)")
+    from cosmosphere_b200 import dumpio
+    p = inputs.lattice(12)
+    inputs.jiggle_ref(p["h"], 7)
+    f = tmp_path / "lat12.dat"
+    dumpio.write_particles(f, p["x"], p["y"], p["z"], p["h"], p["pmass"])
+    out_ref = tmp_path / "h_ref.txt"
+    r = subprocess.run([drv, str(f), str(out_ref)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    q = dumpio.read_particles(f)
+    n = q.n
+    c = capi.Cosmo()
+    c.arrays_init(n)
+    c.upload(capi.POS, np.stack([q["x"], q["y"], q["z"]]))
+    c.upload(capi.HSML, q["h"])
+    c.density(n, q["pmass"])
+    out_ours = tmp_path / "h_ours.txt"
+    dumpio.write_h(out_ours, c.download(capi.HSML, n)[0])
+    assert out_ours.read_bytes() == out_ref.read_bytes()
