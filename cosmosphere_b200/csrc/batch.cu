@@ -45,6 +45,9 @@ struct Batch
     DBuf<int> converged, orderA, orderB, leafSet, leafSet2, leafPre, preLeaf, preSkip, jlist, activeA, activeB, allLeaves;
     DBuf<uint64_t> keysA, keysB, leafKey, leafKey2;
     DBuf<uint32_t> ops, opsScan, nodeCount, leafPreStart, jcount, jOffset, setHist, setBase, jstream;
+    DBuf<uint32_t> jcountPrev, jOffsetPrev;   // the previous walk's lists, kept for reuse
+    DBuf<int> jlistPrev, walked;
+    DBuf<double> listH;                       // h each leaf's list covers (0: none)
     DBuf<int4> items;                 // Newton work items (leaf, window|group|G, m0, m1)
     DBuf<int> leafNext;               // leaf already queued for the next iteration
     DBuf<uint2> leafRange;
@@ -64,6 +67,7 @@ Batch& batch()
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
+constexpr double kBatchListMargin = 1.15;   // gather-radius widening of the forest's lists
 
 __device__ __forceinline__ int set_of_pos(const int* __restrict__ offs, int nsets, long k)
 {
@@ -357,18 +361,44 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
                    const double4* __restrict__ preCenter, const double4* __restrict__ preHalf,
                    const int* __restrict__ preSkip, const int* __restrict__ preLeaf, const DevBox* __restrict__ boxes,
                    uint32_t* __restrict__ jcount, const uint32_t* __restrict__ jOffset, int* __restrict__ jlist,
-                   uint32_t listCap, int* err, const uint2* __restrict__ range, uint32_t* __restrict__ jstream)
+                   uint32_t listCap, int* err, const uint2* __restrict__ range, uint32_t* __restrict__ jstream,
+                   double* __restrict__ listH, int* __restrict__ walked, const uint32_t* __restrict__ jcountPrev,
+                   const uint32_t* __restrict__ jOffsetPrev, const int* __restrict__ jlistPrev)
 {
     const int lane = threadIdx.x & 31;
     const int nAct = *countPtr;
     for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nAct; t += (gridDim.x * blockDim.x) >> 5)
     {
     const int leaf = leaves[t];
+    double hm = hmaxLeaf[leaf];
+    if (!isfinite(hm) || hm <= 0.0) hm = 0.0;
+    // A list built at kBatchListMargin x an earlier hmax and kept by the previous walk is
+    // a superset, in the same ascending order, of the list this hmax needs: it is copied
+    // instead of walked.
+    if (!Fill)
+    {
+        const bool reuse = hm <= listH[leaf] && jcountPrev[leaf] > 0;
+        if (reuse)
+        {
+            if (lane == 0) { jcount[leaf] = jcountPrev[leaf]; walked[leaf] = 0; }
+            continue;
+        }
+    }
+    else if (walked[leaf] == 0)
+    {
+        const uint32_t dst = jOffset[leaf], cnt = jOffset[leaf + 1] - dst, src = jOffsetPrev[leaf];
+        if (jOffset[leaf + 1] > listCap)
+        {
+            if (lane == 0) atomicOr(err, int(kErrListFull));
+            continue;
+        }
+        for (uint32_t k = lane; k < cnt; k += 32) jlist[dst + k] = jlistPrev[src + k];
+        continue;
+    }
     const int s = set[leaf];
     const int ns = setNodeStart[s], ne = setNodeStart[s + 1];
     const double4 ic = preCenter[leafPre[leaf]], is = preHalf[leafPre[leaf]];
-    double hmax = hmaxLeaf[leaf];
-    if (!isfinite(hmax) || hmax <= 0.0) hmax = 0.0;
+    const double hmax = hm * kBatchListMargin;
     const double radHi = kRadKernel * hmax;
     const double ax = is.x + radHi, ay = is.y + radHi, az = is.z + radHi;
     const DevBox bx = boxes[s];
@@ -449,9 +479,24 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
         {
             jcount[leaf] = count;
             jstream[leaf] = stream;
+            listH[leaf] = hmax;
+            walked[leaf] = 1;
         }
     }
     }
+}
+
+// Keep this walk's lists for the next one: counts, offsets and the used part of the list.
+__global__ void keep_lists_kernel(int L, const uint32_t* __restrict__ jcount, const uint32_t* __restrict__ jOffset,
+                                  const int* __restrict__ jlist, uint32_t listCap, uint32_t* __restrict__ jcountPrev,
+                                  uint32_t* __restrict__ jOffsetPrev, int* __restrict__ jlistPrev)
+{
+    const long stride = long(gridDim.x) * blockDim.x;
+    const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (long t = t0; t < L; t += stride) jcountPrev[t] = jcount[t];
+    for (long t = t0; t <= L; t += stride) jOffsetPrev[t] = jOffset[t];
+    const long total = min(long(jOffset[L]), long(listCap));
+    for (long t = t0; t < total; t += stride) jlistPrev[t] = jlist[t];
 }
 
 // Newton-Raphson step of one particle, FP64 (src/density_base.cu:294-333); returns
@@ -724,6 +769,10 @@ static void batch_build(Batch& B)
     B.hmaxLeaf.resize(L, s.st);
     B.jcount.resize(L, s.st);
     B.jstream.resize(L, s.st);
+    B.jcountPrev.resize(L, s.st);
+    B.jOffsetPrev.resize(size_t(L) + 1, s.st);
+    B.walked.resize(L, s.st);
+    B.listH.resize(L, s.st);
     B.leafNext.resize(L, s.st);
     B.items.resize(std::max(B.n, 1), s.st);
     B.jOffset.resize(size_t(L) + 1, s.st);
@@ -752,10 +801,21 @@ static void walk_lists(Batch& B, bool fill, const int* leaves, const int* countP
                                        B.hmaxLeaf.get(),
                                        B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(),
                                        B.boxes.get(), B.jcount.get(), B.jOffset.get(), B.jlist.get(), B.listCap,
-                                       &s.dscal.get()->err, B.leafRange.get(), B.jstream.get());
+                                       &s.dscal.get()->err, B.leafRange.get(), B.jstream.get(), B.listH.get(),
+                                       B.walked.get(), B.jcountPrev.get(), B.jOffsetPrev.get(), B.jlistPrev.get());
     };
     if (fill) go(list_walk_kernel_b<true>);
     else go(list_walk_kernel_b<false>);
+    COSMO_LAUNCHED();
+}
+
+// Keep the lists just filled (all leaves) as the source the next walk copies from.
+static void keep_lists(Batch& B)
+{
+    State& s = B.core;
+    const int L = B.nLeaves;
+    keep_lists_kernel<<<4 * s.numSMs, 256, 0, s.st>>>(L, B.jcount.get(), B.jOffset.get(), B.jlist.get(), B.listCap,
+                                                     B.jcountPrev.get(), B.jOffsetPrev.get(), B.jlistPrev.get());
     COSMO_LAUNCHED();
 }
 
@@ -787,9 +847,11 @@ static void run_items(Batch& B, const int* leaves, const int* countPtr, bool eva
 }
 
 // One Newton-Raphson iteration, every count read on the device: hmax of the active
-// leaves, the gather lists of all leaves (count, scan, fill), the density kernel over
-// the active leaves of all sets, the new active set, and the loop bookkeeping.  Run
-// eagerly, or captured once as the body of a graph's while node.
+// leaves, the gather lists of all leaves (count, scan, fill: a leaf whose hmax is still
+// inside the radius its kept list was walked at copies that list, the others walk), the
+// density kernel over the active leaves of all sets, the lists kept for the next
+// iteration, the new active set, and the loop bookkeeping.  Run eagerly, or captured
+// once as the body of a graph's while node.
 static void nr_iteration(Batch& B, double tolh, double hfact, cudaGraphConditionalHandle handle, int setCond)
 {
     State& s = B.core;
@@ -799,10 +861,11 @@ static void nr_iteration(Batch& B, double tolh, double hfact, cudaGraphCondition
     hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.activeA.get(),
                                                        &ls->nActiveLeaves, B.hmaxLeaf.get());
     COSMO_LAUNCHED();
-    walk_lists(B, false, B.activeA.get(), &ls->nActiveLeaves);
+    walk_lists(B, false, B.allLeaves.get(), &ls->nAll);
     scan_exclusive(s, B.jcount.get(), B.jOffset.get(), L, false);
-    walk_lists(B, true, B.activeA.get(), &ls->nActiveLeaves);
+    walk_lists(B, true, B.allLeaves.get(), &ls->nAll);
     run_items(B, B.activeA.get(), &ls->nActiveLeaves, false, tolh, hfact);
+    keep_lists(B);
     copy_active_kernel<<<iceil(L, 256), 256, 0, s.st>>>(B.activeB.get(), B.activeA.get(), ds, L);
     COSMO_LAUNCHED();
     loop_epilogue_kernel<<<1, 1, 0, s.st>>>(ls, ds, handle, setCond);
@@ -824,7 +887,7 @@ static void final_rho(Batch& B)
     if (total > B.listCap)
     {
         B.listCap = total + total / 4 + 1024;
-        B.jlist.resize(B.listCap, s.st);
+        B.jlist.resize(B.listCap, s.st);   // the kept lists (jlistPrev) stay where they are
     }
     walk_lists(B, true, B.allLeaves.get(), &ls->nAll);
     run_items(B, B.allLeaves.get(), &ls->nAll, true, 0.0, 0.0);
@@ -860,7 +923,9 @@ static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int fla
     init.nAll = L;
     COSMO_CUDA(cudaMemcpyAsync(B.loop.get(), &init, sizeof(LoopState), cudaMemcpyHostToDevice, s.st));
     // Size the list storage from the first iteration's lists (lists grow with h; a build
-    // that outgrows the storage reports it and the solve is repeated with twice as much).
+    // that outgrows the storage reports it and the solve is repeated with twice as much),
+    // then fill and keep them: the first iteration copies them.
+    COSMO_CUDA(cudaMemsetAsync(B.jcountPrev.get(), 0, size_t(L) * sizeof(uint32_t), s.st));
     hmax_leaf_kernel_b<<<iceil(L, 256), 256, 0, s.st>>>(B.xyzh.get(), B.leafRange.get(), B.activeA.get(),
                                                        &B.loop.get()->nActiveLeaves, B.hmaxLeaf.get());
     COSMO_LAUNCHED();
@@ -869,7 +934,10 @@ static int batch_solve(Batch& B, double tolh, double hfact, int maxIter, int fla
     const uint32_t want = (total0 << (1 + attempt)) + 1024;
     if (B.listCap < want) B.listCap = want;
     B.jlist.resize(B.listCap, s.st);
+    B.jlistPrev.resize(B.listCap, s.st);
     s.scanTmp.resize(size_t(iceil(L, 4096)) + 1, s.st);
+    walk_lists(B, true, B.activeA.get(), &B.loop.get()->nActiveLeaves);
+    keep_lists(B);
     COSMO_CUDA(cudaStreamSynchronize(s.st));
     cudaEvent_t t1 = ev(s);
 
