@@ -131,11 +131,11 @@ size_t state_device_bytes(const State& s)
     for (auto* d : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
                     &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
-                    &s.rowItems})
+                    &s.rowItems, &s.jlistPrev, &s.walked})
         add(*d);
     add(s.items);
     for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
-                    &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
+                    &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback, &s.jOffsetPrev})
         add(*d);
     add(s.box);
     add(s.dscal);
@@ -156,11 +156,11 @@ void release_state(State& s)
     for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
                     &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
-                    &s.rowItems})
+                    &s.rowItems, &s.jlistPrev, &s.walked})
         b->release(s.st);
     s.items.release(s.st);
     for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
-                    &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback})
+                    &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback, &s.jOffsetPrev})
         b->release(s.st);
     s.box.release(s.st);
     s.dscal.release(s.st);

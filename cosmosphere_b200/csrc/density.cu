@@ -617,7 +617,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
 
     // The gather lists are built with a widened radius and reused while every active h
     // stays inside it: a superset list in ascending leaf order offers the same accepted
-    // pairs in the same order, so the sums do not change.  hmaxLeaf is still refreshed
+    // pairs in the same order, so the sums do not change.  When an h outgrows its leaf's
+    // list, only the leaves whose hmax left their radius walk again.  hmaxLeaf is still refreshed
     // for the active leaves every iteration, as the reference does, so the exact lists of
     // the last iteration can be rebuilt afterwards.
     bool listsValid = false, listsWidened = false, rowsReady = false;
@@ -629,7 +630,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         hmax_leaves(s, s.activeA.get(), nActiveLeaves);
         if (!listsValid)
         {
-            build_lists(s, false, kListMargin);
+            build_lists(s, false, kListMargin, listsWidened);   // after the first: only outgrown leaves walk
             listsValid = listsWidened = true;
         }
         cudaEvent_t j1 = ev(s);

@@ -149,6 +149,9 @@ struct State
     DBuf<uint32_t> jstream;                     // particles in each leaf's gather list
     DBuf<double> listH;                         // h each leaf's gather list covers
     DBuf<int> jlist;
+    DBuf<uint32_t> jOffsetPrev;                 // an incremental rebuild's copy of the lists it replaces
+    DBuf<int> jlistPrev, walked;
+    uint32_t listTotal = 0;                     // entries of the current lists
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
     DBuf<int> nbl;                              // neighbour rows, kNbl entries per particle
     DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed)
@@ -181,7 +184,7 @@ void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
 // Gather (symmetric = false) or symmetric j-leaf lists for all leaves.  margin > 1 widens
 // the gather radius to R * hmax * margin, so the lists stay valid while h grows by up to
 // that factor; listH records the h each leaf's list covers.
-void build_lists(State& s, bool symmetric, double margin = 1.0);
+void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental = false);
 // The symmetric lists and the symmetric neighbour rows of the current tree and h (the
 // force pass's pairs; every gather pair of the converged h is among them).
 void build_symmetric(State& s);

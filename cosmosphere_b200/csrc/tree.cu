@@ -336,6 +336,8 @@ __global__ void hmax_level_kernel(int first, int last, const int* __restrict__ c
     hmaxPre[bfsToPre[i]] = m;
 }
 
+constexpr double kListLoose = 1.05;   // a kept list may be this much wider than a new one
+
 // ------------------------------------------------------------------ j-leaf list walk
 // One warp per i-leaf.  The tree is scanned in pre-order 32 nodes at a time: every lane
 // tests one node; the nodes before the first rejected one are all reached (an accepted
@@ -352,16 +354,39 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const DevBox* __restrict__ box, uint32_t* __restrict__ jcount,
                  const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err,
                  const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
-                 double* __restrict__ listH)
+                 double* __restrict__ listH, const uint32_t* __restrict__ jOffsetPrev,
+                 const int* __restrict__ jlistPrev, int* __restrict__ walked)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (leaf >= nL) return;
+    double hmax = hmaxLeaf[leaf];
+    if (!isfinite(hmax) || hmax <= 0.0) hmax = 0.0;
+    // Incremental rebuild (walked set): a leaf whose hmax is still inside the radius its
+    // previous list was walked at, and not so far inside that the list is looser than a
+    // new one by more than kListLoose, keeps that list -- a superset, in the same
+    // pre-order, of what this hmax needs -- and the fill pass copies it; the others walk.
+    if (walked != nullptr)
+    {
+        if (!Fill && hmax <= listH[leaf] && listH[leaf] <= hmax * margin * kListLoose)
+        {
+            if (lane == 0)
+            {
+                jcount[leaf] = jOffsetPrev[leaf + 1] - jOffsetPrev[leaf];
+                walked[leaf] = 0;
+            }
+            return;
+        }
+        if (Fill && walked[leaf] == 0)
+        {
+            const uint32_t dst = jOffset[leaf], cnt = jOffset[leaf + 1] - dst, src = jOffsetPrev[leaf];
+            for (uint32_t k = lane; k < cnt; k += 32) jlist[dst + k] = jlistPrev[src + k];
+            return;
+        }
+    }
     const int iNode = leafToInternal[leaf];
     const double icx = centers[3 * iNode], icy = centers[3 * iNode + 1], icz = centers[3 * iNode + 2];
     const double isx = sizes[3 * iNode], isy = sizes[3 * iNode + 1], isz = sizes[3 * iNode + 2];
-    double hmax = hmaxLeaf[leaf];
-    if (!isfinite(hmax) || hmax <= 0.0) hmax = 0.0;
     hmax *= margin;
     const double radHi = kRadKernel * hmax;
     // gather: the i-box inflated by radHi; symmetric: the raw i-box
@@ -453,6 +478,7 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
             jcount[leaf] = count;
             if (jstream != nullptr) jstream[leaf] = stream;
             if (listH != nullptr) listH[leaf] = hmax;
+            if (walked != nullptr) walked[leaf] = 1;
         }
     }
 }
@@ -731,7 +757,7 @@ void hmax_upsweep(State& s)
 }
 
 template<bool Sym, bool Per>
-static void walk(State& s, bool fill, double margin)
+static void walk(State& s, bool fill, double margin, bool incremental)
 {
     const int nL = s.nLeaves;
     const int blocks = iceil(long(nL) * 32, kBlk);
@@ -741,24 +767,51 @@ static void walk(State& s, bool fill, double margin)
                                         s.preLeaf.get(), s.hmaxPre.get(), s.box.get(), s.jcount.get(),
                                         s.jOffset.get(), s.jlist.get(), &s.dscal.get()->err, s.layout.get(),
                                         !fill ? s.jstream.get() : nullptr, margin,
-                                        (!fill && !Sym) ? s.listH.get() : nullptr);
+                                        (!fill && !Sym) ? s.listH.get() : nullptr,
+                                        incremental ? s.jOffsetPrev.get() : nullptr,
+                                        incremental ? s.jlistPrev.get() : nullptr,
+                                        incremental ? s.walked.get() : nullptr);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
     COSMO_LAUNCHED();
 }
 
-// include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.
-void build_lists(State& s, bool symmetric, double margin)
+// include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.  incremental
+// (gather lists only, over the gather lists of the same tree at the same margin): the
+// current lists are kept aside first, and only the leaves whose hmax outgrew them walk.
+void build_lists(State& s, bool symmetric, double margin, bool incremental)
 {
+    const int nL = s.nLeaves;
+    incremental = incremental && !symmetric && !s.listsSym && nL > 0;
+    if (incremental)
+    {
+        s.jOffsetPrev.resize(size_t(nL) + 1, s.st);
+        s.jlistPrev.resize(std::max<uint32_t>(s.listTotal, 1u), s.st);
+        s.walked.resize(nL, s.st);
+        COSMO_CUDA(cudaMemcpyAsync(s.jOffsetPrev.get(), s.jOffset.get(), (size_t(nL) + 1) * sizeof(uint32_t),
+                                   cudaMemcpyDeviceToDevice, s.st));
+        if (s.listTotal > 0)
+            COSMO_CUDA(cudaMemcpyAsync(s.jlistPrev.get(), s.jlist.get(), size_t(s.listTotal) * sizeof(int),
+                                       cudaMemcpyDeviceToDevice, s.st));
+    }
     auto run = [&](bool fill) {
-        if (symmetric) { if (s.periodic) walk<true, true>(s, fill, margin); else walk<true, false>(s, fill, margin); }
-        else { if (s.periodic) walk<false, true>(s, fill, margin); else walk<false, false>(s, fill, margin); }
+        if (symmetric)
+        {
+            if (s.periodic) walk<true, true>(s, fill, margin, false);
+            else walk<true, false>(s, fill, margin, false);
+        }
+        else
+        {
+            if (s.periodic) walk<false, true>(s, fill, margin, incremental);
+            else walk<false, false>(s, fill, margin, incremental);
+        }
     };
     run(false);
-    const uint32_t total = scan_exclusive(s, s.jcount.get(), s.jOffset.get(), s.nLeaves, true);
+    const uint32_t total = scan_exclusive(s, s.jcount.get(), s.jOffset.get(), nL, true);
     s.jlist.resize(std::max<uint32_t>(total, 1u), s.st);
     run(true);
+    s.listTotal = total;
     s.listsSym = symmetric;
 }
 
