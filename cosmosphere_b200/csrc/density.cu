@@ -200,7 +200,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        return pair_r2(dx, dy, dz) * g.w < wide2;
                    },
-                   mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
+                   mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
         if (mine)
         {
             nblCount[i] = rowLen;
@@ -240,7 +240,7 @@ density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl
             const double hinv2 = 1.0 / (hi * hi);
             const float hinv2f = float(hinv2);
             const int cnt = nblCount[i];
-            const int* row = nbl + size_t(i) * kNbl;
+            const int* row = row_of(nbl, uint32_t(i));
             double sr = 0.0, sg = 0.0;
             KahanF kr, kg;
             unsigned int gp = 0;
@@ -270,13 +270,7 @@ density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl
                     kg.add(fmaf(-q, dwk, -3.0f * wk));
                 }
             };
-            int k = 0;
-            for (; k + 4 <= cnt; k += 4)
-            {
-                const int4 q = *reinterpret_cast<const int4*>(row + k);
-                pair(q.x); pair(q.y); pair(q.z); pair(q.w);
-            }
-            for (; k < cnt; ++k) pair(row[k]);
+            for_row(row, cnt, pair);
             if constexpr (Mixed) { sr = kr.value(); sg = kg.value(); }
             pairs += gp;
             double ro, go, ho;
@@ -440,7 +434,7 @@ gradient_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restri
         const double4 ai = acc4[i];
         const double hi = pi.w;
         const double hinv2 = 1.0 / (hi * hi);
-        const int* row = nbl + size_t(i) * kNbl;
+        const int* row = row_of(nbl, uint32_t(i));
         GradSums g;
         auto pair = [&](int j) {
             const double4 pj = ldg4(xyzh + j);
@@ -451,13 +445,7 @@ gradient_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restri
             if (!(q2 < kRadK2)) return;
             g.add(dx, dy, dz, r2, q2, vi, ai, ldg4(vel4 + j), ldg4(acc4 + j), pmass);
         };
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4)
-        {
-            const int4 q = *reinterpret_cast<const int4*>(row + k);
-            pair(q.x); pair(q.y); pair(q.z); pair(q.w);
-        }
-        for (; k < cnt; ++k) pair(row[k]);
+        for_row(row, cnt, pair);
         pairs += g.gp;
         g.finish(uint32_t(i), hi, pmass, rho, gradh, divv, xiOut, ddivvdt);
     }
@@ -607,7 +595,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     const int itemCap = std::max(s.nAlive, 1);
     s.items.resize(itemCap, s.st);
     s.rowItems.resize(itemCap, s.st);
-    s.nbl.resize(size_t(itemCap) * kNbl, s.st);
+    s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
 

@@ -279,7 +279,7 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
                        const double dr2 = pair_r2(dx, dy, dz);
                        return !(dr2 >= kRadK2 * fmax(g.w, pj.w * pj.w) * (1.0 + 1e-10));
                    },
-                   mine ? nbl + size_t(i) * kNbl : nullptr, rowLen);
+                   mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
         if (mine) nblCount[i] = rowLen;
     }
 }
@@ -305,18 +305,12 @@ force_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict_
         const int cnt = nblCount[i];
         ForceAcc A;
         A.load(uint32_t(i), xyzh, vel4, thermo4, prepA, prepB);
-        const int* row = nbl + size_t(i) * kNbl;
+        const int* row = row_of(nbl, uint32_t(i));
         auto pair = [&](int j) {
             A.add<Periodic, Disc>(ldg4(xyzh + j), j, vel4, thermo4, prepA, prepB, lx, ly, lz, pmass, beta, pdv,
                                   shock);
         };
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4)
-        {
-            const int4 q = *reinterpret_cast<const int4*>(row + k);
-            pair(q.x); pair(q.y); pair(q.z); pair(q.w);
-        }
-        for (; k < cnt; ++k) pair(row[k]);
+        for_row(row, cnt, pair);
         pairs += A.gp;
         A.store(uint32_t(i), fx, fy, fz, f4, vsigmax, divvF);
     }
@@ -346,7 +340,7 @@ void build_symmetric(State& s)
     const int grid = std::max(1, std::min(s.numSMs * 8, iceil(nL, kWarpsPerBlock)));
     const int nA = std::max(s.nAlive, 1);
     s.items.resize(nA, s.st);
-    s.nbl.resize(size_t(nA) * kNbl, s.st);
+    s.nbl.resize(row_buffer_entries(size_t(nA)), s.st);
     s.nblCount.resize(nA, s.st);
     begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
     COSMO_LAUNCHED();

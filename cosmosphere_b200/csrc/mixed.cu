@@ -241,7 +241,7 @@ gradient_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __
         const double4 vi = vel4[i];
         const double4 ai = acc4[i];
         const float hinv2f = float(1.0 / (pi.w * pi.w));
-        const int* row = nbl + size_t(i) * kNbl;
+        const int* row = row_of(nbl, uint32_t(i));
         GradSumsF gs;
         const double hinv2 = 1.0 / (pi.w * pi.w);
         auto pair = [&](int j) {
@@ -253,13 +253,7 @@ gradient_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __
             const float r2 = fmaf(fz, fz, fmaf(fy, fy, fx * fx));
             gs.add(fx, fy, fz, r2, r2 * hinv2f, vi, ai, ldg4(vel4 + j), ldg4(acc4 + j), pmf);
         };
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4)
-        {
-            const int4 q = *reinterpret_cast<const int4*>(row + k);
-            pair(q.x); pair(q.y); pair(q.z); pair(q.w);
-        }
-        for (; k < cnt; ++k) pair(row[k]);
+        for_row(row, cnt, pair);
         pairs += gs.gp;
         gs.finish(uint32_t(i), pi.w, pmass, rho, gradh, divv, xiOut, ddivvdt);
     }
@@ -500,7 +494,7 @@ force_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __res
         const int cnt = nblCount[i];
         ForceAccF A;
         A.load(uint32_t(i), xyzh, vel4, thermof, prepAf, prepBf);
-        const int* row = nbl + size_t(i) * kNbl;
+        const int* row = row_of(nbl, uint32_t(i));
         auto pair = [&](int j) {
             const double4 pj = ldg4(xyzh + j);
             double dx = A.p.x - pj.x, dy = A.p.y - pj.y, dz = A.p.z - pj.z;
@@ -510,13 +504,7 @@ force_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __res
             if (dr2 > 0.0f)
                 A.add<Disc>(fx, fy, fz, dr2, float(pj.w), j, vel4, thermof, prepAf, prepBf, pm, bt, pdv, shock);
         };
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4)
-        {
-            const int4 q = *reinterpret_cast<const int4*>(row + k);
-            pair(q.x); pair(q.y); pair(q.z); pair(q.w);
-        }
-        for (; k < cnt; ++k) pair(row[k]);
+        for_row(row, cnt, pair);
         pairs += A.gp;
         A.store(uint32_t(i), fx, fy, fz, f4, vsigmax, divvF);
     }

@@ -9,7 +9,9 @@
  * that then walks a row applies the same exact test to the same candidates in the same
  * order as a walk of the whole list would, so its sums are the same bit for bit.
  *
- * Row layout: kNbl entries per particle (row i at nbl + i * kNbl, 16-byte aligned); a
+ * Row layout: kNbl entries per particle, interleaved over blocks of 32 particles -- entry
+ * k of particle i at nbl[(i / 32) * 32 kNbl + 32 k + i % 32] -- so that the lanes of a warp
+ * over 32 consecutive particles read entry k of all their rows from one 128-byte line.  A
  * count above kNbl marks a row that overflowed, whose particle keeps the group path.
  */
 #pragma once
@@ -19,13 +21,24 @@
 namespace cosmo {
 
 constexpr int kNbl = kQuintic ? 256 : 128;
+constexpr int kRowStride = 32;   // distance between consecutive entries of one row
+
+// Entries the row buffer of n particles holds.
+inline size_t row_buffer_entries(size_t n) { return ((n + 31) / 32) * size_t(32) * kNbl; }
+
+// Entry 0 of particle i's row; entry k is at [k * kRowStride].
+template<class T>
+__device__ __forceinline__ T* row_of(T* nbl, uint32_t i)
+{
+    return nbl + (size_t(i >> 5) * kNbl << 5) + (i & 31u);
+}
 
 // Per-warp shared scratch of rows_group: the double ring, its indices, the group's data.
 constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32;
 
 // Rows of one group.  Lanes [0, ng) own the group's particles, whose per-particle test data
 // gi (a double4: position and one test value) the caller passes; test(gi, pj) is the exact
-// acceptance of the pair.  row is the lane's own row (nullptr if not mine); rowLen
+// acceptance of the pair.  row is the lane's own row (row_of; nullptr if not mine); rowLen
 // receives its length (kNbl + 1 when it overflowed).
 template<class Ranges, class Filter, class Test>
 __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng, const double4& gi, const GroupBox& bx,
@@ -61,11 +74,25 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
             {
                 const int b = __ffs(myMask) - 1;
                 myMask &= myMask - 1;
-                if (len < kNbl) row[len] = ri[(head + b) & (kRing - 1)];
+                if (len < kNbl) row[size_t(len) * kRowStride] = ri[(head + b) & (kRing - 1)];
                 ++len;
             }
         });
     rowLen = len > kNbl ? kNbl + 1 : len;
+}
+
+// f(j) for the cnt entries of a row (row_of), in order, four loads ahead of their use.
+template<class F>
+__device__ __forceinline__ void for_row(const int* __restrict__ row, int cnt, F&& f)
+{
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4)
+    {
+        const int a = __ldg(row + size_t(k) * kRowStride), b = __ldg(row + size_t(k + 1) * kRowStride);
+        const int c = __ldg(row + size_t(k + 2) * kRowStride), d = __ldg(row + size_t(k + 3) * kRowStride);
+        f(a); f(b); f(c); f(d);
+    }
+    for (; k < cnt; ++k) f(__ldg(row + size_t(k) * kRowStride));
 }
 
 // Whether particle i's row is usable (written and not overflowed).
