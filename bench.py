@@ -187,7 +187,7 @@ def run_ensemble(args, rank, world, local, dist):
     (plain and mixed) against 256 sequential plain FP64 single-set solves on the same GPU.
     On N GPUs the sets are packed onto the ranks by particle count (no exchange step);
     each rank times its own share and the job's time is the slowest rank's."""
-    from cosmosphere_b200 import capi, inputs, shard
+    from cosmosphere_b200 import autotune, capi, inputs, shard
     sizes = inputs.ensemble_sizes(args.nsets)
     shares = shard.pack_sets(sizes, world)
     mine = shares[rank]
@@ -197,9 +197,27 @@ def run_ensemble(args, rank, world, local, dist):
     c.set_device(local)
     res = {}
     outs = {}
+    tuned = {}
     for mode in ("fp64", "mixed"):
         c.set_precision(mode == "mixed")
+        untuned_ms = None
+        if args.autotune == "on":
+            # per size class, on this rank's sets, before anything is timed
+            w0 = time.perf_counter()
+            table = autotune.tune(sets, max_particles=args.tune_particles)
+            tuned[mode] = {"seconds": time.perf_counter() - w0, **table.to_json()}
+            b = capi.Batch(sets)
+            b.upload()
+            for _ in range(args.warmup):
+                assert b.density(final_rho=True) == 0
+            tu = 0.0
+            for _ in range(args.steps):
+                assert b.density(final_rho=True) == 0
+                tu += b.scalar("t_total")
+            untuned_ms = 1e3 * shard.reduce_scalar(dist, tu, "max", device=f"cuda:{local}" if dist else None) / args.steps
         b = capi.Batch(sets)
+        if args.autotune == "on":
+            table.apply(b)
         b.upload()
         for _ in range(args.warmup):
             assert b.density(final_rho=True) == 0
@@ -228,7 +246,7 @@ def run_ensemble(args, rank, world, local, dist):
                      "e2e_value": upd_all / args.steps / we,
                      "ms_newton_loop_graph": 1e3 * tnr / args.steps, "graph": b.scalar("graph") == 1.0,
                      "updates_per_solve": upd_all / args.steps, "iters": b.scalar("itersRun"),
-                     "leaves_rank0": b.scalar("nLeaves")}
+                     "leaves_rank0": b.scalar("nLeaves"), "ms_per_solve_untuned": untuned_ms}
     c.set_precision(False)
     # sequential plain FP64 single-set solves
     tseq = 0.0
@@ -259,7 +277,8 @@ def run_ensemble(args, rank, world, local, dist):
                 "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
                 "config": {"workload": f"{args.nsets} sets, log-uniform 1e4..5e5 particles, even: periodic uniform "
                                        "box, odd: Plummer r<20; h = 1.2 x spacing x U[0.8,1.2]; cubic; density/NR "
-                                       "loop as one CUDA graph + rho at the converged h",
+                                       "loop as one CUDA graph + rho at the converged h; launch parameters "
+                                       + ("autotuned per size class" if args.autotune == "on" else "default"),
                            "particles": n_all,
                            "parallelism": f"sets packed on {world} GPU(s), largest first onto the least-loaded "
                                           f"(imbalance {shard.imbalance(sizes, shares):.3f})"},
@@ -271,6 +290,7 @@ def run_ensemble(args, rank, world, local, dist):
                 "speedup_mixed_batched_vs_sequential_fp64": (res["mixed"]["value"]) / (useq / tseq),
                 "speedup_mixed_vs_fp64_batched": res["mixed"]["value"] / res["fp64"]["value"],
                 "accuracy_mixed_vs_fp64": {"h_max_rel": eh, "rho_max_rel": er},
+                "autotune_rank0": tuned or None,
                 "roofline": None, "cpu_baseline": None, "gpu_launches": None}
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -516,6 +536,10 @@ def main():
     ap.add_argument("--serve-load", type=float, default=0.9,
                     help="served: Poisson rate as a multiple of the FP64 loop's request rate")
     ap.add_argument("--nsets", type=int, default=256)
+    ap.add_argument("--autotune", default="on", choices=["on", "off"],
+                    help="ensemble: tune the batched form per size class before timing")
+    ap.add_argument("--tune-particles", type=float, default=2.0e6,
+                    help="ensemble: particles in the sample of each size class the tuner times")
     ap.add_argument("--profile", action="store_true",
                     help="for ncu: set up, run --warmup and --steps device-resident steps, print nothing else")
     args = ap.parse_args()

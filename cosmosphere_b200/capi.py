@@ -23,7 +23,8 @@ EXPORTS = [
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
-    "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_upload",
+    "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_set_tuning",
+    "cosmo_batch_upload",
     "cosmo_batch_density", "cosmo_batch_download", "cosmo_batch_scalar",
     "cosmo_serve_start", "cosmo_serve_submit", "cosmo_serve_continue", "cosmo_serve_wait",
     "cosmo_serve_request_stat", "cosmo_serve_release", "cosmo_serve_stat", "cosmo_serve_stop",
@@ -69,6 +70,8 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_batch_init.restype = I
     L.cosmo_batch_set_params.argtypes = [P, P, P]
     L.cosmo_batch_set_bucket.argtypes = [P]
+    L.cosmo_batch_set_tuning.argtypes = [P, P, P, P]
+    L.cosmo_batch_set_tuning.restype = I
     L.cosmo_batch_upload.argtypes = [P, P, P, P]
     L.cosmo_batch_density.argtypes = [D, D, I, I]
     L.cosmo_batch_density.restype = I
@@ -234,6 +237,19 @@ class Batch:
         self._keep = (pm, per, box)
         cat = lambda k: np.ascontiguousarray(np.concatenate([np.asarray(s[k], dtype=np.float64) for s in sets]))
         self.x, self.y, self.z, self.h = cat("x"), cat("y"), cat("z"), cat("h")
+
+    def set_tuning(self, bucket=None, list_margin=None, split_stream=None, split_work=None):
+        """Per-set launch parameters (each a scalar or one value per set; None keeps it)."""
+        ns = len(self.sizes)
+
+        def arr(v, dt):
+            return None if v is None else np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=dt), (ns,)))
+
+        a = [arr(bucket, np.int32), arr(list_margin, np.float64), arr(split_stream, np.int32),
+             arr(split_work, np.int32)]
+        rc = self.L.cosmo_batch_set_tuning(*[x.ctypes.data if x is not None else None for x in a])
+        if rc != 0:
+            raise ValueError("cosmo_batch_set_tuning rejected a value")
 
     def upload(self):
         self.L.cosmo_batch_upload(self.x.ctypes.data, self.y.ctypes.data, self.z.ctypes.data, self.h.ctypes.data)

@@ -40,6 +40,8 @@ struct Batch
     double tBuild = 0, tNR = 0, tList = 0, tTotal = 0;
     unsigned long long pairs = 0;
     DBuf<int> dOffs, setOf, nAliveSet, setLeafStart, setNodeStart, bucket, setPer;
+    DBuf<double> setMargin;           // per set: gather-radius widening of its lists
+    DBuf<uint2> setSplit;             // per set: stream above which a leaf is cut, work per cut group
     DBuf<double> ux, uy, uz, uh, pmass, setBox6, rho, gradh, hmaxLeaf;
     DBuf<double4> xyzh, preCenter, preHalf;
     DBuf<int> converged, orderA, orderB, leafSet, leafSet2, leafPre, preLeaf, preSkip, jlist, activeA, activeB, allLeaves;
@@ -54,6 +56,7 @@ struct Batch
     DBuf<DevBox> boxes;
     DBuf<LoopState> loop;
     uint32_t listCap = 0;
+    std::vector<double> tuning;       // per set: bucket, list margin, cut stream, cut work
     bool graphUsed = false;
 };
 
@@ -67,7 +70,8 @@ Batch& batch()
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
-constexpr double kBatchListMargin = 1.15;   // gather-radius widening of the forest's lists
+constexpr double kBatchListMargin = 1.15;   // default gather-radius widening of a set's lists
+constexpr int kMinTuneBucket = 8, kMaxTuneBucket = 1024;   // leaf capacities a set may be given
 
 __device__ __forceinline__ int set_of_pos(const int* __restrict__ offs, int nsets, long k)
 {
@@ -363,7 +367,8 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
                    uint32_t* __restrict__ jcount, const uint32_t* __restrict__ jOffset, int* __restrict__ jlist,
                    uint32_t listCap, int* err, const uint2* __restrict__ range, uint32_t* __restrict__ jstream,
                    double* __restrict__ listH, int* __restrict__ walked, const uint32_t* __restrict__ jcountPrev,
-                   const uint32_t* __restrict__ jOffsetPrev, const int* __restrict__ jlistPrev)
+                   const uint32_t* __restrict__ jOffsetPrev, const int* __restrict__ jlistPrev,
+                   const double* __restrict__ setMargin)
 {
     const int lane = threadIdx.x & 31;
     const int nAct = *countPtr;
@@ -372,7 +377,7 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
     const int leaf = leaves[t];
     double hm = hmaxLeaf[leaf];
     if (!isfinite(hm) || hm <= 0.0) hm = 0.0;
-    // A list built at kBatchListMargin x an earlier hmax and kept by the previous walk is
+    // A list built at the set's margin x an earlier hmax and kept by the previous walk is
     // a superset, in the same ascending order, of the list this hmax needs: it is copied
     // instead of walked.
     if (!Fill)
@@ -398,7 +403,7 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
     const int s = set[leaf];
     const int ns = setNodeStart[s], ne = setNodeStart[s + 1];
     const double4 ic = preCenter[leafPre[leaf]], is = preHalf[leafPre[leaf]];
-    const double hmax = hm * kBatchListMargin;
+    const double hmax = hm * setMargin[s];
     const double radHi = kRadKernel * hmax;
     const double ax = is.x + radHi, ay = is.y + radHi, az = is.z + radHi;
     const DevBox bx = boxes[s];
@@ -802,7 +807,8 @@ static void walk_lists(Batch& B, bool fill, const int* leaves, const int* countP
                                        B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(),
                                        B.boxes.get(), B.jcount.get(), B.jOffset.get(), B.jlist.get(), B.listCap,
                                        &s.dscal.get()->err, B.leafRange.get(), B.jstream.get(), B.listH.get(),
-                                       B.walked.get(), B.jcountPrev.get(), B.jOffsetPrev.get(), B.jlistPrev.get());
+                                       B.walked.get(), B.jcountPrev.get(), B.jOffsetPrev.get(), B.jlistPrev.get(),
+                                       B.setMargin.get());
     };
     if (fill) go(list_walk_kernel_b<true>);
     else go(list_walk_kernel_b<false>);
@@ -832,7 +838,7 @@ static void run_items(Batch& B, const int* leaves, const int* countPtr, bool eva
     plan_items_table_kernel<<<s.numSMs * 8, kThreads, 0, s.st>>>(leaves, countPtr, B.leafRange.get(),
                                                                   evalAll ? nullptr : B.converged.get(),
                                                                   B.jstream.get(), B.xyzh.get(), B.items.get(), cap,
-                                                                  ds);
+                                                                  ds, B.leafSet.get(), B.setSplit.get());
     COSMO_LAUNCHED();
     const PreorderTree tree{B.preCenter.get(), B.preHalf.get(), B.preSkip.get(), B.preLeaf.get(), 0, 0};
     auto go = [&](auto kern) {
@@ -1039,6 +1045,20 @@ int cosmo_batch_init(int nsets, const int* offsets)
     COSMO_LAUNCHED();
     std::vector<int> bucket(nsets, int(kBucket)), per(nsets, 0);
     COSMO_CUDA(cudaMemcpyAsync(B.bucket.get(), bucket.data(), size_t(nsets) * 4, cudaMemcpyHostToDevice, s.st));
+    B.setMargin.resize(nsets, s.st);
+    B.setSplit.resize(nsets, s.st);
+    std::vector<double> margin(nsets, kBatchListMargin);
+    std::vector<uint2> split(nsets, make_uint2(kSplitStream, kSplitWork));
+    COSMO_CUDA(cudaMemcpyAsync(B.setMargin.get(), margin.data(), size_t(nsets) * 8, cudaMemcpyHostToDevice, s.st));
+    COSMO_CUDA(cudaMemcpyAsync(B.setSplit.get(), split.data(), size_t(nsets) * 8, cudaMemcpyHostToDevice, s.st));
+    B.tuning.assign(size_t(nsets) * 4, 0.0);
+    for (int k = 0; k < nsets; ++k)
+    {
+        B.tuning[4 * k] = kBucket;
+        B.tuning[4 * k + 1] = kBatchListMargin;
+        B.tuning[4 * k + 2] = kSplitStream;
+        B.tuning[4 * k + 3] = kSplitWork;
+    }
     COSMO_CUDA(cudaMemcpyAsync(B.setPer.get(), per.data(), size_t(nsets) * 4, cudaMemcpyHostToDevice, s.st));
     COSMO_CUDA(cudaStreamSynchronize(s.st));
     return 0;
@@ -1065,6 +1085,41 @@ void cosmo_batch_set_bucket(const int* bucketPerSet)
     State& s = B.core;
     COSMO_CUDA(cudaMemcpyAsync(B.bucket.get(), bucketPerSet, size_t(B.nsets) * 4, cudaMemcpyHostToDevice, s.st));
     COSMO_CUDA(cudaStreamSynchronize(s.st));
+    for (int k = 0; k < B.nsets; ++k) B.tuning[4 * size_t(k)] = bucketPerSet[k];
+}
+
+int cosmo_batch_set_tuning(const int* bucket, const double* listMargin, const int* splitStream, const int* splitWork)
+{
+    Batch& B = batch();
+    State& s = B.core;
+    const int ns = B.nsets;
+    if (ns < 1) return -1;
+    for (int k = 0; k < ns; ++k)
+    {
+        if (bucket && (bucket[k] < kMinTuneBucket || bucket[k] > kMaxTuneBucket)) return -1;
+        if (listMargin && !(listMargin[k] >= 1.0 && listMargin[k] <= 2.0)) return -1;
+        if (splitStream && splitStream[k] < 32) return -1;
+        if (splitWork && splitWork[k] < 32) return -1;
+    }
+    std::vector<double> margin(ns);
+    std::vector<uint2> split(ns);
+    for (int k = 0; k < ns; ++k)
+    {
+        double* t = &B.tuning[4 * size_t(k)];
+        if (bucket) t[0] = bucket[k];
+        if (listMargin) t[1] = listMargin[k];
+        if (splitStream) t[2] = splitStream[k];
+        if (splitWork) t[3] = splitWork[k];
+        margin[k] = t[1];
+        split[k] = make_uint2(uint32_t(t[2]), uint32_t(t[3]));
+    }
+    std::vector<int> bk(ns);
+    for (int k = 0; k < ns; ++k) bk[k] = int(B.tuning[4 * size_t(k)]);
+    COSMO_CUDA(cudaMemcpyAsync(B.bucket.get(), bk.data(), size_t(ns) * 4, cudaMemcpyHostToDevice, s.st));
+    COSMO_CUDA(cudaMemcpyAsync(B.setMargin.get(), margin.data(), size_t(ns) * 8, cudaMemcpyHostToDevice, s.st));
+    COSMO_CUDA(cudaMemcpyAsync(B.setSplit.get(), split.data(), size_t(ns) * 8, cudaMemcpyHostToDevice, s.st));
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    return 0;
 }
 
 void cosmo_batch_upload(const double* x, const double* y, const double* z, const double* h)

@@ -41,9 +41,23 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
 // each, so that no single warp carries the pass's tail; cut items are queued from the
 // front of the buffer and run first (their warps scan the tree for their own box), whole
 // groups from the back.  A window's items hold at most its active particles, so cap = the
-// particle count always suffices.
+// particle count always suffices.  The batched form sets both figures per set (tuned).
 constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
+
+// The cut of one leaf: x = the stream above which it is cut, y = the work of one cut group.
+struct FixedSplit
+{
+    __device__ __forceinline__ uint2 operator()(int) const { return make_uint2(kSplitStream, kSplitWork); }
+};
+
+// The cut of a forest leaf: its set's entry of a per-set table.
+struct SetSplit
+{
+    const int* __restrict__ leafSet;
+    const uint2* __restrict__ setSplit;
+    __device__ __forceinline__ uint2 operator()(int leaf) const { return setSplit[leafSet[leaf]]; }
+};
 
 // Row classification (optional): with rowCount given, an active particle whose
 // neighbour row is complete for its current h (count <= K and h <= rowH) goes to
@@ -56,12 +70,13 @@ struct RowSplit
     int* __restrict__ rowItems;
 };
 
-template<class Ranges>
+template<class Ranges, class Split = FixedSplit>
 __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int nActive, Ranges ranges,
                                            const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
                                            const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
                                            DevScalars* __restrict__ ds, RowSplit rs = RowSplit{nullptr, nullptr, 0,
-                                                                                              nullptr})
+                                                                                              nullptr},
+                                           Split split = Split{})
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -73,7 +88,8 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
         const uint2 rg = ranges(leaf);
         const uint32_t p0 = rg.x, p1 = rg.y;
         const uint32_t S = jstream[leaf];
-        const int gsize = S <= kSplitStream ? 32 : max(1, int(kSplitWork / S));
+        const uint2 cut = split(leaf);
+        const int gsize = S <= cut.x ? 32 : max(1, int(cut.y / S));
         for (uint32_t g = p0; g < p1; g += 64)
         {
             const uint32_t a0 = g + lane, a1 = g + 32 + lane;
@@ -130,13 +146,16 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
     plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, rs);
 }
 
-// The same over a forest's range table, the active count read on the device.
+// The same over a forest's range table, the active count read on the device, each leaf
+// cut by its set's entry of setSplit.
 __global__ void plan_items_table_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr,
                                         const uint2* __restrict__ range, const int* __restrict__ converged,
                                         const uint32_t* __restrict__ jstream, const double4* __restrict__ xyzh,
-                                        int4* __restrict__ items, int cap, DevScalars* __restrict__ ds)
+                                        int4* __restrict__ items, int cap, DevScalars* __restrict__ ds,
+                                        const int* __restrict__ leafSet, const uint2* __restrict__ setSplit)
 {
-    plan_items(leaves, *countPtr, TableRanges{range}, converged, jstream, xyzh, items, cap, ds);
+    plan_items(leaves, *countPtr, TableRanges{range}, converged, jstream, xyzh, items, cap, ds,
+               RowSplit{nullptr, nullptr, 0, nullptr}, SetSplit{leafSet, setSplit});
 }
 
 // A persistent grid: as many blocks of the kernel as fit on the device at once.

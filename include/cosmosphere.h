@@ -105,6 +105,15 @@ int cosmo_batch_init(int nsets, const int* offsets);
 void cosmo_batch_set_params(const double* pmass, const int* periodic, const double* box6);
 /* Leaf capacity of each set's tree (default 64, the reference's BUCKET_SIZE). */
 void cosmo_batch_set_bucket(const int* bucket_per_set);
+/* Per-set launch parameters, as an autotuner picks them (NULL keeps a parameter):
+ * bucket = leaf capacity (8..1024); list_margin = widening of the gather radius the lists
+ * are walked at, which lets them serve later iterations (1..2, default 1.15);
+ * split_stream = gather stream (particles) above which a leaf's active particles are cut
+ * into smaller work items, split_work = the particle-pairs of one cut item (>= 32; default
+ * 4096 and 131072).  None of them changes a result of the plain form.  Returns 0, or -1
+ * (nothing set) when a value is out of range or no batch is initialised. */
+int cosmo_batch_set_tuning(const int* bucket, const double* list_margin, const int* split_stream,
+                           const int* split_work);
 /* Positions and initial h of all sets (host arrays, length offsets[nsets]). */
 void cosmo_batch_upload(const double* x, const double* y, const double* z, const double* h);
 /* Solve every set; 0 ok, 1 some particle unconverged within max_iter (<= 0: 100; at
