@@ -123,7 +123,7 @@ size_t state_device_bytes(const State& s)
     auto add = [&](const auto& buf) { b += buf.cap * sizeof(*buf.p); };
     for (auto* d : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
-                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH})
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH, &s.nblR2})
         add(*d);
     for (auto* d : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) add(*d);
     for (auto* d : {&s.prepAf, &s.prepBf, &s.thermof}) add(*d);
@@ -148,7 +148,7 @@ void release_state(State& s)
     COSMO_CUDA(cudaStreamSynchronize(s.st));
     for (auto* b : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
-                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH})
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH, &s.nblR2})
         b->release(s.st);
     for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) b->release(s.st);
     for (auto* b : {&s.prepAf, &s.prepBf, &s.thermof}) b->release(s.st);

@@ -154,16 +154,17 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
     }
 }
 
-// Newton rows of the still-active particles at their current h (ascending j).  A row is
-// complete while the particle's h stays within kRowMargin of the h it was built at and
-// within the radius its leaf's list covers; rowH records that bound.
+// Newton rows of the still-active particles at their current h: r^2 of every j within
+// kRowMargin of the particle's support, in ascending j.  A row is complete while the
+// particle's h stays within kRowMargin of the h it was built at and within the radius its
+// leaf's list covers; rowH records that bound.
 
 template<bool Periodic>
 __global__ void __launch_bounds__(kThreads)
 newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                    const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                    const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
-                   const double* __restrict__ listH, int* __restrict__ nbl, int* __restrict__ nblCount,
+                   const double* __restrict__ listH, double* __restrict__ nblR2, int* __restrict__ nblCount,
                    double* __restrict__ rowH, DevScalars* __restrict__ ds)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
@@ -200,7 +201,12 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        return pair_r2(dx, dy, dz) * g.w < wide2;
                    },
-                   mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
+                   [&](const double4& pj, int) {   // the owner's own r^2 with j, as the test formed it
+                       double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                       return pair_r2(dx, dy, dz);
+                   },
+                   mine ? row_of(nblR2, uint32_t(i)) : nullptr, rowLen);
         if (mine)
         {
             nblCount[i] = rowLen;
@@ -215,7 +221,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
 // bit; mixed: the mixed pair arithmetic on FP64 separations rounded to FP32, Kahan sums.
 template<bool Periodic, bool Mixed>
 __global__ void __launch_bounds__(kThreads)
-density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl, const int* __restrict__ nblCount,
+density_row_kernel(const int* __restrict__ rowItems, const double* __restrict__ nblR2, const int* __restrict__ nblCount,
                    double4* __restrict__ xyzh, double* __restrict__ rho, double* __restrict__ gradh,
                    int* __restrict__ converged, double pmass, double tolh, double hfact,
                    const DevBox* __restrict__ box, const double* __restrict__ listH,
@@ -224,8 +230,6 @@ density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl
 {
     const int n = ds->rowParticles;
     const int lane = threadIdx.x & 31;
-    double lx = 0, ly = 0, lz = 0;
-    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     unsigned long long pairs = 0;
     for (int t0 = blockIdx.x * blockDim.x; t0 < n; t0 += gridDim.x * blockDim.x)
     {
@@ -240,15 +244,12 @@ density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl
             const double hinv2 = 1.0 / (hi * hi);
             const float hinv2f = float(hinv2);
             const int cnt = nblCount[i];
-            const int* row = row_of(nbl, uint32_t(i));
+            const double* row = row_of(nblR2, uint32_t(i));
             double sr = 0.0, sg = 0.0;
             KahanF kr, kg;
             unsigned int gp = 0;
-            auto pair = [&](int j) {
-                const double4 pj = ldg4(xyzh + j);
-                double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                const double q2 = pair_r2(dx, dy, dz) * hinv2;
+            auto pair = [&](double r2) {
+                const double q2 = r2 * hinv2;
                 if (!(q2 < kRadK2)) return;
                 ++gp;
                 if constexpr (!Mixed)
@@ -261,8 +262,7 @@ density_row_kernel(const int* __restrict__ rowItems, const int* __restrict__ nbl
                 }
                 else
                 {
-                    const float fx = float(dx), fy = float(dy), fz = float(dz);
-                    const float q2f = fmaf(fz, fz, fmaf(fy, fy, fx * fx)) * hinv2f;
+                    const float q2f = float(r2) * hinv2f;
                     const float q = sqrt_q(q2f);
                     float wk, dwk;
                     sph_kernel_f(q2f, q, wk, dwk);
@@ -595,7 +595,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     const int itemCap = std::max(s.nAlive, 1);
     s.items.resize(itemCap, s.st);
     s.rowItems.resize(itemCap, s.st);
-    s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);
+    s.nblR2.resize(row_buffer_entries(size_t(itemCap)), s.st);
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
 
@@ -636,7 +636,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 auto nrows = s.periodic ? newton_rows_kernel<true> : newton_rows_kernel<false>;
                 nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
                     s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
-                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nbl.get(), s.nblCount.get(), s.nblH.get(), ds);
+                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
                 COSMO_LAUNCHED();
                 rowsReady = true;
             }
@@ -663,7 +663,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 auto rk = mx ? (s.periodic ? density_row_kernel<true, true> : density_row_kernel<false, true>)
                              : (s.periodic ? density_row_kernel<true, false> : density_row_kernel<false, false>);
                 rk<<<std::max(1, std::min(iceil(int(nActiveParticles), kThreads), 8 * s.numSMs)), kThreads, 0,
-                     s.st>>>(s.rowItems.get(), s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.rho.get(),
+                     s.st>>>(s.rowItems.get(), s.nblR2.get(), s.nblCount.get(), s.xyzh.get(), s.rho.get(),
                              s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
                              s.particleLeaf.get(), s.leafNext.get(), s.activeB.get(), ds);
                 COSMO_LAUNCHED();

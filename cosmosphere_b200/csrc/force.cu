@@ -279,7 +279,7 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
                        const double dr2 = pair_r2(dx, dy, dz);
                        return !(dr2 >= kRadK2 * fmax(g.w, pj.w * pj.w) * (1.0 + 1e-10));
                    },
-                   mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
+                   [](const double4&, int j) { return j; }, mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
         if (mine) nblCount[i] = rowLen;
     }
 }

@@ -9,6 +9,10 @@
  * that then walks a row applies the same exact test to the same candidates in the same
  * order as a walk of the whole list would, so its sums are the same bit for bit.
  *
+ * An entry is j (the symmetric rows of the gradient and force passes), or r^2 of the pair
+ * (the Newton rows: positions do not move during a density solve, so the later Newton
+ * iterations need only r^2 and h_i, and read no j data at all).
+ *
  * Row layout: kNbl entries per particle, interleaved over blocks of 32 particles -- entry
  * k of particle i at nbl[(i / 32) * 32 kNbl + 32 k + i % 32] -- so that the lanes of a warp
  * over 32 consecutive particles read entry k of all their rows from one 128-byte line.  A
@@ -38,13 +42,14 @@ constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32;
 
 // Rows of one group.  Lanes [0, ng) own the group's particles, whose per-particle test data
 // gi (a double4: position and one test value) the caller passes; test(gi, pj) is the exact
-// acceptance of the pair.  row is the lane's own row (row_of; nullptr if not mine); rowLen
-// receives its length (kNbl + 1 when it overflowed).
-template<class Ranges, class Filter, class Test>
+// acceptance of the pair, and value(pj, j) the entry the owner writes for an accepted j (j
+// itself, or a pair quantity it recomputes from pj).  row is the lane's own row (row_of;
+// nullptr if not mine); rowLen receives its length (kNbl + 1 when it overflowed).
+template<class T, class Ranges, class Filter, class Test, class Value>
 __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng, const double4& gi, const GroupBox& bx,
                                            uint32_t jb, uint32_t nj, const int* __restrict__ jlist, Ranges ranges,
-                                           const double4* __restrict__ xyzh, Filter filter, Test test, int* row,
-                                           int& rowLen)
+                                           const double4* __restrict__ xyzh, Filter filter, Test test, Value value,
+                                           T* row, int& rowLen)
 {
     const int lane = threadIdx.x & 31;
     double4* ring = reinterpret_cast<double4*>(scr);
@@ -74,22 +79,23 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
             {
                 const int b = __ffs(myMask) - 1;
                 myMask &= myMask - 1;
-                if (len < kNbl) row[size_t(len) * kRowStride] = ri[(head + b) & (kRing - 1)];
+                const int sl = (head + b) & (kRing - 1);
+                if (len < kNbl) row[size_t(len) * kRowStride] = value(rg[sl], ri[sl]);
                 ++len;
             }
         });
     rowLen = len > kNbl ? kNbl + 1 : len;
 }
 
-// f(j) for the cnt entries of a row (row_of), in order, four loads ahead of their use.
-template<class F>
-__device__ __forceinline__ void for_row(const int* __restrict__ row, int cnt, F&& f)
+// f(entry) for the cnt entries of a row (row_of), in order, four loads ahead of their use.
+template<class T, class F>
+__device__ __forceinline__ void for_row(const T* __restrict__ row, int cnt, F&& f)
 {
     int k = 0;
     for (; k + 4 <= cnt; k += 4)
     {
-        const int a = __ldg(row + size_t(k) * kRowStride), b = __ldg(row + size_t(k + 1) * kRowStride);
-        const int c = __ldg(row + size_t(k + 2) * kRowStride), d = __ldg(row + size_t(k + 3) * kRowStride);
+        const T a = __ldg(row + size_t(k) * kRowStride), b = __ldg(row + size_t(k + 1) * kRowStride);
+        const T c = __ldg(row + size_t(k + 2) * kRowStride), d = __ldg(row + size_t(k + 3) * kRowStride);
         f(a); f(b); f(c); f(d);
     }
     for (; k < cnt; ++k) f(__ldg(row + size_t(k) * kRowStride));

@@ -153,7 +153,8 @@ struct State
     DBuf<int> jlistPrev, walked;
     uint32_t listTotal = 0;                     // entries of the current lists
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
-    DBuf<int> nbl;                              // neighbour rows, kNbl entries per particle
+    DBuf<int> nbl;                              // symmetric rows (j), kNbl entries per particle
+    DBuf<double> nblR2;                         // Newton rows (r^2), kNbl entries per particle
     DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed)
     DBuf<double> nblH;                          // largest h a Newton row stays complete for
     DBuf<int> rowItems;                         // particles of a Newton iteration on their rows
