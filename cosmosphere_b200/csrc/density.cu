@@ -193,7 +193,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
         const double rmax = warp_max(mine ? rs : 0.0);
         const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
         int rowLen = 0;
-        rows_group(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), bx, jOffset[d.leaf],
+        rows_group<1>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), bx, jOffset[d.leaf],
                    jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
                    [&](const double4& g, const double4& pj) {
@@ -206,7 +206,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        return pair_r2(dx, dy, dz);
                    },
-                   mine ? row_of(nblR2, uint32_t(i)) : nullptr, rowLen);
+                   mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen);
         if (mine)
         {
             nblCount[i] = rowLen;
@@ -244,7 +244,7 @@ density_row_kernel(const int* __restrict__ rowItems, const double* __restrict__ 
             const double hinv2 = 1.0 / (hi * hi);
             const float hinv2f = float(hinv2);
             const int cnt = nblCount[i];
-            const double* row = row_of(nblR2, uint32_t(i));
+            const double* row = row_flat(nblR2, uint32_t(i));
             double sr = 0.0, sg = 0.0;
             KahanF kr, kg;
             unsigned int gp = 0;
@@ -270,7 +270,7 @@ density_row_kernel(const int* __restrict__ rowItems, const double* __restrict__ 
                     kg.add(fmaf(-q, dwk, -3.0f * wk));
                 }
             };
-            for_row(row, cnt, pair);
+            for_flat_row(row, cnt, pair);
             if constexpr (Mixed) { sr = kr.value(); sg = kg.value(); }
             pairs += gp;
             double ro, go, ho;
@@ -595,7 +595,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     const int itemCap = std::max(s.nAlive, 1);
     s.items.resize(itemCap, s.st);
     s.rowItems.resize(itemCap, s.st);
-    s.nblR2.resize(row_buffer_entries(size_t(itemCap)), s.st);
+    s.nblR2.resize(size_t(itemCap) * kNbl, s.st);
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
 

@@ -270,7 +270,7 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
         const double rg = kRadKernel * warp_max(mine ? pi.w : 0.0);
         const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, 0.0, rg);
         int rowLen = 0;
-        rows_group(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, pi.w * pi.w), bx, jOffset[d.leaf],
+        rows_group<kRowStride>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, pi.w * pi.w), bx, jOffset[d.leaf],
                    jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
                    [&](const double4& g, const double4& pj) {

@@ -11,7 +11,10 @@
  *
  * An entry is j (the symmetric rows of the gradient and force passes), or r^2 of the pair
  * (the Newton rows: positions do not move during a density solve, so the later Newton
- * iterations need only r^2 and h_i, and read no j data at all).
+ * iterations need only r^2 and h_i, and read no j data at all).  The Newton rows are flat
+ * (kNbl consecutive doubles per particle): their reader streams its own row 32 bytes at a
+ * time, so the sectors it touches hold only its own entries whichever particles share
+ * its warp.
  *
  * Row layout: kNbl entries per particle, interleaved over blocks of 32 particles -- entry
  * k of particle i at nbl[(i / 32) * 32 kNbl + 32 k + i % 32] -- so that the lanes of a warp
@@ -43,9 +46,10 @@ constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32;
 // Rows of one group.  Lanes [0, ng) own the group's particles, whose per-particle test data
 // gi (a double4: position and one test value) the caller passes; test(gi, pj) is the exact
 // acceptance of the pair, and value(pj, j) the entry the owner writes for an accepted j (j
-// itself, or a pair quantity it recomputes from pj).  row is the lane's own row (row_of;
-// nullptr if not mine); rowLen receives its length (kNbl + 1 when it overflowed).
-template<class T, class Ranges, class Filter, class Test, class Value>
+// itself, or a pair quantity it recomputes from pj).  row is the lane's own row (row_of
+// with Stride kRowStride, or row_flat with Stride 1; nullptr if not mine); rowLen receives
+// its length (kNbl + 1 when it overflowed).
+template<int Stride, class T, class Ranges, class Filter, class Test, class Value>
 __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng, const double4& gi, const GroupBox& bx,
                                            uint32_t jb, uint32_t nj, const int* __restrict__ jlist, Ranges ranges,
                                            const double4* __restrict__ xyzh, Filter filter, Test test, Value value,
@@ -80,11 +84,39 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
                 const int b = __ffs(myMask) - 1;
                 myMask &= myMask - 1;
                 const int sl = (head + b) & (kRing - 1);
-                if (len < kNbl) row[size_t(len) * kRowStride] = value(rg[sl], ri[sl]);
+                if (len < kNbl) row[size_t(len) * Stride] = value(rg[sl], ri[sl]);
                 ++len;
             }
         });
     rowLen = len > kNbl ? kNbl + 1 : len;
+}
+
+// Entry 0 of particle i's row in the flat layout (kNbl consecutive entries per particle).
+template<class T>
+__device__ __forceinline__ T* row_flat(T* nbl, uint32_t i)
+{
+    return nbl + size_t(i) * kNbl;
+}
+
+// f(r2) for the cnt entries of a flat row of doubles, in order, 32 bytes per load (the
+// rows are 32-byte aligned and kNbl is a multiple of 4, so the last load stays in the row).
+template<class F>
+__device__ __forceinline__ void for_flat_row(const double* __restrict__ row, int cnt, F&& f)
+{
+    const double4* r4 = reinterpret_cast<const double4*>(row);
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4)
+    {
+        const double4 v = ldg4(r4 + (k >> 2));
+        f(v.x); f(v.y); f(v.z); f(v.w);
+    }
+    if (k < cnt)
+    {
+        const double4 v = ldg4(r4 + (k >> 2));
+        f(v.x);
+        if (k + 1 < cnt) f(v.y);
+        if (k + 2 < cnt) f(v.z);
+    }
 }
 
 // f(entry) for the cnt entries of a row (row_of), in order, four loads ahead of their use.
