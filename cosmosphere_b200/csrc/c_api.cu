@@ -131,7 +131,7 @@ size_t state_device_bytes(const State& s)
     for (auto* d : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
                     &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
-                    &s.rowItems, &s.jlistPrev, &s.walked})
+                    &s.rowItems, &s.jlistPrev, &s.walked, &s.walkScratch})
         add(*d);
     add(s.items);
     for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
@@ -156,7 +156,7 @@ void release_state(State& s)
     for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
                     &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
-                    &s.rowItems, &s.jlistPrev, &s.walked})
+                    &s.rowItems, &s.jlistPrev, &s.walked, &s.walkScratch})
         b->release(s.st);
     s.items.release(s.st);
     for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,

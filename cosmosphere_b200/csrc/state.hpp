@@ -151,6 +151,7 @@ struct State
     DBuf<int> jlist;
     DBuf<uint32_t> jOffsetPrev;                 // an incremental rebuild's copy of the lists it replaces
     DBuf<int> jlistPrev, walked;
+    DBuf<int> walkScratch;                      // the count pass's copy of each list it walks
     uint32_t listTotal = 0;                     // entries of the current lists
     DBuf<int4> items;                           // Newton work items (leaf, window|group|G, m0, m1)
     DBuf<int> nbl;                              // symmetric rows (j), kNbl entries per particle

@@ -60,11 +60,21 @@ __global__ void bbox_partial_kernel(const double* __restrict__ x, const double* 
 // centred on the particles.
 __global__ void bbox_final_kernel(const double* __restrict__ part, int nb, DevBox* box)
 {
-    if (threadIdx.x != 0) return;
-    double mn[3], mx[3];
-    for (int d = 0; d < 3; ++d) { mn[d] = part[d]; mx[d] = part[3 + d]; }
-    for (int b = 1; b < nb; ++b)
+    // one warp: lanes stride over the block partials, then a shuffle reduction (min and
+    // max are exact, so any order gives the serial result)
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x >= 32) return;
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int b = lane; b < nb; b += 32)
         for (int d = 0; d < 3; ++d) { mn[d] = fmin(mn[d], part[6 * b + d]); mx[d] = fmax(mx[d], part[6 * b + 3 + d]); }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        for (int d = 0; d < 3; ++d)
+        {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    if (lane != 0) return;
     const double sx = mx[0] - mn[0], sy = mx[1] - mn[1], sz = mx[2] - mn[2];
     double span = (sx < sy) ? sy : sx;
     span = (span < sz) ? sz : span;
@@ -337,6 +347,7 @@ __global__ void hmax_level_kernel(int first, int last, const int* __restrict__ c
 }
 
 constexpr double kListLoose = 1.05;   // a kept list may be this much wider than a new one
+constexpr int kWalkScratch = 128;     // list entries per leaf the count pass keeps for the fill
 
 // ------------------------------------------------------------------ j-leaf list walk
 // One warp per i-leaf.  The tree is scanned in pre-order 32 nodes at a time: every lane
@@ -355,11 +366,23 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err,
                  const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
                  double* __restrict__ listH, const uint32_t* __restrict__ jOffsetPrev,
-                 const int* __restrict__ jlistPrev, int* __restrict__ walked)
+                 const int* __restrict__ jlistPrev, int* __restrict__ walked, int* __restrict__ scratch)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (leaf >= nL) return;
+    // The count pass keeps the first kWalkScratch entries of every list it walks in
+    // scratch; the fill pass copies a list that fitted instead of walking it again.
+    if (Fill && scratch != nullptr && (walked == nullptr || walked[leaf] != 0))
+    {
+        const uint32_t dst = jOffset[leaf], cnt = jOffset[leaf + 1] - dst;
+        if (cnt <= uint32_t(kWalkScratch))
+        {
+            const int* src = scratch + leaf * kWalkScratch;
+            for (uint32_t k = lane; k < cnt; k += 32) jlist[dst + k] = src[k];
+            return;
+        }
+    }
     double hmax = hmaxLeaf[leaf];
     if (!isfinite(hmax) || hmax <= 0.0) hmax = 0.0;
     // Incremental rebuild (walked set): a leaf whose hmax is still inside the radius its
@@ -453,8 +476,12 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                     else atomicOr(err, int(kErrListCap));
                 }
             }
-            else if (jstream != nullptr && ((emitMask >> lane) & 1u))
-                stream += layout[pl + 1] - layout[pl];
+            else if ((emitMask >> lane) & 1u)
+            {
+                if (jstream != nullptr) stream += layout[pl + 1] - layout[pl];
+                const uint32_t slot = count + __popc(emitMask & lt);
+                if (scratch != nullptr && slot < uint32_t(kWalkScratch)) scratch[leaf * kWalkScratch + slot] = pl;
+            }
             count += __popc(emitMask);
             if (r >= 32) { next = p + 32; break; }
             int rskip = __shfl_sync(0xffffffffu, skip, r);
@@ -770,7 +797,7 @@ static void walk(State& s, bool fill, double margin, bool incremental)
                                         (!fill && !Sym) ? s.listH.get() : nullptr,
                                         incremental ? s.jOffsetPrev.get() : nullptr,
                                         incremental ? s.jlistPrev.get() : nullptr,
-                                        incremental ? s.walked.get() : nullptr);
+                                        incremental ? s.walked.get() : nullptr, s.walkScratch.get());
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
@@ -795,6 +822,7 @@ void build_lists(State& s, bool symmetric, double margin, bool incremental)
             COSMO_CUDA(cudaMemcpyAsync(s.jlistPrev.get(), s.jlist.get(), size_t(s.listTotal) * sizeof(int),
                                        cudaMemcpyDeviceToDevice, s.st));
     }
+    s.walkScratch.resize(size_t(nL) * kWalkScratch, s.st);
     auto run = [&](bool fill) {
         if (symmetric)
         {
