@@ -772,7 +772,8 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
     achieved = flops / head["t_nr"] / 1e12
     peaks, src = measured_peaks()
     hbm_achieved = BYTES_PER_DENSITY_UPDATE * head["nr_upd"] / head["t_nr"] / 1e9
-    kname = "density_nr_kernel"
+    kname = ("Newton stage, per iteration: density_nr_kernel + newton_rows_kernel + density_row_kernel "
+             "+ plan_items_kernel, timed together by CUDA events")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not quintic:
         cp = workload(args.ref_npartx)
@@ -800,7 +801,10 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
                      "frac": achieved / fp64_peak,
                      "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
                      "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
-                     "traffic": ncu_traffic(kname),
+                     "traffic": ncu_traffic("newton_stage_per_iteration"),
+                     "traffic_note": "DRAM bytes per Newton iteration from ncu (profiles/traffic.json); above the "
+                                     "algorithmic bytes because the Newton rows (r^2 per pair) are written once "
+                                     "and streamed by the later iterations",
                      "hbm": {"achieved": hbm_achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                              "frac": hbm_achieved / peaks.get("hbm_gbs"), "source": src,
                              "byte_convention": "56 B per particle-update"},
