@@ -801,7 +801,8 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
                      "frac": achieved / fp64_peak,
                      "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
                      "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
-                     "traffic": ncu_traffic("newton_stage_per_iteration"),
+                     "traffic": (ncu_traffic("newton_stage_per_iteration")
+                                 if args.workload == "lattice100" and args.npartx == 100 and not quintic else None),
                      "traffic_note": "DRAM bytes per Newton iteration from ncu (profiles/traffic.json); above the "
                                      "algorithmic bytes because the Newton rows (r^2 per pair) are written once "
                                      "and streamed by the later iterations",
