@@ -106,6 +106,35 @@ def test_lattice100_workload_small():
     check_all(c, o)
 
 
+@pytest.mark.parametrize("case", ["plummer_lognormal", "lattice_open"])
+def test_density_only_incremental_lists(case):
+    """Density without gradients: the Newton lists are rebuilt incrementally when an h
+    outgrows its leaf's list (only outgrown or loosened leaves walk, the rest copy), the
+    fill pass copies what the count pass kept (lists up to 128 entries) or walks again
+    (longer lists), and the exact lists of the last iteration are rebuilt at the end.
+    Iteration counts, active counts, h, rho and those final lists equal the oracle's."""
+    if case == "plummer_lognormal":
+        p = inputs.plummer(20000, lnsigma=0.5, seed=7)
+    else:
+        p = inputs.lattice(18)
+        inputs.jiggle_frac(p["h"], 0.2, 0.5, 1.6, 3)
+    n = p.n
+    c = capi.Cosmo()
+    c.arrays_init(n)
+    c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+    c.upload(capi.HSML, p["h"])
+    assert c.density_status(n, p["pmass"], with_gradients=False) == 0
+    o = O.Oracle()
+    assert o.density(p["x"], p["y"], p["z"], p["h"], p["pmass"], with_gradients=False) == 0
+    assert c.scalar("itersRun") == o.scalar("itersRun")
+    np.testing.assert_array_equal(c.array("activePerIter"), o.array("activePerIter"))
+    assert_same(c, o, ["h", "rho", "gradh"])
+    assert_lists_same(c, o)
+    assert c.scalar("pairsDensity") == o.scalar("pairsDensity")
+    if case == "plummer_lognormal":
+        assert int(c.array("jcount").max()) > 128      # some lists take the walking fill
+
+
 def test_periodic_jittered_lattice():
     x, y, z = (np.asarray(v) for v in np.meshgrid(*(np.arange(12) / 12.0,) * 3, indexing="ij"))
     n = x.size
