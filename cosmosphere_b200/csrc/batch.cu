@@ -584,11 +584,11 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
             src.rc = make_double3(c.x, c.y, c.z);
             src.re = make_double3(h.x + ext, h.y + ext, h.z + ext);
         }
-        if (per)
-            density_group<true, Mixed>(sScr[wib], mine, d.ng, pi, bxs.len[0], bxs.len[1], bxs.len[2], src, rhoi,
-                                       gradhi, gp, gc);
-        else
-            density_group<false, Mixed>(sScr[wib], mine, d.ng, pi, 0.0, 0.0, 0.0, src, rhoi, gradhi, gp, gc);
+        // one engine instance for open and periodic sets (zero periods fold nothing): half
+        // the code the warps of a mixed ensemble would otherwise share the instruction
+        // cache with
+        density_group<true, Mixed>(sScr[wib], mine, d.ng, pi, per ? bxs.len[0] : 0.0, per ? bxs.len[1] : 0.0,
+                                   per ? bxs.len[2] : 0.0, src, rhoi, gradhi, gp, gc);
         if (EvalAll)
         {
             // rho and d(rho)/dh at the converged h (src/density_base.cu:635-643)

@@ -12,6 +12,9 @@
  *
  *   plain  the exact FP64 test q^2 = r^2 / h_i^2 < R^2 (src/density_base.cu:270-283) and
  *          FP64 sums in ascending j: bit for bit the oracle's.
+ * The periodic form with zero periods behaves, bit for bit, as the open form (the batched
+ * kernel runs open and periodic sets through the one periodic instance).
+ *
  *   mixed  coordinates relative to the group box centre (at the nearest periodic image
  *          of that centre when the box is small enough for it to be every pair's nearest
  *          image), the test and W, dW in FP32, two group particles per packed f32x2
@@ -160,7 +163,7 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         float* recG = recQ + kRec;
         // relative coordinates at the centre's nearest image are every accepted pair's
         // nearest image when the box (search spheres included) spans under half a period
-        const bool shifted = !Periodic || (bx.ex < 0.5 * lx && bx.ey < 0.5 * ly && bx.ez < 0.5 * lz);
+        const bool shifted = !Periodic || lx == 0.0 || (bx.ex < 0.5 * lx && bx.ey < 0.5 * ly && bx.ez < 0.5 * lz);
         const double sx = shifted && Periodic ? lx : 0.0, sy = shifted && Periodic ? ly : 0.0;
         const double sz = shifted && Periodic ? lz : 0.0;
         gx[lane] = mine ? float(pi.x - bx.cx) : 0.0f;

@@ -54,12 +54,13 @@ __device__ __forceinline__ GroupBox group_box(bool mine, double x, double y, dou
     return b;
 }
 
-// Per-axis distance of a coordinate from a box centre, at the nearest periodic image.
+// Per-axis distance of a coordinate from a box centre, at the nearest periodic image
+// (a zero period, as an open set passes to the periodic form, folds nothing).
 template<bool Periodic>
 __device__ __forceinline__ double axis_dist(double x, double c, double L)
 {
     double d = fabs(x - c);
-    if (Periodic) d = fmin(d, L - d);
+    if (Periodic && L > 0.0) d = fmin(d, L - d);
     return d;
 }
 
@@ -263,7 +264,7 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
 {
     const int lane = threadIdx.x & 31;
     CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz};
-    auto fold = [&](double d, double L) { return Periodic ? fmin(d, L - d) : d; };
+    auto fold = [&](double d, double L) { return (Periodic && L > 0.0) ? fmin(d, L - d) : d; };
     int p = t.n0;
     while (p < t.n1)
     {
