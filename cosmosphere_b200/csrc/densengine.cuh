@@ -75,8 +75,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                 if (ng == 1)
                 {
                     // a single particle (a cut group): every lane evaluates its own pair and
-                    // the sums fold the lanes in order through shuffles, a rejected lane
-                    // adding +0 (which leaves a sum started at +0 unchanged)
+                    // the sums take the accepted lanes in order through shuffles -- the
+                    // serial chain is one add per accepted pair, as in the oracle's loop
                     const double4 g = grp[0];
                     double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
@@ -91,10 +91,12 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                         wv = wk;
                         tv = -q * dwk - 3.0 * wk;
                     }
-                    gp += __popc(__ballot_sync(0xffffffffu, acc));
-#pragma unroll
-                    for (int k = 0; k < 32; ++k)
+                    uint32_t am = __ballot_sync(0xffffffffu, acc);
+                    gp += __popc(am);
+                    while (am)
                     {
+                        const int k = __ffs(am) - 1;
+                        am &= am - 1;
                         sr += __shfl_sync(0xffffffffu, wv, k);
                         sg += __shfl_sync(0xffffffffu, tv, k);
                     }
