@@ -9,6 +9,7 @@
  * still holds an unconverged particle appends the leaf to the next iteration's list.
  */
 #include <algorithm>
+#include <type_traits>
 
 #include "pairstream.cuh"
 #include "state.hpp"
@@ -159,14 +160,16 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
 // particle's h stays within kRowMargin of the h it was built at and within the radius its
 // leaf's list covers; rowH records that bound.
 
-template<bool Periodic>
+template<bool Periodic, bool Mixed>
 __global__ void __launch_bounds__(kThreads)
 newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                    const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                    const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
-                   const double* __restrict__ listH, double* __restrict__ nblR2, int* __restrict__ nblCount,
+                   const double* __restrict__ listH, void* __restrict__ rowsR2, int* __restrict__ nblCount,
                    double* __restrict__ rowH, DevScalars* __restrict__ ds)
 {
+    using R2 = typename std::conditional<Mixed, float, double>::type;   // FP32 rows in the mixed form
+    R2* nblR2 = static_cast<R2*>(rowsR2);
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double lx = 0, ly = 0, lz = 0;
@@ -204,7 +207,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                    [&](const double4& pj, int) {   // the owner's own r^2 with j, as the test formed it
                        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                       return pair_r2(dx, dy, dz);
+                       return R2(pair_r2(dx, dy, dz));
                    },
                    mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen);
         if (mine)
@@ -221,7 +224,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
 // bit; mixed: the mixed pair arithmetic on FP64 separations rounded to FP32, Kahan sums.
 template<bool Periodic, bool Mixed>
 __global__ void __launch_bounds__(kThreads)
-density_row_kernel(const int* __restrict__ rowItems, const double* __restrict__ nblR2, const int* __restrict__ nblCount,
+density_row_kernel(const int* __restrict__ rowItems, const void* __restrict__ rowsR2, const int* __restrict__ nblCount,
                    double4* __restrict__ xyzh, double* __restrict__ rho, double* __restrict__ gradh,
                    int* __restrict__ converged, double pmass, double tolh, double hfact,
                    const DevBox* __restrict__ box, const double* __restrict__ listH,
@@ -244,12 +247,13 @@ density_row_kernel(const int* __restrict__ rowItems, const double* __restrict__ 
             const double hinv2 = 1.0 / (hi * hi);
             const float hinv2f = float(hinv2);
             const int cnt = nblCount[i];
-            const double* row = row_flat(nblR2, uint32_t(i));
+            using R2 = typename std::conditional<Mixed, float, double>::type;
+            const R2* row = row_flat(static_cast<const R2*>(rowsR2), uint32_t(i));
             double sr = 0.0, sg = 0.0;
             KahanF kr, kg;
             unsigned int gp = 0;
-            auto pair = [&](double r2) {
-                const double q2 = r2 * hinv2;
+            auto pair = [&](R2 r2) {
+                const double q2 = double(r2) * hinv2;
                 if (!(q2 < kRadK2)) return;
                 ++gp;
                 if constexpr (!Mixed)
@@ -633,7 +637,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                     s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(),
                     s.xyzh.get(), s.items.get(), itemCap, ds);
                 COSMO_LAUNCHED();
-                auto nrows = s.periodic ? newton_rows_kernel<true> : newton_rows_kernel<false>;
+                auto nrows = s.precision == 1
+                                 ? (s.periodic ? newton_rows_kernel<true, true> : newton_rows_kernel<false, true>)
+                                 : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
                 nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
                     s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
                     s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);

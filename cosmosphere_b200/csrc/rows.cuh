@@ -12,9 +12,9 @@
  * An entry is j (the symmetric rows of the gradient and force passes), or r^2 of the pair
  * (the Newton rows: positions do not move during a density solve, so the later Newton
  * iterations need only r^2 and h_i, and read no j data at all).  The Newton rows are flat
- * (kNbl consecutive doubles per particle): their reader streams its own row 32 bytes at a
- * time, so the sectors it touches hold only its own entries whichever particles share
- * its warp.
+ * (kNbl consecutive entries per particle, FP64, or FP32 in the mixed form): their reader
+ * streams its own row 16-32 bytes at a time, so the sectors it touches hold only its own
+ * entries whichever particles share its warp.
  *
  * Row layout: kNbl entries per particle, interleaved over blocks of 32 particles -- entry
  * k of particle i at nbl[(i / 32) * 32 kNbl + 32 k + i % 32] -- so that the lanes of a warp
@@ -113,6 +113,26 @@ __device__ __forceinline__ void for_flat_row(const double* __restrict__ row, int
     if (k < cnt)
     {
         const double4 v = ldg4(r4 + (k >> 2));
+        f(v.x);
+        if (k + 1 < cnt) f(v.y);
+        if (k + 2 < cnt) f(v.z);
+    }
+}
+
+// The same over a flat row of floats (the mixed form's r^2 rows), 16 bytes per load.
+template<class F>
+__device__ __forceinline__ void for_flat_row(const float* __restrict__ row, int cnt, F&& f)
+{
+    const float4* r4 = reinterpret_cast<const float4*>(row);
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4)
+    {
+        const float4 v = __ldg(r4 + (k >> 2));
+        f(v.x); f(v.y); f(v.z); f(v.w);
+    }
+    if (k < cnt)
+    {
+        const float4 v = __ldg(r4 + (k >> 2));
         f(v.x);
         if (k + 1 < cnt) f(v.y);
         if (k + 2 < cnt) f(v.z);
