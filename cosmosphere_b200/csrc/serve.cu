@@ -116,10 +116,11 @@ double now_s()
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Device bytes a new set of n particles is charged at admission (particle arrays, FP32
-// copies, tree, lists and neighbour rows; about 1 KB/particle measured on the lattice and Plummer sets),
-// until its real footprint is known.
-constexpr long long kBytesPerParticle = 1200;
+// Device bytes a new set of n particles is charged at admission, until its real footprint
+// is known: ≈ 1 KB of particle arrays, FP32 copies, tree and lists, plus the neighbour
+// rows -- 4 bytes (symmetric, j) and 8 bytes (Newton, r^2) per row entry, 128 entries
+// per particle for the cubic kernel and 256 for the quintic one.
+constexpr long long kBytesPerParticle = 1024 + 12 * (kQuintic ? 256 : 128);
 constexpr long long kBytesFixed = 1ll << 20;
 
 struct Request
@@ -531,6 +532,8 @@ double cosmo_serve_stat(const char* name)
     std::lock_guard<std::mutex> lk(S.m);
     const std::string k(name);
     if (k == "device_bytes") return double(g_deviceBytes.load());
+    if (k == "bytes_per_particle") return double(kBytesPerParticle);
+    if (k == "bytes_fixed") return double(kBytesFixed);
     if (k == "budget") return double(S.budget);
     if (k == "resident_sets") return double(S.sets.size());
     if (k == "max_inflight") return S.maxInflight;

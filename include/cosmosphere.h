@@ -163,7 +163,8 @@ double cosmo_serve_request_stat(long request_id, const char* name);
 /* Drop an idle resident set (0), or -1 if unknown or busy. */
 int cosmo_serve_release(long set_id);
 /* Server figures: device_bytes, budget, resident_sets, max_inflight, completed,
- * rejected, evicted, queued, slots. */
+ * rejected, evicted, queued, slots, and the admission estimate of a new set
+ * (bytes_fixed + bytes_per_particle x n). */
 double cosmo_serve_stat(const char* name);
 /* Stop the workers (after the running requests) and release every resident set. */
 int cosmo_serve_stop(void);

@@ -119,7 +119,8 @@ def test_warm_started_continuation(reqs):
 def test_admission_against_the_budget():
     four = [(inputs.uniform_box(8000, seed=40 + k), [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]) for k in range(4)]
     base = capi.load().cosmo_serve_stat(b"device_bytes")
-    est = 2 ** 20 + 1200 * 8000
+    L = capi.load()
+    est = L.cosmo_serve_stat(b"bytes_fixed") + L.cosmo_serve_stat(b"bytes_per_particle") * 8000
     budget = (base + 1.5 * est) / 1e9          # room for one set at a time
     res, stats = serve(four, slots=4, budget=budget)
     assert all(s == 1 for s, _ in res)
@@ -149,7 +150,7 @@ def test_lru_eviction_of_idle_resident_sets():
     finally:
         S.stop()
     base = L.cosmo_serve_stat(b"device_bytes")
-    est = 2 ** 20 + 1200 * 6000
+    est = L.cosmo_serve_stat(b"bytes_fixed") + L.cosmo_serve_stat(b"bytes_per_particle") * 6000
     assert held >= 0.5 * est
     S = capi.Server(slots=1, budget_gb=(base + 2 * held + 0.5 * est) / 1e9)   # two fit, a third does not
     try:
