@@ -48,7 +48,7 @@ struct Batch
     DBuf<uint64_t> keysA, keysB, leafKey, leafKey2;
     DBuf<uint32_t> ops, opsScan, nodeCount, leafPreStart, jcount, jOffset, setHist, setBase, jstream;
     DBuf<uint32_t> jcountPrev, jOffsetPrev;   // the previous walk's lists, kept for reuse
-    DBuf<int> jlistPrev, walked;
+    DBuf<int> jlistPrev, walked, walkScratch;
     DBuf<double> listH;                       // h each leaf's list covers (0: none)
     DBuf<int4> items;                 // Newton work items (leaf, window|group|G, m0, m1)
     DBuf<int> leafNext;               // leaf already queued for the next iteration
@@ -72,6 +72,7 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 constexpr double kBatchListMargin = 1.15;   // default gather-radius widening of a set's lists
 constexpr int kMinTuneBucket = 8, kMaxTuneBucket = 1024;   // leaf capacities a set may be given
+constexpr int kWalkScratchB = 128;   // list entries per leaf the count pass keeps for the fill
 
 __device__ __forceinline__ int set_of_pos(const int* __restrict__ offs, int nsets, long k)
 {
@@ -368,7 +369,7 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
                    uint32_t listCap, int* err, const uint2* __restrict__ range, uint32_t* __restrict__ jstream,
                    double* __restrict__ listH, int* __restrict__ walked, const uint32_t* __restrict__ jcountPrev,
                    const uint32_t* __restrict__ jOffsetPrev, const int* __restrict__ jlistPrev,
-                   const double* __restrict__ setMargin)
+                   const double* __restrict__ setMargin, int* __restrict__ scratch)
 {
     const int lane = threadIdx.x & 31;
     const int nAct = *countPtr;
@@ -389,7 +390,23 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
             continue;
         }
     }
-    else if (walked[leaf] == 0)
+    else if (walked[leaf] != 0)
+    {
+        // a walked list that fitted in the count pass's copy is copied, not walked again
+        const uint32_t dst = jOffset[leaf], cnt = jOffset[leaf + 1] - dst;
+        if (cnt <= uint32_t(kWalkScratchB))
+        {
+            if (jOffset[leaf + 1] > listCap)
+            {
+                if (lane == 0) atomicOr(err, int(kErrListFull));
+                continue;
+            }
+            const int* src = scratch + size_t(leaf) * kWalkScratchB;
+            for (uint32_t k = lane; k < cnt; k += 32) jlist[dst + k] = src[k];
+            continue;
+        }
+    }
+    else
     {
         const uint32_t dst = jOffset[leaf], cnt = jOffset[leaf + 1] - dst, src = jOffsetPrev[leaf];
         if (jOffset[leaf + 1] > listCap)
@@ -461,7 +478,12 @@ list_walk_kernel_b(const int* __restrict__ leaves, const int* __restrict__ count
                 if (slot < cap) jlist[base + slot] = pl;
                 else atomicOr(err, int(kErrListCap));
             }
-            if (!Fill && ((emitMask >> lane) & 1u)) stream += range[pl].y - range[pl].x;
+            if (!Fill && ((emitMask >> lane) & 1u))
+            {
+                stream += range[pl].y - range[pl].x;
+                const uint32_t slot = count + __popc(emitMask & lt);
+                if (slot < uint32_t(kWalkScratchB)) scratch[size_t(leaf) * kWalkScratchB + slot] = pl;
+            }
             count += __popc(emitMask);
             if (r >= 32) { next = p + 32; break; }
             int rskip = __shfl_sync(0xffffffffu, skip, r);
@@ -777,6 +799,7 @@ static void batch_build(Batch& B)
     B.jcountPrev.resize(L, s.st);
     B.jOffsetPrev.resize(size_t(L) + 1, s.st);
     B.walked.resize(L, s.st);
+    B.walkScratch.resize(size_t(L) * kWalkScratchB, s.st);
     B.listH.resize(L, s.st);
     B.leafNext.resize(L, s.st);
     B.items.resize(std::max(B.n, 1), s.st);
@@ -808,7 +831,7 @@ static void walk_lists(Batch& B, bool fill, const int* leaves, const int* countP
                                        B.boxes.get(), B.jcount.get(), B.jOffset.get(), B.jlist.get(), B.listCap,
                                        &s.dscal.get()->err, B.leafRange.get(), B.jstream.get(), B.listH.get(),
                                        B.walked.get(), B.jcountPrev.get(), B.jOffsetPrev.get(), B.jlistPrev.get(),
-                                       B.setMargin.get());
+                                       B.setMargin.get(), B.walkScratch.get());
     };
     if (fill) go(list_walk_kernel_b<true>);
     else go(list_walk_kernel_b<false>);
