@@ -297,6 +297,28 @@ def run_ensemble(args, rank, world, local, dist):
         dist.destroy_process_group()
 
 
+def profile_ensemble(args, local):
+    """For ncu: the ensemble's sets solved as one batch, --warmup + --steps times, with the
+    Newton loop driven from the host (each iteration's launches visible to the profiler),
+    in the precision --precision names (fp64 or mixed), with the default launch parameters
+    or (--autotune on) tuned ones; prints the last solve's counters."""
+    from cosmosphere_b200 import autotune, capi, inputs
+    sets = inputs.ensemble_sets(args.nsets)
+    c = capi.Cosmo()
+    c.set_device(local)
+    c.set_precision(args.precision == "mixed")
+    table = autotune.tune(sets, max_particles=args.tune_particles) if args.autotune == "on" else None
+    b = capi.Batch(sets)
+    if table is not None:
+        table.apply(b)
+    b.upload()
+    for _ in range(args.warmup + args.steps):
+        assert b.density(final_rho=True, graph=False) == 0
+    print(json.dumps({"profile_solves": args.warmup + args.steps,
+                      **{k: b.scalar(k) for k in ["t_total", "t_nr", "t_build", "itersRun", "nLeaves", "updates"]}}),
+          flush=True)
+
+
 def _served_fp64_loop(reqs):
     """The plain FP64 one-request-at-a-time loop through the C-ABI: per request upload,
     density, thermo, force and download of every output; a continuation drifts its set's
@@ -550,7 +572,10 @@ def main():
         run_reference(args, rank, world, local, dist)
         return
     if args.workload == "ensemble":
-        run_ensemble(args, rank, world, local, dist)
+        if args.profile:
+            profile_ensemble(args, local)
+        else:
+            run_ensemble(args, rank, world, local, dist)
         return
     if args.workload == "served":
         run_served(args, rank, world, local, dist)
