@@ -205,7 +205,9 @@ def run_ensemble(args, rank, world, local, dist):
             # per size class, on this rank's sets, before anything is timed
             w0 = time.perf_counter()
             table = autotune.tune(sets, max_particles=args.tune_particles)
-            tuned[mode] = {"seconds": time.perf_counter() - w0, **table.to_json()}
+            table, t_tab, t_def = autotune.confirm(sets, table)
+            tuned[mode] = {"seconds": time.perf_counter() - w0, "confirm_s": {"tuned": t_tab, "default": t_def},
+                           "kept": "tuned" if table.entries else "default", **table.to_json()}
             b = capi.Batch(sets)
             b.upload()
             for _ in range(args.warmup):

@@ -157,6 +157,33 @@ def solve_time(sets, tuning: Tuning, repeats: int = 2, final_rho: bool = True) -
     return best
 
 
+def batch_time(sets, table: "Table", repeats: int = 2, final_rho: bool = True) -> float:
+    """Device time (s) of the batched solve of all these sets with a table's per-class
+    parameters: the minimum over repeats, after one untimed solve."""
+    from . import capi
+    b = capi.Batch(sets)
+    table.apply(b)
+    b.upload()
+    if b.density(final_rho=final_rho) != 0:
+        return math.inf
+    best = math.inf
+    for _ in range(max(1, repeats)):
+        b.upload()
+        if b.density(final_rho=final_rho) != 0:
+            return math.inf
+        best = min(best, b.scalar("t_total"))
+    return best
+
+
+def confirm(sets, table: "Table", repeats: int = 2, timer: Callable = batch_time):
+    """The tuned table or the defaults, whichever solves the whole batch faster: the
+    classes are tuned on samples solved alone, and a setting can lose a few percent once
+    every set shares the GPU.  Returns (table, tuned seconds, default seconds)."""
+    t_tuned = timer(sets, table, repeats)
+    t_default = timer(sets, Table(), repeats)
+    return (table if t_tuned <= t_default else Table()), t_tuned, t_default
+
+
 def tune(sets, max_particles: float = 2.0e6, repeats: int = 2, sweeps: int = 1,
          candidates: Dict[str, tuple] = CANDIDATES, timer: Callable = solve_time,
          classes: Iterable[int] | None = None) -> Table:

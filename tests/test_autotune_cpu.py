@@ -87,3 +87,13 @@ def test_apply_passes_per_set_arrays():
     at.Table({at.size_class(300000): at.Tuning(bucket=128)}).apply(b)
     assert b.kw["bucket"].tolist() == [64, 128]
     assert b.kw["split_work"].tolist() == [131072, 131072]
+
+
+def test_confirm_keeps_the_faster_of_tuned_and_default():
+    tuned = at.Table({14: at.Tuning(bucket=128)})
+    times = {True: 1.0, False: 2.0}
+    t, a, b = at.confirm([], tuned, timer=lambda sets, table, r: times[bool(table.entries)])
+    assert t is tuned and (a, b) == (1.0, 2.0)
+    times = {True: 3.0, False: 2.0}
+    t, a, b = at.confirm([], tuned, timer=lambda sets, table, r: times[bool(table.entries)])
+    assert t.entries == {} and (a, b) == (3.0, 2.0)
