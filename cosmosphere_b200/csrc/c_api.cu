@@ -623,6 +623,7 @@ double cosmo_x_scalar(const char* name)
         if (k == "pairsDensity") return double(s.hscal->pairs[0]);
         if (k == "pairsGrad") return double(s.hscal->pairs[1]);
         if (k == "pairsForce") return double(s.hscal->pairs[2]);
+        if (k == "rowOverflow") return double(s.hscal->rowOverflow);
         if (k == "candDensity") return double(s.hscal->pairs[3]);
         if (k == "unconverged") return s.hscal->unconverged;
     }

@@ -482,6 +482,7 @@ gradient_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __r
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     unsigned long long pairs = 0;
     const double pm = pmass;
+    if (nblCount != nullptr && ds->rowOverflow == 0) return;   // every row complete: nothing to do
     auto wanted = [&](uint32_t a) { return nblCount == nullptr || unsigned(nblCount[a]) > unsigned(kNbl); };
     for (int leaf = warpGlobal; leaf < nL; leaf += nWarps)
     {

@@ -191,6 +191,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     unsigned long long pairs = 0;
     const double pm = pmass;
+    if (nblCount != nullptr && ds->rowOverflow == 0) return;   // every row complete: nothing to do
     auto wanted = [&](uint32_t a) { return nblCount == nullptr || !row_ok(nblCount, a); };
     for (int leaf = warpGlobal; leaf < nL; leaf += nWarps)
     {
@@ -281,6 +282,7 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
                    },
                    [](const double4&, int j) { return j; }, mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
         if (mine) nblCount[i] = rowLen;
+        if (mine && rowLen > kNbl) ds->rowOverflow = 1;
     }
 }
 
@@ -344,6 +346,7 @@ void build_symmetric(State& s)
     s.nblCount.resize(nA, s.st);
     begin_iteration_kernel<<<1, 32, 0, s.st>>>(ds, nullptr, 0);
     COSMO_LAUNCHED();
+    COSMO_CUDA(cudaMemsetAsync(&ds->rowOverflow, 0, sizeof(int), s.st));
     plan_items_kernel<<<grid, kThreads, 0, s.st>>>(nullptr, nL, s.layout.get(), nullptr, s.jstream.get(),
                                                     s.xyzh.get(), s.items.get(), nA, ds);
     COSMO_LAUNCHED();

@@ -93,7 +93,8 @@ struct DevScalars
     int itemsHeavy, itemsLight;  // Newton work items of the current iteration (split, whole)
     int rowParticles;            // particles of the current iteration on their neighbour rows
     int settling;                // unconverged particles whose h moved by less than kSettle
-    int pad[2];
+    int rowOverflow;             // some symmetric row overflowed (its particle takes the group path)
+    int pad[1];
 };
 
 struct Timings

@@ -135,6 +135,22 @@ def test_density_only_incremental_lists(case):
         assert int(c.array("jcount").max()) > 128      # some lists take the walking fill
 
 
+@pytest.mark.parametrize("overflow", [False, True])
+def test_symmetric_row_overflow_takes_the_group_path(overflow):
+    """Particles whose symmetric row would hold more than 128 entries (a compact core in
+    a wide halo of large h) take the group path in the gradient sweep and the force pass;
+    when no row overflows those passes skip the group path altogether.  Either way every
+    field equals the oracle's."""
+    if overflow:
+        p = inputs.plummer(6000, lnsigma=0.9, seed=12)
+    else:
+        p = inputs.lattice(14)
+        inputs.jiggle_ref(p["h"], 42)
+    c, o = run_pair(p)
+    assert c.scalar("rowOverflow") == (1.0 if overflow else 0.0)
+    check_all(c, o)
+
+
 def test_periodic_jittered_lattice():
     x, y, z = (np.asarray(v) for v in np.meshgrid(*(np.arange(12) / 12.0,) * 3, indexing="ij"))
     n = x.size
