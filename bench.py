@@ -824,18 +824,20 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
                    "parallelism": f"replicas x{world}", "l2": "working set above the 126 MB L2 (no flush needed)"},
         "e2e": {"value": head["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
                 "d2h_bytes_per_step": head["d2h"], "ms_per_step": head["e2e_ms_per_step"]},
-        "roofline": {"kernel": kname, "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp64_peak,
-                     "peak_source": "FP64 FMA microkernel run in this bench (MEASURED_PEAKS.json has no FP64 figure)",
-                     "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
+        "roofline": {"kernel": kname, "bound": "hbm", "achieved": hbm_achieved, "peak": peaks.get("hbm_gbs"),
+                     "unit": "GB/s", "frac": hbm_achieved / peaks.get("hbm_gbs"), "peak_source": src,
+                     "byte_convention": "56 B per particle-update (read x, y, z, h; write h, rho, dh, flag)",
+                     "algorithmic_bytes_per_iteration": BYTES_PER_DENSITY_UPDATE * head["nr_upd"]
+                                                        / max(1, head["nr_launches"]),
                      "traffic": (ncu_traffic("newton_stage_per_iteration")
                                  if args.workload == "lattice100" and args.npartx == 100 and not quintic else None),
                      "traffic_note": "DRAM bytes per Newton iteration from ncu (profiles/traffic.json); above the "
                                      "algorithmic bytes because the Newton rows (r^2 per pair) are written once "
                                      "and streamed by the later iterations",
-                     "hbm": {"achieved": hbm_achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                             "frac": hbm_achieved / peaks.get("hbm_gbs"), "source": src,
-                             "byte_convention": "56 B per particle-update"},
+                     "fp64": {"achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                              "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
+                              "peak_source": "FP64 FMA microkernel run in this bench "
+                                             "(MEASURED_PEAKS.json has no FP64 figure)"},
                      "launch_ms": 1e3 * head["t_nr"] / max(1, head["nr_launches"])},
         "kernel_ms_per_step": head["kernel_ms_per_step"],
         "plain_fp64": strip(plain),
