@@ -271,14 +271,18 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
         const double rg = kRadKernel * warp_max(mine ? pi.w : 0.0);
         const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, 0.0, rg);
         int rowLen = 0;
-        rows_group<kRowStride>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, pi.w * pi.w), bx, jOffset[d.leaf],
-                   jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
+        // the force pass's test dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10), with each side's
+        // bound formed once: rounding is monotone, so the bound of the larger h is the
+        // larger bound and max(bound_i, bound_j) is the same double as the test's own
+        auto bound = [](double h) { return kRadK2 * (h * h) * (1.0 + 1e-10); };
+        rows_group<kRowStride>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, bound(pi.w)), bx,
+                   jOffset[d.leaf], jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
                    [&](const double4& g, const double4& pj) {
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        const double dr2 = pair_r2(dx, dy, dz);
-                       return !(dr2 >= kRadK2 * fmax(g.w, pj.w * pj.w) * (1.0 + 1e-10));
+                       return !(dr2 >= fmax(g.w, bound(pj.w)));
                    },
                    [](const double4&, int j) { return j; }, mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
         if (mine) nblCount[i] = rowLen;
