@@ -816,8 +816,10 @@ static void batch_build(Batch& B)
     B.tBuild = elapsed_s(e0, e1);
 }
 
-// The gather lists of the given leaves (count on the device); the counts of all other
-// leaves are zero, so the scan sizes the list storage for these leaves only.
+// The gather lists of the given leaves (count on the device): a leaf whose kept list
+// still covers its hmax copies it, the others walk (the count pass keeps what it walks
+// for the fill pass).  The counts of all other leaves are zero, so the scan sizes the
+// list storage for these leaves only.
 static void walk_lists(Batch& B, bool fill, const int* leaves, const int* countPtr)
 {
     State& s = B.core;
