@@ -127,3 +127,19 @@ def test_final_rho_mixed_within_bound(sets):
         live = h0 > 0
         assert np.max(np.abs(h1[live] / h0[live] - 1)) <= 1e-5, k
         assert np.max(np.abs(r1[live] / r0[live] - 1)) <= 1e-5, k
+
+
+def test_batch_with_tiny_sets():
+    """Sets of one leaf and just over one leaf beside a larger one: each comes out as the
+    same set solved alone."""
+    tiny = []
+    for n in (33, 65, 700):
+        rng = np.random.default_rng(100 + n)
+        x, y, z = rng.random((3, n))
+        tiny.append(dict(inputs.Particles(x=x, y=y, z=z, h=np.full(n, 1.2 * (1.0 / n) ** (1.0 / 3.0)),
+                                          pmass=1.0 / n)))
+    alone = [single(s) for s in tiny]
+    b, (h, rho, gh) = run_batch(tiny)
+    for k, (hs, d) in enumerate(alone):
+        np.testing.assert_array_equal(h[k], hs, err_msg=f"set {k} h")
+        np.testing.assert_array_equal(rho[k], d[0], err_msg=f"set {k} rho")

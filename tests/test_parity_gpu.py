@@ -151,6 +151,17 @@ def test_symmetric_row_overflow_takes_the_group_path(overflow):
     check_all(c, o)
 
 
+@pytest.mark.parametrize("n", [33, 64, 65, 130])
+def test_small_sets_around_one_leaf(n):
+    """A set of one leaf, exactly one full leaf, one particle over (the root splits into
+    eight) and two leaves' worth: every structure and field equals the oracle's."""
+    rng = np.random.default_rng(n)
+    x, y, z = rng.random((3, n))
+    p = inputs.Particles(x=x, y=y, z=z, h=np.full(n, 1.2 * (1.0 / n) ** (1.0 / 3.0)), pmass=1.0 / n)
+    c, o = run_pair(p)
+    check_all(c, o)
+
+
 def test_periodic_jittered_lattice():
     x, y, z = (np.asarray(v) for v in np.meshgrid(*(np.arange(12) / 12.0,) * 3, indexing="ij"))
     n = x.size
