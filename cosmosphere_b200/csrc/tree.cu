@@ -347,7 +347,7 @@ __global__ void hmax_level_kernel(int first, int last, const int* __restrict__ c
 }
 
 constexpr double kListLoose = 1.05;   // a kept list may be this much wider than a new one
-constexpr int kWalkScratch = 128;     // list entries per leaf the count pass keeps for the fill
+constexpr int kWalkScratch = 512;     // list entries per leaf the count pass keeps for the fill
 
 // ------------------------------------------------------------------ j-leaf list walk
 // One warp per i-leaf.  The tree is scanned in pre-order 32 nodes at a time: every lane

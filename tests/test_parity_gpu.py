@@ -110,7 +110,7 @@ def test_lattice100_workload_small():
 def test_density_only_incremental_lists(case):
     """Density without gradients: the Newton lists are rebuilt incrementally when an h
     outgrows its leaf's list (only outgrown or loosened leaves walk, the rest copy), the
-    fill pass copies what the count pass kept (lists up to 128 entries) or walks again
+    fill pass copies what the count pass kept (lists up to 512 entries) or walks again
     (longer lists), and the exact lists of the last iteration are rebuilt at the end.
     Iteration counts, active counts, h, rho and those final lists equal the oracle's."""
     if case == "plummer_lognormal":
@@ -132,7 +132,7 @@ def test_density_only_incremental_lists(case):
     assert_lists_same(c, o)
     assert c.scalar("pairsDensity") == o.scalar("pairsDensity")
     if case == "plummer_lognormal":
-        assert int(c.array("jcount").max()) > 128      # some lists take the walking fill
+        assert int(c.array("jcount").max()) > 512      # some lists take the walking fill
 
 
 @pytest.mark.parametrize("overflow", [False, True])
