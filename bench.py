@@ -569,10 +569,12 @@ def main():
     args = ap.parse_args()
     if not args.profile:
         args.warmup = max(3, args.warmup)
-    rank, world, local, dist = dist_setup(args)
     if args.impl == "reference":
-        run_reference(args, rank, world, local, dist)
+        # host cores only: rank 0 times the CPU arm, the other ranks exit at once; no
+        # process group is needed for that
+        run_reference(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0, None)
         return
+    rank, world, local, dist = dist_setup(args)
     if args.workload == "ensemble":
         if args.profile:
             profile_ensemble(args, local)
