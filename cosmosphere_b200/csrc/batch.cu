@@ -1151,6 +1151,7 @@ void cosmo_batch_upload(const double* x, const double* y, const double* z, const
 {
     Batch& B = batch();
     State& s = B.core;
+    if (B.n < 1) return;   // no batch initialised: nothing to receive
     const size_t bytes = size_t(B.n) * 8;
     COSMO_CUDA(cudaMemcpyAsync(B.ux.get(), x, bytes, cudaMemcpyHostToDevice, s.st));
     COSMO_CUDA(cudaMemcpyAsync(B.uy.get(), y, bytes, cudaMemcpyHostToDevice, s.st));
@@ -1172,6 +1173,7 @@ void cosmo_batch_download(double* h, double* rho, double* gradh)
     Batch& B = batch();
     State& s = B.core;
     const int n = B.n;
+    if (n < 1) return;   // no batch initialised: nothing to send
     scatter_kernel_b<<<iceil(n, 256), 256, 0, s.st>>>(B.orderA.get(), n, B.xyzh.get(), B.rho.get(), B.gradh.get(),
                                                      s.xfer.get());
     COSMO_LAUNCHED();

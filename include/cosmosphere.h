@@ -114,7 +114,8 @@ void cosmo_batch_set_bucket(const int* bucket_per_set);
  * (nothing set) when a value is out of range or no batch is initialised. */
 int cosmo_batch_set_tuning(const int* bucket, const double* list_margin, const int* split_stream,
                            const int* split_work);
-/* Positions and initial h of all sets (host arrays, length offsets[nsets]). */
+/* Positions and initial h of all sets (host arrays, length offsets[nsets]); a no-op
+ * before cosmo_batch_init, as is cosmo_batch_download. */
 void cosmo_batch_upload(const double* x, const double* y, const double* z, const double* h);
 /* Solve every set; 0 ok, 1 some particle unconverged within max_iter (<= 0: 100; at
  * most 128).  flags: COSMO_BATCH_GRAPH runs the whole Newton loop as one CUDA graph
