@@ -21,6 +21,7 @@ EXPORTS = [
     "cosmo_arrays_init", "cosmo_slot_ncomp", "cosmo_upload", "cosmo_upload_sorted", "cosmo_download",
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
+    "cosmo_x_stats_line",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
     "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_set_tuning",
@@ -53,6 +54,8 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_density.argtypes = [I, D, I, P, D, D, I, I]
     L.cosmo_x_density.restype = I
     L.cosmo_x_scalar.argtypes = [ctypes.c_char_p]
+    L.cosmo_x_stats_line.argtypes = [I, P, ctypes.c_char_p, I]
+    L.cosmo_x_stats_line.restype = I
     L.cosmo_x_scalar.restype = D
     L.cosmo_x_array.argtypes = [ctypes.c_char_p, P, ctypes.POINTER(I)]
     L.cosmo_x_array.restype = ctypes.c_long
@@ -156,6 +159,16 @@ class Cosmo:
 
     def force(self, n, pmass, *, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1):
         self.L.force_gpu_c(int(n), float(pmass), float(beta), float(alphau), int(disc), int(pdv), int(shock))
+
+    def stats_line(self, which: int, values) -> str:
+        """One statistics line (0 COSMO_STATS, 1 COSMO_FORCE, 2 COSMO_MEM) formatted by the
+        library from the given values, as its entry points print it."""
+        v = _c(values)
+        buf = ctypes.create_string_buffer(1024)
+        n = self.L.cosmo_x_stats_line(which, v.ctypes.data, buf, len(buf))
+        if n < 0:
+            raise ValueError(which)
+        return buf.value.decode()
 
     def kernel_radius(self) -> float:
         return float(self.L.cosmo_kernel_radius())

@@ -397,6 +397,64 @@ static void upload_slot(int slot, const double* host, int n, bool sorted, const 
 // ------------------------------------------------------------------ stats lines
 static bool env_on(const char* k) { return std::getenv(k) != nullptr; }
 
+// Host high-water mark (VmHWM, kB) of this process, as the reference's COSMO_MEM line
+// reports it (src/dens_c_api.cu:84-92); 0 where /proc is unavailable.
+static long host_peak_kb()
+{
+    long kb = 0;
+    if (FILE* fp = std::fopen("/proc/self/status", "r"))
+    {
+        char line[256];
+        while (std::fgets(line, sizeof line, fp))
+            if (std::strncmp(line, "VmHWM:", 6) == 0)
+            {
+                std::sscanf(line + 6, "%ld", &kb);
+                break;
+            }
+        std::fclose(fp);
+    }
+    return kb;
+}
+
+
+// The three stderr lines, formatted from their values in the order the reference prints
+// them: COSMO_STATS (src/dens_c_api.cu:113-122), COSMO_FORCE (src/force_c_api.cu:74-79)
+// and COSMO_MEM (src/dens_c_api.cu:95-97).  Operators grep these key=value fields, so
+// the keys, their order and the number formats are the reference's.
+// v: n leaves iters vecin upload bbox keysort tree nodes jbuild nrkern gjbuild gradkern
+//    download gpusum solve unaccounted total (ms)
+static int format_dens_stats(char* buf, size_t len, const double* v)
+{
+    return std::snprintf(buf, len,
+                         "COSMO_STATS n=%d leaves=%d iters=%d | vecin=%.2f upload=%.2f bbox=%.2f keysort=%.2f "
+                         "tree=%.2f nodes=%.2f jbuild=%.2f nrkern=%.2f gjbuild=%.2f gradkern=%.2f download=%.2f | "
+                         "gpusum=%.2f solve=%.2f unaccounted=%.2f total=%.2f\n",
+                         int(v[0]), int(v[1]), int(v[2]), v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10], v[11],
+                         v[12], v[13], v[14], v[15], v[16], v[17]);
+}
+// v: n leaves upsweep jbuild upload prep kernel download gpusum wall unaccounted (ms)
+static int format_force_stats(char* buf, size_t len, const double* v)
+{
+    return std::snprintf(buf, len,
+                         "COSMO_FORCE n=%d leaves=%d | upsweep=%.2f jbuild=%.2f upload=%.2f prep=%.2f kernel=%.2f "
+                         "download=%.2f | gpusum=%.2f wall=%.2f unaccounted=%.2f\n",
+                         int(v[0]), int(v[1]), v[2], v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10]);
+}
+// v: n device_used_GB total_GB bytes_per_particle host_peak_GB
+static int format_mem_line(char* buf, size_t len, const double* v)
+{
+    return std::snprintf(buf, len,
+                         "COSMO_MEM n=%d device_used=%.2f GB of %.2f GB (%.0f bytes/particle) host_peak=%.2f GB\n",
+                         int(v[0]), v[1], v[2], v[3], v[4]);
+}
+
+static void print_line(int (*fmt)(char*, size_t, const double*), const double* v)
+{
+    char buf[512];
+    fmt(buf, sizeof buf, v);
+    std::fputs(buf, stderr);
+}
+
 } // namespace cosmo
 
 using namespace cosmo;
@@ -459,6 +517,9 @@ void densityiterate_gpu_c(int n, double pmass, int periodic, const double* box, 
     if (n <= 0) return;
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
+    // vecin= is the host time between entry and the start of the solve, as the reference
+    // reports it (src/dens_c_api.cu:73-76); with the transfers outside the call it is ~0.
+    const auto tv = clk::now();
     const DensResult r = solve_density(s, n, pmass, periodic ? box : nullptr, tolh, hfact, s.maxIter, true);
     const auto t1 = clk::now();
     if (r.status == 1)
@@ -473,22 +534,23 @@ void densityiterate_gpu_c(int n, double pmass, int periodic, const double* box, 
         memReported = true;
         size_t fr = 0, tot = 0;
         COSMO_CUDA(cudaMemGetInfo(&fr, &tot));
-        std::fprintf(stderr, "COSMO_MEM n=%d device_used=%.2f GB of %.2f GB (%.0f bytes/particle)\n", n,
-                     (tot - fr) / 1e9, tot / 1e9, double(tot - fr) / n);
+        const double v[5] = {double(n), (tot - fr) / 1e9, tot / 1e9, double(tot - fr) / n, host_peak_kb() / 1e6};
+        print_line(format_mem_line, v);
     }
     static const bool stats = env_on("COSMO_DENS_STATS");
     if (stats)
     {
         const Timings& t = s.t;
         const double gpu = 1e3 * (t.bbox + t.keysSort + t.tree + t.nodes + t.jbuild + t.nrkern + t.gjbuild + t.gradkern);
-        const double solve = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        std::fprintf(stderr,
-                     "COSMO_STATS n=%d leaves=%d iters=%d | upload=%.2f bbox=%.2f keysort=%.2f tree=%.2f nodes=%.2f "
-                     "jbuild=%.2f nrkern=%.2f gjbuild=%.2f gradkern=%.2f download=%.2f | gpusum=%.2f solve=%.2f "
-                     "unaccounted=%.2f\n",
-                     n, s.nLeaves, s.itersRun, 1e3 * s.uploadSeconds, 1e3 * t.bbox, 1e3 * t.keysSort, 1e3 * t.tree,
-                     1e3 * t.nodes, 1e3 * t.jbuild, 1e3 * t.nrkern, 1e3 * t.gjbuild, 1e3 * t.gradkern,
-                     1e3 * s.downloadSeconds, gpu, solve, solve - gpu);
+        auto ms = [](clk::time_point a, clk::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        const double solve = ms(tv, t1);
+        const double v[18] = {double(n), double(s.nLeaves), double(s.itersRun), ms(t0, tv), 1e3 * s.uploadSeconds,
+                              1e3 * t.bbox, 1e3 * t.keysSort, 1e3 * t.tree, 1e3 * t.nodes, 1e3 * t.jbuild,
+                              1e3 * t.nrkern, 1e3 * t.gjbuild, 1e3 * t.gradkern, 1e3 * s.downloadSeconds, gpu,
+                              solve, solve - gpu, ms(t0, t1)};
+        print_line(format_dens_stats, v);
     }
     s.uploadSeconds = 0.0;
     s.downloadSeconds = 0.0;
@@ -514,12 +576,14 @@ void force_gpu_c(int n, double pmass, double beta, double alphau, int disc_visco
     {
         const double wall = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         const Timings& t = s.t;
-        const double gpu = 1e3 * (t.upsweep + t.fjbuild + t.prep + t.fkern);
-        std::fprintf(stderr,
-                     "COSMO_FORCE n=%d leaves=%d | upsweep=%.2f jbuild=%.2f prep=%.2f kernel=%.2f | gpusum=%.2f "
-                     "wall=%.2f unaccounted=%.2f\n",
-                     s.ngas, s.nLeaves, 1e3 * t.upsweep, 1e3 * t.fjbuild, 1e3 * t.prep, 1e3 * t.fkern, gpu, wall,
-                     wall - gpu);
+        // upload= and download= are the transfers inside the call (src/force_c_api.cu:74-79):
+        // the caller moves THERMO, VEL and FORCE_OUT with cosmo_upload_sorted / cosmo_download,
+        // so the force pass itself moves nothing and both are 0.
+        const double upload = 0.0, download = 0.0;
+        const double gpu = 1e3 * (t.upsweep + t.fjbuild + t.prep + t.fkern) + upload + download;
+        const double v[11] = {double(s.ngas), double(s.nLeaves), 1e3 * t.upsweep, 1e3 * t.fjbuild, upload,
+                              1e3 * t.prep, 1e3 * t.fkern, download, gpu, wall, wall - gpu};
+        print_line(format_force_stats, v);
     }
 }
 
@@ -603,6 +667,20 @@ void cosmo_x_sync(void)
 {
     State& s = state();
     if (s.st) COSMO_CUDA(cudaStreamSynchronize(s.st));
+}
+
+// Format one of the stderr statistics lines from given values (0 COSMO_STATS, 1
+// COSMO_FORCE, 2 COSMO_MEM), exactly as the entry points print it; no device work.
+int cosmo_x_stats_line(int which, const double* values, char* buf, int len)
+{
+    if (!values || !buf || len <= 0) return -1;
+    switch (which)
+    {
+    case 0: return format_dens_stats(buf, size_t(len), values);
+    case 1: return format_force_stats(buf, size_t(len), values);
+    case 2: return format_mem_line(buf, size_t(len), values);
+    default: return -1;
+    }
 }
 
 double cosmo_x_scalar(const char* name)

@@ -87,9 +87,25 @@ extern "C" int cosmo_hilbert_order_noalloc(int n, const double* d_x, const doubl
                      n, kNoallocMaxN, kNoallocScratchBytes);
         return -1;
     }
+    if (periodic && box6 == nullptr)
+    {
+        std::fprintf(stderr, "cosmo_hilbert_order_noalloc: periodic=%d needs box6 (xmin,xmax,ymin,ymax,zmin,zmax)\n",
+                     periodic);
+        return -1;
+    }
+    // An error left pending by the caller's own earlier CUDA calls is not this call's to
+    // report or to clear: refuse before launching, and leave it in place.
+    if (const cudaError_t pending = cudaPeekAtLastError(); pending != cudaSuccess)
+    {
+        std::fprintf(stderr, "cosmo_hilbert_order_noalloc: a CUDA error is pending from before this call (%s)\n",
+                     cudaGetErrorString(pending));
+        return -2;
+    }
     void* scratch = nullptr;
     int sms = 0;
     if (const int e = scratch_for_current_device(&scratch, &sms)) return e;
+    // The calling thread's default stream: it does not wait for, or hold up, work on the
+    // caller's other streams (the legacy default stream would serialise with them).
     return keysort_raw(n, d_x, d_y, d_z, d_h, periodic ? box6 : nullptr, reinterpret_cast<uint64_t*>(d_keys),
-                       d_order, scratch, sms, /*stream=*/0);
+                       d_order, scratch, sms, cudaStreamPerThread);
 }

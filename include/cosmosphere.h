@@ -180,9 +180,12 @@ int cosmo_serve_stop(void);
  * results equal the keys and ordering a density solve of the same particles builds.
  * Scratch is a fixed 7.06 MiB array inside the library, held by every GPU that loads it
  * until exit; n must be in [1, 524288], else it returns -1 (with a message on stderr)
- * and does nothing.  The first call on a device looks up that array's address; make
- * that first call before any stream capture.  Runs on the legacy default stream and
- * returns when done: 0 ok, -1 size rejected, -2 CUDA error, -3 device wait gave up.
+ * and does nothing; so does periodic != 0 with box6 == NULL.  The first call on a device
+ * looks up that array's address; make that first call before any stream capture.  Runs
+ * on the calling thread's default stream (cudaStreamPerThread, which neither waits for
+ * nor holds up the caller's other streams) and returns when done: 0 ok, -1 input
+ * rejected, -2 CUDA error (also when an error from the caller's earlier CUDA calls is
+ * pending on entry; that error is left in place), -3 device wait gave up.
  * Every call uses the same array: calls that overlap on the GPU (from several threads
  * or streams) race and corrupt each other's results. */
 int cosmo_hilbert_order_noalloc(int n, const double* d_x, const double* d_y, const double* d_z,
@@ -201,6 +204,11 @@ int cosmo_x_density(int n, double pmass, int periodic, const double* box, double
 
 /* Wait for the library's stream. */
 void cosmo_x_sync(void);
+
+/* Format a statistics line (0 COSMO_STATS, 1 COSMO_FORCE, 2 COSMO_MEM) from its values,
+ * in the field order the entry points print it; returns the snprintf length or -1.  No
+ * device work. */
+int cosmo_x_stats_line(int which, const double* values, char* buf, int len);
 
 /* Make device dev current for the library (before its first call on this thread). */
 void cosmo_x_set_device(int dev);

@@ -1,6 +1,7 @@
 """Regenerate the golden fixtures in this directory from the reference's own code.
 
-Run in a container that has the reference checkout (default /root/reference):
+Run in a container that has the reference checkout, given as the argument or by the
+environment variable COSMO_REFERENCE_DIR:
     python tests/golden/make_golden.py [REF]
 It compiles, where they lie, the reference's include/kernel.hpp (both kernels) and its
 standalone driver src/main.cu (against a recording stub of the C-ABI), through
@@ -25,7 +26,10 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 ORACLE = os.path.join(REPO, "oracle")
 
 
-def main(ref="/root/reference"):
+def main(ref=None):
+    ref = ref or os.environ.get("COSMO_REFERENCE_DIR")
+    if not ref:
+        sys.exit("give the reference checkout as the argument or in COSMO_REFERENCE_DIR")
     subprocess.run(["make", "-s", "-C", ORACLE, "ref", f"REF={ref}"], check=True)
     q = np.linspace(0.0, 3.2, 2049)
     out = {"q": q}

@@ -59,3 +59,38 @@ def test_fatal_before_any_device_work(call, msg):
     r = _child("import numpy as np\nfrom cosmosphere_b200 import capi\nc = capi.Cosmo()\n" + call)
     assert r.returncode != 0
     assert msg in r.stderr
+
+
+# Field keys of the reference's stderr lines, in print order: COSMO_STATS
+# (src/dens_c_api.cu:113-122), COSMO_FORCE (src/force_c_api.cu:74-79) and COSMO_MEM
+# (src/dens_c_api.cu:95-97).
+REF_KEYS = {
+    0: ["n", "leaves", "iters", "vecin", "upload", "bbox", "keysort", "tree", "nodes", "jbuild", "nrkern",
+        "gjbuild", "gradkern", "download", "gpusum", "solve", "unaccounted", "total"],
+    1: ["n", "leaves", "upsweep", "jbuild", "upload", "prep", "kernel", "download", "gpusum", "wall",
+        "unaccounted"],
+    2: ["n", "device_used", "host_peak"],
+}
+REF_HEAD = {0: "COSMO_STATS", 1: "COSMO_FORCE", 2: "COSMO_MEM"}
+
+
+@pytest.mark.parametrize("which", [0, 1, 2])
+def test_stats_lines_have_the_reference_fields(which):
+    """Each statistics line carries the reference's keys in the reference's order, with
+    two decimals for times, integers for counts, and the '|' group separators."""
+    c = capi.Cosmo()
+    nvals = {0: 18, 1: 11, 2: 5}[which]
+    vals = [1403000.0, 40000.0, 6.0] + [1.234 + k for k in range(nvals - 3)]
+    line = c.stats_line(which, vals)
+    assert line.startswith(REF_HEAD[which] + " ") and line.endswith("\n")
+    keys = re.findall(r"(\w+)=", line)
+    assert keys == REF_KEYS[which]
+    assert "n=1403000 " in line
+    if which == 0:
+        assert line.count(" | ") == 2 and "leaves=40000 iters=6 | vecin=1.23 upload=2.23" in line
+        assert line.rstrip().endswith("total=15.23")
+    elif which == 1:
+        assert line.count(" | ") == 2 and "leaves=40000 | upsweep=6.00 jbuild=1.23 upload=2.23" in line
+    else:
+        assert re.fullmatch(r"COSMO_MEM n=\d+ device_used=\d+\.\d\d GB of \d+\.\d\d GB \(\d+ bytes/particle\) "
+                            r"host_peak=\d+\.\d\d GB\n", line)
