@@ -10,8 +10,14 @@
  * particle's owner lane adds its own records in order.  All lanes work in every phase
  * whatever the group's size or spatial spread.
  *
- *   plain  the exact FP64 test q^2 = r^2 / h_i^2 < R^2 (src/density_base.cu:270-283) and
- *          FP64 sums in ascending j: bit for bit the oracle's.
+ *   plain  a conservative FP32 prefilter decides which (particle, candidate) pairs are
+ *          recorded: coordinates relative to the group box centre, two group particles
+ *          per packed f32x2 instruction, against fp32_bound2(R h_i, eps), where eps
+ *          bounds the FP32 distance error (fp32_margin) -- it can pass a pair the exact
+ *          test rejects, never the reverse.  The records are then evaluated one pair per
+ *          lane with the exact FP64 test q^2 = r^2 / h_i^2 < R^2 (src/density_base.cu:
+ *          270-283) on the FP64 positions, and the owner adds the exact-accepted ones in
+ *          ascending j: the accepted pairs and their order are the oracle's, bit for bit.
  * The periodic form with zero periods behaves, bit for bit, as the open form (the batched
  * kernel runs open and periodic sets through the one periodic instance).
  *
@@ -34,7 +40,7 @@ template<bool Mixed>
 struct DensScratch
 {
     static constexpr int kBytes = Mixed ? (kRing * 16 + 4 * 32 * 4 + 2 * kRec * 4)
-                                        : (kRing * 32 + 32 * 32 + 2 * kRec * 8);
+                                        : (kRing * 32 + 32 * 32 + 4 * 32 * 4 + 2 * kRec * 8 + kRec * 4);
 };
 
 // q = sqrt(q2) in FP32 (q2 >= 0); exact 0 for the self pair.
@@ -61,17 +67,40 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
     {
         double4* ring = reinterpret_cast<double4*>(scr);
         double4* grp = ring + kRing;
-        double* recA = reinterpret_cast<double*>(grp + 32);
+        float* gfx = reinterpret_cast<float*>(grp + 32);   // FP32 offsets from the box centre
+        float* gfy = gfx + 32;
+        float* gfz = gfy + 32;
+        float* gfT = gfz + 32;                              // prefilter bound on r^2
+        double* recA = reinterpret_cast<double*>(gfT + 32);
         double* recB = recA + kRec;
-        if (mine) grp[lane] = make_double4(pi.x, pi.y, pi.z, hinv2);
+        int* recI = reinterpret_cast<int*>(recB + kRec);    // (group particle << 8) | ring slot
+        const double period = Periodic ? fmax(lx, fmax(ly, lz)) : 0.0;
+        const double eps = fp32_margin(bx, period);
+        if (mine)
+        {
+            grp[lane] = make_double4(pi.x, pi.y, pi.z, hinv2);
+            gfx[lane] = float(pi.x - bx.cx);
+            gfy[lane] = float(pi.y - bx.cy);
+            gfz[lane] = float(pi.z - bx.cz);
+            gfT[lane] = fp32_bound2(rs, eps);
+        }
+        else
+        {
+            gfx[lane] = 0.0f;
+            gfy[lane] = 0.0f;
+            gfz[lane] = 0.0f;
+            gfT[lane] = -1.0f;
+        }
         __syncwarp();
+        const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
         double sr = 0.0, sg = 0.0;
         src.template stream<true, false, false, Periodic>(
             ring, nullptr, nullptr, bx, 0.0, 0.0, 0.0, lx, ly, lz,
             [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
             [&](const double4* rg, const float4*, const int*, int head, int count) {
                 gc += count;
-                const double4 pj = rg[(head + (lane < count ? lane : 0)) & (kRing - 1)];
+                const int mySlot = (head + (lane < count ? lane : 0)) & (kRing - 1);
+                const double4 pj = rg[mySlot];
                 if (ng == 1)
                 {
                     // a single particle (a cut group): every lane evaluates its own pair and
@@ -102,49 +131,89 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                     }
                     return;
                 }
+                // the candidate's FP32 offset from the box centre, at its nearest image
+                const float px = float(image_offset(pj.x, bx.cx, lx)), py = float(image_offset(pj.y, bx.cy, ly));
+                const float pz = float(image_offset(pj.z, bx.cz, lz));
                 int nrec = 0, segStart = 0, segCount = 0;
                 auto flush = [&]() {
                     __syncwarp();
+                    // the exact FP64 test and the pair terms, one record per lane
                     for (int r = lane; r < nrec; r += 32)
                     {
-                        const double q2 = recA[r];
-                        const double q = sqrt(q2);
-                        double wk, dwk;
-                        sph_kernel(q2, q, wk, dwk);
-                        recA[r] = wk;
-                        recB[r] = -q * dwk - 3.0 * wk;
+                        const int code = recI[r];
+                        const double4 g = grp[code >> 8];
+                        const double4 q = ring[code & 0xff];
+                        double dx = g.x - q.x, dy = g.y - q.y, dz = g.z - q.z;
+                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                        const double q2 = pair_r2(dx, dy, dz) * g.w;
+                        double wv = -1.0, tv = 0.0;   // W >= 0 for an accepted pair
+                        if (q2 < kRadK2)
+                        {
+                            const double qq = sqrt(q2);
+                            double wk, dwk;
+                            sph_kernel(q2, qq, wk, dwk);
+                            wv = wk;
+                            tv = -qq * dwk - 3.0 * wk;
+                        }
+                        recA[r] = wv;
+                        recB[r] = tv;
                     }
                     __syncwarp();
                     for (int t = 0; t < segCount; ++t)
                     {
-                        sr += recA[segStart + t];
-                        sg += recB[segStart + t];
+                        const double a = recA[segStart + t];
+                        if (a >= 0.0)
+                        {
+                            sr += a;
+                            sg += recB[segStart + t];
+                            ++gp;
+                        }
                     }
-                    gp += segCount;
                     segCount = 0;
                     nrec = 0;
                     __syncwarp();
                 };
-                // four group particles per step: independent FP64 chains for the scheduler
+                const float2 nx = make_float2(-px, -px), ny = make_float2(-py, -py), nz = make_float2(-pz, -pz);
+                // four group particles per step, two per packed FP32 instruction
                 for (int i0 = 0; i0 < ng; i0 += 4)
                 {
                     if (nrec + 4 * 32 > kRec) flush();
-                    double q2u[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
+                    float r2u[4];
+                    if (!Periodic || Lx == 0.0f)   // zero periods (an open set) fold nothing
                     {
-                        const double4 g = grp[min(i0 + u, 31)];
-                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
-                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                        q2u[u] = pair_r2(dx, dy, dz) * g.w;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                        {
+                            const int k = i0 + 2 * h;
+                            const float2 dx = __fadd2_rn(*reinterpret_cast<const float2*>(gfx + k), nx);
+                            const float2 dy = __fadd2_rn(*reinterpret_cast<const float2*>(gfy + k), ny);
+                            const float2 dz = __fadd2_rn(*reinterpret_cast<const float2*>(gfz + k), nz);
+                            float2 r2 = __fmul2_rn(dx, dx);
+                            r2 = __ffma2_rn(dy, dy, r2);
+                            r2 = __ffma2_rn(dz, dz, r2);
+                            r2u[2 * h] = r2.x;
+                            r2u[2 * h + 1] = r2.y;
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                        {
+                            const int k = i0 + u;
+                            const float dx = axis_df<true>(gfx[k], px, Lx);
+                            const float dy = axis_df<true>(gfy[k], py, Ly);
+                            const float dz = axis_df<true>(gfz[k], pz, Lz);
+                            r2u[u] = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        }
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
                     {
-                        const bool acc = lane < count && i0 + u < ng && q2u[u] < kRadK2;
+                        const bool acc = lane < count && i0 + u < ng && r2u[u] < gfT[i0 + u];
                         const uint32_t m = __ballot_sync(0xffffffffu, acc);
                         const int c = __popc(m);
-                        if (acc) recA[nrec + __popc(m & lt)] = q2u[u];
+                        if (acc) recI[nrec + __popc(m & lt)] = ((i0 + u) << 8) | mySlot;
                         if (lane == i0 + u) { segStart = nrec; segCount = c; }
                         nrec += c;
                     }

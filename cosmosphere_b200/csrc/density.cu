@@ -196,18 +196,15 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
         const double rmax = warp_max(mine ? rs : 0.0);
         const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
         int rowLen = 0;
-        rows_group<1>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), bx, jOffset[d.leaf],
-                   jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
+        rows_group<1, Periodic>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), rs, bx, lx, ly, lz,
+                   jOffset[d.leaf], jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
-                   [&](const double4& g, const double4& pj) {
+                   [](const double4&) { return 0.0; },
+                   [&](const double4& g, const double4& pj, int) {   // r^2 within the wide support
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                       return pair_r2(dx, dy, dz) * g.w < wide2;
-                   },
-                   [&](const double4& pj, int) {   // the owner's own r^2 with j, as the test formed it
-                       double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                       return R2(pair_r2(dx, dy, dz));
+                       const double r2 = pair_r2(dx, dy, dz);
+                       return RowEntry<R2>{r2 * g.w < wide2, R2(r2)};
                    },
                    mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen);
         if (mine)

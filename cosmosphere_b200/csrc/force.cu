@@ -275,16 +275,19 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
         // bound formed once: rounding is monotone, so the bound of the larger h is the
         // larger bound and max(bound_i, bound_j) is the same double as the test's own
         auto bound = [](double h) { return kRadK2 * (h * h) * (1.0 + 1e-10); };
-        rows_group<kRowStride>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, bound(pi.w)), bx,
-                   jOffset[d.leaf], jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
+        // prefilter distances: R h (1 + 1e-10) bounds sqrt(bound(h)) for either side
+        rows_group<kRowStride, Periodic>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, bound(pi.w)),
+                   kRadKernel * pi.w * (1.0 + 1e-10), bx, lx, ly, lz, jOffset[d.leaf], jcount[d.leaf], jlist,
+                   LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
-                   [&](const double4& g, const double4& pj) {
+                   [](const double4& pj) { return kRadKernel * pj.w * (1.0 + 1e-10); },
+                   [&](const double4& g, const double4& pj, int j) {
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        const double dr2 = pair_r2(dx, dy, dz);
-                       return !(dr2 >= fmax(g.w, bound(pj.w)));
+                       return RowEntry<int>{!(dr2 >= fmax(g.w, bound(pj.w))), j};
                    },
-                   [](const double4&, int j) { return j; }, mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
+                   mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
         if (mine) nblCount[i] = rowLen;
         if (mine && rowLen > kNbl) ds->rowOverflow = 1;
     }

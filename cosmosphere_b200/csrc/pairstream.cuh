@@ -415,6 +415,19 @@ __device__ __forceinline__ double fp32_margin(const GroupBox& b, double period)
     return 16.0 * A * 5.9604644775390625e-8;
 }
 
+// Bound on the FP32 squared distance r2_f of a pair whose exact distance is below B, for
+// a group whose float offsets carry the absolute error eps of fp32_margin.  Per axis the
+// float separation of offsets a (|a| <= A) and b errs by at most 2^-24 (|a| + |b| + |d|)
+// <= 2^-23 (A + |d|) (open: |b| <= |a| + |d|; periodic: the fold's terms are absolute and
+// inside eps), so over three axes r_f <= r (1 + 2^-23) + eps and r2_f <= r_f^2 (1 + 3 2^-24):
+// r < B implies r2_f < (B (1 + 1e-6) + eps)^2 (1 + 1e-6).  A candidate far outside the
+// group box (a scatter neighbour of large h) is covered by the relative term.
+__device__ __forceinline__ float fp32_bound2(double B, double eps)
+{
+    const double t = B * (1.0 + 1e-6) + eps;
+    return float(t * t * (1.0 + 1e-6));
+}
+
 // Per-axis float distance, at the nearest periodic image when periodic.
 template<bool Periodic>
 __device__ __forceinline__ float axis_df(float a, float b, float L)

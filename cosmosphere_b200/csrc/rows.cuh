@@ -4,10 +4,11 @@
  *
  * The group pass streams a leaf's list through the group filter into the warp's ring and
  * tests each batch with j on the lanes (for each group particle in turn, every lane tests
- * its candidate); the ballot of a group particle's tests is its lane's mask over the
- * batch, and the owner lane appends the masked j, lowest lane first -- ascending j.  A pass
- * that then walks a row applies the same exact test to the same candidates in the same
- * order as a walk of the whole list would, so its sums are the same bit for bit.
+ * its candidate with a conservative FP32 prefilter); the ballot of a group particle's
+ * tests is its lane's mask over the batch, and the owner lane applies the exact FP64 test
+ * to the masked j, lowest lane first, and appends the accepted ones -- ascending j.  A
+ * pass that then walks a row applies the same exact test to the same candidates in the
+ * same order as a walk of the whole list would, so its sums are the same bit for bit.
  *
  * An entry is j (the symmetric rows of the gradient and force passes), or r^2 of the pair
  * (the Newton rows: positions do not move during a density solve, so the later Newton
@@ -40,52 +41,112 @@ __device__ __forceinline__ T* row_of(T* nbl, uint32_t i)
     return nbl + (size_t(i >> 5) * kNbl << 5) + (i & 31u);
 }
 
-// Per-warp shared scratch of rows_group: the double ring, its indices, the group's data.
-constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32;
+// An exact test's verdict on a pair and the entry an accepted pair writes.
+template<class T>
+struct RowEntry
+{
+    bool ok;
+    T v;
+};
 
-// Rows of one group.  Lanes [0, ng) own the group's particles, whose per-particle test data
-// gi (a double4: position and one test value) the caller passes; test(gi, pj) is the exact
-// acceptance of the pair, and value(pj, j) the entry the owner writes for an accepted j (j
-// itself, or a pair quantity it recomputes from pj).  row is the lane's own row (row_of
-// with Stride kRowStride, or row_flat with Stride 1; nullptr if not mine); rowLen receives
-// its length (kNbl + 1 when it overflowed).
-template<int Stride, class T, class Ranges, class Filter, class Test, class Value>
-__device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng, const double4& gi, const GroupBox& bx,
-                                           uint32_t jb, uint32_t nj, const int* __restrict__ jlist, Ranges ranges,
-                                           const double4* __restrict__ xyzh, Filter filter, Test test, Value value,
+// Per-warp shared scratch of rows_group: the double ring, its indices, the group's data
+// and its FP32 offsets and prefilter bounds.
+constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32 + 4 * 32 * 4;
+
+// Rows of one group.  Lanes [0, ng) own the group's particles, whose per-particle data gi
+// (a double4: position and one test value) the caller passes.  A conservative FP32
+// prefilter picks the candidates each particle must test: the pair's float distance
+// against fp32_bound2 of max(Bi, candB(pj)), where Bi (the particle's) and candB (the
+// candidate's, 0 for a gather row) bound the exact test's distance.  exact(gi, pj, j)
+// then applies the exact acceptance of the pair on the FP64 positions and returns it with
+// the entry the owner writes for an accepted j (j itself, or r^2).  row is the lane's own row
+// (row_of with Stride kRowStride, or row_flat with Stride 1; nullptr if not mine); rowLen
+// receives its length (kNbl + 1 when it overflowed).  Entries come in ascending j.
+template<int Stride, bool Periodic, class T, class Ranges, class Filter, class CandB, class Exact>
+__device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng, const double4& gi, double Bi,
+                                           const GroupBox& bx, double lx, double ly, double lz, uint32_t jb,
+                                           uint32_t nj, const int* __restrict__ jlist, Ranges ranges,
+                                           const double4* __restrict__ xyzh, Filter filter, CandB candB, Exact exact,
                                            T* row, int& rowLen)
 {
     const int lane = threadIdx.x & 31;
     double4* ring = reinterpret_cast<double4*>(scr);
     int* ringIdx = reinterpret_cast<int*>(ring + kRing);
     double4* grp = reinterpret_cast<double4*>(ringIdx + kRing);
+    float* gfx = reinterpret_cast<float*>(grp + 32);
+    float* gfy = gfx + 32;
+    float* gfz = gfy + 32;
+    float* gfT = gfz + 32;
+    const double eps = fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0);
     if (mine) grp[lane] = gi;
+    gfx[lane] = mine ? float(gi.x - bx.cx) : 0.0f;
+    gfy[lane] = mine ? float(gi.y - bx.cy) : 0.0f;
+    gfz[lane] = mine ? float(gi.z - bx.cz) : 0.0f;
+    gfT[lane] = mine ? fp32_bound2(Bi, eps) : -1.0f;
     __syncwarp();
+    const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
     int len = 0;
     stream_ranges<true, false, true>(
         ring, nullptr, ringIdx, bx.cx, bx.cy, bx.cz, 0.0, 0.0, 0.0, jb, nj, jlist, ranges, xyzh, filter,
         [&](const double4* rg, const float4*, const int* ri, int head, int count) {
             const double4 pj = rg[(head + (lane < count ? lane : 0)) & (kRing - 1)];
+            const float px = float(image_offset(pj.x, bx.cx, lx)), py = float(image_offset(pj.y, bx.cy, ly));
+            const float pz = float(image_offset(pj.z, bx.cz, lz));
+            const double bj = candB(pj);
+            const float tj = bj > 0.0 ? fp32_bound2(bj, eps) : 0.0f;
+            const float2 nx = make_float2(-px, -px), ny = make_float2(-py, -py), nz = make_float2(-pz, -pz);
             uint32_t myMask = 0;
             for (int i0 = 0; i0 < ng; i0 += 4)
             {
-                bool a[4];
+                float r2u[4];
+                if (!Periodic || Lx == 0.0f)
+                {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) a[u] = lane < count && i0 + u < ng && test(grp[min(i0 + u, 31)], pj);
+                    for (int h = 0; h < 2; ++h)
+                    {
+                        const int k = i0 + 2 * h;
+                        const float2 dx = __fadd2_rn(*reinterpret_cast<const float2*>(gfx + k), nx);
+                        const float2 dy = __fadd2_rn(*reinterpret_cast<const float2*>(gfy + k), ny);
+                        const float2 dz = __fadd2_rn(*reinterpret_cast<const float2*>(gfz + k), nz);
+                        float2 r2 = __fmul2_rn(dx, dx);
+                        r2 = __ffma2_rn(dy, dy, r2);
+                        r2 = __ffma2_rn(dz, dz, r2);
+                        r2u[2 * h] = r2.x;
+                        r2u[2 * h + 1] = r2.y;
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                    {
+                        const int k = i0 + u;
+                        const float dx = axis_df<true>(gfx[k], px, Lx);
+                        const float dy = axis_df<true>(gfy[k], py, Ly);
+                        const float dz = axis_df<true>(gfz[k], pz, Lz);
+                        r2u[u] = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                    }
+                }
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
                 {
-                    const uint32_t m = __ballot_sync(0xffffffffu, a[u]);
+                    const bool a = lane < count && i0 + u < ng && r2u[u] < fmaxf(gfT[i0 + u], tj);
+                    const uint32_t m = __ballot_sync(0xffffffffu, a);
                     if (lane == i0 + u) myMask = m;
                 }
             }
+            // the owner tests its prefiltered candidates exactly, lowest lane (j) first
             while (myMask)
             {
                 const int b = __ffs(myMask) - 1;
                 myMask &= myMask - 1;
                 const int sl = (head + b) & (kRing - 1);
-                if (len < kNbl) row[size_t(len) * Stride] = value(rg[sl], ri[sl]);
-                ++len;
+                const RowEntry<T> e = exact(gi, rg[sl], ri[sl]);
+                if (e.ok)
+                {
+                    if (len < kNbl) row[size_t(len) * Stride] = e.v;
+                    ++len;
+                }
             }
         });
     rowLen = len > kNbl ? kNbl + 1 : len;

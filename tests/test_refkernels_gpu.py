@@ -6,11 +6,13 @@ for sm_100a from the reference's sources (oracle/refkernels.py), run through the
 reference's solve sequence on this library's Hilbert order, leaf layout and leaf cubes.
 This library's h, rho, d(rho)/dh, div v, xi, d(div v)/dt and the six force outputs must
 agree with theirs within 1e-10 relative (the specification's bound for the FP64 form):
-per particle, relative to the larger of |reference value| and 1e-6 of the field's largest
-magnitude (fields such as the lattice forces are sums of cancelling terms, whose
-near-zero results carry an absolute rounding error of the size of the terms).  xi takes
-its nine inputs rounded to float by design (src/density_base.cu:504-510), so a last-bit
-difference before that rounding may move xi by float rounding: its bound is 1e-6.
+per particle, |ours - reference| <= 1e-10 (|reference| + rms of the field).  The rms
+term matters only where a field is a sum of cancelling terms whose result is far below
+the terms themselves -- the pressure forces inside a lattice, div v of random velocities
+-- and whose absolute rounding error is therefore of the size of the terms, not of the
+result.  xi takes its nine inputs rounded to float by design (src/density_base.cu:
+504-510), so a last-bit difference before that rounding may move xi by float rounding:
+its bound is 1e-6.
 The Newton iteration counts and the active count of every iteration must be equal.
 
 The reference's kernels are built with nvcc's default contraction into fused
@@ -27,7 +29,6 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-10
 TOL_XI = 1e-6
-FLOOR = 1e-6
 FIELDS = ["h", "rho", "gradh", "divv", "xi", "ddivvdt"]
 FORCE = ["fx", "fy", "fz", "f4", "vsigmax", "divvF"]
 
@@ -56,9 +57,19 @@ def _thermo(p, hfact):
 
 
 def rel_dev(got, ref):
-    scale = np.maximum(np.abs(ref), FLOOR * np.max(np.abs(ref)))
-    scale = np.where(scale > 0, scale, 1.0)
-    return float(np.max(np.abs(got - ref) / scale)) if ref.size else 0.0
+    """max |got - ref| / (|ref| + rms(ref)) over the particles (0 for an all-zero field
+    matched exactly)."""
+    if ref.size == 0:
+        return 0.0
+    scale = np.abs(ref) + np.sqrt(np.mean(ref * ref))
+    d = np.abs(got - ref)
+    return float(np.max(np.where(scale > 0, d / np.where(scale > 0, scale, 1.0), np.where(d > 0, np.inf, 0.0))))
+
+
+def pointwise_dev(got, ref):
+    """max |got - ref| / |ref| over the particles whose |ref| is at least the field's rms."""
+    big = np.abs(ref) >= np.sqrt(np.mean(ref * ref))
+    return float(np.max(np.abs(got[big] - ref[big]) / np.abs(ref[big]))) if big.any() else 0.0
 
 
 def against_reference(p, *, quintic=False, box=None, disc=0, pdv=1, shock=1, beta=2.0, alphau=0.1):
@@ -94,7 +105,8 @@ def against_reference(p, *, quintic=False, box=None, disc=0, pdv=1, shock=1, bet
         got = c.array(k)
         dev[k] = rel_dev(got, ref[k])
         exact = float(np.mean(got == ref[k]))
-        print(f"  {k:8s} max rel dev {dev[k]:.3e}  bit-equal {100 * exact:.1f}%")
+        print(f"  {k:8s} dev {dev[k]:.3e}  pointwise (|ref| >= rms) {pointwise_dev(got, ref[k]):.3e}  "
+              f"bit-equal {100 * exact:.1f}%")
     bad = {k: d for k, d in dev.items() if d > (TOL_XI if k == "xi" else TOL)}
     assert not bad, bad
     return dev
