@@ -530,11 +530,14 @@ def run_reference(args, rank, world, local, dist):
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"lattice {sample_npx} + 1% jiggle, density+force (sample of lattice 100)",
-                       "particles": p.n, "parallelism": "host threads"},
+            "config": {"workload": lattice_label(sample_npx), "particles": p.n, "parallelism": "host threads"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"lattice-{sample_npx} instance of the lattice-100 generator ({p.n} particles), "
-                                       "one density+force step per step"},
+                             "same_config": sample_npx == args.npartx,
+                             "sample": (f"the workload itself ({p.n} particles), one density+force step of the "
+                                        "CPU oracle (FP64, OpenMP, all host threads) per step")
+                                       if sample_npx == args.npartx else
+                                       f"lattice-{sample_npx} instance of the lattice-100 generator ({p.n} "
+                                       "particles), one density+force step per step"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -546,7 +549,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--npartx", type=int, default=100)
-    ap.add_argument("--ref-npartx", type=int, default=50)
+    ap.add_argument("--ref-npartx", type=int, default=100,
+                    help="lattice size of the CPU arm's workload (default: the timed workload itself)")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="lattice100: leave out the batched-ensemble and served-stream legs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: plain FP64 (the headline value) and mixed in one run")
@@ -595,8 +601,12 @@ def main():
                             "|v| = 0.5 v_circ, u = 0.05, quintic, hfact 1.0, density(NR+gradients)+force, open")
         return
     run_particles(args, rank, world, local, dist, workload(args.npartx), quintic=False, metric=METRIC,
-                  label=f"lattice {args.npartx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, cubic, "
-                        "open boundaries")
+                  label=lattice_label(args.npartx))
+
+
+def lattice_label(npx):
+    return (f"lattice {npx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, cubic, "
+            "open boundaries")
 
 
 def run_file(args, rank, world, local, dist):
@@ -766,6 +776,64 @@ def measure(args, c, p, mixed, hfact, dist, local, profile=False):
     return res
 
 
+def newton_cap_report(c, p, hfact):
+    """The same density solve with the Newton cap at 10 iterations (the iteration cap the
+    specification names; the library's default is the reference's built 100): whether it
+    converges within 10, and how many particles are left unconverged if not."""
+    from cosmosphere_b200 import capi
+    n = p.n
+    c.set_precision(False)
+    c.arrays_init(n)
+    c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+    c.upload(capi.HSML, p["h"])
+    st10 = c.density_status(n, p["pmass"], tolh=1e-4, hfact=hfact, max_iter=10, with_gradients=False)
+    unconv10 = int(c.scalar("unconverged")) if st10 == 1 else 0
+    act10 = [int(a) for a in c.array("activePerIter")]
+    c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+    c.upload(capi.HSML, p["h"])
+    st100 = c.density_status(n, p["pmass"], tolh=1e-4, hfact=hfact, max_iter=100, with_gradients=False)
+    return {"cap": 10, "status": "converged" if st10 == 0 else ("unconverged" if st10 == 1 else f"status {st10}"),
+            "unconverged_particles": unconv10, "active_per_iteration": act10,
+            "iterations_to_converge_with_cap_100": int(c.scalar("itersRun")) if st100 == 0 else None}
+
+
+def run_form_legs(args):
+    """The batched-ensemble and served-stream forms, each run as its own bench.py process
+    on this GPU after the lattice-100 timing; their headline figures are carried on this
+    line (their full lines come from --workload ensemble / served)."""
+    out = {}
+    legs = {"batched_ensemble": ["--workload", "ensemble", "--steps", "3", "--warmup", "1"],
+            "served_stream": ["--workload", "served"]}
+    for name, extra in legs.items():
+        t0 = time.perf_counter()
+        r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--gpus", "1", *extra],
+                           capture_output=True, text=True, timeout=900)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not lines:
+            out[name] = {"error": (r.stderr or r.stdout).strip().splitlines()[-1:] or ["no output"]}
+            continue
+        d = json.loads(lines[-1])
+        d["wall_s"] = time.perf_counter() - t0
+        if name == "batched_ensemble":
+            out[name] = {"metric": d["metric"], "value": d["value"], "unit": d["unit"], "config": d["config"],
+                         "speedup_mixed_batched_vs_sequential_fp64": d["speedup_mixed_batched_vs_sequential_fp64"],
+                         "speedup_mixed_vs_fp64_batched": d["speedup_mixed_vs_fp64_batched"],
+                         "batched_mixed_ms_per_solve": d["batched_mixed"]["ms_per_solve"],
+                         "batched_fp64_ms_per_solve": d["batched_fp64"]["ms_per_solve"],
+                         "sequential_fp64_ms_total": d["sequential_fp64"]["ms_total"],
+                         "accuracy_mixed_vs_fp64": d["accuracy_mixed_vs_fp64"], "steps": d["steps"],
+                         "wall_s": d["wall_s"]}
+        else:
+            sm, fl = d["served_mixed"], d["fp64_loop"]
+            out[name] = {"metric": d["metric"], "value": d["value"], "unit": d["unit"], "config": d["config"],
+                         "p50_ms": sm["stream"]["p50_ms"], "p99_ms": sm["stream"]["p99_ms"],
+                         "fp64_loop_p50_ms": fl["stream"]["p50_ms"], "fp64_loop_p99_ms": fl["stream"]["p99_ms"],
+                         "speedup_saturated_vs_fp64_loop": d["speedup_saturated_vs_fp64_loop"],
+                         "accuracy_mixed_vs_fp64": d["accuracy_mixed_vs_fp64"], "requests": d["steps"],
+                         "wall_s": d["wall_s"]}
+    return out
+
+
 def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
     """One set of particles: the plain FP64 form (the headline value) and the mixed form,
     with the mixed form's error against FP64 on the same inputs."""
@@ -805,11 +873,21 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
              "+ plan_items_kernel, timed together by CUDA events")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not quintic:
-        cp = workload(args.ref_npartx)
+        same = args.ref_npartx == args.npartx and args.workload == "lattice100"
+        cp = p if same else workload(args.ref_npartx)
         u, dt, cores = cpu_oracle_step(cp)
         cpu = {"value": u / dt, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"lattice-{args.ref_npartx} instance of the same generator ({cp.n} particles), "
-                         "one density+force step of the CPU oracle (FP64, OpenMP)"}
+               "same_config": same,
+               "sample": (f"the timed workload itself ({cp.n} particles), one density+force step of the CPU "
+                          "oracle (FP64, OpenMP, all host threads)") if same else
+                         (f"lattice-{args.ref_npartx} instance of the same generator ({cp.n} particles), "
+                          "one density+force step of the CPU oracle (FP64, OpenMP)")}
+    forms = None
+    if rank == 0 and world == 1 and args.workload == "lattice100" and not args.no_forms and not quintic:
+        forms = run_form_legs(args)
+    cap10 = None
+    if args.workload == "plummer":
+        cap10 = newton_cap_report(c, p, hfact)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -847,6 +925,8 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
                                              "speedup_vs_plain": (mixed["value"] / plain["value"]) if plain else None,
                                              "accuracy_vs_fp64": accuracy},
         "cpu_baseline": cpu,
+        "forms": forms,
+        "newton_cap_10": cap10,
         "clocks": clk,
         "gpu_launches": head["launches"],
     }

@@ -21,7 +21,7 @@ EXPORTS = [
     "cosmo_arrays_init", "cosmo_slot_ncomp", "cosmo_upload", "cosmo_upload_sorted", "cosmo_download",
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
-    "cosmo_x_stats_line",
+    "cosmo_x_stats_line", "cosmo_x_set_wait_limit", "cosmo_x_get_wait_limit", "cosmo_x_wait_test",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
     "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_set_tuning",
@@ -56,6 +56,10 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_scalar.argtypes = [ctypes.c_char_p]
     L.cosmo_x_stats_line.argtypes = [I, P, ctypes.c_char_p, I]
     L.cosmo_x_stats_line.restype = I
+    L.cosmo_x_set_wait_limit.argtypes = [ctypes.c_longlong]
+    L.cosmo_x_get_wait_limit.restype = ctypes.c_longlong
+    L.cosmo_x_wait_test.argtypes = [I, I]
+    L.cosmo_x_wait_test.restype = I
     L.cosmo_x_scalar.restype = D
     L.cosmo_x_array.argtypes = [ctypes.c_char_p, P, ctypes.POINTER(I)]
     L.cosmo_x_array.restype = ctypes.c_long
@@ -169,6 +173,15 @@ class Cosmo:
         if n < 0:
             raise ValueError(which)
         return buf.value.decode()
+
+    def set_wait_limit(self, ns: int):
+        self.L.cosmo_x_set_wait_limit(int(ns))
+
+    def wait_limit(self) -> int:
+        return int(self.L.cosmo_x_get_wait_limit())
+
+    def wait_test(self, kind: int, fatal: bool = False) -> int:
+        return int(self.L.cosmo_x_wait_test(int(kind), 1 if fatal else 0))
 
     def kernel_radius(self) -> float:
         return float(self.L.cosmo_kernel_radius())

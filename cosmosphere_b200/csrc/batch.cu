@@ -569,10 +569,13 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
                      const double* __restrict__ pmassSet, double tolh, double hfact, const DevBox* __restrict__ boxes,
                      int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
                      const int* __restrict__ setNodeStart, const int* __restrict__ leafPre,
-                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds)
+                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds, long long waitNs)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
+    __shared__ __align__(128) WarpStage sStage[kWarpsPerBlock];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    stage_init(sStage[wib]);
+    const StageRef stage{&sStage[wib], &ds->err, waitNs};
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     unsigned long long pairs = 0;
     for (;;)
@@ -593,6 +596,7 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
         double rhoi = 0.0, gradhi = 0.0;
         unsigned int gp = 0, gc = 0;
         auto src = list_source(jlist, jOffset[leaf], jcount[leaf], TableRanges{range}, xyzh);
+        src.stage = stage;   // j ranges staged into shared memory by bulk copies
         if (w < nHeavy)
         {
             const double4 c = tree.center[leafPre[leaf]], h = tree.half[leafPre[leaf]];
@@ -726,7 +730,8 @@ static void batch_build(Batch& B)
         {
             onesweep_set_kernel<<<tiles, kSortThreads, 0, s.st>>>(kA, vA, kB, vB, n, 8 * p, B.setBase.get() + 256 * p,
                                                                  s.sortLookback.get() + size_t(p) * tiles * 256,
-                                                                 &ds->sortTiles[8 + p], &ds->err, B.setOf.get());
+                                                                 &ds->sortTiles[8 + p], &ds->err, B.setOf.get(),
+                                                                 wait_limit_ns());
             COSMO_LAUNCHED();
             std::swap(kA, kB);
             std::swap(vA, vB);
@@ -870,7 +875,8 @@ static void run_items(Batch& B, const int* leaves, const int* countPtr, bool eva
         kern<<<persistent_grid(s, kern, kThreads), kThreads, 0, s.st>>>(
             B.items.get(), cap, B.leafSet.get(), B.leafRange.get(), B.jOffset.get(), B.jcount.get(), B.jlist.get(),
             B.xyzh.get(), B.rho.get(), B.gradh.get(), B.converged.get(), B.pmass.get(), tolh, hfact, B.boxes.get(),
-            B.leafNext.get(), B.activeB.get(), tree, B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(), ds);
+            B.leafNext.get(), B.activeB.get(), tree, B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(), ds,
+            wait_limit_ns());
     };
     if (evalAll) { if (s.precision == 1) go(density_batch_kernel<true, true>); else go(density_batch_kernel<false, true>); }
     else { if (s.precision == 1) go(density_batch_kernel<true, false>); else go(density_batch_kernel<false, false>); }

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "state.hpp"
+#include "tma.cuh"
 #include "../../include/cosmosphere.h"
 #include "../../include/cosmo_density.hpp"
 
@@ -209,7 +210,37 @@ void check_dev_err(State& s, const char* where)
     if (e)
         fatal("%s: device error 0x%x (%s%s%s%s)", where, e, (e & kErrSortSpin) ? "sort look-back timeout " : "",
               (e & kErrListCap) ? "j-list capacity " : "", (e & kErrStageWait) ? "staging wait timeout " : "",
-              (e & kErrQueueWait) ? "queue wait timeout" : "");
+              (e & kErrFlagWait) ? "flag wait timeout" : "");
+}
+
+// Limit of every bounded device wait (sort look-back, staging barriers), nanoseconds.
+static std::atomic<long long> g_waitLimitNs{1000000000ll};
+long long wait_limit_ns() { return g_waitLimitNs.load(); }
+
+// Test-only waits that can never be satisfied, through the same bounded-wait code as the
+// library's own: kind 0 polls a flag no block sets (as the sort's look-back polls its
+// predecessor's), kind 1 waits on an mbarrier armed for 32 bytes of bulk copy that is never
+// issued (as a staging wait does).  Each gives up after limitNs and raises its bit.
+__global__ void wait_test_kernel(int kind, const int* flag, int* err, long long limitNs)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (kind == 0)
+    {
+        if (threadIdx.x != 0) return;
+        WaitClock clk;
+        while (*reinterpret_cast<const volatile int*>(flag) == 0)
+            if (clk.over(limitNs)) { atomicOr(err, int(kErrFlagWait)); return; }
+        return;
+    }
+    if (threadIdx.x == 0)
+    {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(&bar, 32u);
+    }
+    __syncwarp();
+    const bool got = mbar_wait_bounded(&bar, 0u, limitNs);
+    if (!__all_sync(0xffffffffu, got) && threadIdx.x == 0) atomicOr(err, int(kErrStageWait));
 }
 
 // Each state records its phase timings with its own pool of events (the served form runs
@@ -667,6 +698,33 @@ void cosmo_x_sync(void)
 {
     State& s = state();
     if (s.st) COSMO_CUDA(cudaStreamSynchronize(s.st));
+}
+
+void cosmo_x_set_wait_limit(long long ns)
+{
+    g_waitLimitNs.store(ns > 0 ? ns : 1000000000ll);
+}
+
+long long cosmo_x_get_wait_limit(void) { return wait_limit_ns(); }
+
+int cosmo_x_wait_test(int kind, int fatal_on_error)
+{
+    if (kind != 0 && kind != 1) return -1;
+    State& s = state();
+    ensure_init(s);
+    DBuf<int> flag;
+    flag.resize(1, s.st);
+    COSMO_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), s.st));
+    COSMO_CUDA(cudaMemsetAsync(&s.dscal.get()->err, 0, sizeof(int), s.st));
+    wait_test_kernel<<<1, 32, 0, s.st>>>(kind, flag.get(), &s.dscal.get()->err, wait_limit_ns());
+    COSMO_LAUNCHED();
+    if (fatal_on_error) check_dev_err(s, "cosmo_x_wait_test");
+    read_scalars(s);
+    const int e = s.hscal->err;
+    COSMO_CUDA(cudaMemsetAsync(&s.dscal.get()->err, 0, sizeof(int), s.st));
+    flag.release(s.st);
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    return e;
 }
 
 // Format one of the stderr statistics lines from given values (0 COSMO_STATS, 1

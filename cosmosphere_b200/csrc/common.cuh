@@ -43,10 +43,6 @@ constexpr uint64_t kKeyEnd   = 1ull << 63;      // one past the largest live key
 constexpr uint64_t kDeadKey  = ~0ull;           // h <= 0: sorted to the end (tree.cuh:99-104)
 constexpr uint32_t kBucket   = 64;              // leaf capacity, BUCKET_SIZE (tree.cuh:53)
 
-// Bounded spins: every wait on another block's flag gives up after this many polls and
-// raises the device error word instead of hanging the GPU.
-constexpr long long kSpinLimit = 1ll << 26;
-
 inline int iceil(long a, long b) { return int((a + b - 1) / b); }
 
 // --------------------------------------------------------------------------------------
@@ -253,7 +249,7 @@ enum DevErr : int
     kErrSortSpin  = 1,      // radix sort look-back gave up waiting
     kErrListCap   = 2,      // a j-list fill found more entries than its count pass
     kErrStageWait = 4,      // a TMA staging wait gave up
-    kErrQueueWait = 8,      // a persistent-queue wait gave up
+    kErrFlagWait  = 8,      // a wait on a flag another block sets gave up (the wait test hook)
     kErrListFull  = 16,     // a j-list build needed more than the preallocated capacity
 };
 

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace cosmo {
 
@@ -135,6 +136,7 @@ struct CandidateRing
     float4* ringf;
     int* ringIdx;
     double cx, cy, cz, lx, ly, lz;
+    StageRef stage;
     int head = 0, cnt = 0;
 
     template<class Batch>
@@ -155,6 +157,11 @@ struct CandidateRing
     __device__ __forceinline__ void feed(uint32_t s0, uint32_t len, int nb, const double4* __restrict__ xyzh,
                                          Filter& filter, Batch& batch)
     {
+        if (stage.ws != nullptr && stage.ws->broken == 0u)
+        {
+            feed_staged(s0, len, nb, xyzh, filter, batch);
+            return;
+        }
         const int lane = threadIdx.x & 31;
         const uint32_t lt = (1u << lane) - 1u;
         const uint32_t incl = warp_incl_scan_u32(len);
@@ -207,6 +214,118 @@ struct CandidateRing
         }
     }
 
+    // Admit one loaded stream position (pj, particle index j) through the filter into the
+    // ring, in order, and hand full batches of 32 to batch.
+    template<class Filter, class Batch>
+    __device__ __forceinline__ void admit(bool valid, const double4& pj, uint32_t j, Filter& filter, Batch& batch)
+    {
+        const int lane = threadIdx.x & 31;
+        const uint32_t lt = (1u << lane) - 1u;
+        const bool pass = valid && filter(pj);
+        const uint32_t m = __ballot_sync(0xffffffffu, pass);
+        if (pass)
+        {
+            const int slot = (head + cnt + __popc(m & lt)) & (kRing - 1);
+            if constexpr (Dbl) ring[slot] = pj;
+            if constexpr (Float)
+                ringf[slot] = make_float4(float(image_offset(pj.x, cx, lx)), float(image_offset(pj.y, cy, ly)),
+                                          float(image_offset(pj.z, cz, lz)), float(pj.w));
+            if constexpr (Index) ringIdx[slot] = int(j);
+        }
+        cnt += __popc(m);
+        __syncwarp();
+        if (cnt >= 32) drain(32, batch);
+    }
+
+    // feed() with the stream staged by bulk copies: chunk c (stream positions 32c ..
+    // 32c + 31) is copied into stage buffer c % kStages as one cp.async.bulk per run of
+    // consecutive particles (a run starts where the particle index does not follow its
+    // predecessor's; Hilbert-ordered leaves make runs of whole leaves and more), issued by
+    // the run's first lane and completing on the buffer's mbarrier.  While chunk c is
+    // filtered, chunk c + 1 is in flight.  A wait that gives up raises kErrStageWait,
+    // waits (bounded) for the copies still in flight, marks the stage broken and returns;
+    // the host then reports the error.
+    template<class Filter, class Batch>
+    __device__ __forceinline__ void feed_staged(uint32_t s0, uint32_t len, int nb, const double4* __restrict__ xyzh,
+                                                Filter& filter, Batch& batch)
+    {
+        const int lane = threadIdx.x & 31;
+        WarpStage& S = *stage.ws;
+        const uint32_t incl = warp_incl_scan_u32(len);
+        const uint32_t excl = incl - len;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        auto locate = [&](uint32_t p) -> uint32_t {
+            int t = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+            {
+                const uint32_t e = __shfl_sync(0xffffffffu, excl, (t + step) & 31);
+                if (t + step < nb && e <= p) t += step;
+            }
+            return __shfl_sync(0xffffffffu, s0, t) + (p - __shfl_sync(0xffffffffu, excl, t));
+        };
+        const uint32_t nChunks = (total + 31u) >> 5;
+        uint32_t phase = S.phase;
+        auto issue = [&](uint32_t c) {
+            const int b = int(c % kStages);
+            const uint32_t p = (c << 5) + uint32_t(lane);
+            const bool valid = p < total;
+            const uint32_t j = locate(p);
+            const uint32_t jp = __shfl_up_sync(0xffffffffu, j, 1);
+            const bool start = valid && (lane == 0 || j != jp + 1u);
+            const uint32_t starts = __ballot_sync(0xffffffffu, start);
+            const int count = int(min(32u, total - (c << 5)));
+            if (lane == 0) mbar_arrive_expect_tx(&S.bar[b], uint32_t(count) * 32u);
+            __syncwarp();
+            if (start)
+            {
+                const uint32_t after = starts & ~((2u << lane) - 1u);
+                const int end = after ? (__ffs(after) - 1) : count;
+                bulk_g2s(&S.buf[b][lane], xyzh + j, uint32_t(end - lane) * 32u, &S.bar[b]);
+            }
+        };
+        for (uint32_t c = 0; c < nChunks && c < uint32_t(kStages); ++c) issue(c);
+        for (uint32_t c = 0; c < nChunks; ++c)
+        {
+            const int b = int(c % kStages);
+            // lane 0 waits under the limit; once it has seen the phase complete, the other
+            // lanes' waits (each lane's own acquire of the copied data) return at once
+            bool got = lane == 0 ? mbar_wait_bounded(&S.bar[b], (phase >> b) & 1u, stage.limitNs) : true;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (got && lane != 0) mbar_wait_bounded(&S.bar[b], (phase >> b) & 1u, stage.limitNs);
+            if (!got)
+            {
+                // give up: the copies still in flight (this chunk's and those after it) must
+                // land before the warp leaves the buffers
+                if (lane == 0) atomicOr(stage.err, int(kErrStageWait));
+                const uint32_t last = min(nChunks, c + uint32_t(kStages));
+                if (lane == 0)
+                {
+                    for (uint32_t d = c; d < last; ++d)
+                    {
+                        const int bd = int(d % kStages);
+                        mbar_wait_bounded(&S.bar[bd], (phase >> bd) & 1u, stage.limitNs);
+                    }
+                    S.broken = 1u;
+                }
+                __syncwarp();
+                return;
+            }
+            phase ^= 1u << b;
+            const uint32_t p = (c << 5) + uint32_t(lane);
+            const bool valid = p < total;
+            double4 pj = make_double4(0, 0, 0, 0);
+            if (valid) pj = S.buf[b][lane];
+            const uint32_t j = Index ? locate(p) : 0u;
+            fence_proxy_async_smem();   // the reads above before the next copy into buffer b
+            __syncwarp();
+            if (c + uint32_t(kStages) < nChunks) issue(c + uint32_t(kStages));
+            admit(valid, pj, j, filter, batch);
+        }
+        if (lane == 0) S.phase = phase;
+        __syncwarp();
+    }
+
     template<class Batch>
     __device__ __forceinline__ void finish(Batch& batch)
     {
@@ -220,10 +339,11 @@ template<bool Dbl, bool Float, bool Index, class Ranges, class Filter, class Bat
 __device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
                                               double cz, double lx, double ly, double lz, uint32_t jb, uint32_t nj,
                                               const int* __restrict__ jlist, Ranges ranges,
-                                              const double4* __restrict__ xyzh, Filter filter, Batch batch)
+                                              const double4* __restrict__ xyzh, Filter filter, Batch batch,
+                                              StageRef stage = StageRef{nullptr, nullptr, 0})
 {
     const int lane = threadIdx.x & 31;
-    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, lx, ly, lz};
+    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, lx, ly, lz, stage};
     for (uint32_t lb = 0; lb < nj; lb += 32)
     {
         const int nb = int(min(32u, nj - lb));
@@ -260,10 +380,10 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
                                             double cz, double sx, double sy, double sz, const PreorderTree& t,
                                             double3 c, double3 e, double3 rc, double3 re, double lx, double ly,
                                             double lz, Ranges ranges, const double4* __restrict__ xyzh,
-                                            Filter filter, Batch batch)
+                                            Filter filter, Batch batch, StageRef stage = StageRef{nullptr, nullptr, 0})
 {
     const int lane = threadIdx.x & 31;
-    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz};
+    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz, stage};
     auto fold = [&](double d, double L) { return (Periodic && L > 0.0) ? fmin(d, L - d) : d; };
     int p = t.n0;
     while (p < t.n1)
@@ -337,6 +457,7 @@ struct GroupSource
     bool walk;
     PreorderTree tree;
     double3 rc, re;
+    StageRef stage;   // the warp's bulk-copy stage, or none (direct loads)
 
     template<bool Dbl, bool Float, bool Index, bool Periodic, class Filter, class Batch>
     __device__ __forceinline__ void stream(double4* ring, float4* ringf, int* ringIdx, const GroupBox& bx, double sx,
@@ -347,10 +468,10 @@ struct GroupSource
             stream_walk<Dbl, Float, Index, Periodic>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, tree,
                                                      make_double3(bx.cx, bx.cy, bx.cz),
                                                      make_double3(bx.ex, bx.ey, bx.ez), rc, re, lx, ly, lz, ranges,
-                                                     xyzh, filter, batch);
+                                                     xyzh, filter, batch, stage);
         else
             stream_ranges<Dbl, Float, Index>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, jb, nj, jlist,
-                                             ranges, xyzh, filter, batch);
+                                             ranges, xyzh, filter, batch, stage);
     }
 };
 
@@ -359,7 +480,7 @@ __device__ __forceinline__ GroupSource<Ranges> list_source(const int* jlist, uin
                                                            const double4* xyzh)
 {
     GroupSource<Ranges> g{jlist, jb, nj, ranges, xyzh, false, PreorderTree{nullptr, nullptr, nullptr, nullptr, 0, 0},
-                          make_double3(0, 0, 0), make_double3(-1, -1, -1)};
+                          make_double3(0, 0, 0), make_double3(-1, -1, -1), StageRef{nullptr, nullptr, 0}};
     return g;
 }
 

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace cosmo {
 namespace {
@@ -156,7 +157,8 @@ template<bool SetDigit>
 __device__ __forceinline__ void
 onesweep_body(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uint64_t* __restrict__ kout,
                   int* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ binBase,
-                  uint32_t* lookback, unsigned int* tileTicket, int* err, const int* __restrict__ setOf)
+                  uint32_t* lookback, unsigned int* tileTicket, int* err, const int* __restrict__ setOf,
+                  long long waitNs)
 {
     __shared__ uint32_t sHist[kSortWarps][256];
     __shared__ uint32_t sBase[256];
@@ -216,13 +218,13 @@ onesweep_body(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uin
             atomicExch(mine, kLbAgg | total);
             uint32_t excl = 0;
             int p = tile - 1;
-            long long spins = 0;
+            WaitClock clk;
             while (p >= 0)
             {
                 const uint32_t s = ld_volatile_u32(lookback + size_t(p) * 256 + d);
                 if ((s & ~kLbMask) == 0u)
                 {
-                    if (++spins > kSpinLimit) { atomicOr(err, int(kErrSortSpin)); break; }
+                    if (clk.over(waitNs)) { atomicOr(err, int(kErrSortSpin)); break; }
                     continue;
                 }
                 excl += s & kLbMask;
@@ -252,17 +254,18 @@ onesweep_body(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uin
 __global__ void __launch_bounds__(kSortThreads)
 onesweep_kernel(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uint64_t* __restrict__ kout,
                 int* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ binBase,
-                uint32_t* lookback, unsigned int* tileTicket, int* err)
+                uint32_t* lookback, unsigned int* tileTicket, int* err, long long waitNs)
 {
-    onesweep_body<false>(kin, vin, kout, vout, n, shift, binBase, lookback, tileTicket, err, nullptr);
+    onesweep_body<false>(kin, vin, kout, vout, n, shift, binBase, lookback, tileTicket, err, nullptr, waitNs);
 }
 
 __global__ void __launch_bounds__(kSortThreads)
 onesweep_set_kernel(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uint64_t* __restrict__ kout,
                     int* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ binBase,
-                    uint32_t* lookback, unsigned int* tileTicket, int* err, const int* __restrict__ setOf)
+                    uint32_t* lookback, unsigned int* tileTicket, int* err, const int* __restrict__ setOf,
+                    long long waitNs)
 {
-    onesweep_body<true>(kin, vin, kout, vout, n, shift, binBase, lookback, tileTicket, err, setOf);
+    onesweep_body<true>(kin, vin, kout, vout, n, shift, binBase, lookback, tileTicket, err, setOf, waitNs);
 }
 
 } // namespace

@@ -552,7 +552,7 @@ void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int 
     {
         onesweep_kernel<<<tiles, kSortThreads, 0, s.st>>>(
             ki, vi, ko, vo, n, 8 * p, s.sortBase.get() + 256 * p,
-            s.sortLookback.get() + size_t(p) * tiles * 256, &ds->sortTiles[p], &ds->err);
+            s.sortLookback.get() + size_t(p) * tiles * 256, &ds->sortTiles[p], &ds->err, wait_limit_ns());
         COSMO_LAUNCHED();
         std::swap(ki, ko);
         vi = vo;
@@ -626,7 +626,8 @@ int keysort_raw(int n, const double* x, const double* y, const double* z, const 
     for (int pass = 0; pass < kSortPasses; ++pass)
     {
         onesweep_kernel<<<tiles, kSortThreads, 0, st>>>(ki, vi, ko, vo, n, 8 * pass, base + 256 * pass,
-                                                        lookback + size_t(pass) * tiles * 256, &tickets[pass], err);
+                                                        lookback + size_t(pass) * tiles * 256, &tickets[pass], err,
+                                                        wait_limit_ns());
         std::swap(ki, ko);
         vi = vo;
         vo = (vo == vB) ? orderOut : vB;

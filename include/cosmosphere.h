@@ -205,6 +205,20 @@ int cosmo_x_density(int n, double pmass, int periodic, const double* box, double
 /* Wait for the library's stream. */
 void cosmo_x_sync(void);
 
+/* Time limit of every bounded device wait (the sort's look-back on its predecessor
+ * tiles, the staging barriers of the bulk copies), in nanoseconds; <= 0 restores the
+ * default of 1 s.  A wait that runs out raises a bit in the device error word, and the
+ * entry point reports it (FATAL, or -3 where a status is returned). */
+void cosmo_x_set_wait_limit(long long ns);
+long long cosmo_x_get_wait_limit(void);
+
+/* Run a device wait that can never be satisfied, through the library's bounded-wait code:
+ * kind 0 polls a flag no block sets, kind 1 waits on a staging mbarrier whose bulk copy is
+ * never issued.  Returns the device error bits it raised (8 flag wait, 4 staging wait) and
+ * clears them, or -1 for an unknown kind; with fatal_on_error the library reports them as
+ * a solve does (a FATAL line and abort). */
+int cosmo_x_wait_test(int kind, int fatal_on_error);
+
 /* Format a statistics line (0 COSMO_STATS, 1 COSMO_FORCE, 2 COSMO_MEM) from its values,
  * in the field order the entry points print it; returns the snprintf length or -1.  No
  * device work. */

@@ -94,3 +94,15 @@ def test_stats_lines_have_the_reference_fields(which):
     else:
         assert re.fullmatch(r"COSMO_MEM n=\d+ device_used=\d+\.\d\d GB of \d+\.\d\d GB \(\d+ bytes/particle\) "
                             r"host_peak=\d+\.\d\d GB\n", line)
+
+
+def test_wait_limit_setting_round_trips():
+    """The bounded-wait limit is a host setting (no device work to set it)."""
+    c = capi.Cosmo()
+    old = c.wait_limit()
+    assert old > 0
+    c.set_wait_limit(12345)
+    assert c.wait_limit() == 12345
+    c.set_wait_limit(0)                 # restores the default
+    assert c.wait_limit() == 1_000_000_000
+    c.set_wait_limit(old)
