@@ -4,7 +4,10 @@
  *
  * Layout in HBM (all Hilbert-ordered arrays are indexed by sorted position k):
  *   caller order   ux uy uz uh | uvx uvy uvz | uax uay uaz    upload targets (f64 SoA)
- *   Hilbert order  xyzh   double4 (x, y, z, h)                 TMA/128-bit friendly
+ *   Hilbert order  xyzh   double4 (x, y, z, h)                 32-byte records: bulk-copied
+ *                                                              into shared memory by the
+ *                                                              Newton kernels, read as two
+ *                                                              128-bit loads elsewhere
  *                  vel4   double4 (vx, vy, vz, 0), acc4 likewise
  *                  thermo4 double4 (pro2, cs, alpha, u)
  *                  prepA  double4 (1/h^2, 1/h, rho(h), 1/rho)   force per-particle factors

@@ -215,3 +215,44 @@ def test_continuations_queued_before_admission(reqs):
         np.testing.assert_array_equal(got["h"], h, err_msg=f"step {k}")
         np.testing.assert_array_equal(got["force"], c.download(capi.FORCE_OUT, n), err_msg=f"step {k}")
     assert np.all((pos >= 0.0) & (pos < 1.0))
+
+
+def test_mixed_same_alone_and_in_the_mix(reqs):
+    """The mixed-precision served form (the form the served bench runs): each request's
+    result in a concurrent mix equals its result served alone within the mixed form's
+    stated tolerance (1e-5 relative in h and rho, 1e-5 of the field's rms elsewhere), and
+    both are within it of the plain FP64 result."""
+    c = capi.Cosmo()
+    plain = []
+    for r in reqs:
+        res, _ = serve([r], slots=1)
+        plain.append(res[0])
+    c.set_precision(True)
+    try:
+        alone = []
+        for r in reqs:
+            res, _ = serve([r], slots=1)
+            alone.append(res[0])
+        mix, stats = serve(reqs, slots=4)
+    finally:
+        c.set_precision(False)
+    assert stats["max_inflight"] >= 2
+
+    def close(a, b, what):
+        for key in ("h", "dens"):
+            x, y = a[key].reshape(-1), b[key].reshape(-1)
+            if key == "dens":
+                x, y = a[key][0], b[key][0]
+            live = np.abs(y) > 0
+            assert np.max(np.abs(x[live] / y[live] - 1.0)) <= 1e-5, (what, key)
+        for key in ("grad", "force"):
+            for comp in range(a[key].shape[0]):
+                x, y = a[key][comp], b[key][comp]
+                rms = np.sqrt(np.mean(y * y))
+                if rms > 0:
+                    assert np.max(np.abs(x - y)) <= 1e-5 * (rms + np.max(np.abs(y))), (what, key, comp)
+
+    for k, ((s0, p0), (s1, a), (s2, b)) in enumerate(zip(plain, alone, mix)):
+        assert s0 == 1 and s1 == 1 and s2 == 1
+        close(b, a, f"request {k}: mix vs alone")
+        close(a, p0, f"request {k}: mixed vs plain")
