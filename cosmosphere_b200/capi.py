@@ -21,7 +21,7 @@ EXPORTS = [
     "cosmo_arrays_init", "cosmo_slot_ncomp", "cosmo_upload", "cosmo_upload_sorted", "cosmo_download",
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
-    "cosmo_x_stats_line", "cosmo_x_set_wait_limit", "cosmo_x_get_wait_limit", "cosmo_x_wait_test",
+    "cosmo_x_stats_line", "cosmo_x_set_option", "cosmo_x_set_wait_limit", "cosmo_x_get_wait_limit", "cosmo_x_wait_test",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
     "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_set_tuning",
@@ -56,6 +56,8 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_scalar.argtypes = [ctypes.c_char_p]
     L.cosmo_x_stats_line.argtypes = [I, P, ctypes.c_char_p, I]
     L.cosmo_x_stats_line.restype = I
+    L.cosmo_x_set_option.argtypes = [ctypes.c_char_p, I]
+    L.cosmo_x_set_option.restype = I
     L.cosmo_x_set_wait_limit.argtypes = [ctypes.c_longlong]
     L.cosmo_x_get_wait_limit.restype = ctypes.c_longlong
     L.cosmo_x_wait_test.argtypes = [I, I]
@@ -173,6 +175,9 @@ class Cosmo:
         if n < 0:
             raise ValueError(which)
         return buf.value.decode()
+
+    def set_option(self, name: str, value: int) -> int:
+        return int(self.L.cosmo_x_set_option(name.encode(), int(value)))
 
     def set_wait_limit(self, ns: int):
         self.L.cosmo_x_set_wait_limit(int(ns))

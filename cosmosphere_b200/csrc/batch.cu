@@ -569,7 +569,7 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
                      const double* __restrict__ pmassSet, double tolh, double hfact, const DevBox* __restrict__ boxes,
                      int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
                      const int* __restrict__ setNodeStart, const int* __restrict__ leafPre,
-                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds, long long waitNs)
+                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds, long long waitNs, int staged)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
     __shared__ __align__(128) WarpStage sStage[kWarpsPerBlock];
@@ -596,7 +596,7 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
         double rhoi = 0.0, gradhi = 0.0;
         unsigned int gp = 0, gc = 0;
         auto src = list_source(jlist, jOffset[leaf], jcount[leaf], TableRanges{range}, xyzh);
-        src.stage = stage;   // j ranges staged into shared memory by bulk copies
+        if (staged) src.stage = stage;   // j ranges staged into shared memory by bulk copies
         if (w < nHeavy)
         {
             const double4 c = tree.center[leafPre[leaf]], h = tree.half[leafPre[leaf]];
@@ -876,7 +876,7 @@ static void run_items(Batch& B, const int* leaves, const int* countPtr, bool eva
             B.items.get(), cap, B.leafSet.get(), B.leafRange.get(), B.jOffset.get(), B.jcount.get(), B.jlist.get(),
             B.xyzh.get(), B.rho.get(), B.gradh.get(), B.converged.get(), B.pmass.get(), tolh, hfact, B.boxes.get(),
             B.leafNext.get(), B.activeB.get(), tree, B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(), ds,
-            wait_limit_ns());
+            wait_limit_ns(), s.staging);
     };
     if (evalAll) { if (s.precision == 1) go(density_batch_kernel<true, true>); else go(density_batch_kernel<false, true>); }
     else { if (s.precision == 1) go(density_batch_kernel<true, false>); else go(density_batch_kernel<false, false>); }

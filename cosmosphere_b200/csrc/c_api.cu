@@ -116,6 +116,8 @@ void ensure_init(State& s)
     s.box.resize(1, s.st);
     if (const char* e = std::getenv("COSMO_MAX_ITER")) s.maxIter = std::max(1, std::atoi(e));
     if (const char* e = std::getenv("COSMO_PRECISION")) s.precision = (std::string(e) == "mixed") ? 1 : 0;
+    if (const char* e = std::getenv("COSMO_STAGING")) s.staging = std::atoi(e) != 0;
+    if (const char* e = std::getenv("COSMO_SYM_PREFILTER")) s.symPrefilter = std::atoi(e) != 0;
 }
 
 size_t state_device_bytes(const State& s)
@@ -698,6 +700,16 @@ void cosmo_x_sync(void)
 {
     State& s = state();
     if (s.st) COSMO_CUDA(cudaStreamSynchronize(s.st));
+}
+
+int cosmo_x_set_option(const char* name, int value)
+{
+    State& s = state();
+    ensure_init(s);
+    const std::string k(name ? name : "");
+    if (k == "staging") { s.staging = value != 0; return 0; }
+    if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
+    return -1;
 }
 
 void cosmo_x_set_wait_limit(long long ns)

@@ -39,9 +39,66 @@ constexpr int kRec = 256;   // pair records per warp
 template<bool Mixed>
 struct DensScratch
 {
-    static constexpr int kBytes = Mixed ? (kRing * 16 + 4 * 32 * 4 + 2 * kRec * 4)
-                                        : (kRing * 32 + 32 * 32 + 4 * 32 * 4 + 2 * kRec * 8 + kRec * 4);
+    static constexpr int kBytes = (Mixed ? (kRing * 16 + 4 * 32 * 4 + 2 * kRec * 4)
+                                         : (kRing * 32 + 32 * 32 + 4 * 32 * 4 + 2 * kRec * 8 + kRec * 4)) +
+                                  2 * 8 * 16;   // sub-group boxes
 };
+
+// Sub-group boxes.  A group whose smoothing lengths spread widely (largest over smallest
+// above kSubSpread) has a box much larger than most of its particles' search spheres -- one
+// wide particle sets it.  Such a group gets one box per four consecutive particles (their
+// search spheres, widened by eps), and a batch of candidates none of which lies inside a
+// sub-group's box skips that sub-group's tests: a candidate outside the box of particle i's
+// search sphere can pass neither the prefilter nor the exact test for i.  Offsets are FP32
+// from the group box centre (c, e: 8 centres and half extents per warp).
+constexpr double kSubSpread = 1.3;
+
+__device__ __forceinline__ bool sub_boxes(float4* sc, float4* se, bool mine, int ng, double hi, double rs,
+                                          double ox, double oy, double oz, double eps)
+{
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    const double hmin = warp_min(mine ? hi : inf), hmax = warp_max(mine ? hi : 0.0);
+    if (!(ng > 4 && hmax > kSubSpread * hmin)) return false;
+    const int lane = threadIdx.x & 31;
+    double lx = mine ? ox - rs : inf, hx = mine ? ox + rs : -inf;
+    double ly = mine ? oy - rs : inf, hy = mine ? oy + rs : -inf;
+    double lz = mine ? oz - rs : inf, hz = mine ? oz + rs : -inf;
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1)
+    {
+        lx = fmin(lx, __shfl_xor_sync(0xffffffffu, lx, o)); hx = fmax(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+        ly = fmin(ly, __shfl_xor_sync(0xffffffffu, ly, o)); hy = fmax(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+        lz = fmin(lz, __shfl_xor_sync(0xffffffffu, lz, o)); hz = fmax(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+    }
+    if ((lane & 3) == 0 && lane < ng)
+    {
+        sc[lane >> 2] = make_float4(float(0.5 * (lx + hx)), float(0.5 * (ly + hy)), float(0.5 * (lz + hz)), 0.0f);
+        se[lane >> 2] = make_float4(__double2float_ru(0.5 * (hx - lx) + eps), __double2float_ru(0.5 * (hy - ly) + eps),
+                                    __double2float_ru(0.5 * (hz - lz) + eps), 0.0f);
+    }
+    __syncwarp();
+    return true;
+}
+
+// The sub-groups whose boxes hold a lane's candidate (px, py, pz), OR-ed over the batch.
+template<bool Periodic>
+__device__ __forceinline__ uint32_t sub_need(const float4* sc, const float4* se, int ng, bool valid, float px,
+                                             float py, float pz, float Lx, float Ly, float Lz)
+{
+    uint32_t m = 0;
+    if (valid)
+    {
+        const int nsub = (ng + 3) >> 2;
+        for (int s = 0; s < nsub; ++s)
+        {
+            const float4 c = sc[s], e = se[s];
+            if (axis_df<Periodic>(px, c.x, Lx) <= e.x && axis_df<Periodic>(py, c.y, Ly) <= e.y &&
+                axis_df<Periodic>(pz, c.z, Lz) <= e.z)
+                m |= 1u << s;
+        }
+    }
+    return __reduce_or_sync(0xffffffffu, m);
+}
 
 // q = sqrt(q2) in FP32 (q2 >= 0); exact 0 for the self pair.
 __device__ __forceinline__ float sqrt_q(float q2) { return q2 > 0.0f ? q2 * rsqrtf(q2) : 0.0f; }
@@ -74,8 +131,11 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         double* recA = reinterpret_cast<double*>(gfT + 32);
         double* recB = recA + kRec;
         int* recI = reinterpret_cast<int*>(recB + kRec);    // (group particle << 8) | ring slot
+        float4* subC = reinterpret_cast<float4*>(recI + kRec);
+        float4* subE = subC + 8;
         const double period = Periodic ? fmax(lx, fmax(ly, lz)) : 0.0;
         const double eps = fp32_margin(bx, period);
+        const bool useSub = sub_boxes(subC, subE, mine, ng, hi, rs, pi.x - bx.cx, pi.y - bx.cy, pi.z - bx.cz, eps);
         if (mine)
         {
             grp[lane] = make_double4(pi.x, pi.y, pi.z, hinv2);
@@ -174,9 +234,15 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                     __syncwarp();
                 };
                 const float2 nx = make_float2(-px, -px), ny = make_float2(-py, -py), nz = make_float2(-pz, -pz);
+                uint32_t need = 0xffffffffu;
+                if (useSub)
+                    need = (Periodic && Lx != 0.0f)
+                               ? sub_need<true>(subC, subE, ng, lane < count, px, py, pz, Lx, Ly, Lz)
+                               : sub_need<false>(subC, subE, ng, lane < count, px, py, pz, Lx, Ly, Lz);
                 // four group particles per step, two per packed FP32 instruction
                 for (int i0 = 0; i0 < ng; i0 += 4)
                 {
+                    if (!((need >> (i0 >> 2)) & 1u)) continue;   // no candidate of the batch in its box
                     if (nrec + 4 * 32 > kRec) flush();
                     float r2u[4];
                     if (!Periodic || Lx == 0.0f)   // zero periods (an open set) fold nothing
@@ -232,6 +298,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         float* gh = gz + 32;
         float* recQ = gh + 32;
         float* recG = recQ + kRec;
+        float4* subC = reinterpret_cast<float4*>(recG + kRec);
+        float4* subE = subC + 8;
         // relative coordinates at the centre's nearest image are every accepted pair's
         // nearest image when the box (search spheres included) spans under half a period
         const bool shifted = !Periodic || lx == 0.0 || (bx.ex < 0.5 * lx && bx.ey < 0.5 * ly && bx.ez < 0.5 * lz);
@@ -243,6 +311,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         gh[lane] = mine ? float(hinv2) : 0.0f;
         __syncwarp();
         const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
+        const bool useSub = sub_boxes(subC, subE, mine, ng, hi, rs, pi.x - bx.cx, pi.y - bx.cy, pi.z - bx.cz,
+                                      fp32_margin(bx, Periodic ? fmax(lx, fmax(ly, lz)) : 0.0));
         KahanF kr, kg, lr, lg;
         src.template stream<false, true, false, Periodic>(
             nullptr, ringf, nullptr, bx, sx, sy, sz, lx, ly, lz,
@@ -299,8 +369,14 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                 };
                 const float2 nx = make_float2(-pf.x, -pf.x), ny = make_float2(-pf.y, -pf.y);
                 const float2 nz = make_float2(-pf.z, -pf.z);
+                uint32_t need = 0xffffffffu;
+                if (useSub)
+                    need = (Periodic && !shifted)
+                               ? sub_need<true>(subC, subE, ng, lane < count, pf.x, pf.y, pf.z, Lx, Ly, Lz)
+                               : sub_need<false>(subC, subE, ng, lane < count, pf.x, pf.y, pf.z, Lx, Ly, Lz);
                 for (int i0 = 0; i0 < ng; i0 += 4)
                 {
+                    if (!((need >> (i0 >> 2)) & 1u)) continue;   // no candidate of the batch in its box
                     if (nrec + 4 * 32 > kRec) flush();
                     float q2u[4];
                     if (!Periodic || shifted)

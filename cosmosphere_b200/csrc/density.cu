@@ -384,7 +384,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
                 s.leafNext.get(), s.activeB.get(),
                 PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
-                s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns());
+                s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns(), s.staging);
             COSMO_LAUNCHED();
             if (rowsReady)
             {

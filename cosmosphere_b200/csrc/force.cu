@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kThreads)
 sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                 const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                 const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
-                int* __restrict__ nbl, int* __restrict__ nblCount, DevScalars* __restrict__ ds)
+                int* __restrict__ nbl, int* __restrict__ nblCount, DevScalars* __restrict__ ds, int prefilter)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -276,18 +276,25 @@ sym_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restr
         // larger bound and max(bound_i, bound_j) is the same double as the test's own
         auto bound = [](double h) { return kRadK2 * (h * h) * (1.0 + 1e-10); };
         // prefilter distances: R h (1 + 1e-10) bounds sqrt(bound(h)) for either side
-        rows_group<kRowStride, Periodic>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, bound(pi.w)),
-                   kRadKernel * pi.w * (1.0 + 1e-10), bx, lx, ly, lz, jOffset[d.leaf], jcount[d.leaf], jlist,
-                   LayoutRanges{layout}, xyzh,
-                   [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); },
-                   [](const double4& pj) { return kRadKernel * pj.w * (1.0 + 1e-10); },
-                   [&](const double4& g, const double4& pj, int j) {
-                       double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
-                       nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                       const double dr2 = pair_r2(dx, dy, dz);
-                       return RowEntry<int>{!(dr2 >= fmax(g.w, bound(pj.w))), j};
-                   },
-                   mine ? row_of(nbl, uint32_t(i)) : nullptr, rowLen);
+        auto filt = [&](const double4& pj) { return in_sym_box<Periodic>(pj, bx, rg, lx, ly, lz); };
+        auto candB = [](const double4& pj) { return kRadKernel * pj.w * (1.0 + 1e-10); };
+        auto exact = [&](const double4& g, const double4& pj, int j) {
+            double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
+            nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+            const double dr2 = pair_r2(dx, dy, dz);
+            return RowEntry<int>{!(dr2 >= fmax(g.w, bound(pj.w))), j};
+        };
+        int* myRow = mine ? row_of(nbl, uint32_t(i)) : nullptr;
+        const double4 gi = make_double4(pi.x, pi.y, pi.z, bound(pi.w));
+        const double Bi = kRadKernel * pi.w * (1.0 + 1e-10);
+        if (prefilter)
+            rows_group<kRowStride, Periodic, true>(sScr[wib], mine, d.ng, gi, Bi, bx, lx, ly, lz, jOffset[d.leaf],
+                                                   jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh, filt, candB,
+                                                   exact, myRow, rowLen);
+        else
+            rows_group<kRowStride, Periodic, false>(sScr[wib], mine, d.ng, gi, Bi, bx, lx, ly, lz, jOffset[d.leaf],
+                                                    jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh, filt, candB,
+                                                    exact, myRow, rowLen);
         if (mine) nblCount[i] = rowLen;
         if (mine && rowLen > kNbl) ds->rowOverflow = 1;
     }
@@ -360,7 +367,7 @@ void build_symmetric(State& s)
     auto rows = s.periodic ? sym_rows_kernel<true> : sym_rows_kernel<false>;
     rows<<<persistent_grid(s, rows, kThreads), kThreads, 0, s.st>>>(
         s.items.get(), nA, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-        s.box.get(), s.nbl.get(), s.nblCount.get(), ds);
+        s.box.get(), s.nbl.get(), s.nblCount.get(), ds, s.symPrefilter);
     COSMO_LAUNCHED();
 }
 

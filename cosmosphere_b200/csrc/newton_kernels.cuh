@@ -82,7 +82,7 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
                   double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
                   int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
                   const int* __restrict__ leafToInternal, const double* __restrict__ centers,
-                  const double* __restrict__ sizes, DevScalars* __restrict__ ds, long long waitNs)
+                  const double* __restrict__ sizes, DevScalars* __restrict__ ds, long long waitNs, int staged)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
     __shared__ __align__(128) WarpStage sStage[kWarpsPerBlock];
@@ -110,7 +110,7 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
         // a cut group (its leaf's list streams far more than it needs) scans the tree for
         // its own box instead, within the region its leaf's list covers
         auto src = list_source(jlist, jOffset[leaf], jcount[leaf], LayoutRanges{layout}, xyzh);
-        src.stage = stage;   // j ranges staged into shared memory by bulk copies
+        if (staged) src.stage = stage;   // j ranges staged into shared memory by bulk copies
         if (w < nHeavy)
         {
             const int in = leafToInternal[leaf];

@@ -24,6 +24,8 @@
  */
 #pragma once
 
+#include <type_traits>
+
 #include "pairstream.cuh"
 
 namespace cosmo {
@@ -62,7 +64,11 @@ constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32 + 4 * 32 * 4;
 // the entry the owner writes for an accepted j (j itself, or r^2).  row is the lane's own row
 // (row_of with Stride kRowStride, or row_flat with Stride 1; nullptr if not mine); rowLen
 // receives its length (kNbl + 1 when it overflowed).  Entries come in ascending j.
-template<int Stride, bool Periodic, class T, class Ranges, class Filter, class CandB, class Exact>
+// Prefilter = false: no FP32 prefilter; every lane applies exact(gi of particle k, its
+// candidate, j) in lockstep over the group particles, and the ballots are the masks (the
+// symmetric rows, whose candidate-dependent bound makes the prefilter pass most pairs).
+template<int Stride, bool Periodic, bool Prefilter = true, class T, class Ranges, class Filter, class CandB,
+         class Exact>
 __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng, const double4& gi, double Bi,
                                            const GroupBox& bx, double lx, double ly, double lz, uint32_t jb,
                                            uint32_t nj, const int* __restrict__ jlist, Ranges ranges,
@@ -89,7 +95,38 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
     stream_ranges<true, false, true>(
         ring, nullptr, ringIdx, bx.cx, bx.cy, bx.cz, 0.0, 0.0, 0.0, jb, nj, jlist, ranges, xyzh, filter,
         [&](const double4* rg, const float4*, const int* ri, int head, int count) {
-            const double4 pj = rg[(head + (lane < count ? lane : 0)) & (kRing - 1)];
+            const int mySlot = (head + (lane < count ? lane : 0)) & (kRing - 1);
+            const double4 pj = rg[mySlot];
+            if constexpr (!Prefilter)
+            {
+                uint32_t mask = 0;
+                for (int i0 = 0; i0 < ng; i0 += 4)
+                {
+                    bool a[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        a[u] = lane < count && i0 + u < ng && exact(grp[min(i0 + u, 31)], pj, ri[mySlot]).ok;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                    {
+                        const uint32_t m = __ballot_sync(0xffffffffu, a[u]);
+                        if (lane == i0 + u) mask = m;
+                    }
+                }
+                while (mask)
+                {
+                    const int b = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const int sl = (head + b) & (kRing - 1);
+                    if (len < kNbl)
+                    {
+                        if constexpr (std::is_same<T, int>::value) row[size_t(len) * Stride] = ri[sl];   // j itself
+                        else row[size_t(len) * Stride] = exact(gi, rg[sl], ri[sl]).v;
+                    }
+                    ++len;
+                }
+                return;
+            }
             const float px = float(image_offset(pj.x, bx.cx, lx)), py = float(image_offset(pj.y, bx.cy, ly));
             const float pz = float(image_offset(pj.z, bx.cz, lz));
             const double bj = candB(pj);

@@ -124,6 +124,12 @@ struct State
     int itersRun = 0, maxIter = 100;
     long long settling0 = 0;                    // settling particles after the first Newton update
     int precision = 0;     // 0 plain FP64 (the drop-in form), 1 mixed FP32/FP64
+    // Kernel variants (results are the same either way): staging = 1 stages the Newton
+    // kernels' j-stream into shared memory by bulk copies (cp.async.bulk + mbarrier)
+    // instead of loading it directly (COSMO_STAGING); symPrefilter = 1 runs the symmetric
+    // row builder's tests through the FP32 prefilter (COSMO_SYM_PREFILTER).
+    int staging = 0;
+    int symPrefilter = 0;
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;

@@ -205,6 +205,13 @@ int cosmo_x_density(int n, double pmass, int periodic, const double* box, double
 /* Wait for the library's stream. */
 void cosmo_x_sync(void);
 
+/* Select a kernel variant of the single-set solve (results do not depend on it):
+ * "staging" 1 stages the Newton kernels' j-stream into shared memory with bulk copies
+ * (cp.async.bulk completing on an mbarrier), 0 (default) loads it directly;
+ * "sym_prefilter" 1 puts the symmetric row builder's tests behind the FP32 prefilter.
+ * Returns 0, or -1 for an unknown name. */
+int cosmo_x_set_option(const char* name, int value);
+
 /* Time limit of every bounded device wait (the sort's look-back on its predecessor
  * tiles, the staging barriers of the bulk copies), in nanoseconds; <= 0 restores the
  * default of 1 s.  A wait that runs out raises a bit in the device error word, and the

@@ -359,3 +359,23 @@ def test_reference_driver_reads_a_particle_file(tmp_path):
     out_ours = tmp_path / "h_ours.txt"
     dumpio.write_h(out_ours, c.download(capi.HSML, n)[0])
     assert out_ours.read_bytes() == out_ref.read_bytes()
+
+
+@pytest.mark.parametrize("option", ["staging", "sym_prefilter"])
+def test_kernel_variants_keep_parity(option):
+    """The bulk-copy staging of the Newton kernels' j-stream and the FP32-prefiltered
+    symmetric row builder are variants of the same passes: with either switched on, every
+    structure and field still equals the oracle's bit for bit (jiggled lattice, and a
+    log-normal quintic Plummer sphere whose groups spread in h)."""
+    for quintic in (False, True):
+        c = capi.Cosmo(quintic)
+        assert c.set_option(option, 1) == 0
+        try:
+            if quintic:
+                p = inputs.plummer(12000, lnsigma=0.5, seed=21)
+            else:
+                p = inputs.lattice100_workload(16)
+            cc, o = run_pair(p, quintic=quintic)
+            check_all(cc, o)
+        finally:
+            c.set_option(option, 0)
