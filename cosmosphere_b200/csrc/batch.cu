@@ -560,7 +560,7 @@ __device__ __forceinline__ bool nr_step_b(double rhoi, double gradhi, double hi,
 // set, taken dynamically by a persistent grid.  Each item carries its leaf; the leaf its
 // set's mass, periodicity and box.  A cut item scans its set's tree for its own box
 // instead of streaming the leaf's whole list.
-template<bool Mixed, bool EvalAll>
+template<bool Mixed, bool EvalAll, bool Staged>
 __global__ void __launch_bounds__(kThreads, 5)   // 20 warps per SM (measured best of 4, 5, 6)
 density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restrict__ leafSet,
                      const uint2* __restrict__ range, const uint32_t* __restrict__ jOffset,
@@ -569,13 +569,17 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
                      const double* __restrict__ pmassSet, double tolh, double hfact, const DevBox* __restrict__ boxes,
                      int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
                      const int* __restrict__ setNodeStart, const int* __restrict__ leafPre,
-                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds, long long waitNs, int staged)
+                     const double* __restrict__ hmaxLeaf, DevScalars* __restrict__ ds, long long waitNs)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
-    __shared__ __align__(128) WarpStage sStage[kWarpsPerBlock];
+    __shared__ __align__(128) WarpStage sStage[Staged ? kWarpsPerBlock : 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    stage_init(sStage[wib]);
-    const StageRef stage{&sStage[wib], &ds->err, waitNs};
+    StageRef stage{nullptr, &ds->err, waitNs};
+    if constexpr (Staged)
+    {
+        stage_init(sStage[wib]);
+        stage.ws = &sStage[wib];
+    }
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     unsigned long long pairs = 0;
     for (;;)
@@ -596,7 +600,7 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
         double rhoi = 0.0, gradhi = 0.0;
         unsigned int gp = 0, gc = 0;
         auto src = list_source(jlist, jOffset[leaf], jcount[leaf], TableRanges{range}, xyzh);
-        if (staged) src.stage = stage;   // j ranges staged into shared memory by bulk copies
+        src.stage = stage;   // Staged: j ranges staged into shared memory by bulk copies
         if (w < nHeavy)
         {
             const double4 c = tree.center[leafPre[leaf]], h = tree.half[leafPre[leaf]];
@@ -613,7 +617,7 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
         // one engine instance for open and periodic sets (zero periods fold nothing): half
         // the code the warps of a mixed ensemble would otherwise share the instruction
         // cache with
-        density_group<true, Mixed>(sScr[wib], mine, d.ng, pi, per ? bxs.len[0] : 0.0, per ? bxs.len[1] : 0.0,
+        density_group<true, Mixed, Staged>(sScr[wib], mine, d.ng, pi, per ? bxs.len[0] : 0.0, per ? bxs.len[1] : 0.0,
                                    per ? bxs.len[2] : 0.0, src, rhoi, gradhi, gp, gc);
         if (EvalAll)
         {
@@ -876,10 +880,19 @@ static void run_items(Batch& B, const int* leaves, const int* countPtr, bool eva
             B.items.get(), cap, B.leafSet.get(), B.leafRange.get(), B.jOffset.get(), B.jcount.get(), B.jlist.get(),
             B.xyzh.get(), B.rho.get(), B.gradh.get(), B.converged.get(), B.pmass.get(), tolh, hfact, B.boxes.get(),
             B.leafNext.get(), B.activeB.get(), tree, B.setNodeStart.get(), B.leafPre.get(), B.hmaxLeaf.get(), ds,
-            wait_limit_ns(), s.staging);
+            wait_limit_ns());
     };
-    if (evalAll) { if (s.precision == 1) go(density_batch_kernel<true, true>); else go(density_batch_kernel<false, true>); }
-    else { if (s.precision == 1) go(density_batch_kernel<true, false>); else go(density_batch_kernel<false, false>); }
+    const bool mx = s.precision == 1, st = s.staging != 0;
+    if (evalAll)
+    {
+        if (mx) st ? go(density_batch_kernel<true, true, true>) : go(density_batch_kernel<true, true, false>);
+        else st ? go(density_batch_kernel<false, true, true>) : go(density_batch_kernel<false, true, false>);
+    }
+    else
+    {
+        if (mx) st ? go(density_batch_kernel<true, false, true>) : go(density_batch_kernel<true, false, false>);
+        else st ? go(density_batch_kernel<false, false, true>) : go(density_batch_kernel<false, false, false>);
+    }
     COSMO_LAUNCHED();
 }
 

@@ -377,14 +377,17 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                           : RowSplit{nullptr, nullptr, 0, nullptr});
             COSMO_LAUNCHED();
             const bool mx = s.precision == 1;
-            NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic)
-                               : (s.periodic ? density_nr_kernel<true, false> : density_nr_kernel<false, false>);
+            NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic, s.staging)
+                          : s.staging ? (s.periodic ? density_nr_kernel<true, false, true>
+                                                    : density_nr_kernel<false, false, true>)
+                                      : (s.periodic ? density_nr_kernel<true, false, false>
+                                                    : density_nr_kernel<false, false, false>);
             nr<<<persistent_grid(s, nr, kThreads), kThreads, 0, s.st>>>(
                 s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
                 s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
                 s.leafNext.get(), s.activeB.get(),
                 PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
-                s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns(), s.staging);
+                s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns());
             COSMO_LAUNCHED();
             if (rowsReady)
             {

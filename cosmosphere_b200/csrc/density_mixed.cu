@@ -9,9 +9,10 @@
 
 namespace cosmo {
 
-NrKernelFn mixed_density_nr_kernel(bool periodic)
+NrKernelFn mixed_density_nr_kernel(bool periodic, bool staged)
 {
-    return periodic ? density_nr_kernel<true, true> : density_nr_kernel<false, true>;
+    if (staged) return periodic ? density_nr_kernel<true, true, true> : density_nr_kernel<false, true, true>;
+    return periodic ? density_nr_kernel<true, true, false> : density_nr_kernel<false, true, false>;
 }
 
 RowsKernelFn mixed_newton_rows_kernel(bool periodic)

@@ -43,12 +43,23 @@ __device__ inline double xi_limiter_m(const double g[9])
     return (fac + trS > 2.220446049250313e-16) ? fac / (fac + trS) : 1.0;
 }
 
-// The mixed form's sums of the post-convergence sweep for one particle: FP32 pair terms
-// with Kahan compensation, combined in FP64, and the FP64 finish of the plain form
-// (src/density_base.cu:635-713).
+// The mixed form's sums of the post-convergence sweep for one particle: FP32 pair terms,
+// rho, d(rho)/dh and div v with Kahan compensation, the 24 velocity- and acceleration-
+// gradient and R-matrix sums as plain FP32 sums (the compensation of 24 more sums held
+// the kernel at 128 registers, four blocks per SM, on a pass that waits on its gathers);
+// all combined in FP64 for the FP64 finish of the plain form (src/density_base.cu:
+// 635-713).  Their error against the FP64 form is measured with the rest.
+struct SumF
+{
+    float s = 0.0f;
+    __device__ __forceinline__ void add(float x) { s += x; }
+    __device__ __forceinline__ double value() const { return double(s); }
+};
+
 struct GradSumsF
 {
-    KahanF srho, sgh, sdiv, sdv[9], sda[9], sr[6];
+    KahanF srho, sgh, sdiv;
+    SumF sdv[9], sda[9], sr[6];
     unsigned int gp = 0;
 
     // One pair: FP32 separation (dx, dy, dz) at the nearest image, r^2 and q^2.
@@ -222,7 +233,7 @@ gradient_mixed_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_
 // by the FP64 test; the separation is formed in FP64 at the nearest image and rounded to
 // FP32, the pair terms are the group path's.
 template<bool Periodic>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 6)
 gradient_row_mixed_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict__ nblCount,
                           const double4* __restrict__ xyzh, const double4* __restrict__ vel4,
                           const double4* __restrict__ acc4, double* __restrict__ rho, double* __restrict__ gradh,

@@ -73,7 +73,14 @@ __device__ __forceinline__ bool newton_step(double rhoi, double gradhi, double h
 // A warp whose group keeps an unconverged particle queues the leaf for the next
 // iteration (once per leaf), and flags the lists stale when an updated h outgrows the
 // radius its leaf's list covers.
-template<bool Periodic, bool Mixed>
+// One Newton iteration over the work items, taken dynamically by a persistent grid of
+// warps: each item's group sums come from density_group (plain FP64, bit for bit the
+// oracle's; or mixed), then the FP64 Newton-Raphson step of src/density_base.cu:294-333.
+// A warp whose group keeps an unconverged particle queues the leaf for the next
+// iteration (once per leaf), and flags the lists stale when an updated h outgrows the
+// radius its leaf's list covers.  Staged: the group's j-stream is staged into shared
+// memory by bulk copies (the WarpStage of its warp) instead of loaded directly.
+template<bool Periodic, bool Mixed, bool Staged>
 __global__ void __launch_bounds__(kThreads, Mixed ? 6 : 5)
 density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
@@ -82,13 +89,12 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
                   double hfact, const DevBox* __restrict__ box, const double* __restrict__ listH,
                   int* __restrict__ leafNext, int* __restrict__ nextLeaves, PreorderTree tree,
                   const int* __restrict__ leafToInternal, const double* __restrict__ centers,
-                  const double* __restrict__ sizes, DevScalars* __restrict__ ds, long long waitNs, int staged)
+                  const double* __restrict__ sizes, DevScalars* __restrict__ ds, long long waitNs)
 {
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][DensScratch<Mixed>::kBytes];
-    __shared__ __align__(128) WarpStage sStage[kWarpsPerBlock];
+    __shared__ __align__(128) WarpStage sStage[Staged ? kWarpsPerBlock : 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    stage_init(sStage[wib]);
-    const StageRef stage{&sStage[wib], &ds->err, waitNs};
+    if constexpr (Staged) stage_init(sStage[wib]);
     double lx = 0, ly = 0, lz = 0;
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
@@ -110,7 +116,7 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
         // a cut group (its leaf's list streams far more than it needs) scans the tree for
         // its own box instead, within the region its leaf's list covers
         auto src = list_source(jlist, jOffset[leaf], jcount[leaf], LayoutRanges{layout}, xyzh);
-        if (staged) src.stage = stage;   // j ranges staged into shared memory by bulk copies
+        if constexpr (Staged) src.stage = StageRef{&sStage[wib], &ds->err, waitNs};   // bulk-copy staging
         if (w < nHeavy)
         {
             const int in = leafToInternal[leaf];
@@ -120,7 +126,7 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
             src.rc = make_double3(centers[3 * in], centers[3 * in + 1], centers[3 * in + 2]);
             src.re = make_double3(sizes[3 * in] + ext, sizes[3 * in + 1] + ext, sizes[3 * in + 2] + ext);
         }
-        density_group<Periodic, Mixed>(sScr[wib], mine, d.ng, pi, lx, ly, lz, src, rhoi, gradhi, gp, gc);
+        density_group<Periodic, Mixed, Staged>(sScr[wib], mine, d.ng, pi, lx, ly, lz, src, rhoi, gradhi, gp, gc);
         bool stillActive = false, settle = false;
         if (mine)
         {
@@ -299,12 +305,12 @@ density_row_kernel(const int* __restrict__ rowItems, const void* __restrict__ ro
 } // namespace
 
 // The three Newton kernels share one signature per kind whatever the form.
-using NrKernelFn = decltype(&density_nr_kernel<false, false>);
+using NrKernelFn = decltype(&density_nr_kernel<false, false, false>);
 using RowsKernelFn = decltype(&newton_rows_kernel<false, false>);
 using RowKernelFn = decltype(&density_row_kernel<false, false>);
 
 // The mixed form's kernels, compiled in density_mixed.cu.
-NrKernelFn mixed_density_nr_kernel(bool periodic);
+NrKernelFn mixed_density_nr_kernel(bool periodic, bool staged);
 RowsKernelFn mixed_newton_rows_kernel(bool periodic);
 RowKernelFn mixed_density_row_kernel(bool periodic);
 

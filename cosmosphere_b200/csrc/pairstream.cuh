@@ -129,7 +129,7 @@ __device__ __forceinline__ double image_offset(double x, double c, double L)
 // on every lane.  The ring keeps what the caller asks for: the FP64 xyzh (Dbl), an FP32
 // copy relative to the group box centre at the nearest periodic image when lx, ly, lz > 0
 // (Float), and the particle index (Index).
-template<bool Dbl, bool Float, bool Index>
+template<bool Dbl, bool Float, bool Index, bool Staged = false>
 struct CandidateRing
 {
     double4* ring;
@@ -157,11 +157,12 @@ struct CandidateRing
     __device__ __forceinline__ void feed(uint32_t s0, uint32_t len, int nb, const double4* __restrict__ xyzh,
                                          Filter& filter, Batch& batch)
     {
-        if (stage.ws != nullptr && stage.ws->broken == 0u)
-        {
-            feed_staged(s0, len, nb, xyzh, filter, batch);
-            return;
-        }
+        if constexpr (Staged)
+            if (stage.ws->broken == 0u)
+            {
+                feed_staged(s0, len, nb, xyzh, filter, batch);
+                return;
+            }
         const int lane = threadIdx.x & 31;
         const uint32_t lt = (1u << lane) - 1u;
         const uint32_t incl = warp_incl_scan_u32(len);
@@ -335,7 +336,7 @@ struct CandidateRing
 
 // Stream the j particles of one i-leaf list (entries jb .. jb + nj of jlist, in order)
 // through the group filter into the ring, 32 list entries at a time.
-template<bool Dbl, bool Float, bool Index, class Ranges, class Filter, class Batch>
+template<bool Dbl, bool Float, bool Index, bool Staged = false, class Ranges, class Filter, class Batch>
 __device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
                                               double cz, double lx, double ly, double lz, uint32_t jb, uint32_t nj,
                                               const int* __restrict__ jlist, Ranges ranges,
@@ -343,7 +344,7 @@ __device__ __forceinline__ void stream_ranges(double4* ring, float4* ringf, int*
                                               StageRef stage = StageRef{nullptr, nullptr, 0})
 {
     const int lane = threadIdx.x & 31;
-    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, lx, ly, lz, stage};
+    CandidateRing<Dbl, Float, Index, Staged> cr{ring, ringf, ringIdx, cx, cy, cz, lx, ly, lz, stage};
     for (uint32_t lb = 0; lb < nj; lb += 32)
     {
         const int nb = int(min(32u, nj - lb));
@@ -375,7 +376,8 @@ struct PreorderTree
 // stackless pre-order scan of the tree 32 nodes at a time (the scan of list_walk_kernel):
 // leaves come out in ascending order, so the stream is in ascending j as a list's is.
 // Used for groups whose leaf list is far longer than their own search region needs.
-template<bool Dbl, bool Float, bool Index, bool Periodic, class Ranges, class Filter, class Batch>
+template<bool Dbl, bool Float, bool Index, bool Periodic, bool Staged = false, class Ranges, class Filter,
+         class Batch>
 __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
                                             double cz, double sx, double sy, double sz, const PreorderTree& t,
                                             double3 c, double3 e, double3 rc, double3 re, double lx, double ly,
@@ -383,7 +385,7 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
                                             Filter filter, Batch batch, StageRef stage = StageRef{nullptr, nullptr, 0})
 {
     const int lane = threadIdx.x & 31;
-    CandidateRing<Dbl, Float, Index> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz, stage};
+    CandidateRing<Dbl, Float, Index, Staged> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz, stage};
     auto fold = [&](double d, double L) { return (Periodic && L > 0.0) ? fmin(d, L - d) : d; };
     int p = t.n0;
     while (p < t.n1)
@@ -459,19 +461,19 @@ struct GroupSource
     double3 rc, re;
     StageRef stage;   // the warp's bulk-copy stage, or none (direct loads)
 
-    template<bool Dbl, bool Float, bool Index, bool Periodic, class Filter, class Batch>
+    template<bool Dbl, bool Float, bool Index, bool Periodic, bool Staged = false, class Filter, class Batch>
     __device__ __forceinline__ void stream(double4* ring, float4* ringf, int* ringIdx, const GroupBox& bx, double sx,
                                            double sy, double sz, double lx, double ly, double lz, Filter filter,
                                            Batch batch) const
     {
         if (walk)
-            stream_walk<Dbl, Float, Index, Periodic>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, tree,
+            stream_walk<Dbl, Float, Index, Periodic, Staged>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, tree,
                                                      make_double3(bx.cx, bx.cy, bx.cz),
                                                      make_double3(bx.ex, bx.ey, bx.ez), rc, re, lx, ly, lz, ranges,
                                                      xyzh, filter, batch, stage);
         else
-            stream_ranges<Dbl, Float, Index>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, jb, nj, jlist,
-                                             ranges, xyzh, filter, batch, stage);
+            stream_ranges<Dbl, Float, Index, Staged>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, jb, nj,
+                                                     jlist, ranges, xyzh, filter, batch, stage);
     }
 };
 
