@@ -531,6 +531,48 @@ uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool
     return uint32_t(s.hsmall[0]);
 }
 
+__global__ void level_keys_kernel(const uint64_t* __restrict__ prefix, int n, uint64_t* __restrict__ lvl)
+{
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) lvl[i] = uint64_t(prefix_level(prefix[i]));
+}
+
+__global__ void gather_prefix_kernel(const uint64_t* __restrict__ prePrefix, const int* __restrict__ bfsToPre, int n,
+                                     uint64_t* __restrict__ bfsPrefix)
+{
+    const long b = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (b < n) bfsPrefix[b] = prePrefix[bfsToPre[b]];
+}
+
+// bfsToPre / bfsPrefix: the pre-order nodes partitioned stably by level (one onesweep
+// pass on the level, below 256), which is their order by prefix.
+static void sort_nodes_by_level(State& s, int n)
+{
+    const int tiles = iceil(n, kSortTile);
+    s.sortHist.resize(kSortPasses * 256, s.st);
+    s.sortBase.resize(kSortPasses * 256, s.st);
+    s.sortLookback.resize(size_t(kSortPasses) * tiles * 256, s.st);
+    DevScalars* ds = s.dscal.get();
+    COSMO_CUDA(cudaMemsetAsync(s.sortHist.get(), 0, kSortPasses * 256 * sizeof(uint32_t), s.st));
+    COSMO_CUDA(cudaMemsetAsync(s.sortLookback.get(), 0, size_t(tiles) * 256 * sizeof(uint32_t), s.st));
+    COSMO_CUDA(cudaMemsetAsync(&ds->sortTiles[0], 0, sizeof(unsigned int), s.st));
+    level_keys_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.prePrefix.get(), n, s.nodeKeysTmp.get());
+    COSMO_LAUNCHED();
+    digit_hist_kernel<<<std::min(iceil(n, kBlk), 4 * s.numSMs), kBlk, 0, s.st>>>(s.nodeKeysTmp.get(), n,
+                                                                                 s.sortHist.get());
+    COSMO_LAUNCHED();
+    digit_base_kernel<<<kSortPasses, 256, 0, s.st>>>(s.sortHist.get(), s.sortBase.get());
+    COSMO_LAUNCHED();
+    // keys out into bfsPrefix (overwritten by the gather below), pre-order indices into bfsToPre
+    onesweep_kernel<<<tiles, kSortThreads, 0, s.st>>>(s.nodeKeysTmp.get(), nullptr, s.bfsPrefix.get(),
+                                                     s.bfsToPre.get(), n, 0, s.sortBase.get(), s.sortLookback.get(),
+                                                     &ds->sortTiles[0], &ds->err, wait_limit_ns());
+    COSMO_LAUNCHED();
+    gather_prefix_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.prePrefix.get(), s.bfsToPre.get(), n,
+                                                            s.bfsPrefix.get());
+    COSMO_LAUNCHED();
+}
+
 void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int n, bool iotaValues)
 {
     if (n <= 0) return;
@@ -723,13 +765,11 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
     node_emit_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.csTree.get(), nL, s.leafPreStart.get(), numNodes,
                                                          s.prePrefix.get(), s.preLeaf.get(), s.preSkip.get());
     COSMO_LAUNCHED();
-    // sort (prefix, pre-order index); prePrefix is the key ping-pong partner
-    COSMO_CUDA(cudaMemcpyAsync(s.bfsPrefix.get(), s.prePrefix.get(), size_t(numNodes) * 8,
-                               cudaMemcpyDeviceToDevice, s.st));
+    // BFS order = the nodes sorted by prefix, i.e. by (level, key).  Pre-order already has
+    // every level's nodes in ascending key, so the sort is a stable partition of the
+    // pre-order sequence by level: one counting pass on the level.
     s.nodeKeysTmp.resize(numNodes, s.st);
-    s.nodeValsTmp.resize(numNodes, s.st);
-    radix_sort_u64(s, s.bfsPrefix.get(), s.nodeKeysTmp.get(), s.bfsToPre.get(), s.nodeValsTmp.get(), numNodes,
-                   true);
+    sort_nodes_by_level(s, numNodes);
     cudaEvent_t e3 = ev(s);
 
     bfs_link_kernel<<<iceil(numNodes, kBlk), kBlk, 0, s.st>>>(
