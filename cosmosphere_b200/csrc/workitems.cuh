@@ -119,23 +119,37 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
             if (nC == 0) continue;
             const int wnd = int((g - p0) >> 6);
             const int whole = (nC + 31) >> 5;
-            // A window whose smoothing lengths spread by more than kGroupSpread is cut into
-            // one-particle items: a group's box is set by its widest particle, so in a spread
-            // window every particle would test the candidates of the widest one's search
-            // region; alone, each scans the tree for its own box.  Grouping changes no
-            // result (every particle's sums run over the same pairs in j order).
+            // A window whose smoothing lengths spread by more than kGroupSpread is grouped by
+            // h (ranks in ascending h) into at least two groups: a group's box is set by its
+            // widest particle, so the narrow ones keep a box nearer their own size.  Grouping
+            // changes no result (every particle's sums run over the same pairs in j order).
             const double inf = __longlong_as_double(0x7ff0000000000000ll);
             const double h0 = act0 ? xyzh[a0].w : inf, h1 = act1 ? xyzh[a1].w : inf;
             const double hmin = warp_min(fmin(h0, h1));
             const double hmax = warp_max(fmax(act0 ? h0 : 0.0, act1 ? h1 : 0.0));
-            const int gsz = (nC > 1 && hmax > kGroupSpread * hmin) ? 1 : gsize;
-            const int G = max(whole, (nC + gsz - 1) / gsz);
-            const bool split = G > whole;   // cut items scan the tree for their own box
+            const bool byH = nC > 1 && hmax > kGroupSpread * hmin;
+            const int cutG = (nC + gsize - 1) / gsize;
+            const int G = max(byH ? max(whole, 2) : whole, cutG);
+            const bool split = cutG > whole;   // cut items (long streams) scan the tree for their box
             int base = 0;
             if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
             base = __shfl_sync(0xffffffffu, base, 0);
-            // group k takes the active ranks [k nC / G, (k + 1) nC / G)
-            const int r0 = __popc(c0 & lt), r1 = __popc(c0) + __popc(c1 & lt);
+            // group k takes the active ranks [k nC / G, (k + 1) nC / G): in slot order, or in
+            // (h, slot) order for a spread window
+            int r0 = __popc(c0 & lt), r1 = __popc(c0) + __popc(c1 & lt);
+            if (byH)
+            {
+                int k0 = 0, k1 = 0;
+                for (int t = 0; t < 32; ++t)
+                {
+                    const double u0 = __shfl_sync(0xffffffffu, h0, t), u1 = __shfl_sync(0xffffffffu, h1, t);
+                    // slots t and 32 + t against this lane's two slots (inactive slots hold inf)
+                    k0 += (u0 < h0 || (u0 == h0 && t < lane)) + (u1 < h0);
+                    k1 += (u0 < h1 || u0 == h1) + (u1 < h1 || (u1 == h1 && t < lane));
+                }
+                r0 = k0;
+                r1 = k1;
+            }
             for (int k = 0; k < G; ++k)
             {
                 const int lo = k * nC / G, hi = (k + 1) * nC / G;
