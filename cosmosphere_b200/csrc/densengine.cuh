@@ -74,9 +74,11 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                 const double4 pj = rg[(head + (lane < count ? lane : 0)) & (kRing - 1)];
                 if (ng == 1)
                 {
-                    // a single particle (a cut group): every lane evaluates its own pair and
-                    // the sums take the accepted lanes in order through shuffles -- the
-                    // serial chain is one add per accepted pair, as in the oracle's loop
+                    // a single particle (a cut group): every lane evaluates its own pair, the
+                    // accepted values are packed into the record buffers in lane (= j) order,
+                    // and the sums add them in that order from broadcast shared-memory loads
+                    // -- one add per accepted pair, as in the oracle's loop, so the chain is
+                    // bound by the add latency alone
                     const double4 g = grp[0];
                     double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                     nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
@@ -91,15 +93,21 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                         wv = wk;
                         tv = -q * dwk - 3.0 * wk;
                     }
-                    uint32_t am = __ballot_sync(0xffffffffu, acc);
-                    gp += __popc(am);
-                    while (am)
+                    const uint32_t am = __ballot_sync(0xffffffffu, acc);
+                    const int c = __popc(am);
+                    gp += c;
+                    if (acc)
                     {
-                        const int k = __ffs(am) - 1;
-                        am &= am - 1;
-                        sr += __shfl_sync(0xffffffffu, wv, k);
-                        sg += __shfl_sync(0xffffffffu, tv, k);
+                        recA[__popc(am & lt)] = wv;
+                        recB[__popc(am & lt)] = tv;
                     }
+                    __syncwarp();
+                    for (int t = 0; t < c; ++t)
+                    {
+                        sr += recA[t];
+                        sg += recB[t];
+                    }
+                    __syncwarp();
                     return;
                 }
                 int nrec = 0, segStart = 0, segCount = 0;
