@@ -709,6 +709,12 @@ int cosmo_x_set_option(const char* name, int value)
     const std::string k(name ? name : "");
     if (k == "staging") { s.staging = value != 0; return 0; }
     if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
+    if (k == "split_stream" || k == "split_work")
+    {
+        if (value < 0) return -1;
+        (k == "split_stream" ? s.splitStream : s.splitWork) = uint32_t(value);
+        return 0;
+    }
     return -1;
 }
 

@@ -55,6 +55,19 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
     const double rs = kRadKernel * hi;
     const double rmax = warp_max(mine ? rs : 0.0);
     const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
+    // A single particle (lane 0) filters its candidates, and cut groups their tree scan,
+    // by its own sphere: the support plus the box's slack (1e-9 of the support, 1e-13 of
+    // |x|), far above the rounding of the exact test, so no accepted pair is lost.
+    double4 sph = make_double4(0.0, 0.0, 0.0, -1.0);
+    if (ng == 1)
+    {
+        const double x0 = __shfl_sync(0xffffffffu, pi.x, 0), y0 = __shfl_sync(0xffffffffu, pi.y, 0);
+        const double z0 = __shfl_sync(0xffffffffu, pi.z, 0);
+        sph = make_double4(x0, y0, z0, rmax + 1e-9 * rmax + 1e-13 * (fabs(x0) + fabs(y0) + fabs(z0)) + 1e-300);
+    }
+    auto gather = [&](const double4& pj) {
+        return sph.w >= 0.0 ? in_gather_sphere<Periodic>(pj, sph, lx, ly, lz) : in_gather_box<Periodic>(pj, bx, lx, ly, lz);
+    };
     gp = 0;
     gc = 0;
     if constexpr (!Mixed)
@@ -67,8 +80,7 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         __syncwarp();
         double sr = 0.0, sg = 0.0;
         src.template stream<true, false, false, Periodic, Staged>(
-            ring, nullptr, nullptr, bx, 0.0, 0.0, 0.0, lx, ly, lz,
-            [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+            ring, nullptr, nullptr, bx, 0.0, 0.0, 0.0, lx, ly, lz, gather,
             [&](const double4* rg, const float4*, const int*, int head, int count) {
                 gc += count;
                 const double4 pj = rg[(head + (lane < count ? lane : 0)) & (kRing - 1)];
@@ -158,7 +170,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                     }
                 }
                 if (nrec > 0) flush();
-            });
+            },
+            sph);
         rhoi = sr;
         gradhi = sg;
     }
@@ -184,8 +197,7 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
         const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
         KahanF kr, kg, lr, lg;
         src.template stream<false, true, false, Periodic, Staged>(
-            nullptr, ringf, nullptr, bx, sx, sy, sz, lx, ly, lz,
-            [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
+            nullptr, ringf, nullptr, bx, sx, sy, sz, lx, ly, lz, gather,
             [&](const double4*, const float4* rf, const int*, int head, int count) {
                 gc += count;
                 const float4 pf = rf[(head + (lane < count ? lane : 0)) & (kRing - 1)];
@@ -283,7 +295,8 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                     }
                 }
                 if (nrec > 0) flush();
-            });
+            },
+            sph);
         rhoi = kr.value();
         gradhi = kg.value();
         if (ng == 1)

@@ -335,6 +335,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     // list, only the leaves whose hmax left their radius walk again.  hmaxLeaf is still refreshed
     // for the active leaves every iteration, as the reference does, so the exact lists of
     // the last iteration can be rebuilt afterwards.
+    FixedSplit cut;
+    if (s.splitStream > 0) cut.stream = s.splitStream;
+    if (s.splitWork > 0) cut.work = s.splitWork;
     bool listsValid = false, listsWidened = false, rowsReady = false;
     int settling0 = 0;
     cudaEvent_t e3 = ev(s);
@@ -357,7 +360,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 COSMO_LAUNCHED();
                 plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
                     s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(),
-                    s.xyzh.get(), s.items.get(), itemCap, ds);
+                    s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut);
                 COSMO_LAUNCHED();
                 RowsKernelFn nrows = s.precision == 1
                                          ? mixed_newton_rows_kernel(s.periodic)
@@ -374,7 +377,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(), s.xyzh.get(),
                 s.items.get(), itemCap, ds,
                 rowsReady ? RowSplit{s.nblCount.get(), s.nblH.get(), kNbl, s.rowItems.get()}
-                          : RowSplit{nullptr, nullptr, 0, nullptr});
+                          : RowSplit{nullptr, nullptr, 0, nullptr},
+                cut);
             COSMO_LAUNCHED();
             const bool mx = s.precision == 1;
             NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic, s.staging)

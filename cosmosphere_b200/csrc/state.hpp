@@ -130,6 +130,10 @@ struct State
     // row builder's tests through the FP32 prefilter (COSMO_SYM_PREFILTER).
     int staging = 0;
     int symPrefilter = 0;
+    // The Newton work queue's leaf cut (0 = the built-in figures): a leaf whose gather
+    // list streams more than splitStream particles is cut into groups of about
+    // splitWork / stream particles (cosmo_x_set_option "split_stream", "split_work").
+    uint32_t splitStream = 0, splitWork = 0;
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;

@@ -46,10 +46,12 @@ constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
 constexpr double kGroupSpread = 1.5;
 
-// The cut of one leaf: x = the stream above which it is cut, y = the work of one cut group.
+// The cut of one leaf: x = the stream above which it is cut, y = the work of one cut group
+// (the same for every leaf; kSplitStream and kSplitWork unless the caller sets others).
 struct FixedSplit
 {
-    __device__ __forceinline__ uint2 operator()(int) const { return make_uint2(kSplitStream, kSplitWork); }
+    uint32_t stream = kSplitStream, work = kSplitWork;
+    __device__ __forceinline__ uint2 operator()(int) const { return make_uint2(stream, work); }
 };
 
 // The cut of a forest leaf: its set's entry of a per-set table.
@@ -166,9 +168,10 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
                                   const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
                                   const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
                                   DevScalars* __restrict__ ds,
-                                  RowSplit rs = RowSplit{nullptr, nullptr, 0, nullptr})
+                                  RowSplit rs = RowSplit{nullptr, nullptr, 0, nullptr},
+                                  FixedSplit split = FixedSplit{})
 {
-    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, rs);
+    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, rs, split);
 }
 
 // The same over a forest's range table, the active count read on the device, each leaf

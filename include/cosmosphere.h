@@ -208,8 +208,11 @@ void cosmo_x_sync(void);
 /* Select a kernel variant of the single-set solve (results do not depend on it):
  * "staging" 1 stages the Newton kernels' j-stream into shared memory with bulk copies
  * (cp.async.bulk completing on an mbarrier), 0 (default) loads it directly;
- * "sym_prefilter" 1 puts the symmetric row builder's tests behind the FP32 prefilter.
- * Returns 0, or -1 for an unknown name. */
+ * "sym_prefilter" 1 puts the symmetric row builder's tests behind the FP32 prefilter;
+ * "split_stream" / "split_work" set the Newton work queue's leaf cut (a leaf whose gather
+ * list streams more than split_stream particles is cut into groups of about
+ * split_work / stream particles that scan the tree for their own box; 0 restores the
+ * built-in 4096 and 131072).  Returns 0, or -1 for an unknown name or a negative value. */
 int cosmo_x_set_option(const char* name, int value);
 
 /* Time limit of every bounded device wait (the sort's look-back on its predecessor

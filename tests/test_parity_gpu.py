@@ -379,3 +379,29 @@ def test_kernel_variants_keep_parity(option):
             check_all(cc, o)
         finally:
             c.set_option(option, 0)
+
+
+def test_one_particle_cut_items_keep_parity():
+    """With the leaf cut lowered so that nearly every leaf is cut into one-particle items
+    (each scanning the tree for the cells on its own support sphere, and filtering its
+    candidates by that sphere), every structure and field still equals the oracle's bit
+    for bit: a log-normal quintic Plummer sphere, and the jiggled periodic lattice."""
+    for quintic in (True, False):
+        c = capi.Cosmo(quintic)
+        assert c.set_option("split_stream", 64) == 0 and c.set_option("split_work", 32) == 0
+        try:
+            if quintic:
+                p = inputs.plummer(12000, lnsigma=0.5, seed=23)
+                cc, o = run_pair(p, quintic=True)
+            else:
+                x, y, z = (np.asarray(v).ravel() for v in np.meshgrid(*(np.arange(12) / 12.0,) * 3, indexing="ij"))
+                n = x.size
+                rng = np.random.default_rng(5)
+                p = inputs.Particles(x=(x + rng.uniform(0, 0.02, n)) % 1.0, y=(y + rng.uniform(0, 0.02, n)) % 1.0,
+                                     z=(z + rng.uniform(0, 0.02, n)) % 1.0, h=np.full(n, 1.2 / 12), pmass=1.0 / n)
+                inputs.jiggle_frac(p["h"], 0.05, 0.65, 1.35, 6)
+                cc, o = run_pair(p, box=[0.0, 1.0, 0.0, 1.0, 0.0, 1.0])
+            check_all(cc, o)
+        finally:
+            c.set_option("split_stream", 0)
+            c.set_option("split_work", 0)
