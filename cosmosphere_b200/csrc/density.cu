@@ -347,7 +347,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         hmax_leaves(s, s.activeA.get(), nActiveLeaves);
         if (!listsValid)
         {
-            build_lists(s, false, kListMargin, listsWidened);   // after the first: only outgrown leaves walk
+            // widened, rounded lists; after the first build only outgrown leaves walk
+            build_lists(s, false, kListMargin, listsWidened, true);
             listsValid = listsWidened = true;
         }
         cudaEvent_t j1 = ev(s);

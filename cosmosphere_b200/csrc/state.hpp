@@ -200,7 +200,7 @@ void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
 // Gather (symmetric = false) or symmetric j-leaf lists for all leaves.  margin > 1 widens
 // the gather radius to R * hmax * margin, so the lists stay valid while h grows by up to
 // that factor; listH records the h each leaf's list covers.
-void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental = false);
+void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental = false, bool rounded = false);
 // The symmetric lists and the symmetric neighbour rows of the current tree and h (the
 // force pass's pairs; every gather pair of the converged h is among them).
 void build_symmetric(State& s);

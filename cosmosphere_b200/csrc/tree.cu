@@ -355,6 +355,12 @@ constexpr int kWalkScratch = 512;     // list entries per leaf the count pass ke
 // node is followed by its successor in pre-order), so their leaves are emitted in order,
 // and the scan resumes after the rejected node's subtree.  Accepted leaves therefore come
 // out in ascending order, nothing is stacked, and nothing can be dropped.
+// Gather test: a node is taken when its cell overlaps the i-leaf's cell widened by the
+// search radius on every axis (include/tree.cuh's test, the lists callers read), or, with
+// rounded set (the Newton loop's own lists), when its cell lies within the search radius
+// of the i-leaf's cell -- the Euclidean gap, so the cube's corners are left out.  Every
+// pair within the radius still has its j-leaf in the list, and a leaf with a large h
+// near the edge of a concentrated set no longer takes in the dense centre its cube reaches.
 template<bool Symmetric, bool Periodic, bool Fill>
 __global__ void __launch_bounds__(kBlk)
 list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
@@ -366,7 +372,8 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const uint32_t* __restrict__ jOffset, int* __restrict__ jlist, int* err,
                  const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
                  double* __restrict__ listH, const uint32_t* __restrict__ jOffsetPrev,
-                 const int* __restrict__ jlistPrev, int* __restrict__ walked, int* __restrict__ scratch)
+                 const int* __restrict__ jlistPrev, int* __restrict__ walked, int* __restrict__ scratch,
+                 int rounded)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -412,6 +419,9 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
     const double isx = sizes[3 * iNode], isy = sizes[3 * iNode + 1], isz = sizes[3 * iNode + 2];
     hmax *= margin;
     const double radHi = kRadKernel * hmax;
+    // the rounded test's radius, with the slack of the group boxes (1e-9 of the radius,
+    // 1e-13 of |centre|) above the rounding of the gaps
+    const double radR = radHi + 1e-9 * radHi + 1e-13 * (fabs(icx) + fabs(icy) + fabs(icz));
     // gather: the i-box inflated by radHi; symmetric: the raw i-box
     const double ax = Symmetric ? isx : isx + radHi;
     const double ay = Symmetric ? isy : isy + radHi;
@@ -448,6 +458,12 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
             {
                 const double rs = fmax(radHi, kRadKernel * hmaxPre[idx]);
                 accept = n2 <= rs * rs;
+            }
+            else if (rounded)
+            {
+                const double e0 = fmax(dd[0] - isx - s.x, 0.0), e1 = fmax(dd[1] - isy - s.y, 0.0);
+                const double e2 = fmax(dd[2] - isz - s.z, 0.0);
+                accept = e0 * e0 + e1 * e1 + e2 * e2 <= radR * radR;
             }
             else accept = n2 <= 0.0;
             skip = preSkip[idx];
@@ -825,7 +841,7 @@ void hmax_upsweep(State& s)
 }
 
 template<bool Sym, bool Per>
-static void walk(State& s, bool fill, double margin, bool incremental)
+static void walk(State& s, bool fill, double margin, bool incremental, bool rounded)
 {
     const int nL = s.nLeaves;
     const int blocks = iceil(long(nL) * 32, kBlk);
@@ -838,7 +854,8 @@ static void walk(State& s, bool fill, double margin, bool incremental)
                                         (!fill && !Sym) ? s.listH.get() : nullptr,
                                         incremental ? s.jOffsetPrev.get() : nullptr,
                                         incremental ? s.jlistPrev.get() : nullptr,
-                                        incremental ? s.walked.get() : nullptr, s.walkScratch.get());
+                                        incremental ? s.walked.get() : nullptr, s.walkScratch.get(),
+                                        rounded ? 1 : 0);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
@@ -848,8 +865,9 @@ static void walk(State& s, bool fill, double margin, bool incremental)
 // include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.  incremental
 // (gather lists only, over the gather lists of the same tree at the same margin): the
 // current lists are kept aside first, and only the leaves whose hmax outgrew them walk.
-void build_lists(State& s, bool symmetric, double margin, bool incremental)
+void build_lists(State& s, bool symmetric, double margin, bool incremental, bool rounded)
 {
+    rounded = rounded && !symmetric;
     const int nL = s.nLeaves;
     incremental = incremental && !symmetric && !s.listsSym && nL > 0;
     if (incremental)
@@ -867,13 +885,13 @@ void build_lists(State& s, bool symmetric, double margin, bool incremental)
     auto run = [&](bool fill) {
         if (symmetric)
         {
-            if (s.periodic) walk<true, true>(s, fill, margin, false);
-            else walk<true, false>(s, fill, margin, false);
+            if (s.periodic) walk<true, true>(s, fill, margin, false, false);
+            else walk<true, false>(s, fill, margin, false, false);
         }
         else
         {
-            if (s.periodic) walk<false, true>(s, fill, margin, incremental);
-            else walk<false, false>(s, fill, margin, incremental);
+            if (s.periodic) walk<false, true>(s, fill, margin, incremental, rounded);
+            else walk<false, false>(s, fill, margin, incremental, rounded);
         }
     };
     run(false);
