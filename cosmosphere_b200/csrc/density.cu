@@ -339,7 +339,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     if (s.splitStream > 0) cut.stream = s.splitStream;
     if (s.splitWork > 0) cut.work = s.splitWork;
     bool listsValid = false, listsWidened = false, rowsReady = false;
-    int settling0 = 0;
+    long long settlingPrev = 0;
     cudaEvent_t e3 = ev(s);
     for (int iter = 0; iter < maxIter; ++iter)
     {
@@ -354,9 +354,10 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         cudaEvent_t j1 = ev(s);
         {
             const int bgrid = std::min(iceil(nL, 256), 4 * s.numSMs);
-            if (iter == 1 && nActiveParticles > 0 && 5 * (long long)settling0 >= 4 * (long long)s.activePerIter[0])
+            if (!rowsReady && iter >= 1 && nActiveParticles > 0 &&
+                5 * (long long)settlingPrev >= 4 * (long long)s.activePerIter[iter - 1])
             {
-                // rows of the still-active particles at their h after the first update
+                // rows of the still-active particles at their h after the last update
                 begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
                 COSMO_LAUNCHED();
                 plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
@@ -413,7 +414,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         s.itersRun = iter + 1;
         nActiveLeaves = s.hscal->nextActive;
         nActiveParticles = s.hscal->unconverged;
-        if (iter == 0) settling0 = s.settling0 = s.hscal->settling;
+        settlingPrev = s.hscal->settling;
+        if (iter == 0) s.settling0 = settlingPrev;
         if (s.hscal->listStale) listsValid = false;
         std::swap(s.activeA, s.activeB);
         if (nActiveParticles == 0) break;

@@ -25,9 +25,9 @@ constexpr int kThreads = 32 * kWarpsPerBlock;
 
 constexpr double kListMargin = 1.15;            // gather-radius widening of the Newton lists
 // Newton rows: each still-active particle's j within kRowMargin of its support at its h
-// after the first update, built when at least 80% of the particles are settling (moved
-// by less than kSettle in that update), for the iterations after it; where fewer settle,
-// too many rows would go stale before they are used.
+// after an update, built once, after the first update in which at least 80% of the
+// particles it moved are settling (still active, moved by less than kSettle), for the
+// iterations after it; while fewer settle, too many rows would go stale before use.
 constexpr double kRowMargin = 1.1;
 constexpr double kSettle = 0.15;
 
