@@ -354,8 +354,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         cudaEvent_t j1 = ev(s);
         {
             const int bgrid = std::min(iceil(nL, 256), 4 * s.numSMs);
-            if (!rowsReady && iter >= 1 && nActiveParticles > 0 &&
-                5 * (long long)settlingPrev >= 4 * (long long)s.activePerIter[iter - 1])
+            if (!rowsReady && iter >= 1 && nActiveParticles > 0 && 5 * settlingPrev >= 4 * nActiveParticles)
             {
                 // rows of the still-active particles at their h after the last update
                 begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);

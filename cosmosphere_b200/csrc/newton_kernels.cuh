@@ -25,9 +25,9 @@ constexpr int kThreads = 32 * kWarpsPerBlock;
 
 constexpr double kListMargin = 1.15;            // gather-radius widening of the Newton lists
 // Newton rows: each still-active particle's j within kRowMargin of its support at its h
-// after an update, built once, after the first update in which at least 80% of the
-// particles it moved are settling (still active, moved by less than kSettle), for the
-// iterations after it; while fewer settle, too many rows would go stale before use.
+// after an update, built once, after the first update that leaves at least 80% of the
+// still-active particles settling (moved by less than kSettle), for the iterations after
+// it; while fewer settle, too many rows would go stale before use.
 constexpr double kRowMargin = 1.1;
 constexpr double kSettle = 0.15;
 
