@@ -911,9 +911,10 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
                                                         / max(1, head["nr_launches"]),
                      "traffic": (ncu_traffic("newton_stage_per_iteration")
                                  if args.workload == "lattice100" and args.npartx == 100 and not quintic else None),
-                     "traffic_note": "DRAM bytes per Newton iteration from ncu (profiles/traffic.json); above the "
-                                     "algorithmic bytes because the Newton rows (r^2 per pair) are written once "
-                                     "and streamed by the later iterations",
+                     "traffic_note": "DRAM bytes per Newton iteration assembled from one-kernel ncu captures "
+                                     "(profiles/traffic.json, method in its note); above the algorithmic bytes "
+                                     "because the Newton rows (r^2 per pair) are written once and streamed by the "
+                                     "later iterations",
                      "fp64": {"achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                               "flop_convention": "30 FLOP per accepted pair + 30 per Newton update",
                               "peak_source": "FP64 FMA microkernel run in this bench "
