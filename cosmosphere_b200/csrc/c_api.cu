@@ -118,6 +118,7 @@ void ensure_init(State& s)
     if (const char* e = std::getenv("COSMO_PRECISION")) s.precision = (std::string(e) == "mixed") ? 1 : 0;
     if (const char* e = std::getenv("COSMO_STAGING")) s.staging = std::atoi(e) != 0;
     if (const char* e = std::getenv("COSMO_SYM_PREFILTER")) s.symPrefilter = std::atoi(e) != 0;
+    if (const char* e = std::getenv("COSMO_SPREAD_GROUPS")) s.spreadGroups = std::max(0, std::min(32, std::atoi(e)));
 }
 
 size_t state_device_bytes(const State& s)
@@ -709,6 +710,12 @@ int cosmo_x_set_option(const char* name, int value)
     const std::string k(name ? name : "");
     if (k == "staging") { s.staging = value != 0; return 0; }
     if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
+    if (k == "spread_groups")
+    {
+        if (value < 0 || value > 32) return -1;
+        s.spreadGroups = value;
+        return 0;
+    }
     if (k == "split_stream" || k == "split_work")
     {
         if (value < 0) return -1;

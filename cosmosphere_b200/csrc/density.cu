@@ -338,6 +338,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     FixedSplit cut;
     if (s.splitStream > 0) cut.stream = s.splitStream;
     if (s.splitWork > 0) cut.work = s.splitWork;
+    const int spreadG = s.spreadGroups > 0 ? s.spreadGroups : kSpreadGroups;
     bool listsValid = false, listsWidened = false, rowsReady = false;
     long long settlingPrev = 0;
     cudaEvent_t e3 = ev(s);
@@ -348,7 +349,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         if (!listsValid)
         {
             // widened, rounded lists; after the first build only outgrown leaves walk
-            build_lists(s, false, kListMargin, listsWidened, true);
+            build_lists(s, false, kListMargin, listsWidened, true, cut.work);
             listsValid = listsWidened = true;
         }
         cudaEvent_t j1 = ev(s);
@@ -361,7 +362,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 COSMO_LAUNCHED();
                 plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
                     s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(),
-                    s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut);
+                    s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
                 COSMO_LAUNCHED();
                 RowsKernelFn nrows = s.precision == 1
                                          ? mixed_newton_rows_kernel(s.periodic)
@@ -379,7 +380,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 s.items.get(), itemCap, ds,
                 rowsReady ? RowSplit{s.nblCount.get(), s.nblH.get(), kNbl, s.rowItems.get()}
                           : RowSplit{nullptr, nullptr, 0, nullptr},
-                cut);
+                cut, spreadG);
             COSMO_LAUNCHED();
             const bool mx = s.precision == 1;
             NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic, s.staging)

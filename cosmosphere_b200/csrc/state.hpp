@@ -134,6 +134,9 @@ struct State
     // list streams more than splitStream particles is cut into groups of about
     // splitWork / stream particles (cosmo_x_set_option "split_stream", "split_work").
     uint32_t splitStream = 0, splitWork = 0;
+    // h-ordered groups a window whose h spreads is cut into, at least (0 = built-in 2;
+    // cosmo_x_set_option "spread_groups")
+    int spreadGroups = 0;
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;
@@ -200,7 +203,8 @@ void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
 // Gather (symmetric = false) or symmetric j-leaf lists for all leaves.  margin > 1 widens
 // the gather radius to R * hmax * margin, so the lists stay valid while h grows by up to
 // that factor; listH records the h each leaf's list covers.
-void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental = false, bool rounded = false);
+void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental = false, bool rounded = false,
+                 uint32_t streamCap = 0);
 // The symmetric lists and the symmetric neighbour rows of the current tree and h (the
 // force pass's pairs; every gather pair of the converged h is among them).
 void build_symmetric(State& s);

@@ -373,7 +373,7 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
                  double* __restrict__ listH, const uint32_t* __restrict__ jOffsetPrev,
                  const int* __restrict__ jlistPrev, int* __restrict__ walked, int* __restrict__ scratch,
-                 int rounded)
+                 int rounded, uint32_t streamCap)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -507,6 +507,22 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
             pos = target - p;
         }
         p = next;
+        // A count walk with a stream cap stops once the list streams more than the cap:
+        // such a leaf is cut into one-particle groups that scan the tree for their own
+        // spheres (the cut gives one particle per group at any stream above the cut's
+        // work figure, which is the cap), so the list itself is never read.  It is left
+        // empty and its stream marked as unbounded.
+        if (!Fill && streamCap != 0u && jstream != nullptr && __reduce_add_sync(0xffffffffu, stream) > streamCap)
+        {
+            if (lane == 0)
+            {
+                jcount[leaf] = 0;
+                jstream[leaf] = 0xffffffffu;
+                if (listH != nullptr) listH[leaf] = hmax;
+                if (walked != nullptr) walked[leaf] = 1;
+            }
+            return;
+        }
     }
     if (!Fill && jstream != nullptr)
     {
@@ -841,7 +857,7 @@ void hmax_upsweep(State& s)
 }
 
 template<bool Sym, bool Per>
-static void walk(State& s, bool fill, double margin, bool incremental, bool rounded)
+static void walk(State& s, bool fill, double margin, bool incremental, bool rounded, uint32_t streamCap)
 {
     const int nL = s.nLeaves;
     const int blocks = iceil(long(nL) * 32, kBlk);
@@ -855,7 +871,7 @@ static void walk(State& s, bool fill, double margin, bool incremental, bool roun
                                         incremental ? s.jOffsetPrev.get() : nullptr,
                                         incremental ? s.jlistPrev.get() : nullptr,
                                         incremental ? s.walked.get() : nullptr, s.walkScratch.get(),
-                                        rounded ? 1 : 0);
+                                        rounded ? 1 : 0, streamCap);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
@@ -865,9 +881,10 @@ static void walk(State& s, bool fill, double margin, bool incremental, bool roun
 // include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.  incremental
 // (gather lists only, over the gather lists of the same tree at the same margin): the
 // current lists are kept aside first, and only the leaves whose hmax outgrew them walk.
-void build_lists(State& s, bool symmetric, double margin, bool incremental, bool rounded)
+void build_lists(State& s, bool symmetric, double margin, bool incremental, bool rounded, uint32_t streamCap)
 {
     rounded = rounded && !symmetric;
+    if (symmetric || !rounded) streamCap = 0;   // the lists a caller reads are always whole
     const int nL = s.nLeaves;
     incremental = incremental && !symmetric && !s.listsSym && nL > 0;
     if (incremental)
@@ -885,13 +902,13 @@ void build_lists(State& s, bool symmetric, double margin, bool incremental, bool
     auto run = [&](bool fill) {
         if (symmetric)
         {
-            if (s.periodic) walk<true, true>(s, fill, margin, false, false);
-            else walk<true, false>(s, fill, margin, false, false);
+            if (s.periodic) walk<true, true>(s, fill, margin, false, false, 0u);
+            else walk<true, false>(s, fill, margin, false, false, 0u);
         }
         else
         {
-            if (s.periodic) walk<false, true>(s, fill, margin, incremental, rounded);
-            else walk<false, false>(s, fill, margin, incremental, rounded);
+            if (s.periodic) walk<false, true>(s, fill, margin, incremental, rounded, streamCap);
+            else walk<false, false>(s, fill, margin, incremental, rounded, streamCap);
         }
     };
     run(false);

@@ -45,6 +45,8 @@ __global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restr
 constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
 constexpr double kGroupSpread = 1.5;
+constexpr uint32_t kStreamUnbounded = 0xffffffffu;   // jstream of a leaf whose walk stopped at the cap
+constexpr int kSpreadGroups = 2;   // at least this many h-ordered groups in a spread window
 
 // The cut of one leaf: x = the stream above which it is cut, y = the work of one cut group
 // (the same for every leaf; kSplitStream and kSplitWork unless the caller sets others).
@@ -79,7 +81,7 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
                                            const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
                                            DevScalars* __restrict__ ds, RowSplit rs = RowSplit{nullptr, nullptr, 0,
                                                                                               nullptr},
-                                           Split split = Split{})
+                                           Split split = Split{}, int spreadGroups = kSpreadGroups)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
@@ -122,7 +124,7 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
             const int wnd = int((g - p0) >> 6);
             const int whole = (nC + 31) >> 5;
             // A window whose smoothing lengths spread by more than kGroupSpread is grouped by
-            // h (ranks in ascending h) into at least two groups: a group's box is set by its
+            // h (ranks in ascending h) into at least spreadGroups groups: a group's box is set by its
             // widest particle, so the narrow ones keep a box nearer their own size.  Grouping
             // changes no result (every particle's sums run over the same pairs in j order).
             const double inf = __longlong_as_double(0x7ff0000000000000ll);
@@ -131,8 +133,10 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
             const double hmax = warp_max(fmax(act0 ? h0 : 0.0, act1 ? h1 : 0.0));
             const bool byH = nC > 1 && hmax > kGroupSpread * hmin;
             const int cutG = (nC + gsize - 1) / gsize;
-            const int G = max(byH ? max(whole, 2) : whole, cutG);
-            const bool split = cutG > whole;   // cut items (long streams) scan the tree for their box
+            const int G = max(byH ? max(whole, min(spreadGroups, nC)) : whole, cutG);
+            // cut items (long streams) scan the tree for their box; so do all items of a leaf
+            // whose list walk stopped at the stream cap (its list is empty)
+            const bool split = cutG > whole || S == kStreamUnbounded;
             int base = 0;
             if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
             base = __shfl_sync(0xffffffffu, base, 0);
@@ -169,9 +173,10 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
                                   const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
                                   DevScalars* __restrict__ ds,
                                   RowSplit rs = RowSplit{nullptr, nullptr, 0, nullptr},
-                                  FixedSplit split = FixedSplit{})
+                                  FixedSplit split = FixedSplit{}, int spreadGroups = kSpreadGroups)
 {
-    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, rs, split);
+    plan_items(leaves, nActive, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, rs, split,
+               spreadGroups);
 }
 
 // The same over a forest's range table, the active count read on the device, each leaf
