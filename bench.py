@@ -549,6 +549,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--npartx", type=int, default=100)
+    ap.add_argument("--periodic", action="store_true",
+                    help="lattice workloads: solve in the unit periodic box [0,1)^3 instead of open boundaries")
     ap.add_argument("--ref-npartx", type=int, default=100,
                     help="lattice size of the CPU arm's workload (default: the timed workload itself)")
     ap.add_argument("--no-forms", action="store_true",
@@ -600,13 +602,16 @@ def main():
                       label=f"Plummer a=1 r<20, {args.plummer_n} particles, h = (m/rho)^(1/3) x lognormal(0.3), "
                             "|v| = 0.5 v_circ, u = 0.05, quintic, hfact 1.0, density(NR+gradients)+force, open")
         return
-    run_particles(args, rank, world, local, dist, workload(args.npartx), quintic=False, metric=METRIC,
-                  label=lattice_label(args.npartx))
+    p = workload(args.npartx)
+    if args.periodic:
+        p["box"] = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+    run_particles(args, rank, world, local, dist, p, quintic=False, metric=METRIC,
+                  label=lattice_label(args.npartx, args.periodic))
 
 
-def lattice_label(npx):
+def lattice_label(npx, periodic=False):
     return (f"lattice {npx} + 1% h-jiggle U[0.65,1.35], density(NR+gradients)+force, cubic, "
-            "open boundaries")
+            + ("unit periodic box" if periodic else "open boundaries"))
 
 
 def run_file(args, rank, world, local, dist):
@@ -683,6 +688,7 @@ def measure(args, c, p, mixed, hfact, dist, local, profile=False):
     from cosmosphere_b200 import capi
     n = p.n
     pm = p["pmass"]
+    box = p.get("box")
     pos = np.ascontiguousarray(np.stack([p["x"], p["y"], p["z"]]))
     hsml = np.ascontiguousarray(p["h"])
     vel = np.ascontiguousarray(np.stack([p["vx"], p["vy"], p["vz"]]))
@@ -702,12 +708,12 @@ def measure(args, c, p, mixed, hfact, dist, local, profile=False):
         c.upload(capi.ACCEL, acc, n)
 
     def step_resident():
-        c.density(n, pm, tolh=1e-4, hfact=hfact)
+        c.density(n, pm, tolh=1e-4, hfact=hfact, periodic_box=box)
         c.force(n, pm, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
 
     def step_e2e():
         upload_inputs()
-        c.density(n, pm, tolh=1e-4, hfact=hfact)
+        c.density(n, pm, tolh=1e-4, hfact=hfact, periodic_box=box)
         c.upload(capi.THERMO, thermo, n, sorted_=True)
         c.force(n, pm, beta=2.0, alphau=0.0, disc=0, pdv=1, shock=1)
         for slot, buf in outs.items():
@@ -715,7 +721,7 @@ def measure(args, c, p, mixed, hfact, dist, local, profile=False):
 
     # inputs resident; THERMO gathered into Hilbert order once (every step sorts the same input)
     upload_inputs()
-    c.density(n, pm, tolh=1e-4, hfact=hfact)
+    c.density(n, pm, tolh=1e-4, hfact=hfact, periodic_box=box)
     c.upload(capi.THERMO, thermo, n, sorted_=True)
     for _ in range(args.warmup):
         step_resident()
@@ -910,7 +916,8 @@ def run_particles(args, rank, world, local, dist, p, quintic, metric, label):
                      "algorithmic_bytes_per_iteration": BYTES_PER_DENSITY_UPDATE * head["nr_upd"]
                                                         / max(1, head["nr_launches"]),
                      "traffic": (ncu_traffic("newton_stage_per_iteration")
-                                 if args.workload == "lattice100" and args.npartx == 100 and not quintic else None),
+                                 if args.workload == "lattice100" and args.npartx == 100 and not quintic
+                                 and not args.periodic else None),
                      "traffic_note": "DRAM bytes per Newton iteration assembled from one-kernel ncu captures "
                                      "(profiles/traffic.json, method in its note); above the algorithmic bytes "
                                      "because the Newton rows (r^2 per pair) are written once and streamed by the "

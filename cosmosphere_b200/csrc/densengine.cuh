@@ -29,12 +29,15 @@ namespace cosmo {
 
 constexpr int kRec = 256;   // pair records per warp
 
-// Per-warp shared scratch of density_group.
+// Per-warp shared scratch of density_group: the ring, the group's particles, the pair
+// records, and at kBoxAt the group's rounded box (read by the filter from shared memory
+// rather than held in registers through the stream).
 template<bool Mixed>
 struct DensScratch
 {
-    static constexpr int kBytes = Mixed ? (kRing * 16 + 4 * 32 * 4 + 2 * kRec * 4)
+    static constexpr int kBoxAt = Mixed ? (kRing * 16 + 4 * 32 * 4 + 2 * kRec * 4)
                                         : (kRing * 32 + 32 * 32 + 2 * kRec * 8);
+    static constexpr int kBytes = kBoxAt + 64;
 };
 
 // q = sqrt(q2) in FP32 (q2 >= 0); exact 0 for the self pair.
@@ -55,19 +58,19 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
     const double rs = kRadKernel * hi;
     const double rmax = warp_max(mine ? rs : 0.0);
     const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-    // A single particle (lane 0) filters its candidates, and cut groups their tree scan,
-    // by its own sphere: the support plus the box's slack (1e-9 of the support, 1e-13 of
-    // |x|), far above the rounding of the exact test, so no accepted pair is lost.
-    double4 sph = make_double4(0.0, 0.0, 0.0, -1.0);
-    if (ng == 1)
+    // Candidates, and the cells of a cut group's tree scan, are taken within the largest
+    // support of the members' own bounding box (a rounded box: a single particle's is its
+    // sphere), with the box's slack (1e-9 of the support, 1e-13 of |c|) on the radius, far
+    // above the rounding of the exact test, so no accepted pair is lost.
+    RoundBox* rbp = reinterpret_cast<RoundBox*>(scr + DensScratch<Mixed>::kBoxAt);
     {
-        const double x0 = __shfl_sync(0xffffffffu, pi.x, 0), y0 = __shfl_sync(0xffffffffu, pi.y, 0);
-        const double z0 = __shfl_sync(0xffffffffu, pi.z, 0);
-        sph = make_double4(x0, y0, z0, rmax + 1e-9 * rmax + 1e-13 * (fabs(x0) + fabs(y0) + fabs(z0)) + 1e-300);
+        const GroupBox pb = group_box(mine, pi.x, pi.y, pi.z, 0.0, rmax);
+        if (lane == 0)
+            *rbp = RoundBox{pb.cx, pb.cy, pb.cz, pb.ex, pb.ey, pb.ez,
+                            rmax + 1e-9 * rmax + 1e-13 * (fabs(pb.cx) + fabs(pb.cy) + fabs(pb.cz)) + 1e-300};
+        __syncwarp();
     }
-    auto gather = [&](const double4& pj) {
-        return sph.w >= 0.0 ? in_gather_sphere<Periodic>(pj, sph, lx, ly, lz) : in_gather_box<Periodic>(pj, bx, lx, ly, lz);
-    };
+    auto gather = [&](const double4& pj) { return in_round_box<Periodic>(pj, *rbp, lx, ly, lz); };
     gp = 0;
     gc = 0;
     if constexpr (!Mixed)
@@ -171,7 +174,7 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                 }
                 if (nrec > 0) flush();
             },
-            sph);
+            rbp);
         rhoi = sr;
         gradhi = sg;
     }
@@ -296,7 +299,7 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                 }
                 if (nrec > 0) flush();
             },
-            sph);
+            rbp);
         rhoi = kr.value();
         gradhi = kg.value();
         if (ng == 1)

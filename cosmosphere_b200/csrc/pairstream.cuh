@@ -73,14 +73,23 @@ __device__ __forceinline__ bool in_gather_box(const double4& p, const GroupBox& 
            axis_dist<Periodic>(p.z, b.cz, lz) <= b.ez;
 }
 
-// Sphere filter (a single-particle group): within radius s.w of (s.x, s.y, s.z), the
-// radius already holding the caller's slack above the exact test's rounding.
-template<bool Periodic>
-__device__ __forceinline__ bool in_gather_sphere(const double4& p, const double4& s, double lx, double ly, double lz)
+// A rounded box: the points within r of the box (c, e) -- the members' own bounding box
+// and their largest support.  Every pair a member accepts has its j inside (the distance
+// from j to the box is at most the distance to that member), and the region leaves out the
+// cube's corners and edges: about a fifth of the cube for a 32-particle group of a uniform
+// lattice, and, for a single particle (a box of zero size), all but its sphere.  r < 0: none.
+struct RoundBox
 {
-    const double dx = axis_dist<Periodic>(p.x, s.x, lx), dy = axis_dist<Periodic>(p.y, s.y, ly);
-    const double dz = axis_dist<Periodic>(p.z, s.z, lz);
-    return dx * dx + dy * dy + dz * dz <= s.w * s.w;
+    double cx, cy, cz, ex, ey, ez, r;
+};
+
+template<bool Periodic>
+__device__ __forceinline__ bool in_round_box(const double4& p, const RoundBox& b, double lx, double ly, double lz)
+{
+    const double gx = fmax(axis_dist<Periodic>(p.x, b.cx, lx) - b.ex, 0.0);
+    const double gy = fmax(axis_dist<Periodic>(p.y, b.cy, ly) - b.ey, 0.0);
+    const double gz = fmax(axis_dist<Periodic>(p.z, b.cz, lz) - b.ez, 0.0);
+    return gx * gx + gy * gy + gz * gz <= b.r * b.r;
 }
 
 // Symmetric filter: within R*max(hmax_group, h_j) of the box of the group's positions.
@@ -382,13 +391,13 @@ struct PreorderTree
 };
 
 // Stream the j particles of every leaf whose cell overlaps the box (c, e) -- and the
-// region (rc, re), when re.x >= 0, and the sphere sph, when sph.w >= 0 -- through the
+// region (rc, re), when re.x >= 0, and the rounded box *rbp, when given -- through the
 // group filter into the ring, found by a stackless pre-order scan of the tree 32 nodes at
 // a time (the scan of list_walk_kernel): leaves come out in ascending order, so the
 // stream is in ascending j as a list's is.  Used for groups whose leaf list is far longer
-// than their own search region needs.  A single particle's box can hold far more than
-// its sphere (a large h near the edge of a centrally concentrated set: the cube reaches
-// the dense core, the sphere does not), so such a group also tests cells on its sphere.
+// than their own search region needs.  A group's cube can hold far more than its rounded
+// box (a large h near the edge of a centrally concentrated set: the cube of a single
+// particle reaches the dense core, its sphere does not), so cells are tested on both.
 template<bool Dbl, bool Float, bool Index, bool Periodic, bool Staged = false, class Ranges, class Filter,
          class Batch>
 __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* ringIdx, double cx, double cy,
@@ -396,7 +405,7 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
                                             double3 c, double3 e, double3 rc, double3 re, double lx, double ly,
                                             double lz, Ranges ranges, const double4* __restrict__ xyzh,
                                             Filter filter, Batch batch, StageRef stage = StageRef{nullptr, nullptr, 0},
-                                            double4 sph = make_double4(0.0, 0.0, 0.0, -1.0))
+                                            const RoundBox* rbp = nullptr)
 {
     const int lane = threadIdx.x & 31;
     CandidateRing<Dbl, Float, Index, Staged> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz, stage};
@@ -417,13 +426,14 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
             if (re.x >= 0.0)
                 accept = accept && fold(fabs(rc.x - nc.x), lx) <= re.x + nh.x &&
                          fold(fabs(rc.y - nc.y), ly) <= re.y + nh.y && fold(fabs(rc.z - nc.z), lz) <= re.z + nh.z;
-            if (sph.w >= 0.0)
+            if (rbp != nullptr)
             {
-                // distance from the sphere's centre to the cell, per axis then squared
-                const double gx = fmax(fold(fabs(sph.x - nc.x), lx) - nh.x, 0.0);
-                const double gy = fmax(fold(fabs(sph.y - nc.y), ly) - nh.y, 0.0);
-                const double gz = fmax(fold(fabs(sph.z - nc.z), lz) - nh.z, 0.0);
-                accept = accept && gx * gx + gy * gy + gz * gz <= sph.w * sph.w;
+                // gap between the rounded box's core and the cell, per axis then squared
+                const RoundBox rb = *rbp;
+                const double gx = fmax(fold(fabs(rb.cx - nc.x), lx) - nh.x - rb.ex, 0.0);
+                const double gy = fmax(fold(fabs(rb.cy - nc.y), ly) - nh.y - rb.ey, 0.0);
+                const double gz = fmax(fold(fabs(rb.cz - nc.z), lz) - nh.z - rb.ez, 0.0);
+                accept = accept && gx * gx + gy * gy + gz * gz <= rb.r * rb.r;
             }
             skip = t.skip[idx];
             pl = t.leaf[idx];
@@ -483,17 +493,17 @@ struct GroupSource
     double3 rc, re;
     StageRef stage;   // the warp's bulk-copy stage, or none (direct loads)
 
-    // sph (sph.w >= 0): the sphere of a single-particle group, for the tree scan's cells
+    // rbp (when given): the group's rounded box, for the tree scan's cells
     template<bool Dbl, bool Float, bool Index, bool Periodic, bool Staged = false, class Filter, class Batch>
     __device__ __forceinline__ void stream(double4* ring, float4* ringf, int* ringIdx, const GroupBox& bx, double sx,
                                            double sy, double sz, double lx, double ly, double lz, Filter filter,
-                                           Batch batch, double4 sph = make_double4(0.0, 0.0, 0.0, -1.0)) const
+                                           Batch batch, const RoundBox* rbp = nullptr) const
     {
         if (walk)
             stream_walk<Dbl, Float, Index, Periodic, Staged>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, tree,
                                                      make_double3(bx.cx, bx.cy, bx.cz),
                                                      make_double3(bx.ex, bx.ey, bx.ez), rc, re, lx, ly, lz, ranges,
-                                                     xyzh, filter, batch, stage, sph);
+                                                     xyzh, filter, batch, stage, rbp);
         else
             stream_ranges<Dbl, Float, Index, Staged>(ring, ringf, ringIdx, bx.cx, bx.cy, bx.cz, sx, sy, sz, jb, nj,
                                                      jlist, ranges, xyzh, filter, batch, stage);

@@ -271,6 +271,14 @@ def test_lattice50_reference_driver_case():
     check_all(c, o)
 
 
+def test_lattice50_unit_periodic_box():
+    """The same lattice in the unit periodic box [0, 1)^3 (the lattice is not fitted to
+    the period, so the rows at the wrap are closer than the spacing), density + force."""
+    p = inputs.lattice(50)
+    c, o = run_pair(p, box=[0.0, 1.0, 0.0, 1.0, 0.0, 1.0], force=True)
+    check_all(c, o)
+
+
 def _child(code, env=None):
     e = dict(os.environ)
     e.update(env or {})
