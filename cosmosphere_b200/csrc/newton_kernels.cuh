@@ -204,14 +204,10 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
         const double rs = kRadKernel * kRowMargin * pi.w;
         const double rmax = warp_max(mine ? rs : 0.0);
         const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-        // candidates within the wide support of the members' own bounding box
-        const GroupBox pb = group_box(mine, pi.x, pi.y, pi.z, 0.0, rmax);
-        const RoundBox rb{pb.cx, pb.cy, pb.cz, pb.ex, pb.ey, pb.ez,
-                          rmax + 1e-9 * rmax + 1e-13 * (fabs(pb.cx) + fabs(pb.cy) + fabs(pb.cz)) + 1e-300};
         int rowLen = 0;
         rows_group<1, Periodic>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), rs, bx, lx, ly, lz,
                    jOffset[d.leaf], jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
-                   [&](const double4& pj) { return in_round_box<Periodic>(pj, rb, lx, ly, lz); },
+                   [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
                    [](const double4&) { return 0.0; },
                    [&](const double4& g, const double4& pj, int) {   // r^2 within the wide support
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;

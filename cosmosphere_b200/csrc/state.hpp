@@ -134,7 +134,7 @@ struct State
     // list streams more than splitStream particles is cut into groups of about
     // splitWork / stream particles (cosmo_x_set_option "split_stream", "split_work").
     uint32_t splitStream = 0, splitWork = 0;
-    // h-ordered groups a window whose h spreads is cut into, at least (0 = built-in 2;
+    // h-ordered groups a window whose h spreads is cut into, at least (0 = built-in 1;
     // cosmo_x_set_option "spread_groups")
     int spreadGroups = 0;
     std::vector<long long> activePerIter;

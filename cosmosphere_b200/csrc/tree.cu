@@ -420,8 +420,11 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
     hmax *= margin;
     const double radHi = kRadKernel * hmax;
     // the rounded test's radius, with the slack of the group boxes (1e-9 of the radius,
-    // 1e-13 of |centre|) above the rounding of the gaps
+    // 1e-13 of |centre|) above the rounding of the gaps.  It is used where the radius is
+    // large against the cell (there the cube's corners hold most of its volume); for a
+    // radius near the cell's size the cube test lists nearly the same leaves for less work.
     const double radR = radHi + 1e-9 * radHi + 1e-13 * (fabs(icx) + fabs(icy) + fabs(icz));
+    const bool round = rounded && radHi > 4.0 * fmax(isx, fmax(isy, isz));
     // gather: the i-box inflated by radHi; symmetric: the raw i-box
     const double ax = Symmetric ? isx : isx + radHi;
     const double ay = Symmetric ? isy : isy + radHi;
@@ -459,7 +462,7 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                 const double rs = fmax(radHi, kRadKernel * hmaxPre[idx]);
                 accept = n2 <= rs * rs;
             }
-            else if (rounded)
+            else if (round)
             {
                 const double e0 = fmax(dd[0] - isx - s.x, 0.0), e1 = fmax(dd[1] - isy - s.y, 0.0);
                 const double e2 = fmax(dd[2] - isz - s.z, 0.0);

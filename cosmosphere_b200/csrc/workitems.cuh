@@ -46,7 +46,7 @@ constexpr uint32_t kSplitStream = 4096;
 constexpr uint32_t kSplitWork = 32u * 4096u;
 constexpr double kGroupSpread = 1.5;
 constexpr uint32_t kStreamUnbounded = 0xffffffffu;   // jstream of a leaf whose walk stopped at the cap
-constexpr int kSpreadGroups = 2;   // at least this many h-ordered groups in a spread window
+constexpr int kSpreadGroups = 1;   // at least this many h-ordered groups in a spread window
 
 // The cut of one leaf: x = the stream above which it is cut, y = the work of one cut group
 // (the same for every leaf; kSplitStream and kSplitWork unless the caller sets others).
@@ -124,9 +124,13 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
             const int wnd = int((g - p0) >> 6);
             const int whole = (nC + 31) >> 5;
             // A window whose smoothing lengths spread by more than kGroupSpread is grouped by
-            // h (ranks in ascending h) into at least spreadGroups groups: a group's box is set by its
-            // widest particle, so the narrow ones keep a box nearer their own size.  Grouping
-            // changes no result (every particle's sums run over the same pairs in j order).
+            // h (ranks in ascending h), into at least spreadGroups groups and however many
+            // its count and cut need: a group's box is set by its widest particle, so the
+            // narrow ones keep a box nearer their own size (measured on B200 for the Plummer
+            // workload: at least one group, i.e. h order only where a window needs two or
+            // more anyway, is fastest; forcing 2, 4 or 8 costs more in groups than it saves
+            // in tests).  Grouping changes no result (every particle's sums run over the same
+            // pairs in j order).
             const double inf = __longlong_as_double(0x7ff0000000000000ll);
             const double h0 = act0 ? xyzh[a0].w : inf, h1 = act1 ? xyzh[a1].w : inf;
             const double hmin = warp_min(fmin(h0, h1));

@@ -214,7 +214,7 @@ void cosmo_x_sync(void);
  * split_work / stream particles that scan the tree for their own box; 0 restores the
  * built-in 4096 and 131072); "spread_groups" sets how many h-ordered groups, at least, a
  * 64-particle window whose smoothing lengths spread by more than 1.5x is cut into (0 restores
- * the built-in 2; also COSMO_SPREAD_GROUPS).  Returns 0, or -1 for an unknown name or a value
+ * the built-in 1; also COSMO_SPREAD_GROUPS).  Returns 0, or -1 for an unknown name or a value
  * out of range. */
 int cosmo_x_set_option(const char* name, int value);
 
