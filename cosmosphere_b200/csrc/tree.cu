@@ -362,7 +362,7 @@ constexpr int kWalkScratch = 512;     // list entries per leaf the count pass ke
 // pair within the radius still has its j-leaf in the list, and a leaf with a large h
 // near the edge of a concentrated set no longer takes in the dense centre its cube reaches.
 template<bool Symmetric, bool Periodic, bool Fill>
-__global__ void __launch_bounds__(kBlk)
+__global__ void __launch_bounds__(kBlk, 5)
 list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const double* __restrict__ centers, const double* __restrict__ sizes,
                  const double* __restrict__ hmaxLeaf, const double4* __restrict__ preCenter,
@@ -514,8 +514,11 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
         // such a leaf is cut into one-particle groups that scan the tree for their own
         // spheres (the cut gives one particle per group at any stream above the cut's
         // work figure, which is the cap), so the list itself is never read.  It is left
-        // empty and its stream marked as unbounded.
-        if (!Fill && streamCap != 0u && jstream != nullptr && __reduce_add_sync(0xffffffffu, stream) > streamCap)
+        // empty and its stream marked as unbounded.  The stream is summed over the lanes
+        // only once the listed leaves could hold more than the cap (kBucket each, leaves
+        // at the deepest level aside: missing one of those only walks a list in full).
+        if (!Fill && streamCap != 0u && jstream != nullptr && uint64_t(count) * kBucket > streamCap &&
+            __reduce_add_sync(0xffffffffu, stream) > streamCap)
         {
             if (lane == 0)
             {
