@@ -617,7 +617,7 @@ density_batch_kernel(const int4* __restrict__ items, int cap, const int* __restr
         // one engine instance for open and periodic sets (zero periods fold nothing): half
         // the code the warps of a mixed ensemble would otherwise share the instruction
         // cache with
-        density_group<true, Mixed, Staged>(sScr[wib], mine, d.ng, pi, per ? bxs.len[0] : 0.0, per ? bxs.len[1] : 0.0,
+        density_group<true, Mixed, Staged, false>(sScr[wib], mine, d.ng, pi, per ? bxs.len[0] : 0.0, per ? bxs.len[1] : 0.0,
                                    per ? bxs.len[2] : 0.0, src, rhoi, gradhi, gp, gc);
         if (EvalAll)
         {

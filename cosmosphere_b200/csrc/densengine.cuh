@@ -46,7 +46,7 @@ __device__ __forceinline__ float sqrt_q(float q2) { return q2 > 0.0f ? q2 * rsqr
 // Sums over the gather list of one group: the lanes [0, ng) own the group's particles
 // (pi, with mine set); rhoi and gradhi receive the un-normalised sums (W and
 // -q dW/dq - 3W over accepted j), gp the accepted pairs and gc the candidates offered.
-template<bool Periodic, bool Mixed, bool Staged = false, class Ranges>
+template<bool Periodic, bool Mixed, bool Staged = false, bool Round = true, class Ranges>
 __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int ng, const double4& pi, double lx,
                                               double ly, double lz, const GroupSource<Ranges>& src, double& rhoi,
                                               double& gradhi, unsigned int& gp, unsigned int& gc)
@@ -58,11 +58,14 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
     const double rs = kRadKernel * hi;
     const double rmax = warp_max(mine ? rs : 0.0);
     const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
-    // Candidates, and the cells of a cut group's tree scan, are taken within the largest
-    // support of the members' own bounding box (a rounded box: a single particle's is its
-    // sphere), with the box's slack (1e-9 of the support, 1e-13 of |c|) on the radius, far
-    // above the rounding of the exact test, so no accepted pair is lost.
-    RoundBox* rbp = reinterpret_cast<RoundBox*>(scr + DensScratch<Mixed>::kBoxAt);
+    // Round: candidates, and the cells of a cut group's tree scan, are taken within the
+    // largest support of the members' own bounding box (a rounded box: a single particle's
+    // is its sphere), with the box's slack (1e-9 of the support, 1e-13 of |c|) on the
+    // radius, far above the rounding of the exact test, so no accepted pair is lost.
+    // Otherwise within the box of the search spheres (the batched kernel: its sets' h do
+    // not scatter, and its registers are tighter).
+    RoundBox* rbp = Round ? reinterpret_cast<RoundBox*>(scr + DensScratch<Mixed>::kBoxAt) : nullptr;
+    if constexpr (Round)
     {
         const GroupBox pb = group_box(mine, pi.x, pi.y, pi.z, 0.0, rmax);
         if (lane == 0)
@@ -70,7 +73,10 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                             rmax + 1e-9 * rmax + 1e-13 * (fabs(pb.cx) + fabs(pb.cy) + fabs(pb.cz)) + 1e-300};
         __syncwarp();
     }
-    auto gather = [&](const double4& pj) { return in_round_box<Periodic>(pj, *rbp, lx, ly, lz); };
+    auto gather = [&](const double4& pj) {
+        if constexpr (Round) return in_round_box<Periodic>(pj, *rbp, lx, ly, lz);
+        else return in_gather_box<Periodic>(pj, bx, lx, ly, lz);
+    };
     gp = 0;
     gc = 0;
     if constexpr (!Mixed)
