@@ -64,7 +64,7 @@ def test_mixed_matches_fp64(case):
     e = errors(mix, ref)
     print(case, e)
     assert e["h_max"] <= 1e-5 and e["rho_max"] <= 1e-5, e
-    assert e["a_rms_norm"] <= 1e-4, e
+    assert e["a_rms_norm"] <= 1e-4 and e["a_max_rel_floor"] <= 1e-4, e
 
 
 def test_precision_switch_round_trips():
