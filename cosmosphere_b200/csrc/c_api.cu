@@ -118,6 +118,7 @@ void ensure_init(State& s)
     if (const char* e = std::getenv("COSMO_PRECISION")) s.precision = (std::string(e) == "mixed") ? 1 : 0;
     if (const char* e = std::getenv("COSMO_STAGING")) s.staging = std::atoi(e) != 0;
     if (const char* e = std::getenv("COSMO_SYM_PREFILTER")) s.symPrefilter = std::atoi(e) != 0;
+    if (const char* e = std::getenv("COSMO_NEWTON_GRAPH")) s.newtonGraph = std::atoi(e) != 0;
     if (const char* e = std::getenv("COSMO_SPREAD_GROUPS")) s.spreadGroups = std::max(0, std::min(32, std::atoi(e)));
 }
 
@@ -710,6 +711,8 @@ int cosmo_x_set_option(const char* name, int value)
     const std::string k(name ? name : "");
     if (k == "staging") { s.staging = value != 0; return 0; }
     if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
+    if (k == "newton_graph") { s.newtonGraph = value != 0; return 0; }
+    if (k == "graph_list_slack") { s.graphListSlack = value; return 0; }
     if (k == "spread_groups")
     {
         if (value < 0 || value > 32) return -1;
@@ -778,6 +781,7 @@ double cosmo_x_scalar(const char* name)
     if (k == "hfact") return s.hfact;
     if (k == "maxIter") return s.maxIter;
     if (k == "settling0") return double(s.settling0);
+    if (k == "loopGraph") return double(s.lastLoopGraph);
     if (s.hscal)
     {
         read_scalars(s);

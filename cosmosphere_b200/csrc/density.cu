@@ -291,10 +291,256 @@ int grid_for(const State& s, int work)
     return std::max(1, std::min(maxBlocks, iceil(work, kWarpsPerBlock)));
 }
 
+// ---------------------------------------------------------- the Newton loop as a graph
+__global__ void newton_loop_init_kernel(NewtonLoop* L, int nLeaves, int nAlive, int maxIter)
+{
+    *L = NewtonLoop{};
+    L->nActiveLeaves = nLeaves;
+    L->nActiveParticles = nAlive;
+    L->maxIter = maxIter;
+}
+
+// First node of an iteration: the list-rebuild and row-build decisions the last
+// iteration's epilogue recorded become the conditions of this iteration's two branches.
+__global__ void newton_decide_kernel(const NewtonLoop* L, cudaGraphConditionalHandle hList,
+                                     cudaGraphConditionalHandle hRows)
+{
+    cudaGraphSetConditional(hList, L->rebuildNext ? 1u : 0u);
+    cudaGraphSetConditional(hRows, L->rowsNext ? 1u : 0u);
+}
+
+__global__ void newton_count_kernel(NewtonLoop* L, int rows)
+{
+    if (rows)
+    {
+        L->rowsReady = 1;
+        ++L->rowBuilds;
+    }
+    else ++L->rebuilds;
+}
+
+// The next active leaves become the active ones (the host loop swaps the two buffers).
+__global__ void newton_copy_active_kernel(const int* __restrict__ src, int* __restrict__ dst,
+                                          const DevScalars* __restrict__ ds, int cap)
+{
+    const int n = min(ds->nextActive, cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) dst[t] = src[t];
+}
+
+// Last node of an iteration: what the host loop read back after it -- the counts, the
+// stale-list flag, the settling particles -- decides the next iteration on the device.
+__global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, cudaGraphConditionalHandle hMore)
+{
+    const int it = L->iter;
+    if (it < kLoopIters) L->activePerIter[it] = L->nActiveParticles;
+    if (it == 0) L->settling0 = ds->settling;
+    const int active = ds->unconverged;
+    L->nActiveLeaves = ds->nextActive;
+    L->nActiveParticles = active;
+    L->iter = it + 1;
+    const int more = (active > 0 && it + 1 < L->maxIter && ds->err == 0) ? 1 : 0;
+    L->rebuildNext = (more && ds->listStale) ? 1 : 0;
+    L->rowsNext = (more && !L->rowsReady && 5ll * ds->settling >= 4ll * active) ? 1 : 0;
+    cudaGraphSetConditional(hMore, unsigned(more));
+}
+
 } // namespace
 
+// The Newton loop of one solve as one graph launch: a while node whose body is one
+// iteration -- the conditions of its two branches, hmax of the active leaves, [the
+// incremental list rebuild], [the Newton rows], the work items, the Newton kernel, the
+// row kernel, the next active leaves and the epilogue that decides the next iteration.
+// Same kernels, same order, same decisions as the host loop, so the same results; the
+// first lists are built before it (their total sizes the storage of the rebuilds).
+// Returns false, having changed nothing the caller keeps, when the graph cannot be built
+// or a rebuild outgrew the storage: the caller then solves again on the host loop.
+static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact, int maxIter, FixedSplit cut,
+                              int spreadG, long long& nActiveParticles)
+{
+    DevScalars* ds = s.dscal.get();
+    const int nL = s.nLeaves;
+    const int itemCap = std::max(s.nAlive, 1);
+    const bool mx = s.precision == 1;
+    cudaEvent_t j0 = ev(s);
+    hmax_leaves(s, s.activeA.get(), nL);
+    build_lists(s, false, kListMargin, false, true, cut.work);
+    const size_t listCap = s.graphListSlack >= 0 ? size_t(s.listTotal) + size_t(s.graphListSlack)
+                                                 : 2 * size_t(s.listTotal) + 65536;
+    s.jlist.resize(std::max<size_t>(listCap, s.jlist.n), s.st, true);
+    s.jlistPrev.resize(s.jlist.cap, s.st);
+    s.listStore = std::min(listCap, s.jlist.cap);
+    s.jOffsetPrev.resize(size_t(nL) + 1, s.st);
+    s.walked.resize(nL, s.st);
+    s.nloop.resize(1, s.st);
+    NewtonLoop* L = s.nloop.get();
+    newton_loop_init_kernel<<<1, 1, 0, s.st>>>(L, nL, s.nAlive, maxIter);
+    COSMO_LAUNCHED();
+    cudaEvent_t j1 = ev(s);
+
+    RowsKernelFn nrows = mx ? mixed_newton_rows_kernel(s.periodic)
+                            : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
+    NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic, s.staging)
+                  : s.staging ? (s.periodic ? density_nr_kernel<true, false, true> : density_nr_kernel<false, false, true>)
+                              : (s.periodic ? density_nr_kernel<true, false, false> : density_nr_kernel<false, false, false>);
+    RowKernelFn rk = mx ? mixed_density_row_kernel(s.periodic)
+                        : (s.periodic ? density_row_kernel<true, false> : density_row_kernel<false, false>);
+    const int gridRows = persistent_grid(s, nrows, kThreads), gridNr = persistent_grid(s, nr, kThreads);
+    const int gridRow = std::max(1, std::min(iceil(s.nAlive, kThreads), 8 * s.numSMs));
+    const int bgrid = std::min(iceil(nL, 256), 4 * s.numSMs);
+    const RowSplit rows{s.nblCount.get(), s.nblH.get(), kNbl, s.rowItems.get()};
+
+    const unsigned long long launches0 = g_launches.load();
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    bool built = false;
+    unsigned long long kMain = 0, kList = 0, kRows = 0;
+    do
+    {
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
+        cudaGraphConditionalHandle hMore, hList, hRows;
+        if (cudaGraphConditionalHandleCreate(&hMore, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+        cudaGraphNodeParams wp = {};
+        wp.type = cudaGraphNodeTypeConditional;
+        wp.conditional.handle = hMore;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        if (cudaGraphAddNode(&wnode, g, nullptr, 0, &wp) != cudaSuccess) break;
+        cudaGraph_t body = wp.conditional.phGraph_out[0];
+        if (cudaGraphConditionalHandleCreate(&hList, body, 0, 0) != cudaSuccess) break;
+        if (cudaGraphConditionalHandleCreate(&hRows, body, 0, 0) != cudaSuccess) break;
+
+        // the branch conditions and hmax of the active leaves
+        unsigned long long c0 = g_launches.load();
+        if (cudaStreamBeginCaptureToGraph(s.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            break;
+        newton_decide_kernel<<<1, 1, 0, s.st>>>(L, hList, hRows);
+        COSMO_LAUNCHED();
+        hmax_leaves(s, s.activeA.get(), nL, &L->nActiveLeaves);
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        const bool infoOk = cudaStreamGetCaptureInfo(s.st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess;
+        std::vector<cudaGraphNode_t> sink(deps, deps + (infoOk ? nd : 0));
+        if (cudaStreamEndCapture(s.st, &body) != cudaSuccess || !infoOk) break;
+        kMain += g_launches.load() - c0;
+
+        // [the incremental list rebuild]
+        cudaGraphNodeParams lp = {};
+        lp.type = cudaGraphNodeTypeConditional;
+        lp.conditional.handle = hList;
+        lp.conditional.type = cudaGraphCondTypeIf;
+        lp.conditional.size = 1;
+        cudaGraphNode_t lnode;
+        if (cudaGraphAddNode(&lnode, body, sink.data(), sink.size(), &lp) != cudaSuccess) break;
+        cudaGraph_t lbody = lp.conditional.phGraph_out[0];
+        c0 = g_launches.load();
+        if (cudaStreamBeginCaptureToGraph(s.st, lbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            break;
+        build_lists_device(s, kListMargin, true, cut.work);
+        newton_count_kernel<<<1, 1, 0, s.st>>>(L, 0);
+        COSMO_LAUNCHED();
+        if (cudaStreamEndCapture(s.st, &lbody) != cudaSuccess) break;
+        kList = g_launches.load() - c0;
+
+        // [the Newton rows of the still-active particles at their current h]
+        cudaGraphNodeParams rp = {};
+        rp.type = cudaGraphNodeTypeConditional;
+        rp.conditional.handle = hRows;
+        rp.conditional.type = cudaGraphCondTypeIf;
+        rp.conditional.size = 1;
+        cudaGraphNode_t rnode;
+        if (cudaGraphAddNode(&rnode, body, &lnode, 1, &rp) != cudaSuccess) break;
+        cudaGraph_t rbody = rp.conditional.phGraph_out[0];
+        c0 = g_launches.load();
+        if (cudaStreamBeginCaptureToGraph(s.st, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            break;
+        begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
+        COSMO_LAUNCHED();
+        plan_items_count_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
+            s.activeA.get(), &L->nActiveLeaves, nullptr, s.layout.get(), s.converged.get(), s.jstream.get(),
+            s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
+        COSMO_LAUNCHED();
+        nrows<<<gridRows, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(),
+                                               s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.box.get(),
+                                               s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
+        COSMO_LAUNCHED();
+        newton_count_kernel<<<1, 1, 0, s.st>>>(L, 1);
+        COSMO_LAUNCHED();
+        if (cudaStreamEndCapture(s.st, &rbody) != cudaSuccess) break;
+        kRows = g_launches.load() - c0;
+
+        // the iteration proper
+        c0 = g_launches.load();
+        if (cudaStreamBeginCaptureToGraph(s.st, body, &rnode, nullptr, 1, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+            break;
+        begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
+        COSMO_LAUNCHED();
+        plan_items_count_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
+            s.activeA.get(), &L->nActiveLeaves, &L->rowsReady, s.layout.get(), s.converged.get(), s.jstream.get(),
+            s.xyzh.get(), s.items.get(), itemCap, ds, rows, cut, spreadG);
+        COSMO_LAUNCHED();
+        nr<<<gridNr, kThreads, 0, s.st>>>(
+            s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+            s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
+            s.leafNext.get(), s.activeB.get(),
+            PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
+            s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns());
+        COSMO_LAUNCHED();
+        rk<<<gridRow, kThreads, 0, s.st>>>(s.rowItems.get(), s.nblR2.get(), s.nblCount.get(), s.xyzh.get(),
+                                          s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact,
+                                          s.box.get(), s.listH.get(), s.particleLeaf.get(), s.leafNext.get(),
+                                          s.activeB.get(), ds);
+        COSMO_LAUNCHED();
+        newton_copy_active_kernel<<<bgrid, 256, 0, s.st>>>(s.activeB.get(), s.activeA.get(), ds, nL);
+        COSMO_LAUNCHED();
+        newton_epilogue_kernel<<<1, 1, 0, s.st>>>(L, ds, hMore);
+        COSMO_LAUNCHED();
+        if (cudaStreamEndCapture(s.st, &body) != cudaSuccess) break;
+        kMain += g_launches.load() - c0;
+            if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) break;
+        built = true;
+    } while (false);
+    s.listStore = 0;
+    // what was captured did not run: the launches counted are those the graph executes
+    g_launches -= g_launches.load() - launches0;
+    if (!built)
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s.st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+        {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(s.st, &junk);
+            if (junk) cudaGraphDestroy(junk);
+        }
+        if (ex) cudaGraphExecDestroy(ex);
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        return false;
+    }
+    COSMO_CUDA(cudaGraphLaunch(ex, s.st));
+    cudaEvent_t j2 = ev(s);
+    NewtonLoop h;
+    uint32_t total = 0;
+    COSMO_CUDA(cudaMemcpyAsync(&total, s.jOffset.get() + nL, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
+    COSMO_CUDA(cudaMemcpyAsync(&h, L, sizeof(NewtonLoop), cudaMemcpyDeviceToHost, s.st));
+    read_scalars(s);
+    COSMO_CUDA(cudaGraphExecDestroy(ex));
+    COSMO_CUDA(cudaGraphDestroy(g));
+    if (s.hscal->err & kErrListFull) return false;
+    g_launches += h.iter * kMain + h.rebuilds * kList + h.rowBuilds * kRows;
+    s.listTotal = total;
+    s.itersRun = h.iter;
+    s.settling0 = h.settling0;
+    s.activePerIter.assign(h.activePerIter, h.activePerIter + std::min(h.iter, kLoopIters));
+    nActiveParticles = h.nActiveParticles;
+    s.t.jbuild += elapsed_s(j0, j1);
+    s.t.nrkern += elapsed_s(j1, j2);
+    return true;
+}
+
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh, double hfact,
-                         int maxIter, bool withGradients)
+                         int maxIter, bool withGradients, bool allowGraph)
 {
     DensResult res{0, 0, 0};
     if (!(hfact > 0.0)) hfact = kHfactDefault;
@@ -341,8 +587,23 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     const int spreadG = s.spreadGroups > 0 ? s.spreadGroups : kSpreadGroups;
     bool listsValid = false, listsWidened = false, rowsReady = false;
     long long settlingPrev = 0;
+    bool graphRan = false;
+    if (allowGraph && s.newtonGraph && maxIter <= kLoopIters && nActiveParticles > 0)
+    {
+        graphRan = newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles);
+        listsWidened = graphRan;
+        if (!graphRan && (s.hscal->err & kErrListFull))
+        {
+            // a list rebuild outgrew the storage the first lists sized: solve again from
+            // the caller's arrays with the host loop, which sizes every build
+            COSMO_CUDA(cudaMemsetAsync(&ds->err, 0, sizeof(int), s.st));
+            s.hscal->err = 0;
+            return solve_density(s, n, pmass, periodicBox, tolh, hfact, maxIter, withGradients, false);
+        }
+    }
+    s.lastLoopGraph = graphRan ? 1 : 0;
     cudaEvent_t e3 = ev(s);
-    for (int iter = 0; iter < maxIter; ++iter)
+    for (int iter = 0; iter < maxIter && !graphRan; ++iter)
     {
         cudaEvent_t j0 = ev(s);
         hmax_leaves(s, s.activeA.get(), nActiveLeaves);

@@ -97,6 +97,9 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
     if constexpr (Staged) stage_init(sStage[wib]);
     double lx = 0, ly = 0, lz = 0;
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    // lists that outgrew their storage in a graph-run loop are incomplete: the solve is
+    // redone on the host loop, so nothing reads them
+    if (ds->err & kErrListFull) return;
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     unsigned long long pairs = 0, cand = 0;
 
@@ -183,6 +186,9 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double lx = 0, ly = 0, lz = 0;
     if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
+    // lists that outgrew their storage in a graph-run loop are incomplete: the solve is
+    // redone on the host loop, so nothing reads them
+    if (ds->err & kErrListFull) return;
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     const double wide2 = kRadK2 * (kRowMargin * kRowMargin);
     for (;;)

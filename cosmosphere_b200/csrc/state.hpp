@@ -100,6 +100,18 @@ struct DevScalars
     int pad[1];
 };
 
+// The single-set Newton loop run as a graph: what the host loop kept in host variables
+// (active counts, the iteration, the list and row decisions) lives here on the device.
+constexpr int kLoopIters = 128;
+struct NewtonLoop
+{
+    int nActiveLeaves, nActiveParticles, iter, maxIter;
+    int rebuildNext, rowsNext, rowsReady, rebuilds;
+    int rowBuilds, pad0;
+    long long settling0;
+    long long activePerIter[kLoopIters];
+};
+
 struct Timings
 {
     double bbox = 0, keysSort = 0, tree = 0, nodes = 0, jbuild = 0, nrkern = 0, gjbuild = 0,
@@ -137,6 +149,17 @@ struct State
     // h-ordered groups a window whose h spreads is cut into, at least (0 = built-in 1;
     // cosmo_x_set_option "spread_groups")
     int spreadGroups = 0;
+    // 1: the Newton loop runs as one graph launch (a while node over the iterations, the
+    // list rebuilds and the row build as conditional nodes: no host read per iteration);
+    // 0: one host round trip per iteration (cosmo_x_set_option "newton_graph",
+    // COSMO_NEWTON_GRAPH).  The results are the same either way.
+    int newtonGraph = 1;
+    // entries of list storage the graph loop adds to the first lists' total (negative: the
+    // built-in, the total again plus 65536); a small figure makes a rebuild outgrow it, so
+    // the fallback to the host loop can be exercised (cosmo_x_set_option "graph_list_slack")
+    long long graphListSlack = -1;
+    size_t listStore = 0;   // list entries a fill may write (0: all jlist holds)
+    int lastLoopGraph = 0;  // the last solve's Newton loop ran as a graph (1) or on the host (0)
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;
@@ -185,6 +208,7 @@ struct State
     DBuf<int> nodeValsTmp;
     DBuf<double> redTmp;
     DBuf<DevScalars> dscal;
+    DBuf<NewtonLoop> nloop;                     // the graph-run Newton loop's state
     DevScalars* hscal = nullptr;                // pinned host mirror
     int* hsmall = nullptr;                      // pinned scratch for small reads (64 ints)
     std::vector<cudaEvent_t> evPool;            // timing events of this state's stream
@@ -199,12 +223,18 @@ void size_particle_arrays(State& s, int n);
 
 // tree.cu
 void build_tree(State& s, const double* periodicBox, bool alsoSortVA);
-void hmax_leaves(State& s, const int* leaves, int nLeavesActive);
+// hmax of the leaves [0, nLeavesActive) of leaves, or of the first *countPtr of them when
+// countPtr is given (a count on the device; nLeavesActive then bounds it).
+void hmax_leaves(State& s, const int* leaves, int nLeavesActive, const int* countPtr = nullptr);
 // Gather (symmetric = false) or symmetric j-leaf lists for all leaves.  margin > 1 widens
 // the gather radius to R * hmax * margin, so the lists stay valid while h grows by up to
 // that factor; listH records the h each leaf's list covers.
 void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental = false, bool rounded = false,
                  uint32_t streamCap = 0);
+// The same incremental gather-list rebuild with no host read (for a captured Newton
+// loop): the fill stays inside the storage jlist already holds, kErrListFull otherwise.
+// jOffsetPrev, jlistPrev (as large as jlist), walked and the walk scratch must be sized.
+void build_lists_device(State& s, double margin, bool rounded, uint32_t streamCap);
 // The symmetric lists and the symmetric neighbour rows of the current tree and h (the
 // force pass's pairs; every gather pair of the converged h is among them).
 void build_symmetric(State& s);
@@ -214,8 +244,9 @@ uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool
 
 // density.cu
 struct DensResult { int itersRun; int unconverged; int status; };
+// allowGraph = false keeps the Newton loop on the host (the graph loop's fallback).
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh,
-                         double hfact, int maxIter, bool withGradients);
+                         double hfact, int maxIter, bool withGradients, bool allowGraph = true);
 
 // mixed.cu
 void launch_gradient_mixed(State& s, double pmass);

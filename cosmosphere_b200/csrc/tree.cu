@@ -308,10 +308,11 @@ __global__ void iota_kernel(int* __restrict__ a, int n)
 // ------------------------------------------------------------------ hmax
 // include/tree.cuh:177-191: largest finite h of each listed leaf.
 __global__ void hmax_leaf_kernel(const double4* __restrict__ xyzh, const uint32_t* __restrict__ layout,
-                                 const int* __restrict__ leaves, int nActive, double* __restrict__ hmax)
+                                 const int* __restrict__ leaves, int nActive, double* __restrict__ hmax,
+                                 const int* __restrict__ countPtr)
 {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= nActive) return;
+    if (t >= (countPtr != nullptr ? *countPtr : nActive)) return;
     const int l = leaves[t];
     double hm = 0.0;
     for (uint32_t j = layout[l]; j < layout[l + 1]; ++j)
@@ -373,11 +374,19 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
                  double* __restrict__ listH, const uint32_t* __restrict__ jOffsetPrev,
                  const int* __restrict__ jlistPrev, int* __restrict__ walked, int* __restrict__ scratch,
-                 int rounded, uint32_t streamCap)
+                 int rounded, uint32_t streamCap, uint32_t listCap)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (leaf >= nL) return;
+    // A fill writes only inside [jOffset[leaf], jOffset[leaf + 1]); a list storage of
+    // listCap entries that the lists outgrew (a build whose total the host did not read
+    // first) is reported, and nothing is written past it.
+    if (Fill && jOffset[leaf + 1] > listCap)
+    {
+        if (lane == 0) atomicOr(err, int(kErrListFull));
+        return;
+    }
     // The count pass keeps the first kWalkScratch entries of every list it walks in
     // scratch; the fill pass copies a list that fitted instead of walking it again.
     if (Fill && scratch != nullptr && (walked == nullptr || walked[leaf] != 0))
@@ -837,11 +846,11 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
     s.t.nodes += elapsed_s(e3, e4);
 }
 
-void hmax_leaves(State& s, const int* leaves, int nActive)
+void hmax_leaves(State& s, const int* leaves, int nActive, const int* countPtr)
 {
     if (nActive <= 0) return;
     hmax_leaf_kernel<<<iceil(nActive, kBlk), kBlk, 0, s.st>>>(s.xyzh.get(), s.layout.get(), leaves, nActive,
-                                                             s.hmaxLeaf.get());
+                                                             s.hmaxLeaf.get(), countPtr);
     COSMO_LAUNCHED();
 }
 
@@ -877,11 +886,38 @@ static void walk(State& s, bool fill, double margin, bool incremental, bool roun
                                         incremental ? s.jOffsetPrev.get() : nullptr,
                                         incremental ? s.jlistPrev.get() : nullptr,
                                         incremental ? s.walked.get() : nullptr, s.walkScratch.get(),
-                                        rounded ? 1 : 0, streamCap);
+                                        rounded ? 1 : 0, streamCap,
+                                        uint32_t(std::min<size_t>(s.listStore ? s.listStore : s.jlist.cap, 0xffffffffu)));
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
     COSMO_LAUNCHED();
+}
+
+// Copy the lists' entries [0, *total) (the total on the device) into dst.
+__global__ void copy_list_kernel(const int* __restrict__ src, int* __restrict__ dst, const uint32_t* __restrict__ total)
+{
+    const uint32_t n = *total;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+// The Newton loop's incremental rebuild of the gather lists with no host read: the
+// current lists are kept aside (their total read on the device), the outgrown leaves
+// walk, and the fill writes into the storage already held (jlist.cap entries); a build
+// that would not fit raises kErrListFull and writes nothing past it.  Every size is fixed
+// when it is issued, so the sequence can be captured into a graph.
+void build_lists_device(State& s, double margin, bool rounded, uint32_t streamCap)
+{
+    const int nL = s.nLeaves;
+    COSMO_CUDA(cudaMemcpyAsync(s.jOffsetPrev.get(), s.jOffset.get(), (size_t(nL) + 1) * sizeof(uint32_t),
+                               cudaMemcpyDeviceToDevice, s.st));
+    copy_list_kernel<<<4 * s.numSMs, 256, 0, s.st>>>(s.jlist.get(), s.jlistPrev.get(), s.jOffset.get() + nL);
+    COSMO_LAUNCHED();
+    if (s.periodic) walk<false, true>(s, false, margin, true, rounded, streamCap);
+    else walk<false, false>(s, false, margin, true, rounded, streamCap);
+    scan_exclusive(s, s.jcount.get(), s.jOffset.get(), nL, false);
+    if (s.periodic) walk<false, true>(s, true, margin, true, rounded, streamCap);
+    else walk<false, false>(s, true, margin, true, rounded, streamCap);
 }
 
 // include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.  incremental

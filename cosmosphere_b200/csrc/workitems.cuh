@@ -183,6 +183,19 @@ __global__ void plan_items_kernel(const int* __restrict__ leaves, int nActive, c
                spreadGroups);
 }
 
+// The same with the active-leaf count read on the device (a graph-run Newton loop), and
+// the row classification used only once *rowsReady is set.
+__global__ void plan_items_count_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr,
+                                        const int* __restrict__ rowsReady, const uint32_t* __restrict__ layout,
+                                        const int* __restrict__ converged, const uint32_t* __restrict__ jstream,
+                                        const double4* __restrict__ xyzh, int4* __restrict__ items, int cap,
+                                        DevScalars* __restrict__ ds, RowSplit rs, FixedSplit split, int spreadGroups)
+{
+    const RowSplit r = (rowsReady != nullptr && *rowsReady) ? rs : RowSplit{nullptr, nullptr, 0, nullptr};
+    plan_items(leaves, *countPtr, LayoutRanges{layout}, converged, jstream, xyzh, items, cap, ds, r, split,
+               spreadGroups);
+}
+
 // The same over a forest's range table, the active count read on the device, each leaf
 // cut by its set's entry of setSplit.
 __global__ void plan_items_table_kernel(const int* __restrict__ leaves, const int* __restrict__ countPtr,

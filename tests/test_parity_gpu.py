@@ -413,3 +413,64 @@ def test_one_particle_cut_items_keep_parity():
         finally:
             c.set_option("split_stream", 0)
             c.set_option("split_work", 0)
+
+
+def _solve_arrays(p, quintic, box=None):
+    n = p.n
+    c = capi.Cosmo(quintic)
+    c.arrays_init(n)
+    c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+    c.upload(capi.HSML, p["h"])
+    c.upload(capi.VEL, np.stack([inputs.gaussian(n, 0, 0.1, 31 + k) for k in range(3)]))
+    c.upload(capi.ACCEL, np.zeros((3, n)))
+    c.density(n, p["pmass"], periodic_box=box, hfact=1.0 if quintic else 1.2)
+    out = {k: c.array(k).copy() for k in ("h", "rho", "gradh", "divv", "xi", "ddivvdt")}
+    out["iters"] = c.scalar("itersRun")
+    out["active"] = c.array("activePerIter").copy()
+    out["graph"] = c.scalar("loopGraph")
+    return out
+
+
+@pytest.mark.parametrize("case", ["lattice", "plummer_lognormal", "periodic"])
+def test_newton_loop_graph_equals_host_loop(case):
+    """The Newton loop run as one graph launch (a while node, with the list rebuilds and
+    the row build as conditional nodes) and the host loop give the same h, rho and
+    gradients bit for bit, in the same iterations with the same active counts."""
+    quintic, box = False, None
+    if case == "lattice":
+        p = inputs.lattice100_workload(20)
+    elif case == "plummer_lognormal":
+        p = inputs.plummer(30000, lnsigma=0.5, seed=17)
+        quintic = True
+    else:
+        p = inputs.uniform_box(20000, seed=8)
+        box = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+    c = capi.Cosmo(quintic)
+    try:
+        assert c.set_option("newton_graph", 1) == 0
+        g = _solve_arrays(p, quintic, box)
+        assert c.set_option("newton_graph", 0) == 0
+        h = _solve_arrays(p, quintic, box)
+    finally:
+        c.set_option("newton_graph", 1)
+    assert g["graph"] == 1 and h["graph"] == 0
+    assert g["iters"] == h["iters"]
+    np.testing.assert_array_equal(g["active"], h["active"])
+    for k in ("h", "rho", "gradh", "divv", "xi", "ddivvdt"):
+        np.testing.assert_array_equal(g[k], h[k], err_msg=k)
+
+
+def test_newton_loop_graph_list_overflow_falls_back():
+    """A graph-run loop whose list rebuild outgrows the storage the first lists sized
+    reports it, and the solve is redone on the host loop: the results still equal the
+    oracle's bit for bit."""
+    c = capi.Cosmo(True)
+    assert c.set_option("graph_list_slack", 1) == 0
+    try:
+        p = inputs.plummer(12000, lnsigma=0.5, seed=29)
+        p["h"] = 0.5 * p["h"]            # h grows every iteration, and the lists with it
+        cc, o = run_pair(p, quintic=True)
+        assert cc.scalar("loopGraph") == 0
+        check_all(cc, o)
+    finally:
+        c.set_option("graph_list_slack", -1)
