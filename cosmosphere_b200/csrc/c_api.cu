@@ -712,7 +712,12 @@ int cosmo_x_set_option(const char* name, int value)
     if (k == "staging") { s.staging = value != 0; return 0; }
     if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
     if (k == "newton_graph") { s.newtonGraph = value != 0; return 0; }
-    if (k == "graph_list_slack") { s.graphListSlack = value; return 0; }
+    if (k == "graph_list_store")
+    {
+        if (value < 0) return -1;
+        s.graphListStorePct = value;
+        return 0;
+    }
     if (k == "spread_groups")
     {
         if (value < 0 || value > 32) return -1;
@@ -782,6 +787,9 @@ double cosmo_x_scalar(const char* name)
     if (k == "maxIter") return s.maxIter;
     if (k == "settling0") return double(s.settling0);
     if (k == "loopGraph") return double(s.lastLoopGraph);
+    if (k == "loopRebuilds") return double(s.lastLoopRebuilds);
+    if (k == "loopRowBuilds") return double(s.lastLoopRowBuilds);
+    if (k == "listTotal") return double(s.listTotal);
     if (s.hscal)
     {
         read_scalars(s);
@@ -882,6 +890,12 @@ long cosmo_x_array(const char* name, void* out, int* dtype)
             COSMO_CUDA(cudaMemcpy(&tot, s.jOffset.get() + nL, 4, cudaMemcpyDeviceToHost));
         }
         return put(s.jlist.get(), tot, 4, 1);
+    }
+    if (k == "loopListEntries")
+    {
+        if (dtype) *dtype = 4;
+        if (out) std::memcpy(out, s.loopListEntries.data(), s.loopListEntries.size() * 8);
+        return long(s.loopListEntries.size());
     }
     if (k == "activePerIter")
     {

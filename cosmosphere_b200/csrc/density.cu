@@ -329,10 +329,15 @@ __global__ void newton_copy_active_kernel(const int* __restrict__ src, int* __re
 
 // Last node of an iteration: what the host loop read back after it -- the counts, the
 // stale-list flag, the settling particles -- decides the next iteration on the device.
-__global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, cudaGraphConditionalHandle hMore)
+__global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, const uint32_t* listTotal,
+                                       cudaGraphConditionalHandle hMore)
 {
     const int it = L->iter;
-    if (it < kLoopIters) L->activePerIter[it] = L->nActiveParticles;
+    if (it < kLoopIters)
+    {
+        L->activePerIter[it] = L->nActiveParticles;
+        L->listEntries[it] = *listTotal;
+    }
     if (it == 0) L->settling0 = ds->settling;
     const int active = ds->unconverged;
     L->nActiveLeaves = ds->nextActive;
@@ -364,8 +369,8 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     cudaEvent_t j0 = ev(s);
     hmax_leaves(s, s.activeA.get(), nL);
     build_lists(s, false, kListMargin, false, true, cut.work);
-    const size_t listCap = s.graphListSlack >= 0 ? size_t(s.listTotal) + size_t(s.graphListSlack)
-                                                 : 2 * size_t(s.listTotal) + 65536;
+    const size_t listCap = s.graphListStorePct > 0 ? size_t(s.listTotal) * size_t(s.graphListStorePct) / 100
+                                                   : 2 * size_t(s.listTotal) + 65536;
     s.jlist.resize(std::max<size_t>(listCap, s.jlist.n), s.st, true);
     s.jlistPrev.resize(s.jlist.cap, s.st);
     s.listStore = std::min(listCap, s.jlist.cap);
@@ -494,7 +499,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
         COSMO_LAUNCHED();
         newton_copy_active_kernel<<<bgrid, 256, 0, s.st>>>(s.activeB.get(), s.activeA.get(), ds, nL);
         COSMO_LAUNCHED();
-        newton_epilogue_kernel<<<1, 1, 0, s.st>>>(L, ds, hMore);
+        newton_epilogue_kernel<<<1, 1, 0, s.st>>>(L, ds, s.jOffset.get() + nL, hMore);
         COSMO_LAUNCHED();
         if (cudaStreamEndCapture(s.st, &body) != cudaSuccess) break;
         kMain += g_launches.load() - c0;
@@ -530,6 +535,9 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     if (s.hscal->err & kErrListFull) return false;
     g_launches += h.iter * kMain + h.rebuilds * kList + h.rowBuilds * kRows;
     s.listTotal = total;
+    s.lastLoopRebuilds = h.rebuilds;
+    s.lastLoopRowBuilds = h.rowBuilds;
+    s.loopListEntries.assign(h.listEntries, h.listEntries + std::min(h.iter, kLoopIters));
     s.itersRun = h.iter;
     s.settling0 = h.settling0;
     s.activePerIter.assign(h.activePerIter, h.activePerIter + std::min(h.iter, kLoopIters));

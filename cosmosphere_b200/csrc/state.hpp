@@ -110,6 +110,7 @@ struct NewtonLoop
     int rowBuilds, pad0;
     long long settling0;
     long long activePerIter[kLoopIters];
+    unsigned int listEntries[kLoopIters];   // gather-list entries each iteration ran on
 };
 
 struct Timings
@@ -154,12 +155,15 @@ struct State
     // 0: one host round trip per iteration (cosmo_x_set_option "newton_graph",
     // COSMO_NEWTON_GRAPH).  The results are the same either way.
     int newtonGraph = 1;
-    // entries of list storage the graph loop adds to the first lists' total (negative: the
-    // built-in, the total again plus 65536); a small figure makes a rebuild outgrow it, so
-    // the fallback to the host loop can be exercised (cosmo_x_set_option "graph_list_slack")
-    long long graphListSlack = -1;
+    // list storage of the graph loop's rebuilds as a percentage of the first lists' total
+    // (0: the built-in, twice the total plus 65536 entries); a figure under 100 makes a
+    // rebuild outgrow it, so the fallback to the host loop can be exercised
+    // (cosmo_x_set_option "graph_list_store")
+    int graphListStorePct = 0;
     size_t listStore = 0;   // list entries a fill may write (0: all jlist holds)
     int lastLoopGraph = 0;  // the last solve's Newton loop ran as a graph (1) or on the host (0)
+    int lastLoopRebuilds = 0, lastLoopRowBuilds = 0;   // its list rebuilds and row builds
+    std::vector<long long> loopListEntries;              // its gather-list entries per iteration
     std::vector<long long> activePerIter;
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;

@@ -214,8 +214,11 @@ void cosmo_x_sync(void);
  * split_work / stream particles that scan the tree for their own box; 0 restores the
  * built-in 4096 and 131072); "spread_groups" sets how many h-ordered groups, at least, a
  * 64-particle window whose smoothing lengths spread by more than 1.5x is cut into (0 restores
- * the built-in 1; also COSMO_SPREAD_GROUPS).  Returns 0, or -1 for an unknown name or a value
- * out of range. */
+ * the built-in 1; also COSMO_SPREAD_GROUPS); "newton_graph" 1 (default) runs the Newton loop
+ * as one graph launch, 0 with a host round trip per iteration (also COSMO_NEWTON_GRAPH);
+ * "graph_list_store" sets the graph loop's list storage as a percentage of its first lists'
+ * total (0: the built-in; under 100 forces the fallback to the host loop, for tests).
+ * Returns 0, or -1 for an unknown name or a value out of range. */
 int cosmo_x_set_option(const char* name, int value);
 
 /* Time limit of every bounded device wait (the sort's look-back on its predecessor

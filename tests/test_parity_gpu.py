@@ -465,12 +465,11 @@ def test_newton_loop_graph_list_overflow_falls_back():
     reports it, and the solve is redone on the host loop: the results still equal the
     oracle's bit for bit."""
     c = capi.Cosmo(True)
-    assert c.set_option("graph_list_slack", 1) == 0
+    assert c.set_option("graph_list_store", 50) == 0    # half the first lists' entries
     try:
         p = inputs.plummer(12000, lnsigma=0.5, seed=29)
-        p["h"] = 0.5 * p["h"]            # h grows every iteration, and the lists with it
         cc, o = run_pair(p, quintic=True)
         assert cc.scalar("loopGraph") == 0
         check_all(cc, o)
     finally:
-        c.set_option("graph_list_slack", -1)
+        c.set_option("graph_list_store", 0)
