@@ -169,6 +169,12 @@ void release_state(State& s)
         b->release(s.st);
     s.box.release(s.st);
     s.dscal.release(s.st);
+    s.nloop.release(s.st);
+    if (s.loopGraphExec) COSMO_CUDA(cudaGraphExecDestroy(s.loopGraphExec));
+    if (s.loopGraphDef) COSMO_CUDA(cudaGraphDestroy(s.loopGraphDef));
+    s.loopGraphExec = nullptr;
+    s.loopGraphDef = nullptr;
+    s.loopGraphKey.clear();
     for (auto& e : s.evPool) COSMO_CUDA(cudaEventDestroy(e));
     s.evPool.clear();
     if (s.hscal)
@@ -788,6 +794,8 @@ double cosmo_x_scalar(const char* name)
     if (k == "settling0") return double(s.settling0);
     if (k == "loopGraph") return double(s.lastLoopGraph);
     if (k == "loopRebuilds") return double(s.lastLoopRebuilds);
+    if (k == "loopGraphBuilds") return double(s.loopGraphBuilds);
+    if (k == "loopGraphUpdates") return double(s.loopGraphUpdates);
     if (k == "loopRowBuilds") return double(s.lastLoopRowBuilds);
     if (k == "listTotal") return double(s.listTotal);
     if (s.hscal)

@@ -42,6 +42,7 @@ constexpr int      kMaxLevel = 21;              // 21 bits per axis, 63-bit keys
 constexpr uint64_t kKeyEnd   = 1ull << 63;      // one past the largest live key
 constexpr uint64_t kDeadKey  = ~0ull;           // h <= 0: sorted to the end (tree.cuh:99-104)
 constexpr uint32_t kBucket   = 64;              // leaf capacity, BUCKET_SIZE (tree.cuh:53)
+constexpr int kWalkScratch   = 512;             // list entries per leaf a count walk keeps for its fill
 
 inline int iceil(long a, long b) { return int((a + b - 1) / b); }
 

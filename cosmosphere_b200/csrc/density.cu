@@ -292,9 +292,11 @@ int grid_for(const State& s, int work)
 }
 
 // ---------------------------------------------------------- the Newton loop as a graph
-__global__ void newton_loop_init_kernel(NewtonLoop* L, int nLeaves, int nAlive, int maxIter)
+__global__ void newton_loop_init_kernel(NewtonLoop* L, int nLeaves, int numNodes, int nAlive, int maxIter)
 {
     *L = NewtonLoop{};
+    L->nLeaves = nLeaves;
+    L->numNodes = numNodes;
     L->nActiveLeaves = nLeaves;
     L->nActiveParticles = nAlive;
     L->maxIter = maxIter;
@@ -329,14 +331,14 @@ __global__ void newton_copy_active_kernel(const int* __restrict__ src, int* __re
 
 // Last node of an iteration: what the host loop read back after it -- the counts, the
 // stale-list flag, the settling particles -- decides the next iteration on the device.
-__global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, const uint32_t* listTotal,
+__global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, const uint32_t* jOffset,
                                        cudaGraphConditionalHandle hMore)
 {
     const int it = L->iter;
     if (it < kLoopIters)
     {
         L->activePerIter[it] = L->nActiveParticles;
-        L->listEntries[it] = *listTotal;
+        L->listEntries[it] = jOffset[L->nLeaves];
     }
     if (it == 0) L->settling0 = ds->settling;
     const int active = ds->unconverged;
@@ -349,6 +351,18 @@ __global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, cons
     cudaGraphSetConditional(hMore, unsigned(more));
 }
 
+// Bytes of the values a captured loop depends on.
+struct KeyBytes
+{
+    std::vector<unsigned char> b;
+    template<class T>
+    void add(const T& v)
+    {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+        b.insert(b.end(), p, p + sizeof(T));
+    }
+};
+
 } // namespace
 
 // The Newton loop of one solve as one graph launch: a while node whose body is one
@@ -356,31 +370,55 @@ __global__ void newton_epilogue_kernel(NewtonLoop* L, const DevScalars* ds, cons
 // incremental list rebuild], [the Newton rows], the work items, the Newton kernel, the
 // row kernel, the next active leaves and the epilogue that decides the next iteration.
 // Same kernels, same order, same decisions as the host loop, so the same results; the
-// first lists are built before it (their total sizes the storage of the rebuilds).
-// Returns false, having changed nothing the caller keeps, when the graph cannot be built
-// or a rebuild outgrew the storage: the caller then solves again on the host loop.
+// first lists are built before it (their total sizes the storage of the rebuilds).  The
+// graph reads the tree's counts on the device and is launched over the capacities of the
+// buffers, so it depends only on the buffers, the options and the solve's scalars: it is
+// captured and instantiated once and launched again by every later solve with the same
+// ones (a time-stepping caller's trees change; its buffers, grown to the largest tree,
+// do not).  Returns false, having changed nothing the caller keeps, when the graph cannot
+// be built or a rebuild outgrew the storage: the caller then solves again on the host loop.
 static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact, int maxIter, FixedSplit cut,
                               int spreadG, long long& nActiveParticles)
 {
     DevScalars* ds = s.dscal.get();
     const int nL = s.nLeaves;
-    const int itemCap = std::max(s.nAlive, 1);
     const bool mx = s.precision == 1;
     cudaEvent_t j0 = ev(s);
     hmax_leaves(s, s.activeA.get(), nL);
     build_lists(s, false, kListMargin, false, true, cut.work);
-    const size_t listCap = s.graphListStorePct > 0 ? size_t(s.listTotal) * size_t(s.graphListStorePct) / 100
-                                                   : 2 * size_t(s.listTotal) + 65536;
-    s.jlist.resize(std::max<size_t>(listCap, s.jlist.n), s.st, true);
-    s.jlistPrev.resize(s.jlist.cap, s.st);
-    s.listStore = std::min(listCap, s.jlist.cap);
-    s.jOffsetPrev.resize(size_t(nL) + 1, s.st);
+    // list storage of the rebuilds: grown to twice the first lists (never shrunk, so the
+    // graph's buffers stay put), or a set share of them for the fallback's test
+    size_t listStore;
+    if (s.graphListStorePct > 0)
+    {
+        listStore = size_t(s.listTotal) * size_t(s.graphListStorePct) / 100;
+        s.jlist.resize(std::max<size_t>(listStore, s.jlist.n), s.st, true);
+    }
+    else
+    {
+        const size_t want = 2 * size_t(s.listTotal) + 65536;
+        if (s.jlist.cap < want) s.jlist.resize(want, s.st, true);
+        listStore = s.jlist.cap;
+    }
+    if (s.jlistPrev.cap < s.jlist.cap) s.jlistPrev.resize(s.jlist.cap, s.st);
+    if (s.jOffsetPrev.cap < s.jOffset.cap) s.jOffsetPrev.resize(s.jOffset.cap, s.st);
     s.walked.resize(nL, s.st);
     s.nloop.resize(1, s.st);
     NewtonLoop* L = s.nloop.get();
-    newton_loop_init_kernel<<<1, 1, 0, s.st>>>(L, nL, s.nAlive, maxIter);
+    newton_loop_init_kernel<<<1, 1, 0, s.st>>>(L, nL, s.numNodes, s.nAlive, maxIter);
     COSMO_LAUNCHED();
     cudaEvent_t j1 = ev(s);
+
+    // launch extents: the buffers' capacities (every buffer was sized for this tree)
+    size_t lc = std::min<size_t>({s.activeA.cap, s.activeB.cap, s.leafNext.cap, s.jcount.cap, s.jstream.cap,
+                                  s.listH.cap, s.hmaxLeaf.cap, s.walked.cap, s.leafToInternal.cap,
+                                  s.walkScratch.cap / size_t(kWalkScratch)});
+    lc = std::min<size_t>({lc, s.jOffset.cap - 1, s.jOffsetPrev.cap - 1, s.layout.cap - 1});
+    const int leafCap = int(std::min<size_t>(lc, size_t(1) << 30));
+    const size_t ic = std::min<size_t>({s.items.cap, s.rowItems.cap, s.nblCount.cap, s.nblH.cap,
+                                        s.nblR2.cap / size_t(kNbl)});
+    const int itemCap = int(std::min<size_t>(ic, size_t(1) << 30));
+    scan_reserve(s, leafCap);
 
     RowsKernelFn nrows = mx ? mixed_newton_rows_kernel(s.periodic)
                             : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
@@ -390,150 +428,193 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     RowKernelFn rk = mx ? mixed_density_row_kernel(s.periodic)
                         : (s.periodic ? density_row_kernel<true, false> : density_row_kernel<false, false>);
     const int gridRows = persistent_grid(s, nrows, kThreads), gridNr = persistent_grid(s, nr, kThreads);
-    const int gridRow = std::max(1, std::min(iceil(s.nAlive, kThreads), 8 * s.numSMs));
-    const int bgrid = std::min(iceil(nL, 256), 4 * s.numSMs);
+    const int gridRow = std::max(1, std::min(iceil(itemCap, kThreads), 8 * s.numSMs));
+    const int bgrid = std::min(iceil(leafCap, 256), 4 * s.numSMs);
+    const int pgrid = grid_for(s, leafCap);
     const RowSplit rows{s.nblCount.get(), s.nblH.get(), kNbl, s.rowItems.get()};
+    const PreorderTree tree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, 0, &L->numNodes};
+    const long long waitNs = wait_limit_ns();
+    const int* dims = &L->nLeaves;
 
-    const unsigned long long launches0 = g_launches.load();
-    cudaGraph_t g = nullptr;
-    cudaGraphExec_t ex = nullptr;
-    bool built = false;
-    unsigned long long kMain = 0, kList = 0, kRows = 0;
-    do
+    KeyBytes key;
+    for (const void* q : {(const void*)L, (const void*)ds, (const void*)s.activeA.get(), (const void*)s.activeB.get(),
+                          (const void*)s.leafNext.get(), (const void*)s.items.get(), (const void*)s.rowItems.get(),
+                          (const void*)s.nblR2.get(), (const void*)s.nblCount.get(), (const void*)s.nblH.get(),
+                          (const void*)s.layout.get(), (const void*)s.converged.get(), (const void*)s.jstream.get(),
+                          (const void*)s.xyzh.get(), (const void*)s.rho.get(), (const void*)s.gradh.get(),
+                          (const void*)s.box.get(), (const void*)s.listH.get(), (const void*)s.preCenter.get(),
+                          (const void*)s.preHalf.get(), (const void*)s.preSkip.get(), (const void*)s.preLeaf.get(),
+                          (const void*)s.leafToInternal.get(), (const void*)s.centers.get(), (const void*)s.sizes.get(),
+                          (const void*)s.jOffset.get(), (const void*)s.jcount.get(), (const void*)s.jlist.get(),
+                          (const void*)s.jlistPrev.get(), (const void*)s.jOffsetPrev.get(), (const void*)s.walked.get(),
+                          (const void*)s.walkScratch.get(), (const void*)s.hmaxLeaf.get(), (const void*)s.hmaxPre.get(),
+                          (const void*)s.particleLeaf.get(), (const void*)s.scanTmp.get(), (const void*)nrows,
+                          (const void*)nr, (const void*)rk})
+        key.add(q);
+    for (long long v : {(long long)leafCap, (long long)itemCap, (long long)gridRows, (long long)gridNr,
+                        (long long)gridRow, (long long)bgrid, (long long)pgrid, (long long)s.periodic,
+                        (long long)spreadG, (long long)cut.stream, (long long)cut.work, (long long)listStore, waitNs,
+                        (long long)s.numSMs})
+        key.add(v);
+    for (double v : {pmass, tolh, hfact}) key.add(v);
+
+    if (!s.loopGraphExec || key.b != s.loopGraphKey)
     {
-        if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
-        cudaGraphConditionalHandle hMore, hList, hRows;
-        if (cudaGraphConditionalHandleCreate(&hMore, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
-        cudaGraphNodeParams wp = {};
-        wp.type = cudaGraphNodeTypeConditional;
-        wp.conditional.handle = hMore;
-        wp.conditional.type = cudaGraphCondTypeWhile;
-        wp.conditional.size = 1;
-        cudaGraphNode_t wnode;
-        if (cudaGraphAddNode(&wnode, g, nullptr, 0, &wp) != cudaSuccess) break;
-        cudaGraph_t body = wp.conditional.phGraph_out[0];
-        if (cudaGraphConditionalHandleCreate(&hList, body, 0, 0) != cudaSuccess) break;
-        if (cudaGraphConditionalHandleCreate(&hRows, body, 0, 0) != cudaSuccess) break;
-
-        // the branch conditions and hmax of the active leaves
-        unsigned long long c0 = g_launches.load();
-        if (cudaStreamBeginCaptureToGraph(s.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
-            break;
-        newton_decide_kernel<<<1, 1, 0, s.st>>>(L, hList, hRows);
-        COSMO_LAUNCHED();
-        hmax_leaves(s, s.activeA.get(), nL, &L->nActiveLeaves);
-        cudaStreamCaptureStatus cs;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t nd = 0;
-        const bool infoOk = cudaStreamGetCaptureInfo(s.st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess;
-        std::vector<cudaGraphNode_t> sink(deps, deps + (infoOk ? nd : 0));
-        if (cudaStreamEndCapture(s.st, &body) != cudaSuccess || !infoOk) break;
-        kMain += g_launches.load() - c0;
-
-        // [the incremental list rebuild]
-        cudaGraphNodeParams lp = {};
-        lp.type = cudaGraphNodeTypeConditional;
-        lp.conditional.handle = hList;
-        lp.conditional.type = cudaGraphCondTypeIf;
-        lp.conditional.size = 1;
-        cudaGraphNode_t lnode;
-        if (cudaGraphAddNode(&lnode, body, sink.data(), sink.size(), &lp) != cudaSuccess) break;
-        cudaGraph_t lbody = lp.conditional.phGraph_out[0];
-        c0 = g_launches.load();
-        if (cudaStreamBeginCaptureToGraph(s.st, lbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
-            break;
-        build_lists_device(s, kListMargin, true, cut.work);
-        newton_count_kernel<<<1, 1, 0, s.st>>>(L, 0);
-        COSMO_LAUNCHED();
-        if (cudaStreamEndCapture(s.st, &lbody) != cudaSuccess) break;
-        kList = g_launches.load() - c0;
-
-        // [the Newton rows of the still-active particles at their current h]
-        cudaGraphNodeParams rp = {};
-        rp.type = cudaGraphNodeTypeConditional;
-        rp.conditional.handle = hRows;
-        rp.conditional.type = cudaGraphCondTypeIf;
-        rp.conditional.size = 1;
-        cudaGraphNode_t rnode;
-        if (cudaGraphAddNode(&rnode, body, &lnode, 1, &rp) != cudaSuccess) break;
-        cudaGraph_t rbody = rp.conditional.phGraph_out[0];
-        c0 = g_launches.load();
-        if (cudaStreamBeginCaptureToGraph(s.st, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
-            break;
-        begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
-        COSMO_LAUNCHED();
-        plan_items_count_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
-            s.activeA.get(), &L->nActiveLeaves, nullptr, s.layout.get(), s.converged.get(), s.jstream.get(),
-            s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
-        COSMO_LAUNCHED();
-        nrows<<<gridRows, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(),
-                                               s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.box.get(),
-                                               s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
-        COSMO_LAUNCHED();
-        newton_count_kernel<<<1, 1, 0, s.st>>>(L, 1);
-        COSMO_LAUNCHED();
-        if (cudaStreamEndCapture(s.st, &rbody) != cudaSuccess) break;
-        kRows = g_launches.load() - c0;
-
-        // the iteration proper
-        c0 = g_launches.load();
-        if (cudaStreamBeginCaptureToGraph(s.st, body, &rnode, nullptr, 1, cudaStreamCaptureModeRelaxed) != cudaSuccess)
-            break;
-        begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
-        COSMO_LAUNCHED();
-        plan_items_count_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
-            s.activeA.get(), &L->nActiveLeaves, &L->rowsReady, s.layout.get(), s.converged.get(), s.jstream.get(),
-            s.xyzh.get(), s.items.get(), itemCap, ds, rows, cut, spreadG);
-        COSMO_LAUNCHED();
-        nr<<<gridNr, kThreads, 0, s.st>>>(
-            s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-            s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
-            s.leafNext.get(), s.activeB.get(),
-            PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
-            s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns());
-        COSMO_LAUNCHED();
-        rk<<<gridRow, kThreads, 0, s.st>>>(s.rowItems.get(), s.nblR2.get(), s.nblCount.get(), s.xyzh.get(),
-                                          s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact,
-                                          s.box.get(), s.listH.get(), s.particleLeaf.get(), s.leafNext.get(),
-                                          s.activeB.get(), ds);
-        COSMO_LAUNCHED();
-        newton_copy_active_kernel<<<bgrid, 256, 0, s.st>>>(s.activeB.get(), s.activeA.get(), ds, nL);
-        COSMO_LAUNCHED();
-        newton_epilogue_kernel<<<1, 1, 0, s.st>>>(L, ds, s.jOffset.get() + nL, hMore);
-        COSMO_LAUNCHED();
-        if (cudaStreamEndCapture(s.st, &body) != cudaSuccess) break;
-        kMain += g_launches.load() - c0;
-            if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) break;
-        built = true;
-    } while (false);
-    s.listStore = 0;
-    // what was captured did not run: the launches counted are those the graph executes
-    g_launches -= g_launches.load() - launches0;
-    if (!built)
-    {
-        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-        if (cudaStreamIsCapturing(s.st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+        if (s.loopGraphExec) COSMO_CUDA(cudaGraphExecDestroy(s.loopGraphExec));
+        if (s.loopGraphDef) COSMO_CUDA(cudaGraphDestroy(s.loopGraphDef));
+        s.loopGraphExec = nullptr;
+        s.loopGraphDef = nullptr;
+        s.loopGraphKey.clear();
+        s.listStore = listStore;
+        const unsigned long long launches0 = g_launches.load();
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        bool built = false;
+        unsigned long long kMain = 0, kList = 0, kRows = 0;
+        do
         {
-            cudaGraph_t junk = nullptr;
-            cudaStreamEndCapture(s.st, &junk);
-            if (junk) cudaGraphDestroy(junk);
+            if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
+            cudaGraphConditionalHandle hMore, hList, hRows;
+            if (cudaGraphConditionalHandleCreate(&hMore, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+            cudaGraphNodeParams wp = {};
+            wp.type = cudaGraphNodeTypeConditional;
+            wp.conditional.handle = hMore;
+            wp.conditional.type = cudaGraphCondTypeWhile;
+            wp.conditional.size = 1;
+            cudaGraphNode_t wnode;
+            if (cudaGraphAddNode(&wnode, g, nullptr, 0, &wp) != cudaSuccess) break;
+            cudaGraph_t body = wp.conditional.phGraph_out[0];
+            if (cudaGraphConditionalHandleCreate(&hList, body, 0, 0) != cudaSuccess) break;
+            if (cudaGraphConditionalHandleCreate(&hRows, body, 0, 0) != cudaSuccess) break;
+
+            // the branch conditions and hmax of the active leaves
+            unsigned long long c0 = g_launches.load();
+            if (cudaStreamBeginCaptureToGraph(s.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+                cudaSuccess)
+                break;
+            newton_decide_kernel<<<1, 1, 0, s.st>>>(L, hList, hRows);
+            COSMO_LAUNCHED();
+            hmax_leaves(s, s.activeA.get(), leafCap, &L->nActiveLeaves);
+            cudaStreamCaptureStatus cs;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            const bool infoOk = cudaStreamGetCaptureInfo(s.st, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess;
+            std::vector<cudaGraphNode_t> sink(deps, deps + (infoOk ? nd : 0));
+            if (cudaStreamEndCapture(s.st, &body) != cudaSuccess || !infoOk) break;
+            kMain += g_launches.load() - c0;
+
+            // [the incremental list rebuild]
+            cudaGraphNodeParams lp = {};
+            lp.type = cudaGraphNodeTypeConditional;
+            lp.conditional.handle = hList;
+            lp.conditional.type = cudaGraphCondTypeIf;
+            lp.conditional.size = 1;
+            cudaGraphNode_t lnode;
+            if (cudaGraphAddNode(&lnode, body, sink.data(), sink.size(), &lp) != cudaSuccess) break;
+            cudaGraph_t lbody = lp.conditional.phGraph_out[0];
+            c0 = g_launches.load();
+            if (cudaStreamBeginCaptureToGraph(s.st, lbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+                cudaSuccess)
+                break;
+            build_lists_device(s, kListMargin, true, cut.work, dims, leafCap);
+            newton_count_kernel<<<1, 1, 0, s.st>>>(L, 0);
+            COSMO_LAUNCHED();
+            if (cudaStreamEndCapture(s.st, &lbody) != cudaSuccess) break;
+            kList = g_launches.load() - c0;
+
+            // [the Newton rows of the still-active particles at their current h]
+            cudaGraphNodeParams rp = {};
+            rp.type = cudaGraphNodeTypeConditional;
+            rp.conditional.handle = hRows;
+            rp.conditional.type = cudaGraphCondTypeIf;
+            rp.conditional.size = 1;
+            cudaGraphNode_t rnode;
+            if (cudaGraphAddNode(&rnode, body, &lnode, 1, &rp) != cudaSuccess) break;
+            cudaGraph_t rbody = rp.conditional.phGraph_out[0];
+            c0 = g_launches.load();
+            if (cudaStreamBeginCaptureToGraph(s.st, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+                cudaSuccess)
+                break;
+            begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), leafCap, dims);
+            COSMO_LAUNCHED();
+            plan_items_count_kernel<<<pgrid, kThreads, 0, s.st>>>(
+                s.activeA.get(), &L->nActiveLeaves, nullptr, s.layout.get(), s.converged.get(), s.jstream.get(),
+                s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
+            COSMO_LAUNCHED();
+            nrows<<<gridRows, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(),
+                                                   s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.box.get(),
+                                                   s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
+            COSMO_LAUNCHED();
+            newton_count_kernel<<<1, 1, 0, s.st>>>(L, 1);
+            COSMO_LAUNCHED();
+            if (cudaStreamEndCapture(s.st, &rbody) != cudaSuccess) break;
+            kRows = g_launches.load() - c0;
+
+            // the iteration proper
+            c0 = g_launches.load();
+            if (cudaStreamBeginCaptureToGraph(s.st, body, &rnode, nullptr, 1, cudaStreamCaptureModeRelaxed) !=
+                cudaSuccess)
+                break;
+            begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), leafCap, dims);
+            COSMO_LAUNCHED();
+            plan_items_count_kernel<<<pgrid, kThreads, 0, s.st>>>(
+                s.activeA.get(), &L->nActiveLeaves, &L->rowsReady, s.layout.get(), s.converged.get(),
+                s.jstream.get(), s.xyzh.get(), s.items.get(), itemCap, ds, rows, cut, spreadG);
+            COSMO_LAUNCHED();
+            nr<<<gridNr, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(),
+                                              s.jlist.get(), s.xyzh.get(), s.rho.get(), s.gradh.get(),
+                                              s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
+                                              s.leafNext.get(), s.activeB.get(), tree, s.leafToInternal.get(),
+                                              s.centers.get(), s.sizes.get(), ds, waitNs);
+            COSMO_LAUNCHED();
+            rk<<<gridRow, kThreads, 0, s.st>>>(s.rowItems.get(), s.nblR2.get(), s.nblCount.get(), s.xyzh.get(),
+                                              s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact,
+                                              s.box.get(), s.listH.get(), s.particleLeaf.get(), s.leafNext.get(),
+                                              s.activeB.get(), ds);
+            COSMO_LAUNCHED();
+            newton_copy_active_kernel<<<bgrid, 256, 0, s.st>>>(s.activeB.get(), s.activeA.get(), ds, leafCap);
+            COSMO_LAUNCHED();
+            newton_epilogue_kernel<<<1, 1, 0, s.st>>>(L, ds, s.jOffset.get(), hMore);
+            COSMO_LAUNCHED();
+            if (cudaStreamEndCapture(s.st, &body) != cudaSuccess) break;
+            kMain += g_launches.load() - c0;
+            if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) break;
+            built = true;
+        } while (false);
+        s.listStore = 0;
+        // what was captured did not run: the launches counted are those the graph executes
+        g_launches -= g_launches.load() - launches0;
+        if (!built)
+        {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (cudaStreamIsCapturing(s.st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+            {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(s.st, &junk);
+                if (junk) cudaGraphDestroy(junk);
+            }
+            if (ex) cudaGraphExecDestroy(ex);
+            if (g) cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+            return false;
         }
-        if (ex) cudaGraphExecDestroy(ex);
-        if (g) cudaGraphDestroy(g);
-        (void)cudaGetLastError();
-        return false;
+        s.loopGraphDef = g;
+        s.loopGraphExec = ex;
+        s.loopGraphKey = key.b;
+        s.loopKernels[0] = kMain;
+        s.loopKernels[1] = kList;
+        s.loopKernels[2] = kRows;
+        ++s.loopGraphBuilds;
     }
-    COSMO_CUDA(cudaGraphLaunch(ex, s.st));
+    COSMO_CUDA(cudaGraphLaunch(s.loopGraphExec, s.st));
     cudaEvent_t j2 = ev(s);
     NewtonLoop h;
     uint32_t total = 0;
     COSMO_CUDA(cudaMemcpyAsync(&total, s.jOffset.get() + nL, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
     COSMO_CUDA(cudaMemcpyAsync(&h, L, sizeof(NewtonLoop), cudaMemcpyDeviceToHost, s.st));
     read_scalars(s);
-    COSMO_CUDA(cudaGraphExecDestroy(ex));
-    COSMO_CUDA(cudaGraphDestroy(g));
     if (s.hscal->err & kErrListFull) return false;
-    g_launches += h.iter * kMain + h.rebuilds * kList + h.rowBuilds * kRows;
+    g_launches += h.iter * s.loopKernels[0] + h.rebuilds * s.loopKernels[1] + h.rowBuilds * s.loopKernels[2];
     s.listTotal = total;
     s.lastLoopRebuilds = h.rebuilds;
     s.lastLoopRowBuilds = h.rowBuilds;

@@ -388,6 +388,7 @@ struct PreorderTree
     const int* __restrict__ skip;
     const int* __restrict__ leaf;
     int n0, n1;
+    const int* n1p = nullptr;   // when given, the end node n1 is read here (a captured graph)
 };
 
 // Stream the j particles of every leaf whose cell overlaps the box (c, e) -- and the
@@ -410,11 +411,12 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
     const int lane = threadIdx.x & 31;
     CandidateRing<Dbl, Float, Index, Staged> cr{ring, ringf, ringIdx, cx, cy, cz, sx, sy, sz, stage};
     auto fold = [&](double d, double L) { return (Periodic && L > 0.0) ? fmin(d, L - d) : d; };
+    const int n1 = t.n1p != nullptr ? *t.n1p : t.n1;
     int p = t.n0;
-    while (p < t.n1)
+    while (p < n1)
     {
         const int idx = p + lane;
-        const bool valid = idx < t.n1;
+        const bool valid = idx < n1;
         bool accept = false;
         int skip = 1, pl = -1;
         if (valid)
@@ -454,7 +456,7 @@ __device__ __forceinline__ void stream_walk(double4* ring, float4* ringf, int* r
             int rskip = __shfl_sync(0xffffffffu, skip, r);
             if (rskip < 1) rskip = 1;   // a subtree holds its root: the scan always advances
             const int target = p + r + rskip;
-            if (target >= p + 32 || target >= t.n1) { next = target; break; }
+            if (target >= p + 32 || target >= n1) { next = target; break; }
             pos = target - p;
         }
         emit &= __ballot_sync(0xffffffffu, pl >= 0);

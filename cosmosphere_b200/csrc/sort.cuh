@@ -60,8 +60,12 @@ __device__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
     return before + inc - v;
 }
 
-__global__ void scan_reduce_kernel(const uint32_t* __restrict__ in, int n, uint32_t* __restrict__ bsum)
+// nPtr (when given): the element count on the device, n then being a bound on it (a scan
+// issued before its count is known, as a captured graph does).
+__global__ void scan_reduce_kernel(const uint32_t* __restrict__ in, int n, uint32_t* __restrict__ bsum,
+                                   const int* __restrict__ nPtr = nullptr)
 {
+    if (nPtr) n = *nPtr;
     const long base = long(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
     uint32_t s = 0;
 #pragma unroll
@@ -72,8 +76,10 @@ __global__ void scan_reduce_kernel(const uint32_t* __restrict__ in, int n, uint3
     if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
 
-__global__ void scan_blocks_kernel(uint32_t* bsum, int nb, uint32_t* totalOut)
+__global__ void scan_blocks_kernel(uint32_t* bsum, int nb, uint32_t* totalOut, uint32_t* out = nullptr,
+                                   const int* __restrict__ nPtr = nullptr)
 {
+    if (nPtr) totalOut = out + *nPtr;   // the total goes after the last element
     // one block of kScanThreads; nb <= kScanTile
     const int base = threadIdx.x * kScanItems;
     uint32_t v[kScanItems], s = 0;
@@ -96,8 +102,9 @@ __global__ void scan_blocks_kernel(uint32_t* bsum, int nb, uint32_t* totalOut)
 }
 
 __global__ void scan_apply_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, int n,
-                                  const uint32_t* __restrict__ boff)
+                                  const uint32_t* __restrict__ boff, const int* __restrict__ nPtr = nullptr)
 {
+    if (nPtr) n = *nPtr;
     const long base = long(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems], s = 0;
 #pragma unroll

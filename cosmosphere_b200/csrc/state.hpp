@@ -105,6 +105,7 @@ struct DevScalars
 constexpr int kLoopIters = 128;
 struct NewtonLoop
 {
+    int nLeaves, numNodes;       // the tree's counts (the graph reads them, so it serves any tree)
     int nActiveLeaves, nActiveParticles, iter, maxIter;
     int rebuildNext, rowsNext, rowsReady, rebuilds;
     int rowBuilds, pad0;
@@ -162,6 +163,14 @@ struct State
     int graphListStorePct = 0;
     size_t listStore = 0;   // list entries a fill may write (0: all jlist holds)
     int lastLoopGraph = 0;  // the last solve's Newton loop ran as a graph (1) or on the host (0)
+    // The graph-run loop's instantiated graph, kept while the parameters it was captured
+    // with (the key: buffers, counts, scalars, launch shapes) stay the same; a solve with
+    // other parameters captures again and updates it in place.
+    cudaGraph_t loopGraphDef = nullptr;
+    cudaGraphExec_t loopGraphExec = nullptr;
+    std::vector<unsigned char> loopGraphKey;
+    unsigned long long loopKernels[3] = {0, 0, 0};   // kernels of the body, the list branch, the rows branch
+    int loopGraphBuilds = 0, loopGraphUpdates = 0;
     int lastLoopRebuilds = 0, lastLoopRowBuilds = 0;   // its list rebuilds and row builds
     std::vector<long long> loopListEntries;              // its gather-list entries per iteration
     std::vector<long long> activePerIter;
@@ -238,13 +247,18 @@ void build_lists(State& s, bool symmetric, double margin = 1.0, bool incremental
 // The same incremental gather-list rebuild with no host read (for a captured Newton
 // loop): the fill stays inside the storage jlist already holds, kErrListFull otherwise.
 // jOffsetPrev, jlistPrev (as large as jlist), walked and the walk scratch must be sized.
-void build_lists_device(State& s, double margin, bool rounded, uint32_t streamCap);
+// The leaf and node counts are read on the device (dims[0], dims[1]); leafCap bounds the
+// leaf count and sizes the launches, so the same sequence serves any tree up to it.
+void build_lists_device(State& s, double margin, bool rounded, uint32_t streamCap, const int* dims, int leafCap);
 // The symmetric lists and the symmetric neighbour rows of the current tree and h (the
 // force pass's pairs; every gather pair of the converged h is among them).
 void build_symmetric(State& s);
 void hmax_upsweep(State& s);
 void radix_sort_u64(State& s, uint64_t* kA, uint64_t* kB, int* vA, int* vB, int n, bool iotaValues);
 uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool readTotal);
+// The same with the element count on the device (*nPtr <= nCap); the total goes to out[*nPtr].
+void scan_exclusive_dev(State& s, const uint32_t* in, uint32_t* out, int nCap, const int* nPtr);
+void scan_reserve(State& s, int nCap);   // size the scan scratch for up to nCap elements
 
 // density.cu
 struct DensResult { int itersRun; int unconverged; int status; };

@@ -348,7 +348,6 @@ __global__ void hmax_level_kernel(int first, int last, const int* __restrict__ c
 }
 
 constexpr double kListLoose = 1.05;   // a kept list may be this much wider than a new one
-constexpr int kWalkScratch = 512;     // list entries per leaf the count pass keeps for the fill
 
 // ------------------------------------------------------------------ j-leaf list walk
 // One warp per i-leaf.  The tree is scanned in pre-order 32 nodes at a time: every lane
@@ -374,10 +373,16 @@ list_walk_kernel(int nL, int numNodes, const int* __restrict__ leafToInternal,
                  const uint32_t* __restrict__ layout, uint32_t* __restrict__ jstream, double margin,
                  double* __restrict__ listH, const uint32_t* __restrict__ jOffsetPrev,
                  const int* __restrict__ jlistPrev, int* __restrict__ walked, int* __restrict__ scratch,
-                 int rounded, uint32_t streamCap, uint32_t listCap)
+                 int rounded, uint32_t streamCap, uint32_t listCap, const int* __restrict__ dims)
 {
     const int lane = threadIdx.x & 31;
     const long leaf = (long(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (dims != nullptr)
+    {
+        // the leaf and node counts on the device (a captured graph); nL bounded them
+        nL = dims[0];
+        numNodes = dims[1];
+    }
     if (leaf >= nL) return;
     // A fill writes only inside [jOffset[leaf], jOffset[leaf + 1]); a list storage of
     // listCap entries that the lists outgrew (a build whose total the host did not read
@@ -576,6 +581,25 @@ uint32_t scan_exclusive(State& s, const uint32_t* in, uint32_t* out, int n, bool
     COSMO_CUDA(cudaMemcpyAsync(s.hsmall, out + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
     COSMO_CUDA(cudaStreamSynchronize(s.st));
     return uint32_t(s.hsmall[0]);
+}
+
+void scan_reserve(State& s, int nCap)
+{
+    s.scanTmp.resize(size_t(std::max(1, iceil(nCap, kScanTile))) + 1, s.st);
+}
+
+void scan_exclusive_dev(State& s, const uint32_t* in, uint32_t* out, int nCap, const int* nPtr)
+{
+    const int nb = std::max(1, iceil(nCap, kScanTile));
+    if (nb > kScanTile) fatal("scan_exclusive: %d elements exceed the scan capacity", nCap);
+    s.scanTmp.resize(size_t(nb) + 1, s.st);
+    uint32_t* bsum = s.scanTmp.get();
+    scan_reduce_kernel<<<nb, kScanThreads, 0, s.st>>>(in, nCap, bsum, nPtr);
+    COSMO_LAUNCHED();
+    scan_blocks_kernel<<<1, kScanThreads, 0, s.st>>>(bsum, nb, nullptr, out, nPtr);
+    COSMO_LAUNCHED();
+    scan_apply_kernel<<<nb, kScanThreads, 0, s.st>>>(in, out, nCap, bsum, nPtr);
+    COSMO_LAUNCHED();
 }
 
 __global__ void level_keys_kernel(const uint64_t* __restrict__ prefix, int n, uint64_t* __restrict__ lvl)
@@ -872,9 +896,10 @@ void hmax_upsweep(State& s)
 }
 
 template<bool Sym, bool Per>
-static void walk(State& s, bool fill, double margin, bool incremental, bool rounded, uint32_t streamCap)
+static void walk(State& s, bool fill, double margin, bool incremental, bool rounded, uint32_t streamCap,
+                 const int* dims = nullptr, int leafCap = 0)
 {
-    const int nL = s.nLeaves;
+    const int nL = dims ? leafCap : s.nLeaves;
     const int blocks = iceil(long(nL) * 32, kBlk);
     auto args = [&](auto kern) {
         kern<<<blocks, kBlk, 0, s.st>>>(nL, s.numNodes, s.leafToInternal.get(), s.centers.get(), s.sizes.get(),
@@ -887,17 +912,19 @@ static void walk(State& s, bool fill, double margin, bool incremental, bool roun
                                         incremental ? s.jlistPrev.get() : nullptr,
                                         incremental ? s.walked.get() : nullptr, s.walkScratch.get(),
                                         rounded ? 1 : 0, streamCap,
-                                        uint32_t(std::min<size_t>(s.listStore ? s.listStore : s.jlist.cap, 0xffffffffu)));
+                                        uint32_t(std::min<size_t>(s.listStore ? s.listStore : s.jlist.cap, 0xffffffffu)),
+                                        dims);
     };
     if (fill) args(list_walk_kernel<Sym, Per, true>);
     else args(list_walk_kernel<Sym, Per, false>);
     COSMO_LAUNCHED();
 }
 
-// Copy the lists' entries [0, *total) (the total on the device) into dst.
-__global__ void copy_list_kernel(const int* __restrict__ src, int* __restrict__ dst, const uint32_t* __restrict__ total)
+// Copy the lists' entries [0, jOffset[*nL]) (counts on the device) into dst.
+__global__ void copy_list_kernel(const int* __restrict__ src, int* __restrict__ dst, const uint32_t* __restrict__ jOffset,
+                                 const int* __restrict__ nL)
 {
-    const uint32_t n = *total;
+    const uint32_t n = jOffset[*nL];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
 }
 
@@ -906,18 +933,17 @@ __global__ void copy_list_kernel(const int* __restrict__ src, int* __restrict__ 
 // walk, and the fill writes into the storage already held (jlist.cap entries); a build
 // that would not fit raises kErrListFull and writes nothing past it.  Every size is fixed
 // when it is issued, so the sequence can be captured into a graph.
-void build_lists_device(State& s, double margin, bool rounded, uint32_t streamCap)
+void build_lists_device(State& s, double margin, bool rounded, uint32_t streamCap, const int* dims, int leafCap)
 {
-    const int nL = s.nLeaves;
-    COSMO_CUDA(cudaMemcpyAsync(s.jOffsetPrev.get(), s.jOffset.get(), (size_t(nL) + 1) * sizeof(uint32_t),
+    COSMO_CUDA(cudaMemcpyAsync(s.jOffsetPrev.get(), s.jOffset.get(), (size_t(leafCap) + 1) * sizeof(uint32_t),
                                cudaMemcpyDeviceToDevice, s.st));
-    copy_list_kernel<<<4 * s.numSMs, 256, 0, s.st>>>(s.jlist.get(), s.jlistPrev.get(), s.jOffset.get() + nL);
+    copy_list_kernel<<<4 * s.numSMs, 256, 0, s.st>>>(s.jlist.get(), s.jlistPrev.get(), s.jOffset.get(), dims);
     COSMO_LAUNCHED();
-    if (s.periodic) walk<false, true>(s, false, margin, true, rounded, streamCap);
-    else walk<false, false>(s, false, margin, true, rounded, streamCap);
-    scan_exclusive(s, s.jcount.get(), s.jOffset.get(), nL, false);
-    if (s.periodic) walk<false, true>(s, true, margin, true, rounded, streamCap);
-    else walk<false, false>(s, true, margin, true, rounded, streamCap);
+    if (s.periodic) walk<false, true>(s, false, margin, true, rounded, streamCap, dims, leafCap);
+    else walk<false, false>(s, false, margin, true, rounded, streamCap, dims, leafCap);
+    scan_exclusive_dev(s, s.jcount.get(), s.jOffset.get(), leafCap, dims);
+    if (s.periodic) walk<false, true>(s, true, margin, true, rounded, streamCap, dims, leafCap);
+    else walk<false, false>(s, true, margin, true, rounded, streamCap, dims, leafCap);
 }
 
 // include/tree.cuh:360-389: count, scan, size, fill -- for ALL leaves.  incremental

@@ -16,8 +16,10 @@ namespace cosmo {
 namespace {
 
 // Zero the per-iteration counters of the Newton work queue and the leaf re-queue flags.
-__global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restrict__ leafNext, int nL)
+__global__ void begin_iteration_kernel(DevScalars* __restrict__ ds, int* __restrict__ leafNext, int nL,
+                                       const int* __restrict__ nLp = nullptr)
 {
+    if (nLp) nL = *nLp;   // the leaf count on the device (a captured graph)
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t == 0)
     {
