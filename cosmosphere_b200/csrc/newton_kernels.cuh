@@ -180,10 +180,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                    const double* __restrict__ listH, void* __restrict__ rowsR2, int* __restrict__ nblCount,
                    double* __restrict__ rowH, DevScalars* __restrict__ ds)
 {
-    // mixed rows hold FP32 r^2; plain rows hold j, its r^2 recomputed from the positions
-    // (the same FP64 operations, so the same bits) by the row iterations: half the bytes
-    // of an FP64 r^2, and the positions are L2-resident
-    using R2 = typename std::conditional<Mixed, float, int>::type;
+    using R2 = typename std::conditional<Mixed, float, double>::type;   // FP32 rows in the mixed form
     R2* nblR2 = static_cast<R2*>(rowsR2);
     __shared__ __align__(16) unsigned char sScr[kWarpsPerBlock][kRowsScratch];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -218,12 +215,11 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                    jOffset[d.leaf], jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
                    [](const double4&) { return 0.0; },
-                   [&](const double4& g, const double4& pj, int j) {   // j within the wide support
+                   [&](const double4& g, const double4& pj, int) {   // r^2 within the wide support
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        const double r2 = pair_r2(dx, dy, dz);
-                       if constexpr (Mixed) return RowEntry<R2>{r2 * g.w < wide2, R2(r2)};
-                       else return RowEntry<R2>{r2 * g.w < wide2, j};
+                       return RowEntry<R2>{r2 * g.w < wide2, R2(r2)};
                    },
                    mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen);
         if (mine)
@@ -249,8 +245,6 @@ density_row_kernel(const int* __restrict__ rowItems, const void* __restrict__ ro
 {
     const int n = ds->rowParticles;
     const int lane = threadIdx.x & 31;
-    double lx = 0, ly = 0, lz = 0;
-    if (Periodic) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     unsigned long long pairs = 0;
     for (int t0 = blockIdx.x * blockDim.x; t0 < n; t0 += gridDim.x * blockDim.x)
     {
@@ -265,23 +259,13 @@ density_row_kernel(const int* __restrict__ rowItems, const void* __restrict__ ro
             const double hinv2 = 1.0 / (hi * hi);
             const float hinv2f = float(hinv2);
             const int cnt = nblCount[i];
-            using R2 = typename std::conditional<Mixed, float, int>::type;
+            using R2 = typename std::conditional<Mixed, float, double>::type;
             const R2* row = row_flat(static_cast<const R2*>(rowsR2), uint32_t(i));
             double sr = 0.0, sg = 0.0;
             KahanF kr, kg;
             unsigned int gp = 0;
-            auto pair = [&](R2 e) {
-                double r2;
-                if constexpr (Mixed) r2 = double(e);
-                else
-                {
-                    // the row builder's r^2 of (i, j), recomputed: same operands, same bits
-                    const double4 pj = ldg4(xyzh + e);
-                    double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
-                    r2 = pair_r2(dx, dy, dz);
-                }
-                const double q2 = r2 * hinv2;
+            auto pair = [&](R2 r2) {
+                const double q2 = double(r2) * hinv2;
                 if (!(q2 < kRadK2)) return;
                 ++gp;
                 if constexpr (!Mixed)
@@ -294,7 +278,7 @@ density_row_kernel(const int* __restrict__ rowItems, const void* __restrict__ ro
                 }
                 else
                 {
-                    const float q2f = float(e) * hinv2f;
+                    const float q2f = float(r2) * hinv2f;
                     const float q = sqrt_q(q2f);
                     float wk, dwk;
                     sph_kernel_f(q2f, q, wk, dwk);

@@ -238,26 +238,6 @@ __device__ __forceinline__ void for_flat_row(const float* __restrict__ row, int 
 }
 
 // f(entry) for the cnt entries of a row (row_of), in order, four loads ahead of their use.
-// f(j) for the cnt entries of a flat row of int (j indices), in order, 16 bytes per load.
-template<class F>
-__device__ __forceinline__ void for_flat_row(const int* __restrict__ row, int cnt, F&& f)
-{
-    const int4* r4 = reinterpret_cast<const int4*>(row);
-    int k = 0;
-    for (; k + 4 <= cnt; k += 4)
-    {
-        const int4 v = __ldg(r4 + (k >> 2));
-        f(v.x); f(v.y); f(v.z); f(v.w);
-    }
-    if (k < cnt)
-    {
-        const int4 v = __ldg(r4 + (k >> 2));
-        f(v.x);
-        if (k + 1 < cnt) f(v.y);
-        if (k + 2 < cnt) f(v.z);
-    }
-}
-
 template<class T, class F>
 __device__ __forceinline__ void for_row(const T* __restrict__ row, int cnt, F&& f)
 {
