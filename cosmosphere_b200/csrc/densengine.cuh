@@ -28,9 +28,6 @@
 namespace cosmo {
 
 constexpr int kRec = 256;   // pair records per warp
-// Mixed form: groups of at least this many particles evaluate with the particles on the
-// lanes (each lane its own particle's pairs); smaller ones with the candidates on the lanes.
-constexpr int kMixedOwnLanes = 12;
 
 // Per-warp shared scratch of density_group: the ring, the group's particles, the pair
 // records, and at kBoxAt the group's rounded box (read by the filter from shared memory
@@ -235,48 +232,6 @@ __device__ __forceinline__ void density_group(unsigned char* scr, bool mine, int
                         lg.add(fmaf(-q, dwk, -3.0f * wk));
                     }
                     gp += __popc(__ballot_sync(0xffffffffu, acc));
-                    return;
-                }
-                if (ng >= kMixedOwnLanes)
-                {
-                    // a full group: every member lane takes the batch's candidates one by
-                    // one from broadcast shared-memory reads and adds its accepted pairs to
-                    // its own compensated sums (no ballots, records or ordered owner sums:
-                    // the mixed form's sums need no particular order)
-                    if (mine)
-                    {
-                        const float px = gx[lane], py = gy[lane], pz = gz[lane], hh = gh[lane];
-                        unsigned int acc = 0;
-#pragma unroll 4
-                        for (int k = 0; k < count; ++k)
-                        {
-                            const float4 c = rf[(head + k) & (kRing - 1)];
-                            float dx, dy, dz;
-                            if (!Periodic || shifted)
-                            {
-                                dx = px - c.x;
-                                dy = py - c.y;
-                                dz = pz - c.z;
-                            }
-                            else
-                            {
-                                dx = axis_df<true>(px, c.x, Lx);
-                                dy = axis_df<true>(py, c.y, Ly);
-                                dz = axis_df<true>(pz, c.z, Lz);
-                            }
-                            const float q2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) * hh;
-                            if (q2 < float(kRadK2))
-                            {
-                                const float q = sqrt_q(q2);
-                                float wk, dwk;
-                                sph_kernel_f(q2, q, wk, dwk);
-                                kr.add(wk);
-                                kg.add(fmaf(-q, dwk, -3.0f * wk));
-                                ++acc;
-                            }
-                        }
-                        gp += acc;
-                    }
                     return;
                 }
                 int nrec = 0, segStart = 0, segCount = 0;
