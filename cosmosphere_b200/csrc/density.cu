@@ -305,11 +305,10 @@ __global__ void newton_loop_init_kernel(NewtonLoop* L, int nLeaves, int numNodes
 // First node of an iteration: the list-rebuild and row-build decisions the last
 // iteration's epilogue recorded become the conditions of this iteration's two branches.
 __global__ void newton_decide_kernel(const NewtonLoop* L, cudaGraphConditionalHandle hList,
-                                     cudaGraphConditionalHandle hRows, cudaGraphConditionalHandle hPlain)
+                                     cudaGraphConditionalHandle hRows)
 {
     cudaGraphSetConditional(hList, L->rebuildNext ? 1u : 0u);
     cudaGraphSetConditional(hRows, L->rowsNext ? 1u : 0u);
-    cudaGraphSetConditional(hPlain, L->rowsNext ? 0u : 1u);
 }
 
 __global__ void newton_count_kernel(NewtonLoop* L, int rows)
@@ -421,9 +420,8 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     const int itemCap = int(std::min<size_t>(ic, size_t(1) << 30));
     scan_reserve(s, leafCap);
 
-    RowsUpdateKernelFn nrows =
-        mx ? mixed_newton_rows_update_kernel(s.periodic)
-           : (s.periodic ? newton_rows_update_kernel<true, false> : newton_rows_update_kernel<false, false>);
+    RowsKernelFn nrows = mx ? mixed_newton_rows_kernel(s.periodic)
+                            : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
     NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic, s.staging)
                   : s.staging ? (s.periodic ? density_nr_kernel<true, false, true> : density_nr_kernel<false, false, true>)
                               : (s.periodic ? density_nr_kernel<true, false, false> : density_nr_kernel<false, false, false>);
@@ -472,13 +470,11 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
         cudaGraph_t g = nullptr;
         cudaGraphExec_t ex = nullptr;
         bool built = false;
-        unsigned long long kMain = 0, kList = 0, kRows = 0, kPlain = 0;
-        const NewtonUpdate up{s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact, s.leafNext.get(),
-                              s.activeB.get()};
+        unsigned long long kMain = 0, kList = 0, kRows = 0;
         do
         {
             if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
-            cudaGraphConditionalHandle hMore, hList, hRows, hPlain;
+            cudaGraphConditionalHandle hMore, hList, hRows;
             if (cudaGraphConditionalHandleCreate(&hMore, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
             cudaGraphNodeParams wp = {};
             wp.type = cudaGraphNodeTypeConditional;
@@ -490,14 +486,13 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
             cudaGraph_t body = wp.conditional.phGraph_out[0];
             if (cudaGraphConditionalHandleCreate(&hList, body, 0, 0) != cudaSuccess) break;
             if (cudaGraphConditionalHandleCreate(&hRows, body, 0, 0) != cudaSuccess) break;
-            if (cudaGraphConditionalHandleCreate(&hPlain, body, 0, 0) != cudaSuccess) break;
 
             // the branch conditions and hmax of the active leaves
             unsigned long long c0 = g_launches.load();
             if (cudaStreamBeginCaptureToGraph(s.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
                 cudaSuccess)
                 break;
-            newton_decide_kernel<<<1, 1, 0, s.st>>>(L, hList, hRows, hPlain);
+            newton_decide_kernel<<<1, 1, 0, s.st>>>(L, hList, hRows);
             COSMO_LAUNCHED();
             hmax_leaves(s, s.activeA.get(), leafCap, &L->nActiveLeaves);
             cudaStreamCaptureStatus cs;
@@ -527,8 +522,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
             if (cudaStreamEndCapture(s.st, &lbody) != cudaSuccess) break;
             kList = g_launches.load() - c0;
 
-            // [the rows iteration: the rows of the still-active particles at their current h,
-            // built by a pass that also takes their Newton step; then the cut items]
+            // [the Newton rows of the still-active particles at their current h]
             cudaGraphNodeParams rp = {};
             rp.type = cudaGraphNodeTypeConditional;
             rp.conditional.handle = hRows;
@@ -549,34 +543,16 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
             COSMO_LAUNCHED();
             nrows<<<gridRows, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(),
                                                    s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.box.get(),
-                                                   s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds,
-                                                   up);
-            COSMO_LAUNCHED();
-            cut_items_only_kernel<<<1, 1, 0, s.st>>>(ds);
-            COSMO_LAUNCHED();
-            nr<<<gridNr, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(),
-                                              s.jlist.get(), s.xyzh.get(), s.rho.get(), s.gradh.get(),
-                                              s.converged.get(), pmass, tolh, hfact, s.box.get(), s.listH.get(),
-                                              s.leafNext.get(), s.activeB.get(), tree, s.leafToInternal.get(),
-                                              s.centers.get(), s.sizes.get(), ds, waitNs);
+                                                   s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
             COSMO_LAUNCHED();
             newton_count_kernel<<<1, 1, 0, s.st>>>(L, 1);
             COSMO_LAUNCHED();
             if (cudaStreamEndCapture(s.st, &rbody) != cudaSuccess) break;
             kRows = g_launches.load() - c0;
 
-            // [every other iteration: the work items (rows-complete particles on their
-            // rows once rows exist), the Newton kernel, the row kernel]
-            cudaGraphNodeParams pp = {};
-            pp.type = cudaGraphNodeTypeConditional;
-            pp.conditional.handle = hPlain;
-            pp.conditional.type = cudaGraphCondTypeIf;
-            pp.conditional.size = 1;
-            cudaGraphNode_t pnode;
-            if (cudaGraphAddNode(&pnode, body, &rnode, 1, &pp) != cudaSuccess) break;
-            cudaGraph_t pbody = pp.conditional.phGraph_out[0];
+            // the iteration proper
             c0 = g_launches.load();
-            if (cudaStreamBeginCaptureToGraph(s.st, pbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+            if (cudaStreamBeginCaptureToGraph(s.st, body, &rnode, nullptr, 1, cudaStreamCaptureModeRelaxed) !=
                 cudaSuccess)
                 break;
             begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), leafCap, dims);
@@ -596,14 +572,6 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
                                               s.box.get(), s.listH.get(), s.particleLeaf.get(), s.leafNext.get(),
                                               s.activeB.get(), ds);
             COSMO_LAUNCHED();
-            if (cudaStreamEndCapture(s.st, &pbody) != cudaSuccess) break;
-            kPlain = g_launches.load() - c0;
-
-            // the next active leaves and the epilogue
-            c0 = g_launches.load();
-            if (cudaStreamBeginCaptureToGraph(s.st, body, &pnode, nullptr, 1, cudaStreamCaptureModeRelaxed) !=
-                cudaSuccess)
-                break;
             newton_copy_active_kernel<<<bgrid, 256, 0, s.st>>>(s.activeB.get(), s.activeA.get(), ds, leafCap);
             COSMO_LAUNCHED();
             newton_epilogue_kernel<<<1, 1, 0, s.st>>>(L, ds, s.jOffset.get(), hMore);
@@ -636,7 +604,6 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
         s.loopKernels[0] = kMain;
         s.loopKernels[1] = kList;
         s.loopKernels[2] = kRows;
-        s.loopKernels[3] = kPlain;
         ++s.loopGraphBuilds;
     }
     COSMO_CUDA(cudaGraphLaunch(s.loopGraphExec, s.st));
@@ -647,8 +614,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     COSMO_CUDA(cudaMemcpyAsync(&h, L, sizeof(NewtonLoop), cudaMemcpyDeviceToHost, s.st));
     read_scalars(s);
     if (s.hscal->err & kErrListFull) return false;
-    g_launches += h.iter * s.loopKernels[0] + h.rebuilds * s.loopKernels[1] + h.rowBuilds * s.loopKernels[2] +
-                  (h.iter - h.rowBuilds) * s.loopKernels[3];
+    g_launches += h.iter * s.loopKernels[0] + h.rebuilds * s.loopKernels[1] + h.rowBuilds * s.loopKernels[2];
     s.listTotal = total;
     s.lastLoopRebuilds = h.rebuilds;
     s.lastLoopRowBuilds = h.rowBuilds;
@@ -739,12 +705,24 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         cudaEvent_t j1 = ev(s);
         {
             const int bgrid = std::min(iceil(nL, 256), 4 * s.numSMs);
-            const bool mx = s.precision == 1;
-            // the rows iteration: rows of the still-active particles at their h after the
-            // last update, built by a pass that also takes this iteration's Newton step of
-            // those particles; the Newton kernel then takes the cut items alone
-            const bool rowsNow =
-                !rowsReady && iter >= 1 && nActiveParticles > 0 && 5 * settlingPrev >= 4 * nActiveParticles;
+            if (!rowsReady && iter >= 1 && nActiveParticles > 0 && 5 * settlingPrev >= 4 * nActiveParticles)
+            {
+                // rows of the still-active particles at their h after the last update
+                begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
+                COSMO_LAUNCHED();
+                plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
+                    s.activeA.get(), nActiveLeaves, s.layout.get(), s.converged.get(), s.jstream.get(),
+                    s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
+                COSMO_LAUNCHED();
+                RowsKernelFn nrows = s.precision == 1
+                                         ? mixed_newton_rows_kernel(s.periodic)
+                                         : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
+                nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
+                    s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
+                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
+                COSMO_LAUNCHED();
+                rowsReady = true;
+            }
             begin_iteration_kernel<<<bgrid, 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
             COSMO_LAUNCHED();
             plan_items_kernel<<<grid_for(s, nActiveLeaves), kThreads, 0, s.st>>>(
@@ -754,20 +732,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                           : RowSplit{nullptr, nullptr, 0, nullptr},
                 cut, spreadG);
             COSMO_LAUNCHED();
-            if (rowsNow)
-            {
-                RowsUpdateKernelFn nrows =
-                    mx ? mixed_newton_rows_update_kernel(s.periodic)
-                       : (s.periodic ? newton_rows_update_kernel<true, false> : newton_rows_update_kernel<false, false>);
-                nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
-                    s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
-                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds,
-                    NewtonUpdate{s.rho.get(), s.gradh.get(), s.converged.get(), pmass, tolh, hfact,
-                                 s.leafNext.get(), s.activeB.get()});
-                COSMO_LAUNCHED();
-                cut_items_only_kernel<<<1, 1, 0, s.st>>>(ds);
-                COSMO_LAUNCHED();
-            }
+            const bool mx = s.precision == 1;
             NrKernelFn nr = mx ? mixed_density_nr_kernel(s.periodic, s.staging)
                           : s.staging ? (s.periodic ? density_nr_kernel<true, false, true>
                                                     : density_nr_kernel<false, false, true>)
@@ -780,8 +745,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 PreorderTree{s.preCenter.get(), s.preHalf.get(), s.preSkip.get(), s.preLeaf.get(), 0, s.numNodes},
                 s.leafToInternal.get(), s.centers.get(), s.sizes.get(), ds, wait_limit_ns());
             COSMO_LAUNCHED();
-            if (rowsNow) rowsReady = true;
-            else if (rowsReady)
+            if (rowsReady)
             {
                 RowKernelFn rk = mx ? mixed_density_row_kernel(s.periodic)
                                     : (s.periodic ? density_row_kernel<true, false> : density_row_kernel<false, false>);

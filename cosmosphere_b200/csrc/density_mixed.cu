@@ -15,9 +15,9 @@ NrKernelFn mixed_density_nr_kernel(bool periodic, bool staged)
     return periodic ? density_nr_kernel<true, true, false> : density_nr_kernel<false, true, false>;
 }
 
-RowsUpdateKernelFn mixed_newton_rows_update_kernel(bool periodic)
+RowsKernelFn mixed_newton_rows_kernel(bool periodic)
 {
-    return periodic ? newton_rows_update_kernel<true, true> : newton_rows_update_kernel<false, true>;
+    return periodic ? newton_rows_kernel<true, true> : newton_rows_kernel<false, true>;
 }
 
 RowKernelFn mixed_density_row_kernel(bool periodic)

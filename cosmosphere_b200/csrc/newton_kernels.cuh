@@ -171,32 +171,14 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
 // kRowMargin of the particle's support, in ascending j.  A row is complete while the
 // particle's h stays within kRowMargin of the h it was built at and within the radius its
 // leaf's list covers; rowH records that bound.
-//
-// The same pass also takes this iteration's Newton step of the particles it builds
-// rows for.  The owner lane meets every candidate's exact r^2 in ascending j as it
-// appends, so it adds the density sums of the pairs inside the support on the way -- the
-// row kernel's arithmetic in the row kernel's order, hence the same bits -- and a row
-// that overflows still gets its full sums.  Cut groups keep the group path (the Newton
-// kernel, run after this pass on the cut items alone).
-struct NewtonUpdate
-{
-    double* rho;
-    double* gradh;
-    int* converged;
-    double pmass, tolh, hfact;
-    int* leafNext;
-    int* nextLeaves;
-};
 
 template<bool Periodic, bool Mixed>
-__device__ __forceinline__ void newton_rows_pass(const int4* __restrict__ items, int cap,
-                                                 const uint32_t* __restrict__ layout,
-                                                 const uint32_t* __restrict__ jOffset,
-                                                 const uint32_t* __restrict__ jcount, const int* __restrict__ jlist,
-                                                 double4* __restrict__ xyzh, const DevBox* __restrict__ box,
-                                                 const double* __restrict__ listH, void* __restrict__ rowsR2,
-                                                 int* __restrict__ nblCount, double* __restrict__ rowH,
-                                                 DevScalars* __restrict__ ds, const NewtonUpdate& up)
+__global__ void __launch_bounds__(kThreads)
+newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
+                   const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
+                   const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
+                   const double* __restrict__ listH, void* __restrict__ rowsR2, int* __restrict__ nblCount,
+                   double* __restrict__ rowH, DevScalars* __restrict__ ds)
 {
     using R2 = typename std::conditional<Mixed, float, double>::type;   // FP32 rows in the mixed form
     R2* nblR2 = static_cast<R2*>(rowsR2);
@@ -209,7 +191,6 @@ __device__ __forceinline__ void newton_rows_pass(const int4* __restrict__ items,
     if (ds->err & kErrListFull) return;
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     const double wide2 = kRadK2 * (kRowMargin * kRowMargin);
-    unsigned long long pairs = 0;
     for (;;)
     {
         const int w = next_item(ds, nHeavy, nItems, cap);
@@ -226,14 +207,10 @@ __device__ __forceinline__ void newton_rows_pass(const int4* __restrict__ items,
         }
         const double4 pi = xyzh[i];
         const double hinv2 = 1.0 / (pi.w * pi.w);
-        const float hinv2f = float(hinv2);
         const double rs = kRadKernel * kRowMargin * pi.w;
         const double rmax = warp_max(mine ? rs : 0.0);
         const GroupBox bx = group_box(mine, pi.x, pi.y, pi.z, rs, rmax);
         int rowLen = 0;
-        double sr = 0.0, sg = 0.0;
-        KahanF kr, kg;
-        unsigned int gp = 0;
         rows_group<1, Periodic>(sScr[wib], mine, d.ng, make_double4(pi.x, pi.y, pi.z, hinv2), rs, bx, lx, ly, lz,
                    jOffset[d.leaf], jcount[d.leaf], jlist, LayoutRanges{layout}, xyzh,
                    [&](const double4& pj) { return in_gather_box<Periodic>(pj, bx, lx, ly, lz); },
@@ -242,35 +219,7 @@ __device__ __forceinline__ void newton_rows_pass(const int4* __restrict__ items,
                        double dx = g.x - pj.x, dy = g.y - pj.y, dz = g.z - pj.z;
                        nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
                        const double r2 = pair_r2(dx, dy, dz);
-                       const bool keep = r2 * g.w < wide2;
-                       {
-                           // the owner's own pair (exact is called by the owner lane alone):
-                           // density_row_kernel's sums on the r^2 the row stores
-                           const R2 e = R2(r2);
-                           const double q2 = double(e) * hinv2;
-                           if (keep && q2 < kRadK2)
-                           {
-                               ++gp;
-                               if constexpr (!Mixed)
-                               {
-                                   const double q = sqrt(q2);
-                                   double wk, dwk;
-                                   sph_kernel(q2, q, wk, dwk);
-                                   sr += wk;
-                                   sg += -q * dwk - 3.0 * wk;
-                               }
-                               else
-                               {
-                                   const float q2f = float(e) * hinv2f;
-                                   const float q = sqrt_q(q2f);
-                                   float wk, dwk;
-                                   sph_kernel_f(q2f, q, wk, dwk);
-                                   kr.add(wk);
-                                   kg.add(fmaf(-q, dwk, -3.0f * wk));
-                               }
-                           }
-                       }
-                       return RowEntry<R2>{keep, R2(r2)};
+                       return RowEntry<R2>{r2 * g.w < wide2, R2(r2)};
                    },
                    mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen);
         if (mine)
@@ -278,55 +227,7 @@ __device__ __forceinline__ void newton_rows_pass(const int4* __restrict__ items,
             nblCount[i] = rowLen;
             rowH[i] = fmin(kRowMargin * pi.w, listH[d.leaf]) * (1.0 - 1e-12);
         }
-        {
-            bool stillActive = false, settle = false;
-            if (mine)
-            {
-                if constexpr (Mixed) { sr = kr.value(); sg = kg.value(); }
-                pairs += gp;
-                double ro, go, ho;
-                int conv;
-                stillActive = newton_step(sr, sg, pi.w, up.pmass, up.hfact, up.tolh, ro, go, ho, conv);
-                up.rho[i] = ro;
-                up.gradh[i] = go;
-                reinterpret_cast<double*>(xyzh + i)[3] = ho;
-                up.converged[i] = conv;
-                if (stillActive && ho > listH[d.leaf]) ds->listStale = 1;
-                settle = stillActive && fabs(ho - pi.w) < kSettle * pi.w;
-            }
-            const uint32_t still = __ballot_sync(0xffffffffu, stillActive);
-            const uint32_t settled = __ballot_sync(0xffffffffu, settle);
-            if (still && lane == 0)
-            {
-                atomicAdd(&ds->settling, __popc(settled));
-                atomicAdd(&ds->unconverged, __popc(still));
-                if (atomicExch(&up.leafNext[d.leaf], 1) == 0) up.nextLeaves[atomicAdd(&ds->nextActive, 1)] = d.leaf;
-            }
-        }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
-    if (lane == 0) atomicAdd(&ds->pairs[0], pairs);
-}
-
-template<bool Periodic, bool Mixed>
-__global__ void __launch_bounds__(kThreads)
-newton_rows_update_kernel(const int4* __restrict__ items, int cap, const uint32_t* __restrict__ layout,
-                          const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
-                          const int* __restrict__ jlist, double4* __restrict__ xyzh, const DevBox* __restrict__ box,
-                          const double* __restrict__ listH, void* __restrict__ rowsR2, int* __restrict__ nblCount,
-                          double* __restrict__ rowH, DevScalars* __restrict__ ds, NewtonUpdate up)
-{
-    newton_rows_pass<Periodic, Mixed>(items, cap, layout, jOffset, jcount, jlist, xyzh, box, listH, rowsR2,
-                                            nblCount, rowH, ds, up);
-}
-
-// After a row-and-update pass: the Newton kernel of the same iteration takes only the cut
-// items, which sit at the front of the queue.
-__global__ void cut_items_only_kernel(DevScalars* ds)
-{
-    ds->itemsLight = 0;
-    ds->workCounter[0] = 0;
 }
 
 // One Newton iteration for the particles whose rows are complete for their h: one lane
@@ -411,12 +312,12 @@ density_row_kernel(const int* __restrict__ rowItems, const void* __restrict__ ro
 
 // The three Newton kernels share one signature per kind whatever the form.
 using NrKernelFn = decltype(&density_nr_kernel<false, false, false>);
-using RowsUpdateKernelFn = decltype(&newton_rows_update_kernel<false, false>);
+using RowsKernelFn = decltype(&newton_rows_kernel<false, false>);
 using RowKernelFn = decltype(&density_row_kernel<false, false>);
 
 // The mixed form's kernels, compiled in density_mixed.cu.
 NrKernelFn mixed_density_nr_kernel(bool periodic, bool staged);
-RowsUpdateKernelFn mixed_newton_rows_update_kernel(bool periodic);
+RowsKernelFn mixed_newton_rows_kernel(bool periodic);
 RowKernelFn mixed_density_row_kernel(bool periodic);
 
 } // namespace cosmo

@@ -169,8 +169,7 @@ struct State
     cudaGraph_t loopGraphDef = nullptr;
     cudaGraphExec_t loopGraphExec = nullptr;
     std::vector<unsigned char> loopGraphKey;
-    // kernels of the body, the list branch, the rows branch, the other iterations' branch
-    unsigned long long loopKernels[4] = {0, 0, 0, 0};
+    unsigned long long loopKernels[3] = {0, 0, 0};   // kernels of the body, the list branch, the rows branch
     int loopGraphBuilds = 0, loopGraphUpdates = 0;
     int lastLoopRebuilds = 0, lastLoopRowBuilds = 0;   // its list rebuilds and row builds
     std::vector<long long> loopListEntries;              // its gather-list entries per iteration
