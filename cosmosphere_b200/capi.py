@@ -22,6 +22,7 @@ EXPORTS = [
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
     "cosmo_x_stats_line", "cosmo_x_set_option", "cosmo_x_set_wait_limit", "cosmo_x_get_wait_limit", "cosmo_x_wait_test",
+    "cosmo_x_set_key_extent", "cosmo_x_refresh_h", "cosmo_x_set_frozen",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
     "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_set_tuning",
@@ -58,6 +59,10 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_stats_line.restype = I
     L.cosmo_x_set_option.argtypes = [ctypes.c_char_p, I]
     L.cosmo_x_set_option.restype = I
+    L.cosmo_x_set_key_extent.argtypes = [ctypes.c_void_p]
+    L.cosmo_x_refresh_h.restype = I
+    L.cosmo_x_set_frozen.argtypes = [ctypes.c_void_p, I]
+    L.cosmo_x_set_frozen.restype = I
     L.cosmo_x_set_wait_limit.argtypes = [ctypes.c_longlong]
     L.cosmo_x_get_wait_limit.restype = ctypes.c_longlong
     L.cosmo_x_wait_test.argtypes = [I, I]
@@ -178,6 +183,25 @@ class Cosmo:
 
     def set_option(self, name: str, value: int) -> int:
         return int(self.L.cosmo_x_set_option(name.encode(), int(value)))
+
+    def set_key_extent(self, ext6=None):
+        """Open boundaries: the extents (xmin, xmax, ymin, ymax, zmin, zmax) the solves' box
+        and keys are made from; None returns to the uploaded particles' own."""
+        if ext6 is None:
+            self.L.cosmo_x_set_key_extent(None)
+        else:
+            self._ext = np.ascontiguousarray(np.asarray(ext6, dtype=np.float64))
+            self.L.cosmo_x_set_key_extent(self._ext.ctypes.data)
+
+    def refresh_h(self) -> int:
+        return int(self.L.cosmo_x_refresh_h())
+
+    def set_frozen(self, mask=None) -> int:
+        """Particles the next solves take as neighbours only (caller order); None clears."""
+        if mask is None:
+            return int(self.L.cosmo_x_set_frozen(None, 0))
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.int32))
+        return int(self.L.cosmo_x_set_frozen(m.ctypes.data, int(m.size)))
 
     def set_wait_limit(self, ns: int):
         self.L.cosmo_x_set_wait_limit(int(ns))

@@ -739,6 +739,39 @@ int cosmo_x_set_option(const char* name, int value)
     return -1;
 }
 
+void cosmo_x_set_key_extent(const double* ext6)
+{
+    State& s = state();
+    s.keyExtentSet = ext6 != nullptr;
+    if (ext6) std::copy(ext6, ext6 + 6, s.keyExtent);
+}
+
+int cosmo_x_set_frozen(const int* mask, int n)
+{
+    State& s = state();
+    ensure_init(s);
+    if (mask == nullptr || n <= 0)
+    {
+        s.frozenFor = 0;
+        return 0;
+    }
+    s.frozen.resize(size_t(n), s.st);
+    COSMO_CUDA(cudaMemcpyAsync(s.frozen.get(), mask, size_t(n) * sizeof(int), cudaMemcpyHostToDevice, s.st));
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    s.frozenFor = n;
+    return 0;
+}
+
+int cosmo_x_refresh_h(void)
+{
+    State& s = state();
+    if (!s.st || s.nLeaves <= 0 || s.orderFor != s.ngas) return -1;
+    hmax_leaves(s, s.allLeaves.get(), s.nLeaves);
+    s.jlistToken = s.rowsToken = 0;
+    COSMO_CUDA(cudaStreamSynchronize(s.st));
+    return 0;
+}
+
 void cosmo_x_set_wait_limit(long long ns)
 {
     g_waitLimitNs.store(ns > 0 ? ns : 1000000000ll);
@@ -793,6 +826,14 @@ double cosmo_x_scalar(const char* name)
     if (k == "maxIter") return s.maxIter;
     if (k == "settling0") return double(s.settling0);
     if (k == "loopGraph") return double(s.lastLoopGraph);
+    if (k == "hmaxSeen" && s.hscal)
+    {
+        read_scalars(s);
+        const unsigned long long b = s.hscal->hmaxSeen;
+        double v;
+        std::memcpy(&v, &b, sizeof v);
+        return v;
+    }
     if (k == "loopRebuilds") return double(s.lastLoopRebuilds);
     if (k == "loopGraphBuilds") return double(s.loopGraphBuilds);
     if (k == "loopGraphUpdates") return double(s.loopGraphUpdates);

@@ -291,6 +291,17 @@ int grid_for(const State& s, int work)
     return std::max(1, std::min(maxBlocks, iceil(work, kWarpsPerBlock)));
 }
 
+// Converged flags of the fixed particles (the caller's mask through the sort order).
+__global__ void freeze_kernel(const int* __restrict__ order, const int* __restrict__ frozen, int nAlive,
+                              int* __restrict__ converged, DevScalars* __restrict__ ds)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool f = k < nAlive && frozen[order[k]] != 0;
+    if (k < nAlive) converged[k] = f ? 1 : 0;
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&ds->frozenAlive, __popc(m));
+}
+
 // ---------------------------------------------------------- the Newton loop as a graph
 __global__ void newton_loop_init_kernel(NewtonLoop* L, int nLeaves, int numNodes, int nAlive, int maxIter)
 {
@@ -405,7 +416,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     s.walked.resize(nL, s.st);
     s.nloop.resize(1, s.st);
     NewtonLoop* L = s.nloop.get();
-    newton_loop_init_kernel<<<1, 1, 0, s.st>>>(L, nL, s.numNodes, s.nAlive, maxIter);
+    newton_loop_init_kernel<<<1, 1, 0, s.st>>>(L, nL, s.numNodes, int(nActiveParticles), maxIter);
     COSMO_LAUNCHED();
     cudaEvent_t j1 = ev(s);
 
@@ -646,6 +657,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     COSMO_CUDA(cudaMemsetAsync(s.gradh.get(), 0, size_t(n) * 8, s.st));
     COSMO_CUDA(cudaMemsetAsync(s.converged.get(), 0, size_t(n) * 4, s.st));
     COSMO_CUDA(cudaMemsetAsync(&ds->pairs[0], 0, sizeof(ds->pairs), s.st));
+    COSMO_CUDA(cudaMemsetAsync(&ds->hmaxSeen, 0, sizeof(ds->hmaxSeen), s.st));
 
     build_tree(s, periodicBox, withGradients);
     s.orderFor = n;
@@ -663,6 +675,16 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     COSMO_CUDA(cudaMemcpyAsync(s.activeA.get(), s.allLeaves.get(), size_t(nL) * 4, cudaMemcpyDeviceToDevice, s.st));
     int nActiveLeaves = nL;
     long long nActiveParticles = s.nAlive;
+    if (s.frozenFor == n && s.nAlive > 0)
+    {
+        // the caller's fixed particles start converged: neighbours only
+        COSMO_CUDA(cudaMemsetAsync(&ds->frozenAlive, 0, sizeof(int), s.st));
+        freeze_kernel<<<iceil(s.nAlive, 256), 256, 0, s.st>>>(s.orderA.get(), s.frozen.get(), s.nAlive,
+                                                             s.converged.get(), ds);
+        COSMO_LAUNCHED();
+        read_scalars(s);
+        nActiveParticles = s.nAlive - s.hscal->frozenAlive;
+    }
 
     // The gather lists are built with a widened radius and reused while every active h
     // stays inside it: a superset list in ascending leaf order offers the same accepted

@@ -97,7 +97,8 @@ struct DevScalars
     int rowParticles;            // particles of the current iteration on their neighbour rows
     int settling;                // unconverged particles whose h moved by less than kSettle
     int rowOverflow;             // some symmetric row overflowed (its particle takes the group path)
-    int pad[1];
+    int frozenAlive;             // live particles a solve keeps fixed (neighbours only)
+    unsigned long long hmaxSeen; // bits of the largest h any leaf had at the start of an iteration
 };
 
 // The single-set Newton loop run as a graph: what the host loop kept in host variables
@@ -162,6 +163,15 @@ struct State
     // (cosmo_x_set_option "graph_list_store")
     int graphListStorePct = 0;
     size_t listStore = 0;   // list entries a fill may write (0: all jlist holds)
+    // Open boundaries: the particle extents the bounding box is made from, when the caller
+    // gives them (a rank of a decomposed set uses the whole set's, so its keys and order
+    // are the whole set's); otherwise the extents of the particles uploaded.
+    // Particles a solve takes as neighbours only (caller order, 1 = fixed): they start
+    // converged, so the Newton loop never updates them (a rank's halo particles).
+    DBuf<int> frozen;
+    int frozenFor = 0;   // the particle count the mask was given for (0: none)
+    bool keyExtentSet = false;
+    double keyExtent[6] = {0, 0, 0, 0, 0, 0};   // xmin, xmax, ymin, ymax, zmin, zmax
     int lastLoopGraph = 0;  // the last solve's Newton loop ran as a graph (1) or on the host (0)
     // The graph-run loop's instantiated graph, kept while the parameters it was captured
     // with (the key: buffers, counts, scalars, launch shapes) stay the same; a solve with

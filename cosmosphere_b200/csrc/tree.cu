@@ -58,6 +58,14 @@ __global__ void bbox_partial_kernel(const double* __restrict__ x, const double* 
 
 // Open boundaries (src/tree.cu:54-72): a cube of side 1.00001 x the largest span,
 // centred on the particles.
+// One block partial holding given extents (min x, y, z then max x, y, z).
+__global__ void set_extent_kernel(double* part, double x0, double x1, double y0, double y1, double z0, double z1)
+{
+    if (threadIdx.x != 0) return;
+    part[0] = x0; part[1] = y0; part[2] = z0;
+    part[3] = x1; part[4] = y1; part[5] = z1;
+}
+
 __global__ void bbox_final_kernel(const double* __restrict__ part, int nb, DevBox* box)
 {
     // one warp: lanes stride over the block partials, then a shuffle reduction (min and
@@ -309,7 +317,7 @@ __global__ void iota_kernel(int* __restrict__ a, int n)
 // include/tree.cuh:177-191: largest finite h of each listed leaf.
 __global__ void hmax_leaf_kernel(const double4* __restrict__ xyzh, const uint32_t* __restrict__ layout,
                                  const int* __restrict__ leaves, int nActive, double* __restrict__ hmax,
-                                 const int* __restrict__ countPtr)
+                                 const int* __restrict__ countPtr, unsigned long long* __restrict__ seen)
 {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= (countPtr != nullptr ? *countPtr : nActive)) return;
@@ -321,6 +329,8 @@ __global__ void hmax_leaf_kernel(const double4* __restrict__ xyzh, const uint32_
         if (isfinite(hj)) hm = fmax(hm, hj);
     }
     hmax[l] = hm;
+    // the largest h of the solve so far (non-negative doubles order as their bit patterns)
+    if (seen != nullptr) atomicMax(seen, (unsigned long long)__double_as_longlong(hm));
 }
 
 // include/tree.cuh:196-217, one level, deepest first.
@@ -764,6 +774,16 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
         set_box_kernel<<<1, 32, 0, s.st>>>(periodicBox[0], periodicBox[1], periodicBox[2], periodicBox[3],
                                             periodicBox[4], periodicBox[5], s.box.get());
     }
+    else if (s.keyExtentSet)
+    {
+        // the caller's extents (a rank of a decomposed set: the whole set's), through the
+        // same box construction
+        s.redTmp.resize(6, s.st);
+        const double* e = s.keyExtent;
+        set_extent_kernel<<<1, 32, 0, s.st>>>(s.redTmp.get(), e[0], e[1], e[2], e[3], e[4], e[5]);
+        COSMO_LAUNCHED();
+        bbox_final_kernel<<<1, 32, 0, s.st>>>(s.redTmp.get(), 1, s.box.get());
+    }
     else
     {
         const int nb = std::min(iceil(n, kBlk), 2 * s.numSMs);
@@ -874,7 +894,7 @@ void hmax_leaves(State& s, const int* leaves, int nActive, const int* countPtr)
 {
     if (nActive <= 0) return;
     hmax_leaf_kernel<<<iceil(nActive, kBlk), kBlk, 0, s.st>>>(s.xyzh.get(), s.layout.get(), leaves, nActive,
-                                                             s.hmaxLeaf.get(), countPtr);
+                                                             s.hmaxLeaf.get(), countPtr, &s.dscal.get()->hmaxSeen);
     COSMO_LAUNCHED();
 }
 

@@ -221,6 +221,25 @@ void cosmo_x_sync(void);
  * Returns 0, or -1 for an unknown name or a value out of range. */
 int cosmo_x_set_option(const char* name, int value);
 
+/* Open boundaries: the particle extents (xmin, xmax, ymin, ymax, zmin, zmax) the next
+ * solves make their bounding box, keys and order from, instead of the uploaded particles'
+ * own; NULL returns to the latter.  A rank of a set decomposed over several GPUs gives the
+ * whole set's extents, so its particles and halo sort in the whole set's order and its
+ * sums run in the order of a solve of the whole set. */
+void cosmo_x_set_key_extent(const double* ext6);
+
+/* Particles the next solves of n particles take as neighbours only (mask in caller order,
+ * nonzero = fixed): they start converged, so the Newton loop never updates them and the
+ * loop ends when the others have converged (a rank's halo particles).  NULL or n <= 0
+ * clears it.  Returns 0. */
+int cosmo_x_set_frozen(const int* mask, int n);
+
+/* After h (HSML) and rho/gradh (DENS_OUT) were replaced with cosmo_upload_sorted -- a
+ * rank of a decomposed set takes its halo particles' converged values from their owners
+ * -- refresh what the force pass derives from h: the leaves' hmax, and the symmetric
+ * lists and rows, rebuilt by the next force pass.  Returns 0, or -1 with no solved set. */
+int cosmo_x_refresh_h(void);
+
 /* Time limit of every bounded device wait (the sort's look-back on its predecessor
  * tiles, the staging barriers of the bulk copies), in nanoseconds; <= 0 restores the
  * default of 1 s.  A wait that runs out raises a bit in the device error word, and the
