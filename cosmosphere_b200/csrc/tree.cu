@@ -320,17 +320,31 @@ __global__ void hmax_leaf_kernel(const double4* __restrict__ xyzh, const uint32_
                                  const int* __restrict__ countPtr, unsigned long long* __restrict__ seen)
 {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= (countPtr != nullptr ? *countPtr : nActive)) return;
-    const int l = leaves[t];
+    const bool on = t < (countPtr != nullptr ? *countPtr : nActive);
     double hm = 0.0;
-    for (uint32_t j = layout[l]; j < layout[l + 1]; ++j)
+    if (on)
     {
-        const double hj = xyzh[j].w;
-        if (isfinite(hj)) hm = fmax(hm, hj);
+        const int l = leaves[t];
+        for (uint32_t j = layout[l]; j < layout[l + 1]; ++j)
+        {
+            const double hj = xyzh[j].w;
+            if (isfinite(hj)) hm = fmax(hm, hj);
+        }
+        hmax[l] = hm;
     }
-    hmax[l] = hm;
-    // the largest h of the solve so far (non-negative doubles order as their bit patterns)
-    if (seen != nullptr) atomicMax(seen, (unsigned long long)__double_as_longlong(hm));
+    // the largest h of the solve so far, one atomic per warp (non-negative doubles order
+    // as their bit patterns)
+    if (seen != nullptr)
+    {
+        unsigned long long b = (unsigned long long)__double_as_longlong(hm);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            const unsigned long long v = __shfl_xor_sync(0xffffffffu, b, o);
+            b = v > b ? v : b;
+        }
+        if ((threadIdx.x & 31) == 0 && b != 0) atomicMax(seen, b);
+    }
 }
 
 // include/tree.cuh:196-217, one level, deepest first.
