@@ -10,6 +10,11 @@ descent over timed solves of a sample of the class's sets, each timed on the dev
 (`t_total`, CUDA events around the whole batched solve) and taken as the minimum of a
 few repeats.
 
+Beside the per-class parameters, the batch as a whole picks how the Newton kernel feeds
+its j-stream -- loaded directly, or staged into shared memory by bulk copies
+(`cp.async.bulk` on an mbarrier) -- by timing the whole batch both ways (one launch serves
+every set, so this choice cannot differ by class).
+
 None of the parameters changes a plain-FP64 result: every pair test is exact and each
 particle's sums run over its accepted pairs in ascending j whatever the tree, the lists
 or the cut, so a tuned solve returns the same h, rho and d(rho)/dh bit for bit.  In the
@@ -101,9 +106,11 @@ def coordinate_descent(cost: Callable[[Tuning], float], start: Tuning = DEFAULT,
 class Table:
     """Tuned parameters per size class, with the default for classes never tuned."""
 
-    def __init__(self, entries: Dict[int, Tuning] | None = None, times: Dict[int, dict] | None = None):
+    def __init__(self, entries: Dict[int, Tuning] | None = None, times: Dict[int, dict] | None = None,
+                 staging: int = 0):
         self.entries: Dict[int, Tuning] = dict(entries or {})
         self.times: Dict[int, dict] = dict(times or {})
+        self.staging = int(staging)   # the batch's j-stream feed: 1 staged, 0 direct
 
     def for_size(self, n: int) -> Tuning:
         return self.entries.get(size_class(n), DEFAULT)
@@ -117,17 +124,21 @@ class Table:
                 "split_work": np.array([t.split_work for t in ts], dtype=np.int32)}
 
     def apply(self, batch) -> None:
-        """Set every set of a capi.Batch to its class's parameters."""
+        """Set every set of a capi.Batch to its class's parameters, and the batch's feed."""
         batch.set_tuning(**self.per_set(batch.sizes))
+        batch.set_staging(bool(self.staging))
+
+    def with_staging(self, staging: int) -> "Table":
+        return Table(self.entries, self.times, staging)
 
     def to_json(self) -> dict:
         return {"classes": {str(k): asdict(v) for k, v in sorted(self.entries.items())},
-                "times": {str(k): v for k, v in sorted(self.times.items())}}
+                "times": {str(k): v for k, v in sorted(self.times.items())}, "staging": self.staging}
 
     @classmethod
     def from_json(cls, d: dict) -> "Table":
         ent = {int(k): Tuning(**v) for k, v in d.get("classes", {}).items()}
-        return cls(ent, {int(k): v for k, v in d.get("times", {}).items()})
+        return cls(ent, {int(k): v for k, v in d.get("times", {}).items()}, int(d.get("staging", 0)))
 
     def save(self, path: str | os.PathLike) -> None:
         with open(path, "w") as f:
@@ -176,12 +187,19 @@ def batch_time(sets, table: "Table", repeats: int = 2, final_rho: bool = True) -
 
 
 def confirm(sets, table: "Table", repeats: int = 2, timer: Callable = batch_time):
-    """The tuned table or the defaults, whichever solves the whole batch faster: the
-    classes are tuned on samples solved alone, and a setting can lose a few percent once
-    every set shares the GPU.  Returns (table, tuned seconds, default seconds)."""
-    t_tuned = timer(sets, table, repeats)
-    t_default = timer(sets, Table(), repeats)
-    return (table if t_tuned <= t_default else Table()), t_tuned, t_default
+    """The tuned table or the defaults, each with the direct and the staged j-stream feed,
+    whichever solves the whole batch fastest: the classes are tuned on samples solved
+    alone, and a setting can lose a few percent once every set shares the GPU.  Returns
+    (table, tuned seconds, default seconds), the seconds of each with its better feed."""
+    times = {}
+    for name, base in (("tuned", table), ("default", Table())):
+        for st in (0, 1):
+            times[(name, st)] = timer(sets, base.with_staging(st), repeats)
+    t_tuned = min(times[("tuned", 0)], times[("tuned", 1)])
+    t_default = min(times[("default", 0)], times[("default", 1)])
+    name, st = min(times, key=lambda k: (times[k], k[0] != "tuned", k[1]))
+    best = (table if name == "tuned" else Table()).with_staging(st)
+    return best, t_tuned, t_default
 
 
 def tune(sets, max_particles: float = 2.0e6, repeats: int = 2, sweeps: int = 1,

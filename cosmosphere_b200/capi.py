@@ -22,7 +22,7 @@ EXPORTS = [
     "cosmo_pin_host", "cosmo_unpin_host", "cosmo_kernel_radius", "densityiterate_gpu_c", "force_gpu_c",
     "cosmo_x_set_max_iter", "cosmo_x_density", "cosmo_x_sync", "cosmo_x_scalar", "cosmo_x_array",
     "cosmo_x_stats_line", "cosmo_x_set_option", "cosmo_x_set_wait_limit", "cosmo_x_get_wait_limit", "cosmo_x_wait_test",
-    "cosmo_x_set_key_extent", "cosmo_x_refresh_h", "cosmo_x_set_frozen",
+    "cosmo_x_set_key_extent", "cosmo_x_refresh_h", "cosmo_x_set_frozen", "cosmo_batch_set_staging",
     "cosmo_x_set_device", "cosmo_x_mark", "cosmo_x_mark_elapsed", "cosmo_x_launches", "cosmo_x_fp64_peak",
     "cosmo_hilbert_order_noalloc", "cosmo_set_precision", "cosmo_get_precision",
     "cosmo_batch_init", "cosmo_batch_set_params", "cosmo_batch_set_bucket", "cosmo_batch_set_tuning",
@@ -61,6 +61,7 @@ def _bind(L: ctypes.CDLL) -> ctypes.CDLL:
     L.cosmo_x_set_option.restype = I
     L.cosmo_x_set_key_extent.argtypes = [ctypes.c_void_p]
     L.cosmo_x_refresh_h.restype = I
+    L.cosmo_batch_set_staging.argtypes = [I]
     L.cosmo_x_set_frozen.argtypes = [ctypes.c_void_p, I]
     L.cosmo_x_set_frozen.restype = I
     L.cosmo_x_set_wait_limit.argtypes = [ctypes.c_longlong]
@@ -292,6 +293,10 @@ class Batch:
         self._keep = (pm, per, box)
         cat = lambda k: np.ascontiguousarray(np.concatenate([np.asarray(s[k], dtype=np.float64) for s in sets]))
         self.x, self.y, self.z, self.h = cat("x"), cat("y"), cat("z"), cat("h")
+
+    def set_staging(self, on: bool):
+        """The batched Newton kernel's j-stream feed: staged by bulk copies or direct."""
+        self.L.cosmo_batch_set_staging(1 if on else 0)
 
     def set_tuning(self, bucket=None, list_margin=None, split_stream=None, split_work=None):
         """Per-set launch parameters (each a scalar or one value per set; None keeps it)."""

@@ -1132,6 +1132,13 @@ void cosmo_batch_set_bucket(const int* bucketPerSet)
     for (int k = 0; k < B.nsets; ++k) B.tuning[4 * size_t(k)] = bucketPerSet[k];
 }
 
+void cosmo_batch_set_staging(int on)
+{
+    Batch& B = batch();
+    ensure_init(B.core);
+    B.core.staging = on != 0 ? 1 : 0;
+}
+
 int cosmo_batch_set_tuning(const int* bucket, const double* listMargin, const int* splitStream, const int* splitWork)
 {
     Batch& B = batch();

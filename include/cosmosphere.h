@@ -105,6 +105,11 @@ int cosmo_batch_init(int nsets, const int* offsets);
 void cosmo_batch_set_params(const double* pmass, const int* periodic, const double* box6);
 /* Leaf capacity of each set's tree (default 64, the reference's BUCKET_SIZE). */
 void cosmo_batch_set_bucket(const int* bucket_per_set);
+/* The batched Newton kernel's j-stream feed for every set of the batch: 1 staged into
+ * shared memory by bulk copies, 0 (default) loaded directly.  Results do not depend on
+ * it; the autotuner picks it for the whole batch. */
+void cosmo_batch_set_staging(int on);
+
 /* Per-set launch parameters, as an autotuner picks them (NULL keeps a parameter):
  * bucket = leaf capacity (8..1024); list_margin = widening of the gather radius the lists
  * are walked at, which lets them serve later iterations (1..2, default 1.15);

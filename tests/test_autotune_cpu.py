@@ -83,17 +83,32 @@ def test_apply_passes_per_set_arrays():
         def set_tuning(self, **kw):
             self.kw = kw
 
+        def set_staging(self, on):
+            self.staging = on
+
     b = FakeBatch()
     at.Table({at.size_class(300000): at.Tuning(bucket=128)}).apply(b)
     assert b.kw["bucket"].tolist() == [64, 128]
     assert b.kw["split_work"].tolist() == [131072, 131072]
+    assert b.staging is False
+    at.Table({}, staging=1).apply(b)
+    assert b.staging is True
 
 
 def test_confirm_keeps_the_faster_of_tuned_and_default():
     tuned = at.Table({14: at.Tuning(bucket=128)})
     times = {True: 1.0, False: 2.0}
     t, a, b = at.confirm([], tuned, timer=lambda sets, table, r: times[bool(table.entries)])
-    assert t is tuned and (a, b) == (1.0, 2.0)
+    assert t.entries == tuned.entries and t.staging == 0 and (a, b) == (1.0, 2.0)
     times = {True: 3.0, False: 2.0}
     t, a, b = at.confirm([], tuned, timer=lambda sets, table, r: times[bool(table.entries)])
     assert t.entries == {} and (a, b) == (3.0, 2.0)
+
+
+def test_confirm_picks_the_batch_feed():
+    tuned = at.Table({14: at.Tuning(bucket=128)})
+    cost = {(True, 0): 2.0, (True, 1): 1.5, (False, 0): 2.5, (False, 1): 2.4}
+    t, a, b = at.confirm([], tuned, timer=lambda sets, table, r: cost[(bool(table.entries), table.staging)])
+    assert t.entries == tuned.entries and t.staging == 1 and (a, b) == (1.5, 2.4)
+    t2 = at.Table.from_json(t.to_json())
+    assert t2.staging == 1 and t2.entries == t.entries
