@@ -175,6 +175,7 @@ void release_state(State& s)
     s.loopGraphExec = nullptr;
     s.loopGraphDef = nullptr;
     s.loopGraphKey.clear();
+    s.loopKeyPending.clear();
     for (auto& e : s.evPool) COSMO_CUDA(cudaEventDestroy(e));
     s.evPool.clear();
     if (s.hscal)

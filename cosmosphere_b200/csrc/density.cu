@@ -388,8 +388,10 @@ struct KeyBytes
 // ones (a time-stepping caller's trees change; its buffers, grown to the largest tree,
 // do not).  Returns false, having changed nothing the caller keeps, when the graph cannot
 // be built or a rebuild outgrew the storage: the caller then solves again on the host loop.
-static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact, int maxIter, FixedSplit cut,
-                              int spreadG, long long& nActiveParticles)
+enum class LoopGraph { Ran, Deferred, Failed };
+
+static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double hfact, int maxIter, FixedSplit cut,
+                                   int spreadG, long long& nActiveParticles)
 {
     DevScalars* ds = s.dscal.get();
     const int nL = s.nLeaves;
@@ -471,6 +473,15 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
 
     if (!s.loopGraphExec || key.b != s.loopGraphKey)
     {
+        // a graph is built for parameters met a second time in a row (a stepping caller's
+        // solves, whose buffers have stopped growing); a one-off solve -- another set, a
+        // new particle mass, a buffer that grew -- runs on the host loop, with the first
+        // lists already built, instead of paying a capture and an instantiation
+        if (key.b != s.loopKeyPending)
+        {
+            s.loopKeyPending = key.b;
+            return LoopGraph::Deferred;
+        }
         if (s.loopGraphExec) COSMO_CUDA(cudaGraphExecDestroy(s.loopGraphExec));
         if (s.loopGraphDef) COSMO_CUDA(cudaGraphDestroy(s.loopGraphDef));
         s.loopGraphExec = nullptr;
@@ -607,7 +618,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
             if (ex) cudaGraphExecDestroy(ex);
             if (g) cudaGraphDestroy(g);
             (void)cudaGetLastError();
-            return false;
+            return LoopGraph::Failed;
         }
         s.loopGraphDef = g;
         s.loopGraphExec = ex;
@@ -624,7 +635,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     COSMO_CUDA(cudaMemcpyAsync(&total, s.jOffset.get() + nL, sizeof(uint32_t), cudaMemcpyDeviceToHost, s.st));
     COSMO_CUDA(cudaMemcpyAsync(&h, L, sizeof(NewtonLoop), cudaMemcpyDeviceToHost, s.st));
     read_scalars(s);
-    if (s.hscal->err & kErrListFull) return false;
+    if (s.hscal->err & kErrListFull) return LoopGraph::Failed;
     g_launches += h.iter * s.loopKernels[0] + h.rebuilds * s.loopKernels[1] + h.rowBuilds * s.loopKernels[2];
     s.listTotal = total;
     s.lastLoopRebuilds = h.rebuilds;
@@ -636,7 +647,7 @@ static bool newton_loop_graph(State& s, double pmass, double tolh, double hfact,
     nActiveParticles = h.nActiveParticles;
     s.t.jbuild += elapsed_s(j0, j1);
     s.t.nrkern += elapsed_s(j1, j2);
-    return true;
+    return LoopGraph::Ran;
 }
 
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh, double hfact,
@@ -701,9 +712,12 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     bool graphRan = false;
     if (allowGraph && s.newtonGraph && maxIter <= kLoopIters && nActiveParticles > 0)
     {
-        graphRan = newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles);
+        const LoopGraph lg = newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles);
+        graphRan = lg == LoopGraph::Ran;
         listsWidened = graphRan;
-        if (!graphRan && (s.hscal->err & kErrListFull))
+        // deferred: the first lists are built and valid for the host loop's first iteration
+        if (lg == LoopGraph::Deferred) listsValid = listsWidened = true;
+        if (lg == LoopGraph::Failed && (s.hscal->err & kErrListFull))
         {
             // a list rebuild outgrew the storage the first lists sized: solve again from
             // the caller's arrays with the host loop, which sizes every build

@@ -448,7 +448,9 @@ def test_newton_loop_graph_equals_host_loop(case):
     c = capi.Cosmo(quintic)
     try:
         assert c.set_option("newton_graph", 1) == 0
-        g = _solve_arrays(p, quintic, box)
+        # the graph is built when a solve's parameters repeat (buffers settled)
+        for _ in range(3):
+            g = _solve_arrays(p, quintic, box)
         assert c.set_option("newton_graph", 0) == 0
         h = _solve_arrays(p, quintic, box)
     finally:
@@ -477,8 +479,11 @@ def test_newton_loop_graph_list_overflow_falls_back():
     assert c.set_option("graph_list_store", 50) == 0    # half the first lists' entries
     try:
         p = inputs.plummer(12000, lnsigma=0.5, seed=29)
-        cc, o = run_pair(p, quintic=True)
-        assert cc.scalar("loopGraph") == 0
-        check_all(cc, o)
+        builds = c.scalar("loopGraphBuilds")
+        for _ in range(3):     # the graph is built once the parameters repeat
+            cc, o = run_pair(p, quintic=True)
+            assert cc.scalar("loopGraph") == 0
+            check_all(cc, o)
+        assert c.scalar("loopGraphBuilds") > builds
     finally:
         c.set_option("graph_list_store", 0)
