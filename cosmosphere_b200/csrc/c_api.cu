@@ -941,6 +941,18 @@ long cosmo_x_array(const char* name, void* out, int* dtype)
         }
         return put(s.jlist.get(), tot, 4, 1);
     }
+    if (k == "loopKey")
+    {
+        // the parameters the last solve's Newton-loop graph was keyed on, as 8-byte words
+        const size_t w = (s.loopKeyLast.size() + 7) / 8;
+        if (dtype) *dtype = 4;
+        if (out)
+        {
+            std::memset(out, 0, w * 8);
+            std::memcpy(out, s.loopKeyLast.data(), s.loopKeyLast.size());
+        }
+        return long(w);
+    }
     if (k == "loopListEntries")
     {
         if (dtype) *dtype = 4;

@@ -471,6 +471,7 @@ static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double h
         key.add(v);
     for (double v : {pmass, tolh, hfact}) key.add(v);
 
+    s.loopKeyLast = key.b;
     if (!s.loopGraphExec || key.b != s.loopGraphKey)
     {
         // a graph is built for parameters met a second time in a row (a stepping caller's
@@ -683,6 +684,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
 
+    // the host loop swaps the two active-leaf buffers every iteration: put them back in
+    // one order, so that a graph captured with them serves the next solve too
+    if (s.activeA.get() > s.activeB.get()) std::swap(s.activeA, s.activeB);
     COSMO_CUDA(cudaMemcpyAsync(s.activeA.get(), s.allLeaves.get(), size_t(nL) * 4, cudaMemcpyDeviceToDevice, s.st));
     int nActiveLeaves = nL;
     long long nActiveParticles = s.nAlive;

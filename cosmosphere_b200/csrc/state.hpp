@@ -180,6 +180,7 @@ struct State
     cudaGraphExec_t loopGraphExec = nullptr;
     std::vector<unsigned char> loopGraphKey;
     std::vector<unsigned char> loopKeyPending;   // parameters met once, not yet built for
+    std::vector<unsigned char> loopKeyLast;      // the last solve's parameters (a diagnostic)
     unsigned long long loopKernels[3] = {0, 0, 0};   // kernels of the body, the list branch, the rows branch
     int loopGraphBuilds = 0, loopGraphUpdates = 0;
     int lastLoopRebuilds = 0, lastLoopRowBuilds = 0;   // its list rebuilds and row builds
