@@ -218,6 +218,7 @@ def run_ensemble(args, rank, world, local, dist):
             tuned[mode] = {"seconds": time.perf_counter() - w0, "confirm_s": {"tuned": t_tab, "default": t_def},
                            "kept": "tuned" if table.entries else "default", **table.to_json()}
             b = capi.Batch(sets)
+            b.set_staging(False)          # the untuned form: the library's default feed
             b.upload()
             for _ in range(args.warmup):
                 assert b.density(final_rho=True) == 0
