@@ -19,9 +19,14 @@ namespace {
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
 
+// The per-particle factors.  grkfac (prepB.x) is also written to the unused fourth
+// component of vel4, so that a pair reads the j side's velocity and grkfac in one 32-byte
+// record; the pair derives the j side's pr and auterm from prepA and thermo4 with the
+// prep's own operations, so those are the same bits as prepB.y and prepB.z.
 __global__ void force_prep_kernel(const double4* __restrict__ xyzh, const double* __restrict__ gradh,
                                   const double4* __restrict__ thermo4, int n, double pmass, double alphau,
-                                  double hfact, double4* __restrict__ prepA, double4* __restrict__ prepB)
+                                  double hfact, double4* __restrict__ prepA, double4* __restrict__ prepB,
+                                  double4* __restrict__ vel4)
 {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -30,6 +35,7 @@ __global__ void force_prep_kernel(const double4* __restrict__ xyzh, const double
     {
         prepA[i] = make_double4(0, 0, 0, 0);
         prepB[i] = make_double4(0, 0, 0, 0);
+        vel4[i].w = 0.0;
         return;
     }
     const double hsq = 1.0 / (hi * hi);
@@ -41,8 +47,10 @@ __global__ void force_prep_kernel(const double4* __restrict__ xyzh, const double
     const double oinv = (omega > 0.0) ? (1 / omega) : 1.0;
     const double pro2 = thermo4[i].x;
     prepA[i] = make_double4(hsq, 1.0 / hi, rho, 1.0 / rho);
-    prepB[i] = make_double4(h4 * kCnormk * oinv, pro2 * rho * rho, 0.5 * pmass * (1.0 / rho) * alphau,
+    const double grkfac = h4 * kCnormk * oinv;
+    prepB[i] = make_double4(grkfac, pro2 * rho * rho, 0.5 * pmass * (1.0 / rho) * alphau,
                             kCnormk * oinv * h4 / rho);
+    vel4[i].w = grkfac;
 }
 
 // The i-side quantities of one particle and its force sums.
@@ -61,12 +69,13 @@ struct ForceAcc
     }
 
     // One pair with j (src/force.cu:232-383): the exact tests dr^2 > 0 and
-    // dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10), then the i-side and j-side terms.
+    // dr^2 < R^2 max(h_i^2, h_j^2)(1 + 1e-10), then the i-side and j-side terms.  The j
+    // side is four 32-byte records (xyzh, prepA, vel4 with grkfac, thermo4).
     template<bool Periodic, bool Disc>
     __device__ __forceinline__ void add(const double4& pj, int j, const double4* __restrict__ vel4,
                                         const double4* __restrict__ thermo4, const double4* __restrict__ prepA,
-                                        const double4* __restrict__ prepB, double lx, double ly, double lz,
-                                        double pm, double beta, int pdv, int shock)
+                                        double lx, double ly, double lz, double pm, double alphau, double beta,
+                                        int pdv, int shock)
     {
         double dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
         nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
@@ -87,10 +96,11 @@ struct ForceAcc
         const double dvx = v.x - vj.x, dvy = v.y - vj.y, dvz = v.z - vj.z;
         const double projv = dvx * rx + dvy * ry + dvz * rz;
         const double4 tj = ldg4(thermo4 + j);
-        const double4 bj = ldg4(prepB + j);
         const double rhoj = aj.z, rho1j = aj.w, pro2j = tj.x;
         const double vwavej = tj.y, alphaj = tj.z, enj = tj.w;
-        const double prj = bj.y, autermj = bj.z;
+        // the prep's pro2 * rho * rho and 0.5 * pmass * (1 / rho) * alphau, operation for
+        // operation
+        const double prj = pro2j * rhoj * rhoj, autermj = 0.5 * pm * rho1j * alphau;
         const double vsigi = fmax(vwavei - beta * projv, 0.0);
         const double vsigavi = fmax(alphai * vwavei - beta * projv, 0.0);
         const double vsigj = fmax(vwavej - beta * projv, 0.0);
@@ -145,7 +155,7 @@ struct ForceAcc
             double wk, dwk;
             const double q = dr * aj.y;
             sph_kernel(qj2, q, wk, dwk);
-            const double gkj = dwk * bj.x;
+            const double gkj = dwk * vj.w;
             const double gpj = pm * (pro2j + qr2j) * gkj;
             jtx -= gpj * rx; jty -= gpj * ry; jtz -= gpj * rz;
             f4s += vsigu * denij * autermj * gkj;
@@ -176,8 +186,8 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
              const double4* __restrict__ vel4, const double4* __restrict__ thermo4,
              const double4* __restrict__ prepA, const double4* __restrict__ prepB, double* __restrict__ fx,
              double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ f4,
-             double* __restrict__ vsigmax, double* __restrict__ divvF, double pmass, double beta, int pdv,
-             int shock, const DevBox* __restrict__ box, const int* __restrict__ nblCount,
+             double* __restrict__ vsigmax, double* __restrict__ divvF, double pmass, double alphau, double beta,
+             int pdv, int shock, const DevBox* __restrict__ box, const int* __restrict__ nblCount,
              DevScalars* __restrict__ ds)
 {
     __shared__ double4 sRing[kWarpsPerBlock][kRing];
@@ -230,7 +240,7 @@ force_kernel(int nL, const uint32_t* __restrict__ layout, const uint32_t* __rest
                     return r2_f32<Periodic>(xf, yf, zf, pf, Lx, Ly, Lz) <= r * r;
                   },
                   [&](const double4& pj, const float4&, int j) {
-                    A.add<Periodic, Disc>(pj, j, vel4, thermo4, prepA, prepB, lx, ly, lz, pm, beta, pdv, shock);
+                    A.add<Periodic, Disc>(pj, j, vel4, thermo4, prepA, lx, ly, lz, pm, alphau, beta, pdv, shock);
                   });
                 });
             if (!mine) continue;
@@ -309,7 +319,7 @@ force_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict_
                  const double4* __restrict__ thermo4, const double4* __restrict__ prepA,
                  const double4* __restrict__ prepB, double* __restrict__ fx, double* __restrict__ fy,
                  double* __restrict__ fz, double* __restrict__ f4, double* __restrict__ vsigmax,
-                 double* __restrict__ divvF, double pmass, double beta, int pdv, int shock,
+                 double* __restrict__ divvF, double pmass, double alphau, double beta, int pdv, int shock,
                  const DevBox* __restrict__ box, DevScalars* __restrict__ ds)
 {
     double lx = 0, ly = 0, lz = 0;
@@ -323,8 +333,8 @@ force_row_kernel(int nAlive, const int* __restrict__ nbl, const int* __restrict_
         A.load(uint32_t(i), xyzh, vel4, thermo4, prepA, prepB);
         const int* row = row_of(nbl, uint32_t(i));
         auto pair = [&](int j) {
-            A.add<Periodic, Disc>(ldg4(xyzh + j), j, vel4, thermo4, prepA, prepB, lx, ly, lz, pmass, beta, pdv,
-                                  shock);
+            A.add<Periodic, Disc>(ldg4(xyzh + j), j, vel4, thermo4, prepA, lx, ly, lz, pmass, alphau, beta,
+                                  pdv, shock);
         };
         for_row(row, cnt, pair);
         pairs += A.gp;
@@ -390,7 +400,8 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
     }
     cudaEvent_t p0 = ev(s);
     force_prep_kernel<<<iceil(n, 256), 256, 0, s.st>>>(s.xyzh.get(), s.gradh.get(), s.thermo4.get(), n, pmass,
-                                                       alphau, s.hfact, s.prepA.get(), s.prepB.get());
+                                                       alphau, s.hfact, s.prepA.get(), s.prepB.get(),
+                                                       s.vel4.get());
     COSMO_LAUNCHED();
     cudaEvent_t p1 = ev(s);
     const int nL = s.nLeaves;
@@ -399,14 +410,14 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
         kern<<<grid, kThreads, 0, s.st>>>(nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
                                           s.xyzh.get(), s.vel4.get(), s.thermo4.get(), s.prepA.get(),
                                           s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(),
-                                          s.vsigmax.get(), s.divvF.get(), pmass, beta, pdv ? 1 : 0,
+                                          s.vsigmax.get(), s.divvF.get(), pmass, alphau, beta, pdv ? 1 : 0,
                                           shock ? 1 : 0, s.box.get(), s.nblCount.get(), ds);
     };
     auto launchRows = [&](auto kern) {
         kern<<<std::max(1, std::min(iceil(s.nAlive, kThreads), 8 * s.numSMs)), kThreads, 0, s.st>>>(
             s.nAlive, s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.vel4.get(), s.thermo4.get(), s.prepA.get(),
             s.prepB.get(), s.fx.get(), s.fy.get(), s.fz.get(), s.f4.get(), s.vsigmax.get(), s.divvF.get(), pmass,
-            beta, pdv ? 1 : 0, shock ? 1 : 0, s.box.get(), ds);
+            alphau, beta, pdv ? 1 : 0, shock ? 1 : 0, s.box.get(), ds);
     };
     // one lane per particle over its symmetric row; the group pass covers only the rows
     // that overflowed
