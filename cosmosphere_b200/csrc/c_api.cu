@@ -119,6 +119,7 @@ void ensure_init(State& s)
     if (const char* e = std::getenv("COSMO_STAGING")) s.staging = std::atoi(e) != 0;
     if (const char* e = std::getenv("COSMO_SYM_PREFILTER")) s.symPrefilter = std::atoi(e) != 0;
     if (const char* e = std::getenv("COSMO_NEWTON_GRAPH")) s.newtonGraph = std::atoi(e) != 0;
+    if (const char* e = std::getenv("COSMO_SYM_FROM_ROWS")) s.symFromRows = std::atoi(e) != 0;
     if (const char* e = std::getenv("COSMO_SPREAD_GROUPS")) s.spreadGroups = std::max(0, std::min(32, std::atoi(e)));
 }
 
@@ -128,7 +129,7 @@ size_t state_device_bytes(const State& s)
     auto add = [&](const auto& buf) { b += buf.cap * sizeof(*buf.p); };
     for (auto* d : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
-                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH, &s.nblR2})
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH, &s.nblR2, &s.hs})
         add(*d);
     for (auto* d : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) add(*d);
     for (auto* d : {&s.prepAf, &s.prepBf, &s.thermof}) add(*d);
@@ -136,9 +137,12 @@ size_t state_device_bytes(const State& s)
     for (auto* d : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
                     &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
-                    &s.rowItems, &s.jlistPrev, &s.walked, &s.walkScratch})
+                    &s.rowItems, &s.jlistPrev, &s.walked, &s.walkScratch, &s.coverFlag, &s.coverLeaves, &s.extraCnt,
+                    &s.extraBucket, &s.nblJ})
         add(*d);
     add(s.items);
+    add(s.extras);
+    add(s.extraOff);
     for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
                     &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback, &s.jOffsetPrev})
         add(*d);
@@ -153,7 +157,7 @@ void release_state(State& s)
     COSMO_CUDA(cudaStreamSynchronize(s.st));
     for (auto* b : {&s.ux, &s.uy, &s.uz, &s.uh, &s.uvx, &s.uvy, &s.uvz, &s.uax, &s.uay, &s.uaz, &s.rho, &s.gradh,
                     &s.divv, &s.xi, &s.ddivvdt, &s.fx, &s.fy, &s.fz, &s.f4, &s.vsigmax, &s.divvF, &s.xfer, &s.centers,
-                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH, &s.nblR2})
+                    &s.sizes, &s.hmaxLeaf, &s.hmaxNode, &s.hmaxPre, &s.redTmp, &s.listH, &s.nblH, &s.nblR2, &s.hs})
         b->release(s.st);
     for (auto* b : {&s.xyzh, &s.vel4, &s.acc4, &s.thermo4, &s.prepA, &s.prepB, &s.preCenter, &s.preHalf}) b->release(s.st);
     for (auto* b : {&s.prepAf, &s.prepBf, &s.thermof}) b->release(s.st);
@@ -161,9 +165,12 @@ void release_state(State& s)
     for (auto* b : {&s.orderA, &s.orderB, &s.particleLeaf, &s.converged, &s.preLeaf, &s.preSkip, &s.bfsToPre,
                     &s.preToBfs, &s.childOffsets, &s.internalToLeaf, &s.levelRange, &s.leafToInternal, &s.jlist,
                     &s.activeA, &s.activeB, &s.allLeaves, &s.nodeValsTmp, &s.leafNext, &s.nbl, &s.nblCount,
-                    &s.rowItems, &s.jlistPrev, &s.walked, &s.walkScratch})
+                    &s.rowItems, &s.jlistPrev, &s.walked, &s.walkScratch, &s.coverFlag, &s.coverLeaves, &s.extraCnt,
+                    &s.extraBucket, &s.nblJ})
         b->release(s.st);
     s.items.release(s.st);
+    s.extras.release(s.st);
+    s.extraOff.release(s.st);
     for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
                     &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback, &s.jOffsetPrev})
         b->release(s.st);
@@ -719,6 +726,12 @@ int cosmo_x_set_option(const char* name, int value)
     if (k == "staging") { s.staging = value != 0; return 0; }
     if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
     if (k == "newton_graph") { s.newtonGraph = value != 0; return 0; }
+    if (k == "sym_from_rows")
+    {
+        s.symFromRows = value != 0;
+        s.symRowsSkip = 0;
+        return 0;
+    }
     if (k == "graph_list_store")
     {
         if (value < 0) return -1;
@@ -839,11 +852,14 @@ double cosmo_x_scalar(const char* name)
     if (k == "loopGraphBuilds") return double(s.loopGraphBuilds);
     if (k == "loopGraphUpdates") return double(s.loopGraphUpdates);
     if (k == "loopRowBuilds") return double(s.lastLoopRowBuilds);
+    if (k == "rowsFromNewton") return s.rowsFromNewton ? 1.0 : 0.0;
     if (k == "listTotal") return double(s.listTotal);
     if (s.hscal)
     {
         read_scalars(s);
         if (k == "pairsDensity") return double(s.hscal->pairs[0]);
+        if (k == "extraCount") return double(s.hscal->extraCount);
+        if (k == "coverNeed") return double(s.hscal->coverNeed);
         if (k == "pairsGrad") return double(s.hscal->pairs[1]);
         if (k == "pairsForce") return double(s.hscal->pairs[2]);
         if (k == "rowOverflow") return double(s.hscal->rowOverflow);
@@ -920,15 +936,31 @@ long cosmo_x_array(const char* name, void* out, int* dtype)
     if (k == "centers") return put(s.centers.get(), 3 * nN, 8, 0);
     if (k == "sizes") return put(s.sizes.get(), 3 * nN, 8, 0);
     if (k == "hmax_leaf") return put(s.hmaxLeaf.get(), nL, 8, 0);
+    // hmax per node is the force pass's upsweep; when the force pass ran over rows made
+    // from the Newton rows it was not needed, and is made when asked for
+    if ((k == "hmax_node" || ((k == "jcount" || k == "jOffset" || k == "jlist") && s.forceSinceSolve)) &&
+        !s.hmaxNodeDone && nL > 0)
+    {
+        hmax_upsweep(s);
+        s.hmaxNodeDone = true;
+        COSMO_CUDA(cudaStreamSynchronize(s.st));
+    }
     if (k == "hmax_node") return put(s.hmaxNode.get(), nN, 8, 0);
     // the reference's state holds the gather lists after a density solve and the
-    // symmetric ones after a force pass; this library builds the symmetric ones with the
-    // gradient sweep, so the gather view is rebuilt (exactly) when asked for before a force
-    if ((k == "jcount" || k == "jOffset" || k == "jlist") && s.listsSym && !s.forceSinceSolve && nL > 0)
+    // symmetric ones after a force pass.  This library builds the symmetric ones with the
+    // gradient sweep, or none (rows from the Newton rows), and ends a solve with the
+    // Newton loop's widened lists: each view is rebuilt (exactly) when asked for
+    if ((k == "jcount" || k == "jOffset" || k == "jlist") && nL > 0)
     {
-        build_lists(s, false);
-        s.jlistToken = 0;
-        COSMO_CUDA(cudaStreamSynchronize(s.st));
+        const bool gatherView = !s.forceSinceSolve && (s.listsSym || s.listsLoose);
+        const bool symView = s.forceSinceSolve && !s.listsSym;
+        if (gatherView || symView)
+        {
+            build_lists(s, symView);
+            s.listsLoose = false;
+            s.jlistToken = symView ? s.token : 0;
+            COSMO_CUDA(cudaStreamSynchronize(s.st));
+        }
     }
     if (k == "jcount") return put(s.jcount.get(), nL, 4, 2);
     if (k == "jOffset") return put(s.jOffset.get(), nL + 1, 4, 2);

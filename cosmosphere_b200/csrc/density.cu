@@ -268,6 +268,171 @@ __global__ void gradient_dead_kernel(int nAlive, int n, double* __restrict__ div
     divv[i] = 0.0; ddivvdt[i] = 0.0; xiOut[i] = 1.0;
 }
 
+// Rows from the Newton rows: whether each live particle's row covers its converged h
+// with the force test's slack to spare (written this solve, not overflowed, and
+// h (1 + 1e-9) <= the radius it is complete within, kept in acc4.w).  flag = 1 if it
+// does; a leaf with particles that do not is listed, and they are counted.
+__global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, const double4* __restrict__ xyzh,
+                                 const int* __restrict__ nblCount, const double4* __restrict__ acc4,
+                                 const uint32_t* __restrict__ jstream, uint32_t streamCut, int* __restrict__ flag,
+                                 int* __restrict__ leaves, double* __restrict__ hs, DevScalars* __restrict__ ds)
+{
+    const int lane = threadIdx.x & 31;
+    const int nWarps = (gridDim.x * blockDim.x) >> 5;
+    for (int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; leaf < nL; leaf += nWarps)
+    {
+        const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
+        int miss = 0;
+        for (uint32_t a = p0 + lane; a < p1; a += 32)
+        {
+            const double h = xyzh[a].w;
+            const bool ok = unsigned(nblCount[a]) <= unsigned(kNbl) && h * (1.0 + 1e-9) <= acc4[a].w;
+            flag[a] = ok ? 1 : 0;
+            hs[a] = h;
+            miss += ok ? 0 : 1;
+        }
+        miss = __reduce_add_sync(0xffffffffu, miss);
+        if (lane == 0 && miss > 0)
+        {
+            atomicAdd(&ds->coverNeed, miss);
+            // a leaf whose stream the work queue cuts keeps the group path: no row for it
+            if (jstream[leaf] > streamCut) atomicAdd(&ds->mergeOverflow, 1);
+            leaves[atomicAdd(&ds->coverLeaves, 1)] = leaf;
+        }
+    }
+}
+
+// The symmetric rows from the Newton rows, for every live particle whose row covers its
+// converged h: the j of its Newton row (flat, ascending, r^2 beside each -- the same
+// double as the force pass's dr^2) that the force pass takes,
+// dr^2 < R^2 max(h_i^2, h_j^2) (1 + 1e-10) -- sym_rows_kernel's test -- written in the
+// same order into the interleaved rows of the gradient and force passes (hs: h in the
+// sorted order, 8 bytes a particle).  A pair the force pass takes because of this
+// particle's support (dr^2 < R^2 h_i^2 (1 + 1e-10)) is in j's Newton row too unless dr^2
+// reaches the radius j's row covers (acc4.w, with 1e-9 to spare; only a pair beyond j's
+// own support can); such a pair is appended as (j << 32 | i), for i to be merged into
+// j's row.
+__global__ void __launch_bounds__(kThreads)
+sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __restrict__ rowsR2,
+                     int* __restrict__ nblCount, const double* __restrict__ hs, const double4* __restrict__ acc4,
+                     int* __restrict__ nbl, unsigned long long* __restrict__ extras, int extraCap,
+                     DevScalars* __restrict__ ds)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nAlive; i += gridDim.x * blockDim.x)
+    {
+        const int cnt = nblCount[i];
+        const double hi = hs[i];
+        const double bi = kRadK2 * (hi * hi) * (1.0 + 1e-10);
+        const int4* inJ = reinterpret_cast<const int4*>(row_flat(rowsJ, uint32_t(i)));
+        const double4* inR = reinterpret_cast<const double4*>(row_flat(rowsR2, uint32_t(i)));
+        int* out = row_of(nbl, uint32_t(i));
+        int w = 0;
+        auto entry = [&](int j, double dr2) {
+            const double hj = __ldg(hs + j);
+            const double bj = kRadK2 * (hj * hj) * (1.0 + 1e-10);
+            if (!(dr2 >= fmax(bi, bj))) out[size_t(w++) * kRowStride] = j;
+            if (dr2 < bi && !(dr2 < kRadK2 * (hj * hj)))
+            {
+                const double ch = __ldg(&acc4[j].w);
+                if (!(dr2 < kRadK2 * (ch * ch) * (1.0 - 1e-9)))
+                {
+                    const int k = atomicAdd(&ds->extraCount, 1);
+                    if (k < extraCap) extras[k] = (static_cast<unsigned long long>(j) << 32) | uint32_t(i);
+                }
+            }
+        };
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4)
+        {
+            const int4 v = __ldg(inJ + (k >> 2));
+            const double4 r = ldg4(inR + (k >> 2));
+            entry(v.x, r.x); entry(v.y, r.y); entry(v.z, r.z); entry(v.w, r.w);
+        }
+        if (k < cnt)
+        {
+            const int4 v = __ldg(inJ + (k >> 2));
+            const double4 r = ldg4(inR + (k >> 2));
+            entry(v.x, r.x);
+            if (k + 1 < cnt) entry(v.y, r.y);
+            if (k + 2 < cnt) entry(v.z, r.z);
+        }
+        nblCount[i] = w;
+    }
+}
+
+// The extras of each row owner (their number read on the device, at most cap of them):
+// counted, then placed at the owner's offset.
+__global__ void extras_count_kernel(const unsigned long long* __restrict__ extras, int cap,
+                                    const DevScalars* __restrict__ ds, int* __restrict__ cnt)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < min(ds->extraCount, cap)) atomicAdd(&cnt[int(extras[k] >> 32)], 1);
+}
+
+__global__ void extras_place_kernel(const unsigned long long* __restrict__ extras, int cap,
+                                    const DevScalars* __restrict__ ds, const uint32_t* __restrict__ off,
+                                    int* __restrict__ cnt, int* __restrict__ bucket)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= min(ds->extraCount, cap)) return;
+    const int t = int(extras[k] >> 32);
+    bucket[off[t] + uint32_t(atomicSub(&cnt[t], 1) - 1)] = int(uint32_t(extras[k]));
+}
+
+// Each row owner merges its extras into its row: sorted, those the row already holds
+// dropped, the rest merged in from the back so the row stays ascending.  A row that would
+// exceed kNbl sets mergeOverflow (the symmetric rows are then built instead).
+__global__ void extras_merge_kernel(int nA, const uint32_t* __restrict__ off, int* __restrict__ bucket,
+                                    int* __restrict__ nbl, int* __restrict__ nblCount, DevScalars* __restrict__ ds)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nA) return;
+    const uint32_t b0 = off[t], e = off[t + 1] - b0;
+    if (e == 0) return;
+    const int cnt = nblCount[t];
+    if (cnt + int(e) > 2 * kNbl)
+    {
+        ds->mergeOverflow = 1;
+        return;
+    }
+    int* ex = bucket + b0;
+    for (uint32_t a = 1; a < e; ++a)
+    {
+        const int v = ex[a];
+        uint32_t k = a;
+        for (; k > 0 && ex[k - 1] > v; --k) ex[k] = ex[k - 1];
+        ex[k] = v;
+    }
+    int* row = row_of(nbl, uint32_t(t));
+    auto at = [&](int k) -> int& { return row[size_t(k) * kRowStride]; };
+    uint32_t u = 0;
+    for (uint32_t a = 0; a < e; ++a)
+    {
+        const int v = ex[a];
+        int lo = 0, hi = cnt;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (at(mid) < v) lo = mid + 1;
+            else hi = mid;
+        }
+        if (!(lo < cnt && at(lo) == v)) ex[u++] = v;
+    }
+    if (u == 0) return;
+    if (cnt + int(u) > kNbl)
+    {
+        ds->mergeOverflow = 1;
+        return;
+    }
+    int r = cnt - 1, x = int(u) - 1, w = cnt + int(u) - 1;
+    while (x >= 0)
+    {
+        if (r >= 0 && at(r) > ex[x]) at(w--) = at(r--);
+        else at(w--) = ex[x--];
+    }
+    nblCount[t] = cnt + int(u);
+}
+
 __global__ void hmax_live_kernel(const double4* __restrict__ xyzh, int nAlive, double* __restrict__ part)
 {
     double m = 0.0;
@@ -391,7 +556,7 @@ struct KeyBytes
 enum class LoopGraph { Ran, Deferred, Failed };
 
 static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double hfact, int maxIter, FixedSplit cut,
-                                   int spreadG, long long& nActiveParticles)
+                                   int spreadG, long long& nActiveParticles, int* rowsJ, double4* rowsCover)
 {
     DevScalars* ds = s.dscal.get();
     const int nL = s.nLeaves;
@@ -462,7 +627,7 @@ static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double h
                           (const void*)s.jlistPrev.get(), (const void*)s.jOffsetPrev.get(), (const void*)s.walked.get(),
                           (const void*)s.walkScratch.get(), (const void*)s.hmaxLeaf.get(), (const void*)s.hmaxPre.get(),
                           (const void*)s.particleLeaf.get(), (const void*)s.scanTmp.get(), (const void*)nrows,
-                          (const void*)nr, (const void*)rk})
+                          (const void*)nr, (const void*)rk, (const void*)rowsJ, (const void*)rowsCover})
         key.add(q);
     for (long long v : {(long long)leafCap, (long long)itemCap, (long long)gridRows, (long long)gridNr,
                         (long long)gridRow, (long long)bgrid, (long long)pgrid, (long long)s.periodic,
@@ -566,7 +731,8 @@ static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double h
             COSMO_LAUNCHED();
             nrows<<<gridRows, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(),
                                                    s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.box.get(),
-                                                   s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
+                                                   s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds,
+                                                   rowsJ, rowsCover);
             COSMO_LAUNCHED();
             newton_count_kernel<<<1, 1, 0, s.st>>>(L, 1);
             COSMO_LAUNCHED();
@@ -651,6 +817,78 @@ static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double h
     return LoopGraph::Ran;
 }
 
+constexpr int kSymRowsSkip = 8;   // solves that write no index rows after one that could not use them
+
+// After a converged solve whose Newton rows wrote their j: whether every live particle's
+// row covers its converged h.  The particles whose rows do not (those that converged
+// before the rows were built, or outgrew them) get rows now, at their converged h, from
+// the same lists; false if some still do not (a leaf that streams too much, a row that
+// overflows) or too many lack one, and the symmetric rows are built instead.
+static bool cover_rows(State& s, int itemCap, FixedSplit cut, int spreadG)
+{
+    DevScalars* ds = s.dscal.get();
+    const int nL = s.nLeaves;
+    s.coverFlag.resize(itemCap, s.st);
+    s.coverLeaves.resize(nL, s.st);
+    s.hs.resize(itemCap, s.st);
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        COSMO_CUDA(cudaMemsetAsync(&ds->coverNeed, 0, 2 * sizeof(int), s.st));
+        COSMO_CUDA(cudaMemsetAsync(&ds->mergeOverflow, 0, sizeof(int), s.st));   // here: leaves with no row
+        row_cover_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
+            nL, s.layout.get(), s.xyzh.get(), s.nblCount.get(), s.acc4.get(), s.jstream.get(), cut.stream,
+            s.coverFlag.get(), s.coverLeaves.get(), s.hs.get(), ds);
+        COSMO_LAUNCHED();
+        read_scalars(s);
+        const int need = s.hscal->coverNeed;
+        if (need == 0) return true;
+        if (pass == 1 || need > s.nAlive / 4 || s.hscal->mergeOverflow > 0) return false;
+        begin_iteration_kernel<<<std::min(iceil(nL, 256), 4 * s.numSMs), 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
+        COSMO_LAUNCHED();
+        plan_items_count_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
+            s.coverLeaves.get(), &ds->coverLeaves, nullptr, s.layout.get(), s.coverFlag.get(), s.jstream.get(),
+            s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
+        COSMO_LAUNCHED();
+        RowsKernelFn nrows = s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>;
+        nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
+            s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
+            s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds, s.nblJ.get(),
+            s.acc4.get());
+        COSMO_LAUNCHED();
+    }
+    return false;
+}
+
+// The symmetric rows from the covering Newton rows (sym_from_rows_kernel), then the
+// pairs other particles' supports add, merged into their rows -- all on the device, the
+// extras' number read there.  Whether they all fitted is known from extraCount (at most
+// extraCap) and mergeOverflow once the stream has been read.
+static void sym_rows_from_newton(State& s, int extraCap)
+{
+    DevScalars* ds = s.dscal.get();
+    const int nA = s.nAlive;
+    s.extras.resize(extraCap, s.st);
+    s.extraCnt.resize(nA, s.st);
+    s.extraOff.resize(size_t(nA) + 1, s.st);
+    s.extraBucket.resize(extraCap, s.st);
+    COSMO_CUDA(cudaMemsetAsync(&ds->extraCount, 0, 2 * sizeof(int), s.st));   // extraCount, mergeOverflow
+    COSMO_CUDA(cudaMemsetAsync(&ds->rowOverflow, 0, sizeof(int), s.st));
+    COSMO_CUDA(cudaMemsetAsync(s.extraCnt.get(), 0, size_t(nA) * sizeof(int), s.st));
+    sym_from_rows_kernel<<<std::max(1, std::min(iceil(nA, kThreads), 16 * s.numSMs)), kThreads, 0, s.st>>>(
+        nA, s.nblJ.get(), s.nblR2.get(), s.nblCount.get(), s.hs.get(), s.acc4.get(), s.nbl.get(), s.extras.get(),
+        extraCap, ds);
+    COSMO_LAUNCHED();
+    extras_count_kernel<<<iceil(extraCap, 256), 256, 0, s.st>>>(s.extras.get(), extraCap, ds, s.extraCnt.get());
+    COSMO_LAUNCHED();
+    scan_exclusive(s, reinterpret_cast<const uint32_t*>(s.extraCnt.get()), s.extraOff.get(), nA, false);
+    extras_place_kernel<<<iceil(extraCap, 256), 256, 0, s.st>>>(s.extras.get(), extraCap, ds, s.extraOff.get(),
+                                                               s.extraCnt.get(), s.extraBucket.get());
+    COSMO_LAUNCHED();
+    extras_merge_kernel<<<iceil(nA, 256), 256, 0, s.st>>>(nA, s.extraOff.get(), s.extraBucket.get(), s.nbl.get(),
+                                                         s.nblCount.get(), ds);
+    COSMO_LAUNCHED();
+}
+
 DensResult solve_density(State& s, int n, double pmass, const double* periodicBox, double tolh, double hfact,
                          int maxIter, bool withGradients, bool allowGraph)
 {
@@ -683,6 +921,26 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.nblR2.resize(size_t(itemCap) * kNbl, s.st);
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
+    // The Newton rows also write their j (and the radius each covers, in acc4.w) when the
+    // gradient and force passes may run over them: a plain solve with gradients whose
+    // particles all start active (with fixed particles, leaves that never walk would hold
+    // no list this solve)
+    int* rowsJ = nullptr;
+    double4* rowsCover = nullptr;
+    // after a solve whose rows did not all cover (a workload with leaves the work queue
+    // cuts, say), the next few solves do not write them
+    const bool tryRows = s.symRowsSkip == 0;
+    if (s.symRowsSkip > 0) --s.symRowsSkip;
+    if (withGradients && s.symFromRows && s.precision == 0 && s.frozenFor != n && tryRows)
+    {
+        s.nblJ.resize(size_t(itemCap) * kNbl, s.st);
+        s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);
+        rowsJ = s.nblJ.get();
+        rowsCover = s.acc4.get();
+    }
+    s.rowsFromNewton = false;
+    s.hmaxNodeDone = true;
+    s.listsLoose = false;
 
     // the host loop swaps the two active-leaf buffers every iteration: put them back in
     // one order, so that a graph captured with them serves the next solve too
@@ -716,7 +974,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     bool graphRan = false;
     if (allowGraph && s.newtonGraph && maxIter <= kLoopIters && nActiveParticles > 0)
     {
-        const LoopGraph lg = newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles);
+        const LoopGraph lg =
+            newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles, rowsJ, rowsCover);
         graphRan = lg == LoopGraph::Ran;
         listsWidened = graphRan;
         // deferred: the first lists are built and valid for the host loop's first iteration
@@ -759,7 +1018,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                                          : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
                 nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
                     s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
-                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds);
+                    s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds,
+                    rowsJ, rowsCover);
                 COSMO_LAUNCHED();
                 rowsReady = true;
             }
@@ -846,15 +1106,25 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
             return res;
         }
     }
-    bool symBuilt = false;
+    bool symBuilt = false, fromRows = false;
     if (withGradients)
     {
-        // hmax of every leaf at the converged h, then the symmetric lists and rows of the
-        // force pass: at the converged h they hold every pair of the gather sweep too
+        // hmax of every leaf at the converged h; then the symmetric rows of the gradient
+        // and force passes (at the converged h they hold every pair of the gather sweep
+        // too): taken from the Newton rows when every live particle's row covers its
+        // converged h, otherwise built from the symmetric lists
         cudaEvent_t g0 = ev(s);
         hmax_leaves(s, s.allLeaves.get(), nL);
-        build_symmetric(s);
-        symBuilt = true;
+        const bool rowsBuilt = graphRan ? s.lastLoopRowBuilds > 0 : rowsReady;
+        fromRows = rowsJ && s.nAlive > 0 && rowsBuilt && cover_rows(s, itemCap, cut, spreadG);
+        const int extraCap = itemCap;
+        if (fromRows)
+            sym_rows_from_newton(s, extraCap);
+        else
+        {
+            build_symmetric(s);
+            symBuilt = true;
+        }
         cudaEvent_t g1 = ev(s);
         const int grid = grid_for(s, nL);
         if (s.precision == 1)
@@ -866,13 +1136,14 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 s.nAlive, s.nbl.get(), s.nblCount.get(), s.xyzh.get(), s.vel4.get(), s.acc4.get(), s.rho.get(),
                 s.gradh.get(), s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass, s.box.get(), ds);
             COSMO_LAUNCHED();
+            // the group sweep of the rows that overflowed (none: it returns at once)
             auto gk = s.periodic ? gradient_kernel<true> : gradient_kernel<false>;
             gk<<<grid, kThreads, 0, s.st>>>(nL, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
                                             s.xyzh.get(), s.vel4.get(), s.acc4.get(), s.rho.get(), s.gradh.get(),
                                             s.divv.get(), s.xi.get(), s.ddivvdt.get(), pmass, s.box.get(),
                                             s.nblCount.get(), ds);
+            COSMO_LAUNCHED();
         }
-        COSMO_LAUNCHED();
         if (n > s.nAlive)
         {
             gradient_dead_kernel<<<iceil(n - s.nAlive, 256), 256, 0, s.st>>>(s.nAlive, n, s.divv.get(), s.xi.get(),
@@ -881,6 +1152,9 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         }
         cudaEvent_t g2 = ev(s);
         read_scalars(s);
+        // the rows serve the force pass if every extra was kept and merged
+        if (fromRows) s.rowsFromNewton = s.hscal->extraCount <= extraCap && s.hscal->mergeOverflow == 0;
+        if (rowsJ && !s.rowsFromNewton) s.symRowsSkip = kSymRowsSkip;
         s.t.gjbuild += elapsed_s(g0, g1);
         s.t.gradkern += elapsed_s(g1, g2);
     }
@@ -888,6 +1162,13 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     ++s.token;
     s.forceSinceSolve = false;
     if (symBuilt) s.jlistToken = s.rowsToken = s.token;
+    if (s.rowsFromNewton)
+    {
+        s.rowsToken = s.token;
+        s.hmaxNodeDone = false;
+    }
+    // the lists held are the Newton loop's widened gather lists
+    s.listsLoose = withGradients && !symBuilt && listsWidened;
     return res;
 }
 

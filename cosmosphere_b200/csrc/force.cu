@@ -389,11 +389,15 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
     cudaEvent_t e0 = ev(s);
     s.forceSinceSolve = true;
     // The symmetric lists and rows are cached per tree (src/force.cu:19-24); the density
-    // solve's gradient sweep has normally built them already.
-    if (s.jlistToken != s.token || s.rowsToken != s.token || !s.listsSym)
+    // solve's gradient sweep has normally built the rows already (from the Newton rows, or
+    // with the symmetric lists).
+    const bool rowsReady = s.rowsToken == s.token && (s.rowsFromNewton || (s.jlistToken == s.token && s.listsSym));
+    if (!rowsReady)
     {
         build_symmetric(s);
         s.jlistToken = s.rowsToken = s.token;
+        s.rowsFromNewton = false;
+        s.hmaxNodeDone = true;
         cudaEvent_t e2 = ev(s);
         COSMO_CUDA(cudaStreamSynchronize(s.st));
         s.t.fjbuild += elapsed_s(e0, e2);
@@ -428,9 +432,14 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
         if (s.periodic) { if (disc) launchRows(force_row_kernel<true, true>); else launchRows(force_row_kernel<true, false>); }
         else { if (disc) launchRows(force_row_kernel<false, true>); else launchRows(force_row_kernel<false, false>); }
         COSMO_LAUNCHED();
-        if (s.periodic) { if (disc) launch(force_kernel<true, true>); else launch(force_kernel<true, false>); }
-        else { if (disc) launch(force_kernel<false, true>); else launch(force_kernel<false, false>); }
-        COSMO_LAUNCHED();
+        if (!s.rowsFromNewton)
+        {
+            // the group pass of the rows that overflowed (none: it returns at once); rows
+            // from the Newton rows never overflow
+            if (s.periodic) { if (disc) launch(force_kernel<true, true>); else launch(force_kernel<true, false>); }
+            else { if (disc) launch(force_kernel<false, true>); else launch(force_kernel<false, false>); }
+            COSMO_LAUNCHED();
+        }
     }
     if (n > s.nAlive)
     {

@@ -170,7 +170,9 @@ density_nr_kernel(const int4* __restrict__ items, int cap, const uint32_t* __res
 // Newton rows of the still-active particles at their current h: r^2 of every j within
 // kRowMargin of the particle's support, in ascending j.  A row is complete while the
 // particle's h stays within kRowMargin of the h it was built at and within the radius its
-// leaf's list covers; rowH records that bound.
+// leaf's list covers; rowH records that bound.  With rowsJ given, each row's j are also
+// written (flat, beside the r^2), so that at the converged h the symmetric rows of the
+// gradient and force passes can be taken from them.
 
 template<bool Periodic, bool Mixed>
 __global__ void __launch_bounds__(kThreads)
@@ -178,7 +180,8 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                    const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                    const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
                    const double* __restrict__ listH, void* __restrict__ rowsR2, int* __restrict__ nblCount,
-                   double* __restrict__ rowH, DevScalars* __restrict__ ds)
+                   double* __restrict__ rowH, DevScalars* __restrict__ ds, int* __restrict__ rowsJ,
+                   double4* __restrict__ acc4)
 {
     using R2 = typename std::conditional<Mixed, float, double>::type;   // FP32 rows in the mixed form
     R2* nblR2 = static_cast<R2*>(rowsR2);
@@ -221,11 +224,16 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                        const double r2 = pair_r2(dx, dy, dz);
                        return RowEntry<R2>{r2 * g.w < wide2, R2(r2)};
                    },
-                   mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen);
+                   mine ? row_flat(nblR2, uint32_t(i)) : nullptr, rowLen,
+                   mine && rowsJ ? row_flat(rowsJ, uint32_t(i)) : nullptr);
         if (mine)
         {
             nblCount[i] = rowLen;
-            rowH[i] = fmin(kRowMargin * pi.w, listH[d.leaf]) * (1.0 - 1e-12);
+            const double rh = fmin(kRowMargin * pi.w, listH[d.leaf]) * (1.0 - 1e-12);
+            rowH[i] = rh;
+            // with the index rows: the radius this row is complete within, in the fourth
+            // component of the particle's acceleration (otherwise unused)
+            if (rowsJ) acc4[i].w = rh;
         }
     }
 }

@@ -63,7 +63,9 @@ constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32 + 4 * 32 * 4;
 // then applies the exact acceptance of the pair on the FP64 positions and returns it with
 // the entry the owner writes for an accepted j (j itself, or r^2).  row is the lane's own row
 // (row_of with Stride kRowStride, or row_flat with Stride 1; nullptr if not mine); rowLen
-// receives its length (kNbl + 1 when it overflowed).  Entries come in ascending j.
+// receives its length (kNbl + 1 when it overflowed).  Entries come in ascending j.  rowJ,
+// when given (the lane's own row in a second buffer of the same layout), receives each
+// accepted j beside the entry, so that a row of r^2 is also a row of neighbour indices.
 // Prefilter = false: no FP32 prefilter; every lane applies exact(gi of particle k, its
 // candidate, j) in lockstep over the group particles, and the ballots are the masks (the
 // symmetric rows, whose candidate-dependent bound makes the prefilter pass most pairs).
@@ -73,7 +75,7 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
                                            const GroupBox& bx, double lx, double ly, double lz, uint32_t jb,
                                            uint32_t nj, const int* __restrict__ jlist, Ranges ranges,
                                            const double4* __restrict__ xyzh, Filter filter, CandB candB, Exact exact,
-                                           T* row, int& rowLen)
+                                           T* row, int& rowLen, int* rowJ = nullptr)
 {
     const int lane = threadIdx.x & 31;
     double4* ring = reinterpret_cast<double4*>(scr);
@@ -122,6 +124,7 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
                     {
                         if constexpr (std::is_same<T, int>::value) row[size_t(len) * Stride] = ri[sl];   // j itself
                         else row[size_t(len) * Stride] = exact(gi, rg[sl], ri[sl]).v;
+                        if (rowJ) rowJ[size_t(len) * Stride] = ri[sl];
                     }
                     ++len;
                 }
@@ -181,7 +184,11 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
                 const RowEntry<T> e = exact(gi, rg[sl], ri[sl]);
                 if (e.ok)
                 {
-                    if (len < kNbl) row[size_t(len) * Stride] = e.v;
+                    if (len < kNbl)
+                    {
+                        row[size_t(len) * Stride] = e.v;
+                        if (rowJ) rowJ[size_t(len) * Stride] = ri[sl];
+                    }
                     ++len;
                 }
             }

@@ -99,6 +99,10 @@ struct DevScalars
     int rowOverflow;             // some symmetric row overflowed (its particle takes the group path)
     int frozenAlive;             // live particles a solve keeps fixed (neighbours only)
     unsigned long long hmaxSeen; // bits of the largest h any leaf had at the start of an iteration
+    int coverNeed;               // live particles whose Newton row does not cover their converged h
+    int coverLeaves;             // leaves holding such particles
+    int extraCount;              // pairs a Newton row may miss from the other side (appended)
+    int mergeOverflow;           // a row with its extras would exceed kNbl
 };
 
 // The single-set Newton loop run as a graph: what the host loop kept in host variables
@@ -135,7 +139,12 @@ struct State
     double boxHost[6] = {0, 0, 0, 0, 0, 0};
     uint64_t token = 0, jlistToken = 0, rowsToken = 0;
     bool listsSym = false;                      // the lists held are the symmetric ones
+    bool listsLoose = false;                    // the lists held are the Newton loop's widened ones
     bool forceSinceSolve = false;               // a force pass ran on the current tree
+    // The symmetric rows of the current tree come from the Newton rows (their j, with the
+    // pairs another particle's support adds merged in): the symmetric lists and hmax per
+    // node were not built, and are built only if asked for (hmaxNodeDone once done).
+    bool rowsFromNewton = false, hmaxNodeDone = true;
     int itersRun = 0, maxIter = 100;
     long long settling0 = 0;                    // settling particles after the first Newton update
     int precision = 0;     // 0 plain FP64 (the drop-in form), 1 mixed FP32/FP64
@@ -157,6 +166,12 @@ struct State
     // 0: one host round trip per iteration (cosmo_x_set_option "newton_graph",
     // COSMO_NEWTON_GRAPH).  The results are the same either way.
     int newtonGraph = 1;
+    // 1: the gradient and force passes run over the Newton rows' j when every live
+    // particle's row covers its converged h (the symmetric lists and rows are not built);
+    // 0: the symmetric lists and rows are built after every solve (cosmo_x_set_option
+    // "sym_from_rows", COSMO_SYM_FROM_ROWS).  The results are the same either way.
+    int symFromRows = 1;
+    int symRowsSkip = 0;   // solves left that do not try it (after one that could not)
     // list storage of the graph loop's rebuilds as a percentage of the first lists' total
     // (0: the built-in, twice the total plus 65536 entries); a figure under 100 makes a
     // rebuild outgrow it, so the fallback to the host loop can be exercised
@@ -224,6 +239,13 @@ struct State
     DBuf<int> nblCount;                         // entries of each row (> kNbl: overflowed)
     DBuf<double> nblH;                          // largest h a Newton row stays complete for
     DBuf<int> rowItems;                         // particles of a Newton iteration on their rows
+    DBuf<int> nblJ;                             // the Newton rows' j (flat, beside nblR2)
+    DBuf<double> hs;                            // h in the sorted order (rows from the Newton rows)
+    DBuf<int> coverFlag, coverLeaves;           // rows to complete after a solve: particle flags, leaves
+    DBuf<unsigned long long> extras;            // (row owner << 32 | j) a row must gain
+    DBuf<int> extraCnt;                         // extras per particle
+    DBuf<uint32_t> extraOff;                    // their offsets (exclusive scan)
+    DBuf<int> extraBucket;                      // the extras' j, grouped by owner
     DBuf<int> leafNext;                         // leaf already queued for the next iteration
     DBuf<int> activeA, activeB, allLeaves;
 

@@ -222,7 +222,11 @@ void cosmo_x_sync(void);
  * the built-in 1; also COSMO_SPREAD_GROUPS); "newton_graph" 1 (default) runs the Newton loop
  * as one graph launch, 0 with a host round trip per iteration (also COSMO_NEWTON_GRAPH);
  * "graph_list_store" sets the graph loop's list storage as a percentage of its first lists'
- * total (0: the built-in; under 100 forces the fallback to the host loop, for tests).
+ * total (0: the built-in; under 100 forces the fallback to the host loop, for tests);
+ * "sym_from_rows" 1 (default) runs the gradient and force passes over the Newton rows' j
+ * (with the pairs other particles' supports add merged in) when every live particle's row
+ * covers its converged h, 0 builds the symmetric lists and rows after every solve (also
+ * COSMO_SYM_FROM_ROWS).
  * Returns 0, or -1 for an unknown name or a value out of range. */
 int cosmo_x_set_option(const char* name, int value);
 

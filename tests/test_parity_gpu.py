@@ -487,3 +487,53 @@ def test_newton_loop_graph_list_overflow_falls_back():
         assert c.scalar("loopGraphBuilds") > builds
     finally:
         c.set_option("graph_list_store", 0)
+
+
+def _step_arrays(p, quintic=False, box=None):
+    c, o = run_pair(p, quintic=quintic, box=box)
+    out = {k: c.array(k).copy() for k in FIELDS + FORCE}
+    for k in ("pairsDensity", "pairsGrad", "pairsForce", "rowsFromNewton", "extraCount"):
+        out[k] = c.scalar(k)
+    return c, o, out
+
+
+@pytest.mark.parametrize("case", ["lattice_open", "periodic", "plummer_quintic", "dead"])
+def test_rows_from_newton_rows(case):
+    """The gradient and force passes over the Newton rows' j, with the pairs another
+    particle's larger support adds merged in, equal the oracle's bit for bit, and equal
+    the passes over the symmetric rows built from the symmetric lists; the lists and hmax
+    per node asked for afterwards are the reference's.  On the open lattice the surface
+    particles' larger h adds such pairs to their neighbours' rows."""
+    quintic, box = False, None
+    if case == "lattice_open":
+        p = inputs.lattice100_workload(20)
+    elif case == "periodic":
+        x, y, z = (np.asarray(v).ravel() for v in np.meshgrid(*(np.arange(14) / 14.0,) * 3, indexing="ij"))
+        n = x.size
+        rng = np.random.default_rng(3)
+        p = inputs.Particles(x=(x + rng.uniform(0, 0.02, n)) % 1.0, y=(y + rng.uniform(0, 0.02, n)) % 1.0,
+                             z=(z + rng.uniform(0, 0.02, n)) % 1.0, h=np.full(n, 1.2 / 14), pmass=1.0 / n)
+        inputs.jiggle_frac(p["h"], 0.05, 0.65, 1.35, 4)
+        box = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+    elif case == "plummer_quintic":
+        p = inputs.plummer(12000, lnsigma=0.3, seed=42)
+        quintic = True
+    else:
+        p = inputs.lattice100_workload(20)
+        p["h"][np.arange(5, p.n, 37)] = -1.0
+    cc = capi.Cosmo(quintic)
+    try:
+        assert cc.set_option("sym_from_rows", 1) == 0
+        c, o, a = _step_arrays(p, quintic, box)
+        check_all(c, o)
+        assert cc.set_option("sym_from_rows", 0) == 0
+        _, _, b = _step_arrays(p, quintic, box)
+    finally:
+        cc.set_option("sym_from_rows", 1)
+    if case in ("lattice_open", "periodic", "dead"):
+        assert a["rowsFromNewton"] == 1
+    if case == "lattice_open":
+        assert a["extraCount"] > 0
+    assert b["rowsFromNewton"] == 0
+    for k in FIELDS + FORCE + ["pairsDensity", "pairsGrad", "pairsForce"]:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
