@@ -51,6 +51,13 @@ struct RowEntry
     T v;
 };
 
+// Four consecutive j of a flat row in one vector store (the row's first entry and every
+// fourth are aligned to four entries).
+__device__ __forceinline__ void store4(int* p, int a, int b, int c, int d)
+{
+    *reinterpret_cast<int4*>(p) = make_int4(a, b, c, d);
+}
+
 // Per-warp shared scratch of rows_group: the double ring, its indices, the group's data
 // and its FP32 offsets and prefilter bounds.
 constexpr int kRowsScratch = kRing * 32 + kRing * 4 + 32 * 32 + 4 * 32 * 4;
@@ -94,6 +101,7 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
     __syncwarp();
     const float Lx = float(lx), Ly = float(ly), Lz = float(lz);
     int len = 0;
+    int k0 = 0, k1 = 0, k2 = 0, k3 = 0;   // a flat row's last four j, not yet written
     stream_ranges<true, false, true>(
         ring, nullptr, ringIdx, bx.cx, bx.cy, bx.cz, 0.0, 0.0, 0.0, jb, nj, jlist, ranges, xyzh, filter,
         [&](const double4* rg, const float4*, const int* ri, int head, int count) {
@@ -184,7 +192,19 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
                 const RowEntry<T> e = exact(gi, rg[sl], ri[sl]);
                 if (e.ok)
                 {
-                    if (len < kNbl)
+                    if constexpr (Stride == 1)
+                    {
+                        // a flat row: the entry stored at once; its j (when asked for) kept
+                        // with the last three in registers and written as one vector store
+                        // when the fourth arrives
+                        if (len < kNbl) row[len] = e.v;
+                        if (rowJ)
+                        {
+                            k0 = k1; k1 = k2; k2 = k3; k3 = ri[sl];
+                            if ((len & 3) == 3 && len < kNbl) store4(rowJ + (len - 3), k0, k1, k2, k3);
+                        }
+                    }
+                    else if (len < kNbl)
                     {
                         row[size_t(len) * Stride] = e.v;
                         if (rowJ) rowJ[size_t(len) * Stride] = ri[sl];
@@ -193,6 +213,16 @@ __device__ __forceinline__ void rows_group(unsigned char* scr, bool mine, int ng
                 }
             }
         });
+    if constexpr (Stride == 1)
+    {
+        // the last, partial group of four j (its unused slots hold nothing a reader uses)
+        const int m = len & 3;
+        if (rowJ != nullptr && m != 0 && len < kNbl)
+        {
+            const int ja = m == 1 ? k3 : (m == 2 ? k2 : k1), jb = m == 1 ? k3 : (m == 2 ? k3 : k2);
+            store4(rowJ + (len - m), ja, jb, k3, k3);
+        }
+    }
     rowLen = len > kNbl ? kNbl + 1 : len;
 }
 
