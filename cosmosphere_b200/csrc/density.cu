@@ -327,8 +327,7 @@ sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __
         const double4* inR = reinterpret_cast<const double4*>(row_flat(rowsR2, uint32_t(i)));
         int* out = row_of(nbl, uint32_t(i));
         int w = 0;
-        auto entry = [&](int j, double dr2) {
-            const double hj = __ldg(hs + j);
+        auto entry = [&](int j, double dr2, double hj) {
             const double bj = kRadK2 * (hj * hj) * (1.0 + 1e-10);
             if (!(dr2 >= fmax(bi, bj))) out[size_t(w++) * kRowStride] = j;
             if (dr2 < bi && !(dr2 < kRadK2 * (hj * hj)))
@@ -341,20 +340,33 @@ sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __
                 }
             }
         };
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4)
+        // groups of four entries in a two-stage pipeline: while a group is tested, the next
+        // group's h and the one after's j and r^2 are in flight (a row's groups lie within
+        // its kNbl entries; slots past the count read this particle's own h)
+        const int nq = (cnt + 3) >> 2;
+        const int me = i;
+        auto ldj = [&](int q) { return q < nq ? __ldg(inJ + q) : make_int4(me, me, me, me); };
+        auto ldr = [&](int q) { return q < nq ? ldg4(inR + q) : make_double4(0.0, 0.0, 0.0, 0.0); };
+        auto ldh = [&](int q, const int4& v) {
+            const int left = cnt - 4 * q;
+            return make_double4(__ldg(hs + (left > 0 ? v.x : me)), __ldg(hs + (left > 1 ? v.y : me)),
+                                __ldg(hs + (left > 2 ? v.z : me)), __ldg(hs + (left > 3 ? v.w : me)));
+        };
+        int4 v0 = ldj(0), v1 = ldj(1);
+        double4 r0 = ldr(0), r1 = ldr(1);
+        double4 h0 = ldh(0, v0);
+        for (int q = 0; q < nq; ++q)
         {
-            const int4 v = __ldg(inJ + (k >> 2));
-            const double4 r = ldg4(inR + (k >> 2));
-            entry(v.x, r.x); entry(v.y, r.y); entry(v.z, r.z); entry(v.w, r.w);
-        }
-        if (k < cnt)
-        {
-            const int4 v = __ldg(inJ + (k >> 2));
-            const double4 r = ldg4(inR + (k >> 2));
-            entry(v.x, r.x);
-            if (k + 1 < cnt) entry(v.y, r.y);
-            if (k + 2 < cnt) entry(v.z, r.z);
+            const double4 h1 = ldh(q + 1, v1);
+            const int4 v2 = ldj(q + 2);
+            const double4 r2 = ldr(q + 2);
+            const int left = cnt - 4 * q;
+            entry(v0.x, r0.x, h0.x);
+            if (left > 1) entry(v0.y, r0.y, h0.y);
+            if (left > 2) entry(v0.z, r0.z, h0.z);
+            if (left > 3) entry(v0.w, r0.w, h0.w);
+            v0 = v1; r0 = r1; h0 = h1;
+            v1 = v2; r1 = r2;
         }
         nblCount[i] = w;
     }
@@ -927,17 +939,19 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     // no list this solve)
     int* rowsJ = nullptr;
     double4* rowsCover = nullptr;
-    // after a solve whose rows did not all cover (a workload with leaves the work queue
-    // cuts, say), the next few solves do not write them
-    const bool tryRows = s.symRowsSkip == 0;
-    if (s.symRowsSkip > 0) --s.symRowsSkip;
-    if (withGradients && s.symFromRows && s.precision == 0 && s.frozenFor != n && tryRows)
+    if (s.precision == 0)
     {
         s.nblJ.resize(size_t(itemCap) * kNbl, s.st);
         s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);
         rowsJ = s.nblJ.get();
         rowsCover = s.acc4.get();
     }
+    // after a solve whose rows did not all cover (a workload with leaves the work queue
+    // cuts, say), the next few solves do not write them
+    const bool tryRows = s.symRowsSkip == 0;
+    if (s.symRowsSkip > 0) --s.symRowsSkip;
+    const bool writeJ = rowsJ && withGradients && s.symFromRows && s.frozenFor != n && tryRows;
+    COSMO_CUDA(cudaMemsetAsync(&ds->rowsJOn, writeJ ? 1 : 0, sizeof(int), s.st));
     s.rowsFromNewton = false;
     s.hmaxNodeDone = true;
     s.listsLoose = false;
@@ -1116,7 +1130,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         cudaEvent_t g0 = ev(s);
         hmax_leaves(s, s.allLeaves.get(), nL);
         const bool rowsBuilt = graphRan ? s.lastLoopRowBuilds > 0 : rowsReady;
-        fromRows = rowsJ && s.nAlive > 0 && rowsBuilt && cover_rows(s, itemCap, cut, spreadG);
+        fromRows = writeJ && s.nAlive > 0 && rowsBuilt && cover_rows(s, itemCap, cut, spreadG);
         const int extraCap = itemCap;
         if (fromRows)
             sym_rows_from_newton(s, extraCap);
@@ -1154,7 +1168,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         read_scalars(s);
         // the rows serve the force pass if every extra was kept and merged
         if (fromRows) s.rowsFromNewton = s.hscal->extraCount <= extraCap && s.hscal->mergeOverflow == 0;
-        if (rowsJ && !s.rowsFromNewton) s.symRowsSkip = kSymRowsSkip;
+        if (writeJ && !s.rowsFromNewton) s.symRowsSkip = kSymRowsSkip;
         s.t.gjbuild += elapsed_s(g0, g1);
         s.t.gradkern += elapsed_s(g1, g2);
     }

@@ -192,6 +192,9 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
     // lists that outgrew their storage in a graph-run loop are incomplete: the solve is
     // redone on the host loop, so nothing reads them
     if (ds->err & kErrListFull) return;
+    // the index rows are written when the solve asks for them (a flag, so that a graph
+    // captured with the buffer serves solves that do and solves that do not)
+    if (!ds->rowsJOn) rowsJ = nullptr;
     const int nHeavy = ds->itemsHeavy, nItems = nHeavy + ds->itemsLight;
     const double wide2 = kRadK2 * (kRowMargin * kRowMargin);
     for (;;)

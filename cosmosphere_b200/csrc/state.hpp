@@ -103,6 +103,7 @@ struct DevScalars
     int coverLeaves;             // leaves holding such particles
     int extraCount;              // pairs a Newton row may miss from the other side (appended)
     int mergeOverflow;           // a row with its extras would exceed kNbl
+    int rowsJOn;                 // the Newton row builder writes the index rows (nonzero)
 };
 
 // The single-set Newton loop run as a graph: what the host loop kept in host variables
