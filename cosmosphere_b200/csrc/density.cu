@@ -270,10 +270,10 @@ __global__ void gradient_dead_kernel(int nAlive, int n, double* __restrict__ div
 
 // Rows from the Newton rows: whether each live particle's row covers its converged h
 // with the force test's slack to spare (written this solve, not overflowed, and
-// h (1 + 1e-9) <= the radius it is complete within, kept in acc4.w).  flag = 1 if it
-// does; a leaf with particles that do not is listed, and they are counted.
+// h (1 + 1e-9) <= rowH, the h it is complete for, cleared at the start of the solve).
+// flag = 1 if it does; a leaf with particles that do not is listed, and they are counted.
 __global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, const double4* __restrict__ xyzh,
-                                 const int* __restrict__ nblCount, const double4* __restrict__ acc4,
+                                 const int* __restrict__ nblCount, const double* __restrict__ rowH,
                                  const uint32_t* __restrict__ jstream, uint32_t streamCut, int* __restrict__ flag,
                                  int* __restrict__ leaves, double* __restrict__ hs, DevScalars* __restrict__ ds)
 {
@@ -286,7 +286,7 @@ __global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, co
         for (uint32_t a = p0 + lane; a < p1; a += 32)
         {
             const double h = xyzh[a].w;
-            const bool ok = unsigned(nblCount[a]) <= unsigned(kNbl) && h * (1.0 + 1e-9) <= acc4[a].w;
+            const bool ok = unsigned(nblCount[a]) <= unsigned(kNbl) && h * (1.0 + 1e-9) <= rowH[a];
             flag[a] = ok ? 1 : 0;
             hs[a] = h;
             miss += ok ? 0 : 1;
@@ -309,12 +309,12 @@ __global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, co
 // same order into the interleaved rows of the gradient and force passes (hs: h in the
 // sorted order, 8 bytes a particle).  A pair the force pass takes because of this
 // particle's support (dr^2 < R^2 h_i^2 (1 + 1e-10)) is in j's Newton row too unless dr^2
-// reaches the radius j's row covers (acc4.w, with 1e-9 to spare; only a pair beyond j's
+// reaches the radius j's row covers (R rowH, with 1e-9 to spare; only a pair beyond j's
 // own support can); such a pair is appended as (j << 32 | i), for i to be merged into
 // j's row.
 __global__ void __launch_bounds__(kThreads)
 sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __restrict__ rowsR2,
-                     int* __restrict__ nblCount, const double* __restrict__ hs, const double4* __restrict__ acc4,
+                     int* __restrict__ nblCount, const double* __restrict__ hs, const double* __restrict__ rowH,
                      int* __restrict__ nbl, unsigned long long* __restrict__ extras, int extraCap,
                      DevScalars* __restrict__ ds)
 {
@@ -332,7 +332,7 @@ sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __
             if (!(dr2 >= fmax(bi, bj))) out[size_t(w++) * kRowStride] = j;
             if (dr2 < bi && !(dr2 < kRadK2 * (hj * hj)))
             {
-                const double ch = __ldg(&acc4[j].w);
+                const double ch = __ldg(rowH + j);
                 if (!(dr2 < kRadK2 * (ch * ch) * (1.0 - 1e-9)))
                 {
                     const int k = atomicAdd(&ds->extraCount, 1);
@@ -568,7 +568,7 @@ struct KeyBytes
 enum class LoopGraph { Ran, Deferred, Failed };
 
 static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double hfact, int maxIter, FixedSplit cut,
-                                   int spreadG, long long& nActiveParticles, int* rowsJ, double4* rowsCover)
+                                   int spreadG, long long& nActiveParticles, int* rowsJ)
 {
     DevScalars* ds = s.dscal.get();
     const int nL = s.nLeaves;
@@ -639,7 +639,7 @@ static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double h
                           (const void*)s.jlistPrev.get(), (const void*)s.jOffsetPrev.get(), (const void*)s.walked.get(),
                           (const void*)s.walkScratch.get(), (const void*)s.hmaxLeaf.get(), (const void*)s.hmaxPre.get(),
                           (const void*)s.particleLeaf.get(), (const void*)s.scanTmp.get(), (const void*)nrows,
-                          (const void*)nr, (const void*)rk, (const void*)rowsJ, (const void*)rowsCover})
+                          (const void*)nr, (const void*)rk, (const void*)rowsJ})
         key.add(q);
     for (long long v : {(long long)leafCap, (long long)itemCap, (long long)gridRows, (long long)gridNr,
                         (long long)gridRow, (long long)bgrid, (long long)pgrid, (long long)s.periodic,
@@ -744,7 +744,7 @@ static LoopGraph newton_loop_graph(State& s, double pmass, double tolh, double h
             nrows<<<gridRows, kThreads, 0, s.st>>>(s.items.get(), itemCap, s.layout.get(), s.jOffset.get(),
                                                    s.jcount.get(), s.jlist.get(), s.xyzh.get(), s.box.get(),
                                                    s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds,
-                                                   rowsJ, rowsCover);
+                                                   rowsJ);
             COSMO_LAUNCHED();
             newton_count_kernel<<<1, 1, 0, s.st>>>(L, 1);
             COSMO_LAUNCHED();
@@ -848,7 +848,7 @@ static bool cover_rows(State& s, int itemCap, FixedSplit cut, int spreadG)
         COSMO_CUDA(cudaMemsetAsync(&ds->coverNeed, 0, 2 * sizeof(int), s.st));
         COSMO_CUDA(cudaMemsetAsync(&ds->mergeOverflow, 0, sizeof(int), s.st));   // here: leaves with no row
         row_cover_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
-            nL, s.layout.get(), s.xyzh.get(), s.nblCount.get(), s.acc4.get(), s.jstream.get(), cut.stream,
+            nL, s.layout.get(), s.xyzh.get(), s.nblCount.get(), s.nblH.get(), s.jstream.get(), cut.stream,
             s.coverFlag.get(), s.coverLeaves.get(), s.hs.get(), ds);
         COSMO_LAUNCHED();
         read_scalars(s);
@@ -864,8 +864,7 @@ static bool cover_rows(State& s, int itemCap, FixedSplit cut, int spreadG)
         RowsKernelFn nrows = s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>;
         nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
             s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
-            s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds, s.nblJ.get(),
-            s.acc4.get());
+            s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds, s.nblJ.get());
         COSMO_LAUNCHED();
     }
     return false;
@@ -887,7 +886,7 @@ static void sym_rows_from_newton(State& s, int extraCap)
     COSMO_CUDA(cudaMemsetAsync(&ds->rowOverflow, 0, sizeof(int), s.st));
     COSMO_CUDA(cudaMemsetAsync(s.extraCnt.get(), 0, size_t(nA) * sizeof(int), s.st));
     sym_from_rows_kernel<<<std::max(1, std::min(iceil(nA, kThreads), 16 * s.numSMs)), kThreads, 0, s.st>>>(
-        nA, s.nblJ.get(), s.nblR2.get(), s.nblCount.get(), s.hs.get(), s.acc4.get(), s.nbl.get(), s.extras.get(),
+        nA, s.nblJ.get(), s.nblR2.get(), s.nblCount.get(), s.hs.get(), s.nblH.get(), s.nbl.get(), s.extras.get(),
         extraCap, ds);
     COSMO_LAUNCHED();
     extras_count_kernel<<<iceil(extraCap, 256), 256, 0, s.st>>>(s.extras.get(), extraCap, ds, s.extraCnt.get());
@@ -933,18 +932,15 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.nblR2.resize(size_t(itemCap) * kNbl, s.st);
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
-    // The Newton rows also write their j (and the radius each covers, in acc4.w) when the
-    // gradient and force passes may run over them: a plain solve with gradients whose
-    // particles all start active (with fixed particles, leaves that never walk would hold
-    // no list this solve)
+    // The Newton rows also write their j when the gradient and force passes may run over
+    // them: a plain solve with gradients whose particles all start active (with fixed
+    // particles, leaves that never walk would hold no list this solve)
     int* rowsJ = nullptr;
-    double4* rowsCover = nullptr;
     if (s.precision == 0)
     {
         s.nblJ.resize(size_t(itemCap) * kNbl, s.st);
         s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);
         rowsJ = s.nblJ.get();
-        rowsCover = s.acc4.get();
     }
     // after a solve whose rows did not all cover (a workload with leaves the work queue
     // cuts, say), the next few solves do not write them
@@ -952,6 +948,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     if (s.symRowsSkip > 0) --s.symRowsSkip;
     const bool writeJ = rowsJ && withGradients && s.symFromRows && s.frozenFor != n && tryRows;
     COSMO_CUDA(cudaMemsetAsync(&ds->rowsJOn, writeJ ? 1 : 0, sizeof(int), s.st));
+    // rowH = 0: no row this solve (the coverage check reads it for every live particle)
+    if (writeJ) COSMO_CUDA(cudaMemsetAsync(s.nblH.get(), 0, size_t(itemCap) * sizeof(double), s.st));
     s.rowsFromNewton = false;
     s.hmaxNodeDone = true;
     s.listsLoose = false;
@@ -989,7 +987,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     if (allowGraph && s.newtonGraph && maxIter <= kLoopIters && nActiveParticles > 0)
     {
         const LoopGraph lg =
-            newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles, rowsJ, rowsCover);
+            newton_loop_graph(s, pmass, tolh, hfact, maxIter, cut, spreadG, nActiveParticles, rowsJ);
         graphRan = lg == LoopGraph::Ran;
         listsWidened = graphRan;
         // deferred: the first lists are built and valid for the host loop's first iteration
@@ -1033,7 +1031,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
                 nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
                     s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(),
                     s.xyzh.get(), s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds,
-                    rowsJ, rowsCover);
+                    rowsJ);
                 COSMO_LAUNCHED();
                 rowsReady = true;
             }

@@ -180,8 +180,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
                    const uint32_t* __restrict__ jOffset, const uint32_t* __restrict__ jcount,
                    const int* __restrict__ jlist, const double4* __restrict__ xyzh, const DevBox* __restrict__ box,
                    const double* __restrict__ listH, void* __restrict__ rowsR2, int* __restrict__ nblCount,
-                   double* __restrict__ rowH, DevScalars* __restrict__ ds, int* __restrict__ rowsJ,
-                   double4* __restrict__ acc4)
+                   double* __restrict__ rowH, DevScalars* __restrict__ ds, int* __restrict__ rowsJ)
 {
     using R2 = typename std::conditional<Mixed, float, double>::type;   // FP32 rows in the mixed form
     R2* nblR2 = static_cast<R2*>(rowsR2);
@@ -232,11 +231,7 @@ newton_rows_kernel(const int4* __restrict__ items, int cap, const uint32_t* __re
         if (mine)
         {
             nblCount[i] = rowLen;
-            const double rh = fmin(kRowMargin * pi.w, listH[d.leaf]) * (1.0 - 1e-12);
-            rowH[i] = rh;
-            // with the index rows: the radius this row is complete within, in the fourth
-            // component of the particle's acceleration (otherwise unused)
-            if (rowsJ) acc4[i].w = rh;
+            rowH[i] = fmin(kRowMargin * pi.w, listH[d.leaf]) * (1.0 - 1e-12);
         }
     }
 }
