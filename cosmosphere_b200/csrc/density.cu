@@ -279,6 +279,13 @@ __global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, co
 {
     const int lane = threadIdx.x & 31;
     const int nWarps = (gridDim.x * blockDim.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        // the counters of the passes that follow (nothing else touches them here)
+        ds->extraCount = 0;
+        ds->mergeOverflow = 0;
+        ds->rowOverflow = 0;
+    }
     for (int leaf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; leaf < nL; leaf += nWarps)
     {
         const uint32_t p0 = layout[leaf], p1 = layout[leaf + 1];
@@ -296,7 +303,7 @@ __global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, co
         {
             atomicAdd(&ds->coverNeed, miss);
             // a leaf whose stream the work queue cuts keeps the group path: no row for it
-            if (jstream[leaf] > streamCut) atomicAdd(&ds->mergeOverflow, 1);
+            if (jstream[leaf] > streamCut) atomicAdd(&ds->coverCut, 1);
             leaves[atomicAdd(&ds->coverLeaves, 1)] = leaf;
         }
     }
@@ -316,10 +323,11 @@ __global__ void __launch_bounds__(kThreads)
 sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __restrict__ rowsR2,
                      int* __restrict__ nblCount, const double* __restrict__ hs, const double* __restrict__ rowH,
                      int* __restrict__ nbl, unsigned long long* __restrict__ extras, int extraCap,
-                     DevScalars* __restrict__ ds)
+                     int* __restrict__ extraCnt, DevScalars* __restrict__ ds)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nAlive; i += gridDim.x * blockDim.x)
     {
+        extraCnt[i] = 0;
         const int cnt = nblCount[i];
         const double hi = hs[i];
         const double bi = kRadK2 * (hi * hi) * (1.0 + 1e-10);
@@ -845,8 +853,7 @@ static bool cover_rows(State& s, int itemCap, FixedSplit cut, int spreadG)
     s.hs.resize(itemCap, s.st);
     for (int pass = 0; pass < 2; ++pass)
     {
-        COSMO_CUDA(cudaMemsetAsync(&ds->coverNeed, 0, 2 * sizeof(int), s.st));
-        COSMO_CUDA(cudaMemsetAsync(&ds->mergeOverflow, 0, sizeof(int), s.st));   // here: leaves with no row
+        COSMO_CUDA(cudaMemsetAsync(&ds->coverNeed, 0, 3 * sizeof(int), s.st));   // need, leaves, cut
         row_cover_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
             nL, s.layout.get(), s.xyzh.get(), s.nblCount.get(), s.nblH.get(), s.jstream.get(), cut.stream,
             s.coverFlag.get(), s.coverLeaves.get(), s.hs.get(), ds);
@@ -854,7 +861,7 @@ static bool cover_rows(State& s, int itemCap, FixedSplit cut, int spreadG)
         read_scalars(s);
         const int need = s.hscal->coverNeed;
         if (need == 0) return true;
-        if (pass == 1 || need > s.nAlive / 4 || s.hscal->mergeOverflow > 0) return false;
+        if (pass == 1 || need > s.nAlive / 4 || s.hscal->coverCut > 0) return false;
         begin_iteration_kernel<<<std::min(iceil(nL, 256), 4 * s.numSMs), 256, 0, s.st>>>(ds, s.leafNext.get(), nL);
         COSMO_LAUNCHED();
         plan_items_count_kernel<<<grid_for(s, nL), kThreads, 0, s.st>>>(
@@ -882,12 +889,11 @@ static void sym_rows_from_newton(State& s, int extraCap)
     s.extraCnt.resize(nA, s.st);
     s.extraOff.resize(size_t(nA) + 1, s.st);
     s.extraBucket.resize(extraCap, s.st);
-    COSMO_CUDA(cudaMemsetAsync(&ds->extraCount, 0, 2 * sizeof(int), s.st));   // extraCount, mergeOverflow
-    COSMO_CUDA(cudaMemsetAsync(&ds->rowOverflow, 0, sizeof(int), s.st));
-    COSMO_CUDA(cudaMemsetAsync(s.extraCnt.get(), 0, size_t(nA) * sizeof(int), s.st));
+    // extraCount, mergeOverflow and rowOverflow were zeroed by the coverage check; each
+    // particle's extras count by the compaction
     sym_from_rows_kernel<<<std::max(1, std::min(iceil(nA, kThreads), 16 * s.numSMs)), kThreads, 0, s.st>>>(
         nA, s.nblJ.get(), s.nblR2.get(), s.nblCount.get(), s.hs.get(), s.nblH.get(), s.nbl.get(), s.extras.get(),
-        extraCap, ds);
+        extraCap, s.extraCnt.get(), ds);
     COSMO_LAUNCHED();
     extras_count_kernel<<<iceil(extraCap, 256), 256, 0, s.st>>>(s.extras.get(), extraCap, ds, s.extraCnt.get());
     COSMO_LAUNCHED();
@@ -914,13 +920,18 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.t = Timings{};
     ev_reset(s);
     DevScalars* ds = s.dscal.get();
-    COSMO_CUDA(cudaMemsetAsync(s.rho.get(), 0, size_t(n) * 8, s.st));
-    COSMO_CUDA(cudaMemsetAsync(s.gradh.get(), 0, size_t(n) * 8, s.st));
-    COSMO_CUDA(cudaMemsetAsync(s.converged.get(), 0, size_t(n) * 4, s.st));
-    COSMO_CUDA(cudaMemsetAsync(&ds->pairs[0], 0, sizeof(ds->pairs), s.st));
-    COSMO_CUDA(cudaMemsetAsync(&ds->hmaxSeen, 0, sizeof(ds->hmaxSeen), s.st));
+    // The Newton rows also write their j when the gradient and force passes may run over
+    // them: a plain solve with gradients whose particles all start active (with fixed
+    // particles, leaves that never walk would hold no list this solve).  After a solve
+    // whose rows did not all cover (a workload with leaves the work queue cuts, say), the
+    // next few solves do not write them.
+    const bool tryRows = s.symRowsSkip == 0;
+    if (s.symRowsSkip > 0) --s.symRowsSkip;
+    const bool writeJ = s.precision == 0 && withGradients && s.symFromRows && s.frozenFor != n && tryRows;
 
-    build_tree(s, periodicBox, withGradients);
+    // the tree; its particle gather also zeroes rho, gradh, the convergence flags, the
+    // Newton rows' h (0: no row this solve) and the pair counters
+    build_tree(s, periodicBox, withGradients, writeJ);
     s.orderFor = n;
     const int nL = s.nLeaves;
     s.activeA.resize(nL, s.st);
@@ -932,9 +943,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     s.nblR2.resize(size_t(itemCap) * kNbl, s.st);
     s.nblCount.resize(itemCap, s.st);
     s.nblH.resize(itemCap, s.st);
-    // The Newton rows also write their j when the gradient and force passes may run over
-    // them: a plain solve with gradients whose particles all start active (with fixed
-    // particles, leaves that never walk would hold no list this solve)
+    // the index rows' buffer is passed whenever the form has one (the Newton-loop graph
+    // keeps one key); the gather set the device switch from writeJ
     int* rowsJ = nullptr;
     if (s.precision == 0)
     {
@@ -942,14 +952,6 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);
         rowsJ = s.nblJ.get();
     }
-    // after a solve whose rows did not all cover (a workload with leaves the work queue
-    // cuts, say), the next few solves do not write them
-    const bool tryRows = s.symRowsSkip == 0;
-    if (s.symRowsSkip > 0) --s.symRowsSkip;
-    const bool writeJ = rowsJ && withGradients && s.symFromRows && s.frozenFor != n && tryRows;
-    COSMO_CUDA(cudaMemsetAsync(&ds->rowsJOn, writeJ ? 1 : 0, sizeof(int), s.st));
-    // rowH = 0: no row this solve (the coverage check reads it for every live particle)
-    if (writeJ) COSMO_CUDA(cudaMemsetAsync(s.nblH.get(), 0, size_t(itemCap) * sizeof(double), s.st));
     s.rowsFromNewton = false;
     s.hmaxNodeDone = true;
     s.listsLoose = false;

@@ -26,9 +26,10 @@ constexpr int kThreads = 32 * kWarpsPerBlock;
 __global__ void force_prep_kernel(const double4* __restrict__ xyzh, const double* __restrict__ gradh,
                                   const double4* __restrict__ thermo4, int n, double pmass, double alphau,
                                   double hfact, double4* __restrict__ prepA, double4* __restrict__ prepB,
-                                  double4* __restrict__ vel4)
+                                  double4* __restrict__ vel4, DevScalars* __restrict__ ds)
 {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i == 0) ds->pairs[2] = 0;   // the force pass's pair counter
     if (i >= n) return;
     const double hi = xyzh[i].w;
     if (!(hi > 0.0))
@@ -385,7 +386,6 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
 {
     const int n = s.ngas;
     DevScalars* ds = s.dscal.get();
-    COSMO_CUDA(cudaMemsetAsync(&ds->pairs[2], 0, sizeof(unsigned long long), s.st));
     cudaEvent_t e0 = ev(s);
     s.forceSinceSolve = true;
     // The symmetric lists and rows are cached per tree (src/force.cu:19-24); the density
@@ -405,7 +405,7 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
     cudaEvent_t p0 = ev(s);
     force_prep_kernel<<<iceil(n, 256), 256, 0, s.st>>>(s.xyzh.get(), s.gradh.get(), s.thermo4.get(), n, pmass,
                                                        alphau, s.hfact, s.prepA.get(), s.prepB.get(),
-                                                       s.vel4.get());
+                                                       s.vel4.get(), ds);
     COSMO_LAUNCHED();
     cudaEvent_t p1 = ev(s);
     const int nL = s.nLeaves;

@@ -101,6 +101,7 @@ struct DevScalars
     unsigned long long hmaxSeen; // bits of the largest h any leaf had at the start of an iteration
     int coverNeed;               // live particles whose Newton row does not cover their converged h
     int coverLeaves;             // leaves holding such particles
+    int coverCut;                // those of them in leaves the work queue cuts (no row for them)
     int extraCount;              // pairs a Newton row may miss from the other side (appended)
     int mergeOverflow;           // a row with its extras would exceed kNbl
     int rowsJOn;                 // the Newton row builder writes the index rows (nonzero)
@@ -270,7 +271,7 @@ size_t state_device_bytes(const State& s);
 void size_particle_arrays(State& s, int n);
 
 // tree.cu
-void build_tree(State& s, const double* periodicBox, bool alsoSortVA);
+void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJOn = false);
 // hmax of the leaves [0, nLeavesActive) of leaves, or of the first *countPtr of them when
 // countPtr is given (a count on the device; nLeavesActive then bounds it).
 void hmax_leaves(State& s, const int* leaves, int nLeavesActive, const int* countPtr = nullptr);

@@ -135,6 +135,20 @@ __global__ void alive_kernel(const uint64_t* __restrict__ keys, int n, DevScalar
     if (!dead && i == n - 1) ds->nAlive = n;
 }
 
+// What a solve starts from zero, set by the gather (one pass over the particles instead
+// of a memset per array): rho, gradh, the convergence flags and the Newton rows' h, the
+// scalars' pair counters and hmax seen, the index-row switch, and the leaf tree's seed.
+struct SolveReset
+{
+    double* rho;
+    double* gradh;
+    int* converged;
+    double* rowH;
+    uint64_t* csTree;
+    DevScalars* ds;
+    int rowsJOn;
+};
+
 __global__ void gather_particles_kernel(const int* __restrict__ order, int n,
                                         const double* __restrict__ ux, const double* __restrict__ uy,
                                         const double* __restrict__ uz, const double* __restrict__ uh,
@@ -142,9 +156,17 @@ __global__ void gather_particles_kernel(const int* __restrict__ order, int n,
                                         const double* __restrict__ uvy, const double* __restrict__ uvz,
                                         const double* __restrict__ uax, const double* __restrict__ uay,
                                         const double* __restrict__ uaz, double4* __restrict__ vel4,
-                                        double4* __restrict__ acc4, int alsoVA)
+                                        double4* __restrict__ acc4, int alsoVA, SolveReset r)
 {
     const long k = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k == 0)
+    {
+        for (int p = 0; p < 4; ++p) r.ds->pairs[p] = 0;
+        r.ds->hmaxSeen = 0;
+        r.ds->rowsJOn = r.rowsJOn;
+        r.csTree[0] = 0;
+        r.csTree[1] = kKeyEnd;
+    }
     if (k >= n) return;
     const int i = order[k];
     xyzh[k] = make_double4(ux[i], uy[i], uz[i], uh[i]);
@@ -153,6 +175,10 @@ __global__ void gather_particles_kernel(const int* __restrict__ order, int n,
         vel4[k] = make_double4(uvx[i], uvy[i], uvz[i], 0.0);
         acc4[k] = make_double4(uax[i], uay[i], uaz[i], 0.0);
     }
+    r.rho[k] = 0.0;
+    r.gradh[k] = 0.0;
+    r.converged[k] = 0;
+    r.rowH[k] = 0.0;
 }
 
 // ------------------------------------------------------------------ leaf tree
@@ -776,7 +802,7 @@ int keysort_raw(int n, const double* x, const double* y, const double* z, const 
     return e ? -3 : 0;
 }
 
-void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
+void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJOn)
 {
     const int n = s.ngas;
     DevScalars* ds = s.dscal.get();
@@ -816,19 +842,18 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA)
     radix_sort_u64(s, s.keysA.get(), s.keysB.get(), s.orderA.get(), s.orderB.get(), n, true);
     alive_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.keysA.get(), n, ds);
     COSMO_LAUNCHED();
-    gather_particles_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(
+    // cornerstone leaf tree from the single-root seed (src/tree.cu:126-136), written by the
+    // gather with the rest of what a solve starts from zero
+    s.csTree.resize(2, s.st);
+    s.nblH.resize(std::max(n, 1), s.st);
+    gather_particles_kernel<<<iceil(std::max(n, 1), kBlk), kBlk, 0, s.st>>>(
         s.orderA.get(), n, s.ux.get(), s.uy.get(), s.uz.get(), s.uh.get(), s.xyzh.get(), s.uvx.get(),
         s.uvy.get(), s.uvz.get(), s.uax.get(), s.uay.get(), s.uaz.get(), s.vel4.get(), s.acc4.get(),
-        alsoSortVA ? 1 : 0);
+        alsoSortVA ? 1 : 0,
+        SolveReset{s.rho.get(), s.gradh.get(), s.converged.get(), s.nblH.get(), s.csTree.get(), ds, rowsJOn ? 1 : 0});
     COSMO_LAUNCHED();
     cudaEvent_t e2 = ev(s);
 
-    // cornerstone leaf tree from the single-root seed (src/tree.cu:126-136)
-    s.csTree.resize(2, s.st);
-    {
-        const uint64_t seed[2] = {0, kKeyEnd};
-        COSMO_CUDA(cudaMemcpyAsync(s.csTree.get(), seed, sizeof(seed), cudaMemcpyHostToDevice, s.st));
-    }
     int nL = 1;
     for (int round = 0; round < 64; ++round)
     {
