@@ -258,7 +258,7 @@ onesweep_body(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uin
 }
 
 
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 3)
 onesweep_kernel(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uint64_t* __restrict__ kout,
                 int* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ binBase,
                 uint32_t* lookback, unsigned int* tileTicket, int* err, long long waitNs)
