@@ -143,7 +143,7 @@ size_t state_device_bytes(const State& s)
     add(s.items);
     add(s.extras);
     add(s.extraOff);
-    for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
+    for (auto* d : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.startBounds, &s.nodeCount, &s.leafPreStart, &s.jcount,
                     &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback, &s.jOffsetPrev})
         add(*d);
     add(s.box);
@@ -171,7 +171,7 @@ void release_state(State& s)
     s.items.release(s.st);
     s.extras.release(s.st);
     s.extraOff.release(s.st);
-    for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.nodeCount, &s.leafPreStart, &s.jcount,
+    for (auto* b : {&s.counts, &s.ops, &s.opsScan, &s.layout, &s.startBounds, &s.nodeCount, &s.leafPreStart, &s.jcount,
                     &s.jstream, &s.jOffset, &s.scanTmp, &s.sortHist, &s.sortBase, &s.sortLookback, &s.jOffsetPrev})
         b->release(s.st);
     s.box.release(s.st);

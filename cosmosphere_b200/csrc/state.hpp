@@ -105,6 +105,7 @@ struct DevScalars
     int extraCount;              // pairs a Newton row may miss from the other side (appended)
     int mergeOverflow;           // a row with its extras would exceed kNbl
     int rowsJOn;                 // the Newton row builder writes the index rows (nonzero)
+    int leafStart;               // leaves of the grid the leaf tree's refinement starts from
 };
 
 // The single-set Newton loop run as a graph: what the host loop kept in host variables
@@ -220,6 +221,7 @@ struct State
     DBuf<DevBox> box;
     DBuf<uint64_t> csTree, csTree2;
     DBuf<uint32_t> counts, ops, opsScan, layout;
+    DBuf<uint32_t> startBounds;                 // where each level-4 cell starts in the sorted keys
     DBuf<uint64_t> prePrefix, bfsPrefix;
     DBuf<uint32_t> nodeCount, leafPreStart;
     DBuf<int> preLeaf, preSkip, bfsToPre, preToBfs;

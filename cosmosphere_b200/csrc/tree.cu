@@ -137,14 +137,13 @@ __global__ void alive_kernel(const uint64_t* __restrict__ keys, int n, DevScalar
 
 // What a solve starts from zero, set by the gather (one pass over the particles instead
 // of a memset per array): rho, gradh, the convergence flags and the Newton rows' h, the
-// scalars' pair counters and hmax seen, the index-row switch, and the leaf tree's seed.
+// scalars' pair counters and hmax seen, and the index-row switch.
 struct SolveReset
 {
     double* rho;
     double* gradh;
     int* converged;
     double* rowH;
-    uint64_t* csTree;
     DevScalars* ds;
     int rowsJOn;
 };
@@ -164,8 +163,6 @@ __global__ void gather_particles_kernel(const int* __restrict__ order, int n,
         for (int p = 0; p < 4; ++p) r.ds->pairs[p] = 0;
         r.ds->hmaxSeen = 0;
         r.ds->rowsJOn = r.rowsJOn;
-        r.csTree[0] = 0;
-        r.csTree[1] = kKeyEnd;
     }
     if (k >= n) return;
     const int i = order[k];
@@ -222,6 +219,62 @@ __global__ void leaf_split_kernel(const uint64_t* __restrict__ tree, int nL, con
         for (int o = 0; o < 8; ++o) out[p + o] = a + uint64_t(o) * child;
     }
     else out[p] = a;
+}
+
+// Where the leaf tree's refinement starts.  From the root, every node holding more than
+// kBucket live particles splits into its eight children each round, so a node above the
+// coarsest level at which some node holds kBucket or fewer is always split: the rounds
+// that lead there produce the complete grid of that level whatever the particles.
+// leaf_bounds_kernel finds where each of the 4096 level-4 cells starts in the sorted live
+// keys (one binary search a thread); leaf_start_kernel takes each level's smallest count
+// from those bounds and writes the complete grid of level L0 = 1 + the deepest level (at
+// most 4) whose every node holds more than kBucket (0 when the root itself holds no
+// more): 8^L0 leaves, their bounds in tree, the count in *nOut.  The rounds that follow
+// from it give the tree the rounds from the root would.
+constexpr int kStartLevels = 4;
+constexpr int kStartCells = 1 << (3 * kStartLevels);
+
+__global__ void leaf_bounds_kernel(const uint64_t* __restrict__ keys, const DevScalars* __restrict__ ds,
+                                   uint32_t* __restrict__ bounds)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > kStartCells) return;
+    const uint32_t na = uint32_t(ds->nAlive);
+    bounds[c] = c == kStartCells ? na
+                                 : lower_bound_u64(keys, na, uint64_t(c) << (3 * (kMaxLevel - kStartLevels)));
+}
+
+__global__ void __launch_bounds__(1024)
+leaf_start_kernel(const uint32_t* __restrict__ bounds, const DevScalars* __restrict__ ds,
+                  uint64_t* __restrict__ tree, int* __restrict__ nOut)
+{
+    __shared__ uint32_t lmin[kStartLevels + 1];
+    __shared__ int sL0;
+    const uint32_t na = uint32_t(ds->nAlive);
+    const int t = threadIdx.x;
+    if (t <= kStartLevels) lmin[t] = 0xffffffffu;
+    __syncthreads();
+    for (int l = 1; l <= kStartLevels; ++l)
+    {
+        const int cells = 1 << (3 * l), span = kStartCells / cells;
+        for (int c = t; c < cells; c += blockDim.x) atomicMin(&lmin[l], bounds[(c + 1) * span] - bounds[c * span]);
+    }
+    __syncthreads();
+    if (t == 0)
+    {
+        int L0 = 0;
+        if (na > kBucket)
+        {
+            L0 = 1;
+            for (int l = 1; l <= kStartLevels && lmin[l] > kBucket; ++l) L0 = l + 1;
+        }
+        sL0 = L0;
+        *nOut = 1 << (3 * L0);
+    }
+    __syncthreads();
+    const int L0 = sL0, cells = 1 << (3 * L0);
+    for (int c = t; c < cells; c += blockDim.x) tree[c] = uint64_t(c) << (3 * (kMaxLevel - L0));
+    if (t == 0) tree[cells] = kKeyEnd;
 }
 
 // ------------------------------------------------------------------ linked octree
@@ -842,19 +895,25 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJ
     radix_sort_u64(s, s.keysA.get(), s.keysB.get(), s.orderA.get(), s.orderB.get(), n, true);
     alive_kernel<<<iceil(n, kBlk), kBlk, 0, s.st>>>(s.keysA.get(), n, ds);
     COSMO_LAUNCHED();
-    // cornerstone leaf tree from the single-root seed (src/tree.cu:126-136), written by the
-    // gather with the rest of what a solve starts from zero
-    s.csTree.resize(2, s.st);
     s.nblH.resize(std::max(n, 1), s.st);
     gather_particles_kernel<<<iceil(std::max(n, 1), kBlk), kBlk, 0, s.st>>>(
         s.orderA.get(), n, s.ux.get(), s.uy.get(), s.uz.get(), s.uh.get(), s.xyzh.get(), s.uvx.get(),
         s.uvy.get(), s.uvz.get(), s.uax.get(), s.uay.get(), s.uaz.get(), s.vel4.get(), s.acc4.get(),
         alsoSortVA ? 1 : 0,
-        SolveReset{s.rho.get(), s.gradh.get(), s.converged.get(), s.nblH.get(), s.csTree.get(), ds, rowsJOn ? 1 : 0});
+        SolveReset{s.rho.get(), s.gradh.get(), s.converged.get(), s.nblH.get(), ds, rowsJOn ? 1 : 0});
     COSMO_LAUNCHED();
     cudaEvent_t e2 = ev(s);
 
-    int nL = 1;
+    // cornerstone leaf tree (src/tree.cu:126-136): the refinement from the root, started at
+    // the complete grid of the level above which every node splits
+    s.csTree.resize((size_t(1) << (3 * kStartLevels + 3)) + 1, s.st);
+    s.startBounds.resize(kStartCells + 1, s.st);
+    leaf_bounds_kernel<<<iceil(kStartCells + 1, 256), 256, 0, s.st>>>(s.keysA.get(), ds, s.startBounds.get());
+    COSMO_LAUNCHED();
+    leaf_start_kernel<<<1, 1024, 0, s.st>>>(s.startBounds.get(), ds, s.csTree.get(), &ds->leafStart);
+    COSMO_LAUNCHED();
+    read_scalars(s);
+    int nL = s.hscal->leafStart;
     for (int round = 0; round < 64; ++round)
     {
         s.counts.resize(nL, s.st);
