@@ -221,9 +221,9 @@ void read_scalars(State& s)
     COSMO_CUDA(cudaStreamSynchronize(s.st));
 }
 
-void check_dev_err(State& s, const char* where)
+void check_dev_err(State& s, const char* where, bool reread)
 {
-    read_scalars(s);
+    if (reread) read_scalars(s);
     const int e = s.hscal->err;
     if (e)
         fatal("%s: device error 0x%x (%s%s%s%s)", where, e, (e & kErrSortSpin) ? "sort look-back timeout " : "",

@@ -1093,7 +1093,8 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         COSMO_CUDA(cudaEventSynchronize(j1));
         s.t.jbuild += elapsed_s(j0, j1);
     }
-    check_dev_err(s, "solveDensH");
+    check_dev_err(s, "solveDensH", listsWidened && !withGradients);
+    tree_timings(s);
     res.itersRun = s.itersRun;
     res.unconverged = int(nActiveParticles);
     if (nActiveParticles > 0)
@@ -1172,7 +1173,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         s.t.gjbuild += elapsed_s(g0, g1);
         s.t.gradkern += elapsed_s(g1, g2);
     }
-    check_dev_err(s, "solveDensH");
+    check_dev_err(s, "solveDensH", false);
     ++s.token;
     s.forceSinceSolve = false;
     if (symBuilt) s.jlistToken = s.rowsToken = s.token;

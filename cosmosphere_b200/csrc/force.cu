@@ -452,7 +452,7 @@ void compute_forces(State& s, double pmass, double beta, double alphau, bool dis
     read_scalars(s);
     s.t.prep += elapsed_s(p0, p1);
     s.t.fkern += elapsed_s(p1, p2);
-    check_dev_err(s, "force_gpu_c");
+    check_dev_err(s, "force_gpu_c", false);
 }
 
 } // namespace cosmo

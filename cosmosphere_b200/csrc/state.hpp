@@ -204,6 +204,7 @@ struct State
     int lastLoopRebuilds = 0, lastLoopRowBuilds = 0;   // its list rebuilds and row builds
     std::vector<long long> loopListEntries;              // its gather-list entries per iteration
     std::vector<long long> activePerIter;
+    cudaEvent_t treeEv[5] = {};   // the last tree build's stage marks (read after the next sync)
     double uploadSeconds = 0.0, downloadSeconds = 0.0;
     Timings t;
 
@@ -274,6 +275,7 @@ void size_particle_arrays(State& s, int n);
 
 // tree.cu
 void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJOn = false);
+void tree_timings(State& s);   // the last tree build's stage times, once its marks have passed
 // hmax of the leaves [0, nLeavesActive) of leaves, or of the first *countPtr of them when
 // countPtr is given (a count on the device; nLeavesActive then bounds it).
 void hmax_leaves(State& s, const int* leaves, int nLeavesActive, const int* countPtr = nullptr);
@@ -322,6 +324,8 @@ cudaEvent_t ev(State& s);            // record an event on the state's stream (p
 void ev_reset(State& s);
 
 void read_scalars(State& s);         // dscal -> hscal, synchronising the stream
-void check_dev_err(State& s, const char* where);
+// FATAL if the device raised an error bit; reread = false when the scalars were just read
+// (nothing has run since)
+void check_dev_err(State& s, const char* where, bool reread = true);
 
 } // namespace cosmo

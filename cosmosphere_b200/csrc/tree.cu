@@ -913,6 +913,7 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJ
     leaf_start_kernel<<<1, 1024, 0, s.st>>>(s.startBounds.get(), ds, s.csTree.get(), &ds->leafStart);
     COSMO_LAUNCHED();
     read_scalars(s);
+    s.nAlive = s.hscal->nAlive;   // counted by alive_kernel before the gather
     int nL = s.hscal->leafStart;
     for (int round = 0; round < 64; ++round)
     {
@@ -979,13 +980,20 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJ
     iota_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.allLeaves.get(), nL);
     COSMO_LAUNCHED();
     cudaEvent_t e4 = ev(s);
+    // the stage times are taken once the stream has been read again (tree_timings)
+    const cudaEvent_t marks[5] = {e0, e1, e2, e3, e4};
+    std::copy(marks, marks + 5, s.treeEv);
+}
 
-    read_scalars(s);
-    s.nAlive = s.hscal->nAlive;
-    s.t.bbox += elapsed_s(e0, e1);
-    s.t.keysSort += elapsed_s(e1, e2);
-    s.t.tree += elapsed_s(e2, e3);
-    s.t.nodes += elapsed_s(e3, e4);
+void tree_timings(State& s)
+{
+    if (!s.treeEv[4]) return;
+    COSMO_CUDA(cudaEventSynchronize(s.treeEv[4]));
+    s.t.bbox += elapsed_s(s.treeEv[0], s.treeEv[1]);
+    s.t.keysSort += elapsed_s(s.treeEv[1], s.treeEv[2]);
+    s.t.tree += elapsed_s(s.treeEv[2], s.treeEv[3]);
+    s.t.nodes += elapsed_s(s.treeEv[3], s.treeEv[4]);
+    s.treeEv[4] = nullptr;
 }
 
 void hmax_leaves(State& s, const int* leaves, int nActive, const int* countPtr)
