@@ -106,6 +106,7 @@ struct DevScalars
     int mergeOverflow;           // a row with its extras would exceed kNbl
     int rowsJOn;                 // the Newton row builder writes the index rows (nonzero)
     int leafStart;               // leaves of the grid the leaf tree's refinement starts from
+    int leafDone;                // that grid is the leaf tree (no node of it holds more than kBucket)
 };
 
 // The single-set Newton loop run as a graph: what the host loop kept in host variables

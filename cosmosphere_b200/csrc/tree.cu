@@ -225,16 +225,18 @@ __global__ void leaf_split_kernel(const uint64_t* __restrict__ tree, int nL, con
 // kBucket live particles splits into its eight children each round, so a node above the
 // coarsest level at which some node holds kBucket or fewer is always split: the rounds
 // that lead there produce the complete grid of that level whatever the particles.
-// leaf_bounds_kernel finds where each of the 4096 level-4 cells starts in the sorted live
-// keys (one binary search a thread); leaf_start_kernel takes each level's smallest count
-// from those bounds and writes the complete grid of level L0 = 1 + the deepest level (at
-// most 4) whose every node holds more than kBucket (0 when the root itself holds no
-// more): 8^L0 leaves, their bounds in tree, the count in *nOut.  The rounds that follow
-// from it give the tree the rounds from the root would.
-constexpr int kStartLevels = 4;
+// leaf_bounds_kernel finds where each of the 32768 level-5 cells starts in the sorted
+// live keys (one binary search a thread); leaf_start_kernel takes each level's smallest
+// count from those bounds and writes the complete grid of level L0 = 1 + the deepest
+// level (at most 5) whose every node holds more than kBucket (0 when the root itself
+// holds no more): 8^L0 leaves, their bounds in tree, the count in ds->leafStart.  When no
+// node of that grid holds more than kBucket either (L0 at most 5, where its counts are
+// known), the grid is the tree: its counts are written and ds->leafDone set.  Otherwise
+// the rounds that follow from it give the tree the rounds from the root would.
+constexpr int kStartLevels = 5;
 constexpr int kStartCells = 1 << (3 * kStartLevels);
 
-__global__ void leaf_bounds_kernel(const uint64_t* __restrict__ keys, const DevScalars* __restrict__ ds,
+__global__ void leaf_bounds_kernel(const uint64_t* __restrict__ keys, DevScalars* __restrict__ ds,
                                    uint32_t* __restrict__ bounds)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -245,19 +247,28 @@ __global__ void leaf_bounds_kernel(const uint64_t* __restrict__ keys, const DevS
 }
 
 __global__ void __launch_bounds__(1024)
-leaf_start_kernel(const uint32_t* __restrict__ bounds, const DevScalars* __restrict__ ds,
-                  uint64_t* __restrict__ tree, int* __restrict__ nOut)
+leaf_start_kernel(const uint32_t* __restrict__ bounds, DevScalars* __restrict__ ds, uint64_t* __restrict__ tree,
+                  uint32_t* __restrict__ counts)
 {
-    __shared__ uint32_t lmin[kStartLevels + 1];
+    __shared__ uint32_t lmin[kStartLevels + 1], lmax[kStartLevels + 1];
     __shared__ int sL0;
     const uint32_t na = uint32_t(ds->nAlive);
     const int t = threadIdx.x;
-    if (t <= kStartLevels) lmin[t] = 0xffffffffu;
+    if (t <= kStartLevels)
+    {
+        lmin[t] = t == 0 ? na : 0xffffffffu;
+        lmax[t] = t == 0 ? na : 0u;
+    }
     __syncthreads();
     for (int l = 1; l <= kStartLevels; ++l)
     {
         const int cells = 1 << (3 * l), span = kStartCells / cells;
-        for (int c = t; c < cells; c += blockDim.x) atomicMin(&lmin[l], bounds[(c + 1) * span] - bounds[c * span]);
+        for (int c = t; c < cells; c += blockDim.x)
+        {
+            const uint32_t k = bounds[(c + 1) * span] - bounds[c * span];
+            atomicMin(&lmin[l], k);
+            atomicMax(&lmax[l], k);
+        }
     }
     __syncthreads();
     if (t == 0)
@@ -269,11 +280,18 @@ leaf_start_kernel(const uint32_t* __restrict__ bounds, const DevScalars* __restr
             for (int l = 1; l <= kStartLevels && lmin[l] > kBucket; ++l) L0 = l + 1;
         }
         sL0 = L0;
-        *nOut = 1 << (3 * L0);
+        ds->leafStart = 1 << (3 * L0);
+        ds->leafDone = (L0 <= kStartLevels && lmax[L0] <= kBucket) ? 1 : 0;
     }
     __syncthreads();
     const int L0 = sL0, cells = 1 << (3 * L0);
-    for (int c = t; c < cells; c += blockDim.x) tree[c] = uint64_t(c) << (3 * (kMaxLevel - L0));
+    const bool done = L0 <= kStartLevels && lmax[L0] <= kBucket;
+    const int span = L0 <= kStartLevels ? kStartCells / cells : 0;
+    for (int c = t; c < cells; c += blockDim.x)
+    {
+        tree[c] = uint64_t(c) << (3 * (kMaxLevel - L0));
+        if (done) counts[c] = bounds[(c + 1) * span] - bounds[c * span];
+    }
     if (t == 0) tree[cells] = kKeyEnd;
 }
 
@@ -908,14 +926,16 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJ
     // the complete grid of the level above which every node splits
     s.csTree.resize((size_t(1) << (3 * kStartLevels + 3)) + 1, s.st);
     s.startBounds.resize(kStartCells + 1, s.st);
+    s.counts.resize(kStartCells, s.st);
     leaf_bounds_kernel<<<iceil(kStartCells + 1, 256), 256, 0, s.st>>>(s.keysA.get(), ds, s.startBounds.get());
     COSMO_LAUNCHED();
-    leaf_start_kernel<<<1, 1024, 0, s.st>>>(s.startBounds.get(), ds, s.csTree.get(), &ds->leafStart);
+    leaf_start_kernel<<<1, 1024, 0, s.st>>>(s.startBounds.get(), ds, s.csTree.get(), s.counts.get());
     COSMO_LAUNCHED();
     read_scalars(s);
     s.nAlive = s.hscal->nAlive;   // counted by alive_kernel before the gather
     int nL = s.hscal->leafStart;
-    for (int round = 0; round < 64; ++round)
+    const bool startIsTree = s.hscal->leafDone != 0;
+    for (int round = 0; round < 64 && !startIsTree; ++round)
     {
         s.counts.resize(nL, s.st);
         s.ops.resize(nL, s.st);
