@@ -961,7 +961,10 @@ void build_tree(State& s, const double* periodicBox, bool alsoSortVA, bool rowsJ
     s.leafPreStart.resize(size_t(nL) + 1, s.st);
     node_count_kernel<<<iceil(nL, kBlk), kBlk, 0, s.st>>>(s.csTree.get(), nL, s.nodeCount.get());
     COSMO_LAUNCHED();
-    const int numNodes = int(scan_exclusive(s, s.nodeCount.get(), s.leafPreStart.get(), nL, true));
+    // every internal node of the refinement has eight children, so the octree of nL leaves
+    // has (nL - 1) / 7 internal nodes: the node count needs no read of the scan's total
+    scan_exclusive(s, s.nodeCount.get(), s.leafPreStart.get(), nL, false);
+    const int numNodes = nL + (nL - 1) / 7;
     s.numNodes = numNodes;
     for (auto* b : {&s.prePrefix, &s.bfsPrefix}) b->resize(numNodes, s.st);
     for (auto* b : {&s.preLeaf, &s.preSkip, &s.bfsToPre, &s.preToBfs, &s.childOffsets, &s.internalToLeaf})
