@@ -85,45 +85,54 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
                                                                                               nullptr},
                                            Split split = Split{}, int spreadGroups = kSpreadGroups)
 {
+    // The block's warps take one leaf each per step and reserve their rows and items
+    // together: each warp's counts go to shared memory, one thread makes one global
+    // reservation per counter for the block, and each warp writes at its share of it
+    // (one atomic per block and counter instead of one per warp and window: the counters
+    // are single addresses that every warp of the grid adds to).
+    __shared__ int sCnt[3][32];   // per warp: row particles, cut groups, whole groups
+    __shared__ int sBase[3];
+    __shared__ int sWin[32];
     const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nWarps = (gridDim.x * blockDim.x) >> 5;
-    for (int w = warp; w < nActive; w += nWarps)
+    const int wib = threadIdx.x >> 5, nWib = blockDim.x >> 5;
+    for (int w0 = blockIdx.x * nWib; w0 < nActive; w0 += gridDim.x * nWib)
     {
-        const int leaf = leaves ? leaves[w] : w;
-        const uint2 rg = ranges(leaf);
+        const int w = w0 + wib;
+        const bool have = w < nActive;
+        const int leaf = have ? (leaves ? leaves[w] : w) : 0;
+        const uint2 rg = have ? ranges(leaf) : make_uint2(0u, 0u);
         const uint32_t p0 = rg.x, p1 = rg.y;
-        const uint32_t S = jstream[leaf];
+        const uint32_t S = have ? jstream[leaf] : 0u;
         const uint2 cut = split(leaf);
         const int gsize = S <= cut.x ? 32 : max(1, int(cut.y / S));
-        for (uint32_t g = p0; g < p1; g += 64)
+        if (lane == 0) sWin[wib] = int((p1 - p0 + 63) >> 6);
+        __syncthreads();
+        int rounds = 0;
+        for (int k = 0; k < nWib; ++k) rounds = max(rounds, sWin[k]);
+        __syncthreads();   // sWin is written again by the next step
+        for (int r = 0; r < rounds; ++r)
         {
+            const uint32_t g = p0 + 64u * uint32_t(r);
+            const bool win = g < p1;   // warp-uniform
             const uint32_t a0 = g + lane, a1 = g + 32 + lane;
-            bool act0 = a0 < p1 && (!converged || converged[a0] == 0);
-            bool act1 = a1 < p1 && (!converged || converged[a1] == 0);
+            bool act0 = win && a0 < p1 && (!converged || converged[a0] == 0);
+            bool act1 = win && a1 < p1 && (!converged || converged[a1] == 0);
+            bool row0 = false, row1 = false;
             if (rs.rowCount != nullptr)
             {
                 auto rowOK = [&](uint32_t a) {
                     return unsigned(rs.rowCount[a]) <= unsigned(rs.K) && xyzh[a].w <= rs.rowH[a];
                 };
-                const bool row0 = act0 && rowOK(a0), row1 = act1 && rowOK(a1);
-                const uint32_t q0 = __ballot_sync(0xffffffffu, row0), q1 = __ballot_sync(0xffffffffu, row1);
-                if (q0 | q1)
-                {
-                    int base = 0;
-                    if (lane == 0) base = atomicAdd(&ds->rowParticles, __popc(q0) + __popc(q1));
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    if (row0) rs.rowItems[base + __popc(q0 & lt)] = int(a0);
-                    if (row1) rs.rowItems[base + __popc(q0) + __popc(q1 & lt)] = int(a1);
-                }
+                row0 = act0 && rowOK(a0);
+                row1 = act1 && rowOK(a1);
                 act0 = act0 && !row0;
                 act1 = act1 && !row1;
             }
+            const uint32_t q0 = __ballot_sync(0xffffffffu, row0), q1 = __ballot_sync(0xffffffffu, row1);
             const uint32_t c0 = __ballot_sync(0xffffffffu, act0), c1 = __ballot_sync(0xffffffffu, act1);
             const int nC = __popc(c0) + __popc(c1);
-            if (nC == 0) continue;
-            const int wnd = int((g - p0) >> 6);
+            const int wnd = win ? int((g - p0) >> 6) : 0;
             const int whole = (nC + 31) >> 5;
             // A window whose smoothing lengths spread by more than kGroupSpread is grouped by
             // h (ranks in ascending h), into at least spreadGroups groups and however many
@@ -139,37 +148,68 @@ __device__ __forceinline__ void plan_items(const int* __restrict__ leaves, int n
             const double hmax = warp_max(fmax(act0 ? h0 : 0.0, act1 ? h1 : 0.0));
             const bool byH = nC > 1 && hmax > kGroupSpread * hmin;
             const int cutG = (nC + gsize - 1) / gsize;
-            const int G = max(byH ? max(whole, min(spreadGroups, nC)) : whole, cutG);
+            const int G = nC == 0 ? 0 : max(byH ? max(whole, min(spreadGroups, nC)) : whole, cutG);
             // cut items (long streams) scan the tree for their box; so do all items of a leaf
             // whose list walk stopped at the stream cap (its list is empty)
-            const bool split = cutG > whole || S == kStreamUnbounded;
-            int base = 0;
-            if (lane == 0) base = atomicAdd(split ? &ds->itemsHeavy : &ds->itemsLight, G);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            // group k takes the active ranks [k nC / G, (k + 1) nC / G): in slot order, or in
-            // (h, slot) order for a spread window
-            int r0 = __popc(c0 & lt), r1 = __popc(c0) + __popc(c1 & lt);
-            if (byH)
+            const bool splitW = cutG > whole || S == kStreamUnbounded;
+            if (lane == 0)
             {
-                int k0 = 0, k1 = 0;
-                for (int t = 0; t < 32; ++t)
+                sCnt[0][wib] = __popc(q0) + __popc(q1);
+                sCnt[1][wib] = splitW ? G : 0;
+                sCnt[2][wib] = splitW ? 0 : G;
+            }
+            __syncthreads();
+            if (threadIdx.x < 3)
+            {
+                // the block's reservation: exclusive prefixes over its warps, one atomic
+                const int c = threadIdx.x;
+                int run = 0;
+                for (int k = 0; k < nWib; ++k)
                 {
-                    const double u0 = __shfl_sync(0xffffffffu, h0, t), u1 = __shfl_sync(0xffffffffu, h1, t);
-                    // slots t and 32 + t against this lane's two slots (inactive slots hold inf)
-                    k0 += (u0 < h0 || (u0 == h0 && t < lane)) + (u1 < h0);
-                    k1 += (u0 < h1 || u0 == h1) + (u1 < h1 || (u1 == h1 && t < lane));
+                    const int v = sCnt[c][k];
+                    sCnt[c][k] = run;
+                    run += v;
                 }
-                r0 = k0;
-                r1 = k1;
+                int* ctr = c == 0 ? &ds->rowParticles : (c == 1 ? &ds->itemsHeavy : &ds->itemsLight);
+                sBase[c] = run > 0 ? atomicAdd(ctr, run) : 0;
             }
-            for (int k = 0; k < G; ++k)
+            __syncthreads();
+            if (q0 | q1)
             {
-                const int lo = k * nC / G, hi = (k + 1) * nC / G;
-                const uint32_t i0 = __ballot_sync(0xffffffffu, act0 && r0 >= lo && r0 < hi);
-                const uint32_t i1 = __ballot_sync(0xffffffffu, act1 && r1 >= lo && r1 < hi);
-                const int idx = split ? base + k : cap - 1 - (base + k);
-                if (lane == 0 && idx >= 0 && idx < cap) items[idx] = make_int4(leaf, (wnd << 16) | 1, int(i0), int(i1));
+                const int base = sBase[0] + sCnt[0][wib];
+                if (row0) rs.rowItems[base + __popc(q0 & lt)] = int(a0);
+                if (row1) rs.rowItems[base + __popc(q0) + __popc(q1 & lt)] = int(a1);
             }
+            if (G > 0)
+            {
+                const int base = splitW ? sBase[1] + sCnt[1][wib] : sBase[2] + sCnt[2][wib];
+                // group k takes the active ranks [k nC / G, (k + 1) nC / G): in slot order,
+                // or in (h, slot) order for a spread window
+                int r0 = __popc(c0 & lt), r1 = __popc(c0) + __popc(c1 & lt);
+                if (byH)
+                {
+                    int k0 = 0, k1 = 0;
+                    for (int t = 0; t < 32; ++t)
+                    {
+                        const double u0 = __shfl_sync(0xffffffffu, h0, t), u1 = __shfl_sync(0xffffffffu, h1, t);
+                        // slots t and 32 + t against this lane's two slots (inactive slots hold inf)
+                        k0 += (u0 < h0 || (u0 == h0 && t < lane)) + (u1 < h0);
+                        k1 += (u0 < h1 || u0 == h1) + (u1 < h1 || (u1 == h1 && t < lane));
+                    }
+                    r0 = k0;
+                    r1 = k1;
+                }
+                for (int k = 0; k < G; ++k)
+                {
+                    const int lo = k * nC / G, hi = (k + 1) * nC / G;
+                    const uint32_t i0 = __ballot_sync(0xffffffffu, act0 && r0 >= lo && r0 < hi);
+                    const uint32_t i1 = __ballot_sync(0xffffffffu, act1 && r1 >= lo && r1 < hi);
+                    const int idx = splitW ? base + k : cap - 1 - (base + k);
+                    if (lane == 0 && idx >= 0 && idx < cap)
+                        items[idx] = make_int4(leaf, (wnd << 16) | 1, int(i0), int(i1));
+                }
+            }
+            __syncthreads();   // the shared counts are reused by the next round
         }
     }
 }
