@@ -318,13 +318,21 @@ __global__ void row_cover_kernel(int nL, const uint32_t* __restrict__ layout, co
 // particle's support (dr^2 < R^2 h_i^2 (1 + 1e-10)) is in j's Newton row too unless dr^2
 // reaches the radius j's row covers (R rowH, with 1e-9 to spare; only a pair beyond j's
 // own support can); such a pair is appended as (j << 32 | i), for i to be merged into
-// j's row.
+// j's row.  The mixed form's rows hold that double rounded to float (within 2^-24 of
+// it): where it lies within 1e-6 of a bound the test uses, dr^2 is taken again from the
+// positions, so every test decides as on the double and the rows are the same.
+template<class T, bool Periodic>
 __global__ void __launch_bounds__(kThreads)
-sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __restrict__ rowsR2,
+sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const T* __restrict__ rowsR2,
                      int* __restrict__ nblCount, const double* __restrict__ hs, const double* __restrict__ rowH,
-                     int* __restrict__ nbl, unsigned long long* __restrict__ extras, int extraCap,
-                     int* __restrict__ extraCnt, DevScalars* __restrict__ ds)
+                     const double4* __restrict__ xyzh, const DevBox* __restrict__ box, int* __restrict__ nbl,
+                     unsigned long long* __restrict__ extras, int extraCap, int* __restrict__ extraCnt,
+                     DevScalars* __restrict__ ds)
 {
+    constexpr bool kExact = std::is_same<T, double>::value;
+    using R4 = typename std::conditional<kExact, double4, float4>::type;
+    double lx = 0, ly = 0, lz = 0;
+    if (Periodic && !kExact) { lx = box->len[0]; ly = box->len[1]; lz = box->len[2]; }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nAlive; i += gridDim.x * blockDim.x)
     {
         extraCnt[i] = 0;
@@ -332,16 +340,30 @@ sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __
         const double hi = hs[i];
         const double bi = kRadK2 * (hi * hi) * (1.0 + 1e-10);
         const int4* inJ = reinterpret_cast<const int4*>(row_flat(rowsJ, uint32_t(i)));
-        const double4* inR = reinterpret_cast<const double4*>(row_flat(rowsR2, uint32_t(i)));
+        const R4* inR = reinterpret_cast<const R4*>(row_flat(rowsR2, uint32_t(i)));
         int* out = row_of(nbl, uint32_t(i));
         int w = 0;
         auto entry = [&](int j, double dr2, double hj) {
+            bool exact = kExact;
+            auto near = [&](double bound) { return fabs(dr2 - bound) <= 1e-6 * bound; };
+            auto retake = [&]() {
+                if (exact) return;
+                const double4 pa = xyzh[i], pb = ldg4(xyzh + j);
+                double dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+                nearest_image<Periodic>(dx, dy, dz, lx, ly, lz);
+                dr2 = pair_r2(dx, dy, dz);
+                exact = true;
+            };
             const double bj = kRadK2 * (hj * hj) * (1.0 + 1e-10);
+            const double own = kRadK2 * (hj * hj);
+            if (!exact && (near(fmax(bi, bj)) || near(bi) || near(own))) retake();
             if (!(dr2 >= fmax(bi, bj))) out[size_t(w++) * kRowStride] = j;
-            if (dr2 < bi && !(dr2 < kRadK2 * (hj * hj)))
+            if (dr2 < bi && !(dr2 < own))
             {
                 const double ch = __ldg(rowH + j);
-                if (!(dr2 < kRadK2 * (ch * ch) * (1.0 - 1e-9)))
+                const double cover = kRadK2 * (ch * ch) * (1.0 - 1e-9);
+                if (!exact && near(cover)) retake();
+                if (!(dr2 < cover))
                 {
                     const int k = atomicAdd(&ds->extraCount, 1);
                     if (k < extraCap) extras[k] = (static_cast<unsigned long long>(j) << 32) | uint32_t(i);
@@ -354,25 +376,29 @@ sym_from_rows_kernel(int nAlive, const int* __restrict__ rowsJ, const double* __
         const int nq = (cnt + 3) >> 2;
         const int me = i;
         auto ldj = [&](int q) { return q < nq ? __ldg(inJ + q) : make_int4(me, me, me, me); };
-        auto ldr = [&](int q) { return q < nq ? ldg4(inR + q) : make_double4(0.0, 0.0, 0.0, 0.0); };
+        auto ldr = [&](int q) {
+            R4 z{};
+            if constexpr (kExact) return q < nq ? ldg4(inR + q) : z;
+            else return q < nq ? __ldg(inR + q) : z;
+        };
         auto ldh = [&](int q, const int4& v) {
             const int left = cnt - 4 * q;
             return make_double4(__ldg(hs + (left > 0 ? v.x : me)), __ldg(hs + (left > 1 ? v.y : me)),
                                 __ldg(hs + (left > 2 ? v.z : me)), __ldg(hs + (left > 3 ? v.w : me)));
         };
         int4 v0 = ldj(0), v1 = ldj(1);
-        double4 r0 = ldr(0), r1 = ldr(1);
+        R4 r0 = ldr(0), r1 = ldr(1);
         double4 h0 = ldh(0, v0);
         for (int q = 0; q < nq; ++q)
         {
             const double4 h1 = ldh(q + 1, v1);
             const int4 v2 = ldj(q + 2);
-            const double4 r2 = ldr(q + 2);
+            const R4 r2 = ldr(q + 2);
             const int left = cnt - 4 * q;
-            entry(v0.x, r0.x, h0.x);
-            if (left > 1) entry(v0.y, r0.y, h0.y);
-            if (left > 2) entry(v0.z, r0.z, h0.z);
-            if (left > 3) entry(v0.w, r0.w, h0.w);
+            entry(v0.x, double(r0.x), h0.x);
+            if (left > 1) entry(v0.y, double(r0.y), h0.y);
+            if (left > 2) entry(v0.z, double(r0.z), h0.z);
+            if (left > 3) entry(v0.w, double(r0.w), h0.w);
             v0 = v1; r0 = r1; h0 = h1;
             v1 = v2; r1 = r2;
         }
@@ -868,7 +894,9 @@ static bool cover_rows(State& s, int itemCap, FixedSplit cut, int spreadG)
             s.coverLeaves.get(), &ds->coverLeaves, nullptr, s.layout.get(), s.coverFlag.get(), s.jstream.get(),
             s.xyzh.get(), s.items.get(), itemCap, ds, RowSplit{nullptr, nullptr, 0, nullptr}, cut, spreadG);
         COSMO_LAUNCHED();
-        RowsKernelFn nrows = s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>;
+        RowsKernelFn nrows = s.precision == 1
+                                 ? mixed_newton_rows_kernel(s.periodic)
+                                 : (s.periodic ? newton_rows_kernel<true, false> : newton_rows_kernel<false, false>);
         nrows<<<persistent_grid(s, nrows, kThreads), kThreads, 0, s.st>>>(
             s.items.get(), itemCap, s.layout.get(), s.jOffset.get(), s.jcount.get(), s.jlist.get(), s.xyzh.get(),
             s.box.get(), s.listH.get(), s.nblR2.get(), s.nblCount.get(), s.nblH.get(), ds, s.nblJ.get());
@@ -891,9 +919,20 @@ static void sym_rows_from_newton(State& s, int extraCap)
     s.extraBucket.resize(extraCap, s.st);
     // extraCount, mergeOverflow and rowOverflow were zeroed by the coverage check; each
     // particle's extras count by the compaction
-    sym_from_rows_kernel<<<std::max(1, std::min(iceil(nA, kThreads), 16 * s.numSMs)), kThreads, 0, s.st>>>(
-        nA, s.nblJ.get(), s.nblR2.get(), s.nblCount.get(), s.hs.get(), s.nblH.get(), s.nbl.get(), s.extras.get(),
-        extraCap, s.extraCnt.get(), ds);
+    const int grid = std::max(1, std::min(iceil(nA, kThreads), 16 * s.numSMs));
+    auto compact = [&](auto kern, const auto* rows) {
+        kern<<<grid, kThreads, 0, s.st>>>(nA, s.nblJ.get(), rows, s.nblCount.get(), s.hs.get(), s.nblH.get(),
+                                          s.xyzh.get(), s.box.get(), s.nbl.get(), s.extras.get(), extraCap,
+                                          s.extraCnt.get(), ds);
+    };
+    // the mixed form's Newton rows hold FP32 r^2 in the same buffer
+    const float* rowsF = reinterpret_cast<const float*>(s.nblR2.get());
+    if (s.precision == 1)
+    {
+        if (s.periodic) compact(sym_from_rows_kernel<float, true>, rowsF);
+        else compact(sym_from_rows_kernel<float, false>, rowsF);
+    }
+    else compact(sym_from_rows_kernel<double, false>, s.nblR2.get());
     COSMO_LAUNCHED();
     extras_count_kernel<<<iceil(extraCap, 256), 256, 0, s.st>>>(s.extras.get(), extraCap, ds, s.extraCnt.get());
     COSMO_LAUNCHED();
@@ -921,13 +960,13 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     ev_reset(s);
     DevScalars* ds = s.dscal.get();
     // The Newton rows also write their j when the gradient and force passes may run over
-    // them: a plain solve with gradients whose particles all start active (with fixed
-    // particles, leaves that never walk would hold no list this solve).  After a solve
+    // them: a solve with gradients whose particles all start active (with fixed particles,
+    // leaves that never walk would hold no list this solve).  After a solve
     // whose rows did not all cover (a workload with leaves the work queue cuts, say), the
     // next few solves do not write them.
     const bool tryRows = s.symRowsSkip == 0;
     if (s.symRowsSkip > 0) --s.symRowsSkip;
-    const bool writeJ = s.precision == 0 && withGradients && s.symFromRows && s.frozenFor != n && tryRows;
+    const bool writeJ = withGradients && s.symFromRows && s.frozenFor != n && tryRows;
 
     // the tree; its particle gather also zeroes rho, gradh, the convergence flags, the
     // Newton rows' h (0: no row this solve) and the pair counters
@@ -946,7 +985,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
     // the index rows' buffer is passed whenever the form has one (the Newton-loop graph
     // keeps one key); the gather set the device switch from writeJ
     int* rowsJ = nullptr;
-    if (s.precision == 0)
+    if (s.precision == 0 || s.precision == 1)
     {
         s.nblJ.resize(size_t(itemCap) * kNbl, s.st);
         s.nbl.resize(row_buffer_entries(size_t(itemCap)), s.st);

@@ -537,3 +537,55 @@ def test_rows_from_newton_rows(case):
     assert b["rowsFromNewton"] == 0
     for k in FIELDS + FORCE + ["pairsDensity", "pairsGrad", "pairsForce"]:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+@pytest.mark.parametrize("case", ["lattice_open", "periodic"])
+def test_rows_from_newton_rows_mixed(case):
+    """The mixed form's symmetric rows taken from its Newton rows (FP32 r^2, with dr^2
+    taken again from the positions wherever it lies near a bound) are the rows built from
+    the symmetric lists entry for entry, so its outputs are the same bits either way."""
+    box = None
+    if case == "lattice_open":
+        p = inputs.lattice100_workload(20)
+    else:
+        x, y, z = (np.asarray(v).ravel() for v in np.meshgrid(*(np.arange(14) / 14.0,) * 3, indexing="ij"))
+        n = x.size
+        rng = np.random.default_rng(3)
+        p = inputs.Particles(x=(x + rng.uniform(0, 0.02, n)) % 1.0, y=(y + rng.uniform(0, 0.02, n)) % 1.0,
+                             z=(z + rng.uniform(0, 0.02, n)) % 1.0, h=np.full(n, 1.2 / 14), pmass=1.0 / n)
+        inputs.jiggle_frac(p["h"], 0.05, 0.65, 1.35, 4)
+        box = [0.0, 1.0, 0.0, 1.0, 0.0, 1.0]
+    n = p.n
+    v, a = _vel_acc(p)
+    th = _thermo(p, 1.2)
+
+    def run():
+        c = capi.Cosmo(False)
+        c.set_precision(True)
+        try:
+            c.arrays_init(n)
+            c.upload(capi.POS, np.stack([p["x"], p["y"], p["z"]]))
+            c.upload(capi.HSML, p["h"])
+            c.upload(capi.VEL, v)
+            c.upload(capi.ACCEL, a)
+            c.density(n, p["pmass"], periodic_box=box, hfact=1.2)
+            c.upload(capi.THERMO, th, sorted_=True)
+            c.force(n, p["pmass"], beta=2.0, alphau=0.1)
+            out = {k: c.array(k).copy() for k in FIELDS + FORCE}
+            out["rowsFromNewton"] = c.scalar("rowsFromNewton")
+            out["pairsForce"] = c.scalar("pairsForce")
+        finally:
+            c.set_precision(False)
+        return out
+
+    cc = capi.Cosmo(False)
+    try:
+        assert cc.set_option("sym_from_rows", 1) == 0
+        a1 = run()
+        assert cc.set_option("sym_from_rows", 0) == 0
+        b0 = run()
+    finally:
+        cc.set_option("sym_from_rows", 1)
+    assert a1["rowsFromNewton"] == 1 and b0["rowsFromNewton"] == 0
+    for k in FIELDS + FORCE + ["pairsForce"]:
+        np.testing.assert_array_equal(a1[k], b0[k], err_msg=k)
