@@ -726,6 +726,13 @@ int cosmo_x_set_option(const char* name, int value)
     if (k == "staging") { s.staging = value != 0; return 0; }
     if (k == "sym_prefilter") { s.symPrefilter = value != 0; return 0; }
     if (k == "newton_graph") { s.newtonGraph = value != 0; return 0; }
+    if (k == "sym_extra_cap")
+    {
+        if (value < 0) return -1;
+        s.symExtraCap = value;
+        s.symRowsSkip = 0;
+        return 0;
+    }
     if (k == "sym_from_rows")
     {
         s.symFromRows = value != 0;

@@ -1171,7 +1171,7 @@ DensResult solve_density(State& s, int n, double pmass, const double* periodicBo
         hmax_leaves(s, s.allLeaves.get(), nL);
         const bool rowsBuilt = graphRan ? s.lastLoopRowBuilds > 0 : rowsReady;
         fromRows = writeJ && s.nAlive > 0 && rowsBuilt && cover_rows(s, itemCap, cut, spreadG);
-        const int extraCap = itemCap;
+        const int extraCap = s.symExtraCap > 0 ? std::min(s.symExtraCap, itemCap) : itemCap;
         if (fromRows)
             sym_rows_from_newton(s, extraCap);
         else

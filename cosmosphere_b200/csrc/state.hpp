@@ -176,6 +176,10 @@ struct State
     // "sym_from_rows", COSMO_SYM_FROM_ROWS).  The results are the same either way.
     int symFromRows = 1;
     int symRowsSkip = 0;   // solves left that do not try it (after one that could not)
+    // pairs the other side's supports may add that the rows' merge holds (0: one per live
+    // particle); a smaller figure sends the force pass back to the list-built rows when
+    // more are found (cosmo_x_set_option "sym_extra_cap", a test of that fallback)
+    int symExtraCap = 0;
     // list storage of the graph loop's rebuilds as a percentage of the first lists' total
     // (0: the built-in, twice the total plus 65536 entries); a figure under 100 makes a
     // rebuild outgrow it, so the fallback to the host loop can be exercised

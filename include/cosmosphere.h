@@ -226,7 +226,10 @@ void cosmo_x_sync(void);
  * "sym_from_rows" 1 (default) runs the gradient and force passes over the Newton rows' j
  * (with the pairs other particles' supports add merged in) when every live particle's row
  * covers its converged h, 0 builds the symmetric lists and rows after every solve (also
- * COSMO_SYM_FROM_ROWS).
+ * COSMO_SYM_FROM_ROWS); "sym_extra_cap" k > 0 holds at most k of the pairs other
+ * particles' supports add to those rows (0: the built-in, one per live particle), so that
+ * a solve that finds more hands the force pass to the list-built rows (a test of that
+ * fallback).
  * Returns 0, or -1 for an unknown name or a value out of range. */
 int cosmo_x_set_option(const char* name, int value);
 

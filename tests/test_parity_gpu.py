@@ -589,3 +589,21 @@ def test_rows_from_newton_rows_mixed(case):
     assert a1["rowsFromNewton"] == 1 and b0["rowsFromNewton"] == 0
     for k in FIELDS + FORCE + ["pairsForce"]:
         np.testing.assert_array_equal(a1[k], b0[k], err_msg=k)
+
+
+def test_rows_from_newton_rows_extras_fallback():
+    """When the pairs other particles' supports add to the rows taken from the Newton rows
+    do not all fit (here the merge holds one), the force pass builds the symmetric rows from
+    the symmetric lists instead: every structure and field still equals the oracle's."""
+    p = inputs.lattice100_workload(20)
+    cc = capi.Cosmo(False)
+    try:
+        assert cc.set_option("sym_from_rows", 1) == 0
+        assert cc.set_option("sym_extra_cap", 1) == 0
+        c, o = run_pair(p)
+        assert c.scalar("extraCount") > 1
+        assert c.scalar("rowsFromNewton") == 0
+        check_all(c, o)
+    finally:
+        cc.set_option("sym_extra_cap", 0)
+        cc.set_option("sym_from_rows", 1)
